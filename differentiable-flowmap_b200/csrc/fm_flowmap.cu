@@ -1,0 +1,583 @@
+// fm_flowmap.cu -- flow-map transport kernels and their C ABI (sm_100a).
+//
+// Gather kernels (one thread per output node, B-spline taps read through the
+// read-only path; the 128^3 working set sits in the 126 MB L2) for:
+//   advect_u_grid / advect_scalar_grid   (3D/flowmap.py:202-320)
+//   RK_grid / RK_grid_only_psi           (3D/flowmap.py:85-179)
+//   advect_u / advect_scalar (pullback)  (3D/flowmap.py:51-79), BFECC epilogues
+//   accumulate_init / accumulate_init_new(3D/flowmap.py:485-545)
+//   calculate_nabla_u_w / _scalar_adjoint(3D/flowmap.py:359-403)
+//   reset_to_identity, add_fields
+#include "fm_common.cuh"
+#include "fm_internal.h"
+
+namespace fm {
+
+constexpr int kThreads = 256;
+
+// Midpoint (RK2) / RK4 backtrace from X through u0 (3D/flowmap.py:210-219, :257-262).
+template <typename T, int D, int RK>
+__device__ __forceinline__ void backtrace(const Mac<T>& u0, const fm_grid& g, const T* X, T dx, T dt, T* p) {
+  T v1[3], v2[3], q[3] = {0, 0, 0};
+  interp_mac_val<T, D>(u0, g, X, dx, v1);
+#pragma unroll
+  for (int a = 0; a < D; ++a) q[a] = X[a] - v1[a] * dt * (T)0.5;
+  interp_mac_val<T, D>(u0, g, q, dx, v2);
+  if (RK == 2) {
+#pragma unroll
+    for (int a = 0; a < D; ++a) p[a] = X[a] - v2[a] * dt;
+    return;
+  }
+  T v3[3], v4[3];
+#pragma unroll
+  for (int a = 0; a < D; ++a) q[a] = X[a] - v2[a] * dt * (T)0.5;
+  interp_mac_val<T, D>(u0, g, q, dx, v3);
+#pragma unroll
+  for (int a = 0; a < D; ++a) q[a] = X[a] - v3[a] * dt;
+  interp_mac_val<T, D>(u0, g, q, dx, v4);
+#pragma unroll
+  for (int a = 0; a < D; ++a) p[a] = X[a] - (v1[a] + (T)2 * v2[a] + (T)2 * v3[a] + v4[a]) / (T)6.0 * dt;
+}
+
+template <typename T, int D, int RK>
+__global__ void __launch_bounds__(kThreads) k_advect_u_grid(fm_grid g, T dx, T dt, Mac<T> u0, Mac<T> u1,
+                                                            MacW<T> u2) {
+  const int c = blockIdx.y;
+  const Shape s = face_shape(g, c);
+  const long q = (long)blockIdx.x * blockDim.x + threadIdx.x;
+  if (q >= s.size()) return;
+  int i, j, k;
+  unflatten(s, q, i, j, k);
+  T X[3] = {0, 0, 0}, p[3] = {0, 0, 0};
+  node_pos<T, D>(c, i, j, k, dx, X);
+  backtrace<T, D, RK>(u0, g, X, dx, dt, p);
+  u2.c[c][q] = interp_mac_comp<T, D>(u1, g, c, p, dx);
+}
+
+template <typename T, int D, int RK>
+__global__ void __launch_bounds__(kThreads) k_advect_scalar_grid(fm_grid g, T dx, T dt, Mac<T> u0,
+                                                                 const T* __restrict__ s1, T* __restrict__ s2) {
+  const Shape s = cell_shape(g);
+  const long q = (long)blockIdx.x * blockDim.x + threadIdx.x;
+  if (q >= s.size()) return;
+  int i, j, k;
+  unflatten(s, q, i, j, k);
+  T X[3] = {0, 0, 0}, p[3] = {0, 0, 0};
+  node_pos<T, D>(-1, i, j, k, dx, X);
+  backtrace<T, D, RK>(u0, g, X, dx, dt, p);
+  s2[q] = interp_val<T, D, 2>(s1, s, p, dx, (T)0.5, (T)0.5, (T)0.5);
+}
+
+// One march job: a flow map psi (D planes) on grid `face` (-1 = centre),
+// optionally with its Jacobian rows T (D planes).
+template <typename T>
+struct MarchJob {
+  T* psi;
+  T* Tm;
+  int face;
+};
+template <typename T>
+struct MarchJobs {
+  MarchJob<T> j[4];
+};
+
+template <typename T, int D>
+__device__ __forceinline__ void matvec(const T G[3][3], const T* v, T* out) {
+#pragma unroll
+  for (int a = 0; a < D; ++a) {
+    T acc = 0;
+#pragma unroll
+    for (int b = 0; b < D; ++b) acc += G[a][b] * v[b];
+    out[a] = acc;
+  }
+}
+
+// RK2_grid / RK4_grid (with T) and RK*_grid_only_psi (without).
+template <typename T, int D, int RK>
+__global__ void __launch_bounds__(kThreads) k_march(fm_grid g, T dx, T dt, MarchJobs<T> jobs, Mac<T> u) {
+  const MarchJob<T> job = jobs.j[blockIdx.y];
+  const Shape s = job.face >= 0 ? face_shape(g, job.face) : cell_shape(g);
+  const long N = s.size();
+  const long q = (long)blockIdx.x * blockDim.x + threadIdx.x;
+  if (q >= N) return;
+  const bool wt = job.Tm != nullptr;
+  T P[3] = {0, 0, 0}, Tv[3] = {0, 0, 0};
+#pragma unroll
+  for (int a = 0; a < D; ++a) {
+    P[a] = job.psi[a * N + q];
+    if (wt) Tv[a] = job.Tm[a * N + q];
+  }
+  const T neg_dt = -dt;
+  const T h = (T)0.5 * neg_dt;
+  T G[3][3];
+  T k1[3], k2[3], q1[3] = {0, 0, 0}, t1[3] = {0, 0, 0}, d1[3] = {0, 0, 0}, d2[3] = {0, 0, 0};
+  if (wt) interp_mac_grad<T, D, 2>(u, g, P, dx, k1, G);
+  else interp_mac_val<T, D>(u, g, P, dx, k1);
+  if (wt) matvec<T, D>(G, Tv, d1);
+#pragma unroll
+  for (int a = 0; a < D; ++a) { q1[a] = P[a] + h * k1[a]; t1[a] = Tv[a] + h * d1[a]; }
+  if (wt) { interp_mac_grad<T, D, 2>(u, g, q1, dx, k2, G); matvec<T, D>(G, t1, d2); }
+  else interp_mac_val<T, D>(u, g, q1, dx, k2);
+  if (RK == 2) {
+#pragma unroll
+    for (int a = 0; a < D; ++a) {
+      job.psi[a * N + q] = P[a] + neg_dt * k2[a];
+      if (wt) job.Tm[a * N + q] = Tv[a] + neg_dt * d2[a];
+    }
+    return;
+  }
+  T k3[3], k4[3], d3[3] = {0, 0, 0}, d4[3] = {0, 0, 0};
+#pragma unroll
+  for (int a = 0; a < D; ++a) { q1[a] = P[a] + h * k2[a]; t1[a] = Tv[a] + h * d2[a]; }
+  if (wt) { interp_mac_grad<T, D, 2>(u, g, q1, dx, k3, G); matvec<T, D>(G, t1, d3); }
+  else interp_mac_val<T, D>(u, g, q1, dx, k3);
+#pragma unroll
+  for (int a = 0; a < D; ++a) { q1[a] = P[a] + neg_dt * k3[a]; t1[a] = Tv[a] + neg_dt * d3[a]; }
+  if (wt) { interp_mac_grad<T, D, 2>(u, g, q1, dx, k4, G); matvec<T, D>(G, t1, d4); }
+  else interp_mac_val<T, D>(u, g, q1, dx, k4);
+  const T c6 = neg_dt * (T)1 / (T)6;
+#pragma unroll
+  for (int a = 0; a < D; ++a) {
+    job.psi[a * N + q] = P[a] + c6 * (k1[a] + (T)2 * k2[a] + (T)2 * k3[a] + k4[a]);
+    if (wt) job.Tm[a * N + q] = Tv[a] + c6 * (d1[a] + (T)2 * d2[a] + (T)2 * d3[a] + d4[a]);
+  }
+}
+
+// out_c = alpha * (T_c . u0(psi_c) + beta * base_c)
+template <typename T, int D>
+__global__ void __launch_bounds__(kThreads) k_pullback_u(fm_grid g, T dx, Mac<T> u0, MacW<T> out, Mac<T> Tm,
+                                                         Mac<T> psi, T alpha, T beta, Mac<T> base) {
+  const int c = blockIdx.y;
+  const Shape s = face_shape(g, c);
+  const long N = s.size();
+  const long q = (long)blockIdx.x * blockDim.x + threadIdx.x;
+  if (q >= N) return;
+  T p[3] = {0, 0, 0}, v[3];
+#pragma unroll
+  for (int a = 0; a < D; ++a) p[a] = psi.c[c][a * N + q];
+  interp_mac_val<T, D>(u0, g, p, dx, v);
+  T acc = 0;
+#pragma unroll
+  for (int a = 0; a < D; ++a) acc += Tm.c[c][a * N + q] * v[a];
+  if (beta != (T)0) acc = acc + beta * base.c[c][q];
+  out.c[c][q] = alpha * acc;
+}
+
+template <typename T, int D>
+__global__ void __launch_bounds__(kThreads) k_pullback_scalar(fm_grid g, T dx, const T* __restrict__ s0,
+                                                              T* out, const T* __restrict__ psi, T alpha, T beta,
+                                                              const T* base) {
+  const Shape s = cell_shape(g);
+  const long N = s.size();
+  const long q = (long)blockIdx.x * blockDim.x + threadIdx.x;
+  if (q >= N) return;
+  T p[3] = {0, 0, 0};
+#pragma unroll
+  for (int a = 0; a < D; ++a) p[a] = psi[a * N + q];
+  T acc = interp_val<T, D, 2>(s0, s, p, dx, (T)0.5, (T)0.5, (T)0.5);
+  if (beta != (T)0) acc = acc + beta * base[q];
+  out[q] = alpha * acc;
+}
+
+template <typename T, int D, bool AB3>
+__global__ void __launch_bounds__(kThreads) k_accumulate(fm_grid g, T dx, T dt, int ind, Mac<T> f, MacW<T> init,
+                                                         Mac<T> F, Mac<T> phi, MacW<T> Hp, MacW<T> Hpp) {
+  const int c = blockIdx.y;
+  const Shape s = face_shape(g, c);
+  const long N = s.size();
+  const long q = (long)blockIdx.x * blockDim.x + threadIdx.x;
+  if (q >= N) return;
+  T p[3] = {0, 0, 0}, v[3];
+#pragma unroll
+  for (int a = 0; a < D; ++a) p[a] = phi.c[c][a * N + q];
+  interp_mac_val<T, D>(f, g, p, dx, v);
+  T Fv = 0, Fv23 = 0, Fv16 = 0;
+#pragma unroll
+  for (int a = 0; a < D; ++a) {
+    const T Fa = F.c[c][a * N + q];
+    Fv += Fa * v[a];
+    if (AB3) { Fv23 += ((T)23 * Fa) * v[a]; Fv16 += ((T)16 * Fa) * v[a]; }
+  }
+  T acc = init.c[c][q];
+  if (!AB3 || ind == 0) {
+    acc += Fv * dt;
+  } else {
+    const T hp = Hp.c[c][q];
+    if (ind == 1) acc += (Fv23 - Fv16 + (T)5 * hp) / (T)12 * dt;
+    else acc += (Fv23 - (T)16 * hp + (T)5 * Hpp.c[c][q]) / (T)12 * dt;
+    Hpp.c[c][q] = hp;
+    Hp.c[c][q] = Fv;
+  }
+  init.c[c][q] = acc;
+}
+
+template <typename T, int D, int ORDER>
+__global__ void __launch_bounds__(kThreads) k_nabla_u_w(fm_grid g, T dx, Mac<T> u, Mac<T> w, MacW<T> r) {
+  const int c = blockIdx.y;
+  const Shape s = face_shape(g, c);
+  const long q = (long)blockIdx.x * blockDim.x + threadIdx.x;
+  if (q >= s.size()) return;
+  int i, j, k;
+  unflatten(s, q, i, j, k);
+  T X[3] = {0, 0, 0};
+  node_pos<T, D>(c, i, j, k, dx, X);
+  T acc = 0;
+#pragma unroll
+  for (int a = 0; a < D; ++a) {
+    const Shape sa = face_shape(g, a);
+    const T b0 = a == 0 ? (T)0 : (T)0.5, b1 = a == 1 ? (T)0 : (T)0.5, b2 = a == 2 ? (T)0 : (T)0.5;
+    T uv, gr[3];
+    interp_grad<T, D, ORDER>(u.c[a], sa, X, dx, b0, b1, b2, uv, gr);
+    const T wv = interp_val<T, D, ORDER>(w.c[a], sa, X, dx, b0, b1, b2);
+    acc += gr[c] * wv;
+  }
+  r.c[c][q] = acc;
+}
+
+template <typename T, int D>
+__global__ void __launch_bounds__(kThreads) k_nabla_scalar_adj(fm_grid g, T dx, const T* __restrict__ sc,
+                                                               const T* __restrict__ adj, MacW<T> r) {
+  const int c = blockIdx.y;
+  const Shape s = face_shape(g, c);
+  const long q = (long)blockIdx.x * blockDim.x + threadIdx.x;
+  if (q >= s.size()) return;
+  int i, j, k;
+  unflatten(s, q, i, j, k);
+  T X[3] = {0, 0, 0};
+  node_pos<T, D>(c, i, j, k, dx, X);
+  const Shape cs = cell_shape(g);
+  T v, gr[3];
+  interp_grad<T, D, 3>(sc, cs, X, dx, (T)0.5, (T)0.5, (T)0.5, v, gr);
+  const T av = interp_val<T, D, 3>(adj, cs, X, dx, (T)0.5, (T)0.5, (T)0.5);
+  r.c[c][q] = gr[c] * av;
+}
+
+template <typename T, int D>
+__global__ void k_reset_identity(fm_grid g, T dx, MarchJobs<T> jobs) {
+  const MarchJob<T> job = jobs.j[blockIdx.y];
+  if (!job.psi && !job.Tm) return;
+  const Shape s = job.face >= 0 ? face_shape(g, job.face) : cell_shape(g);
+  const long N = s.size();
+  const long q = (long)blockIdx.x * blockDim.x + threadIdx.x;
+  if (q >= N) return;
+  int i, j, k;
+  unflatten(s, q, i, j, k);
+  T X[3] = {0, 0, 0};
+  node_pos<T, D>(job.face, i, j, k, dx, X);
+#pragma unroll
+  for (int a = 0; a < D; ++a) {
+    if (job.psi) job.psi[a * N + q] = X[a];
+    if (job.Tm) job.Tm[a * N + q] = (a == job.face) ? (T)1 : (T)0;
+  }
+}
+
+template <typename T>
+__global__ void k_add_fields(long n, const T* f1, const T* f2, T* dest, T m) {
+  for (long q = (long)blockIdx.x * blockDim.x + threadIdx.x; q < n; q += (long)gridDim.x * blockDim.x)
+    dest[q] = f1[q] + m * f2[q];
+}
+
+// ---------------------------------------------------------------------------
+// host-side launch helpers
+// ---------------------------------------------------------------------------
+static inline long max_face(const fm_grid& g) {
+  long m = 0;
+  for (int c = 0; c < g.dim; ++c) m = face_shape(g, c).size() > m ? face_shape(g, c).size() : m;
+  return m;
+}
+static inline dim3 grid_for(long n, int ycount) {
+  return dim3((unsigned)((n + kThreads - 1) / kThreads), (unsigned)ycount, 1);
+}
+
+template <typename T>
+static Mac<T> mac(const void* x, const void* y, const void* z) {
+  Mac<T> m;
+  m.c[0] = (const T*)x; m.c[1] = (const T*)y; m.c[2] = (const T*)z;
+  return m;
+}
+template <typename T>
+static MacW<T> macw(void* x, void* y, void* z) {
+  MacW<T> m;
+  m.c[0] = (T*)x; m.c[1] = (T*)y; m.c[2] = (T*)z;
+  return m;
+}
+static inline bool mac_ok(const fm_grid& g, const void* x, const void* y, const void* z) {
+  return x && y && (g.dim == 2 || z);
+}
+
+#define FM_DISPATCH_D(g, ...)                 \
+  do {                                        \
+    if ((g).dim == 3) { constexpr int D = 3; __VA_ARGS__; } \
+    else { constexpr int D = 2; __VA_ARGS__; } \
+  } while (0)
+
+template <typename T>
+static int advect_u_grid_t(const fm_grid& g, int rk, double dx, double dt, Mac<T> u0, Mac<T> u1, MacW<T> u2,
+                           cudaStream_t st) {
+  dim3 grid = grid_for(max_face(g), g.dim);
+  FM_DISPATCH_D(g, if (rk == 2) k_advect_u_grid<T, D, 2><<<grid, kThreads, 0, st>>>(g, (T)dx, (T)dt, u0, u1, u2);
+                else k_advect_u_grid<T, D, 4><<<grid, kThreads, 0, st>>>(g, (T)dx, (T)dt, u0, u1, u2));
+  return check_launch();
+}
+
+template <typename T>
+static int advect_scalar_grid_t(const fm_grid& g, int rk, double dx, double dt, Mac<T> u0, const T* s1, T* s2,
+                                cudaStream_t st) {
+  dim3 grid = grid_for(cell_shape(g).size(), 1);
+  FM_DISPATCH_D(g, if (rk == 2) k_advect_scalar_grid<T, D, 2><<<grid, kThreads, 0, st>>>(g, (T)dx, (T)dt, u0, s1, s2);
+                else k_advect_scalar_grid<T, D, 4><<<grid, kThreads, 0, st>>>(g, (T)dx, (T)dt, u0, s1, s2));
+  return check_launch();
+}
+
+template <typename T>
+static int march_t(const fm_grid& g, int rk, double dx, double dt, const MarchJobs<T>& jobs, int njobs, Mac<T> u,
+                   cudaStream_t st) {
+  if (njobs == 0) return FM_OK;
+  long n = cell_shape(g).size();
+  for (int i = 0; i < njobs; ++i) {
+    long m = jobs.j[i].face >= 0 ? face_shape(g, jobs.j[i].face).size() : cell_shape(g).size();
+    n = m > n ? m : n;
+  }
+  dim3 grid = grid_for(n, njobs);
+  FM_DISPATCH_D(g, if (rk == 2) k_march<T, D, 2><<<grid, kThreads, 0, st>>>(g, (T)dx, (T)dt, jobs, u);
+                else k_march<T, D, 4><<<grid, kThreads, 0, st>>>(g, (T)dx, (T)dt, jobs, u));
+  return check_launch();
+}
+
+}  // namespace fm
+
+using namespace fm;
+
+#define FM_STREAM(s) ((cudaStream_t)(s))
+
+extern "C" {
+
+int fm_advect_u_grid(const fm_grid* g, int dtype, int rk, double dx, double dt, const void* u0x, const void* u0y,
+                     const void* u0z, const void* u1x, const void* u1y, const void* u1z, void* u2x, void* u2y,
+                     void* u2z, void* stream) {
+  int st = validate_grid(g, dtype);
+  if (st) return st;
+  if ((rk != 2 && rk != 4) || !mac_ok(*g, u0x, u0y, u0z) || !mac_ok(*g, u1x, u1y, u1z) || !mac_ok(*g, u2x, u2y, u2z))
+    return FM_ERR_ARG;
+  if (dtype == FM_F32)
+    return advect_u_grid_t<float>(*g, rk, dx, dt, mac<float>(u0x, u0y, u0z), mac<float>(u1x, u1y, u1z),
+                                  macw<float>(u2x, u2y, u2z), FM_STREAM(stream));
+  return advect_u_grid_t<double>(*g, rk, dx, dt, mac<double>(u0x, u0y, u0z), mac<double>(u1x, u1y, u1z),
+                                 macw<double>(u2x, u2y, u2z), FM_STREAM(stream));
+}
+
+int fm_advect_scalar_grid(const fm_grid* g, int dtype, int rk, double dx, double dt, const void* u0x,
+                          const void* u0y, const void* u0z, const void* s1, void* s2, void* stream) {
+  int st = validate_grid(g, dtype);
+  if (st) return st;
+  if ((rk != 2 && rk != 4) || !mac_ok(*g, u0x, u0y, u0z) || !s1 || !s2) return FM_ERR_ARG;
+  if (dtype == FM_F32)
+    return advect_scalar_grid_t<float>(*g, rk, dx, dt, mac<float>(u0x, u0y, u0z), (const float*)s1, (float*)s2,
+                                       FM_STREAM(stream));
+  return advect_scalar_grid_t<double>(*g, rk, dx, dt, mac<double>(u0x, u0y, u0z), (const double*)s1, (double*)s2,
+                                      FM_STREAM(stream));
+}
+
+int fm_rk_grid(const fm_grid* g, int dtype, int rk, double dx, double dt, int face, void* psi, void* T,
+               const void* ux, const void* uy, const void* uz, void* stream) {
+  int st = validate_grid(g, dtype);
+  if (st) return st;
+  if ((rk != 2 && rk != 4) || !psi || face < -1 || face >= g->dim || (face == -1 && T) || !mac_ok(*g, ux, uy, uz))
+    return FM_ERR_ARG;
+  if (dtype == FM_F32) {
+    MarchJobs<float> jobs{};
+    jobs.j[0] = MarchJob<float>{(float*)psi, (float*)T, face};
+    return march_t<float>(*g, rk, dx, dt, jobs, 1, mac<float>(ux, uy, uz), FM_STREAM(stream));
+  }
+  MarchJobs<double> jobs{};
+  jobs.j[0] = MarchJob<double>{(double*)psi, (double*)T, face};
+  return march_t<double>(*g, rk, dx, dt, jobs, 1, mac<double>(ux, uy, uz), FM_STREAM(stream));
+}
+
+int fm_march_map(const fm_grid* g, int dtype, int rk, double dx, double dt, void* psi_c, void* psi_x, void* T_x,
+                 void* psi_y, void* T_y, void* psi_z, void* T_z, const void* ux, const void* uy, const void* uz,
+                 void* stream) {
+  int st = validate_grid(g, dtype);
+  if (st) return st;
+  if ((rk != 2 && rk != 4) || !mac_ok(*g, ux, uy, uz)) return FM_ERR_ARG;
+  void* ps[3] = {psi_x, psi_y, psi_z};
+  void* ts[3] = {T_x, T_y, T_z};
+  for (int c = 0; c < g->dim; ++c)
+    if (!ps[c] || !ts[c]) return FM_ERR_ARG;
+  if (dtype == FM_F32) {
+    MarchJobs<float> jobs{};
+    int n = 0;
+    for (int c = 0; c < g->dim; ++c) jobs.j[n++] = MarchJob<float>{(float*)ps[c], (float*)ts[c], c};
+    if (psi_c) jobs.j[n++] = MarchJob<float>{(float*)psi_c, nullptr, -1};
+    return march_t<float>(*g, rk, dx, dt, jobs, n, mac<float>(ux, uy, uz), FM_STREAM(stream));
+  }
+  MarchJobs<double> jobs{};
+  int n = 0;
+  for (int c = 0; c < g->dim; ++c) jobs.j[n++] = MarchJob<double>{(double*)ps[c], (double*)ts[c], c};
+  if (psi_c) jobs.j[n++] = MarchJob<double>{(double*)psi_c, nullptr, -1};
+  return march_t<double>(*g, rk, dx, dt, jobs, n, mac<double>(ux, uy, uz), FM_STREAM(stream));
+}
+
+int fm_pullback_u(const fm_grid* g, int dtype, double dx, const void* u0x, const void* u0y, const void* u0z,
+                  void* outx, void* outy, void* outz, const void* Tx, const void* Ty, const void* Tz,
+                  const void* psix, const void* psiy, const void* psiz, double alpha, double beta,
+                  const void* basex, const void* basey, const void* basez, void* stream) {
+  int st = validate_grid(g, dtype);
+  if (st) return st;
+  if (!mac_ok(*g, u0x, u0y, u0z) || !mac_ok(*g, outx, outy, outz) || !mac_ok(*g, Tx, Ty, Tz) ||
+      !mac_ok(*g, psix, psiy, psiz) || (beta != 0.0 && !mac_ok(*g, basex, basey, basez)))
+    return FM_ERR_ARG;
+  dim3 grid = grid_for(max_face(*g), g->dim);
+  cudaStream_t s = FM_STREAM(stream);
+  if (dtype == FM_F32) {
+    FM_DISPATCH_D(*g, k_pullback_u<float, D><<<grid, kThreads, 0, s>>>(
+                          *g, (float)dx, mac<float>(u0x, u0y, u0z), macw<float>(outx, outy, outz),
+                          mac<float>(Tx, Ty, Tz), mac<float>(psix, psiy, psiz), (float)alpha, (float)beta,
+                          mac<float>(basex, basey, basez)));
+  } else {
+    FM_DISPATCH_D(*g, k_pullback_u<double, D><<<grid, kThreads, 0, s>>>(
+                          *g, dx, mac<double>(u0x, u0y, u0z), macw<double>(outx, outy, outz),
+                          mac<double>(Tx, Ty, Tz), mac<double>(psix, psiy, psiz), alpha, beta,
+                          mac<double>(basex, basey, basez)));
+  }
+  return check_launch();
+}
+
+int fm_pullback_scalar(const fm_grid* g, int dtype, double dx, const void* s0, void* out, const void* psi,
+                       double alpha, double beta, const void* base, void* stream) {
+  int st = validate_grid(g, dtype);
+  if (st) return st;
+  if (!s0 || !out || !psi || (beta != 0.0 && !base)) return FM_ERR_ARG;
+  dim3 grid = grid_for(cell_shape(*g).size(), 1);
+  cudaStream_t s = FM_STREAM(stream);
+  if (dtype == FM_F32) {
+    FM_DISPATCH_D(*g, k_pullback_scalar<float, D><<<grid, kThreads, 0, s>>>(
+                          *g, (float)dx, (const float*)s0, (float*)out, (const float*)psi, (float)alpha,
+                          (float)beta, (const float*)base));
+  } else {
+    FM_DISPATCH_D(*g, k_pullback_scalar<double, D><<<grid, kThreads, 0, s>>>(
+                          *g, dx, (const double*)s0, (double*)out, (const double*)psi, alpha, beta,
+                          (const double*)base));
+  }
+  return check_launch();
+}
+
+int fm_accumulate_init(const fm_grid* g, int dtype, double dx, double dt, int ab3, int ind, const void* fx,
+                       const void* fy, const void* fz, void* initx, void* inity, void* initz, const void* Fx,
+                       const void* Fy, const void* Fz, const void* phix, const void* phiy, const void* phiz,
+                       void* Hpx, void* Hppx, void* Hpy, void* Hppy, void* Hpz, void* Hppz, void* stream) {
+  int st = validate_grid(g, dtype);
+  if (st) return st;
+  if (!mac_ok(*g, fx, fy, fz) || !mac_ok(*g, initx, inity, initz) || !mac_ok(*g, Fx, Fy, Fz) ||
+      !mac_ok(*g, phix, phiy, phiz) || ind < 0)
+    return FM_ERR_ARG;
+  if (ab3 && (!mac_ok(*g, Hpx, Hpy, Hpz) || !mac_ok(*g, Hppx, Hppy, Hppz))) return FM_ERR_ARG;
+  dim3 grid = grid_for(max_face(*g), g->dim);
+  cudaStream_t s = FM_STREAM(stream);
+  if (dtype == FM_F32) {
+    auto f = mac<float>(fx, fy, fz);
+    auto in = macw<float>(initx, inity, initz);
+    auto F = mac<float>(Fx, Fy, Fz);
+    auto ph = mac<float>(phix, phiy, phiz);
+    auto hp = macw<float>(Hpx, Hpy, Hpz);
+    auto hpp = macw<float>(Hppx, Hppy, Hppz);
+    FM_DISPATCH_D(*g, if (ab3) k_accumulate<float, D, true><<<grid, kThreads, 0, s>>>(*g, (float)dx, (float)dt, ind,
+                                                                                       f, in, F, ph, hp, hpp);
+                  else k_accumulate<float, D, false><<<grid, kThreads, 0, s>>>(*g, (float)dx, (float)dt, ind, f,
+                                                                               in, F, ph, hp, hpp));
+  } else {
+    auto f = mac<double>(fx, fy, fz);
+    auto in = macw<double>(initx, inity, initz);
+    auto F = mac<double>(Fx, Fy, Fz);
+    auto ph = mac<double>(phix, phiy, phiz);
+    auto hp = macw<double>(Hpx, Hpy, Hpz);
+    auto hpp = macw<double>(Hppx, Hppy, Hppz);
+    FM_DISPATCH_D(*g, if (ab3) k_accumulate<double, D, true><<<grid, kThreads, 0, s>>>(*g, dx, dt, ind, f, in, F,
+                                                                                        ph, hp, hpp);
+                  else k_accumulate<double, D, false><<<grid, kThreads, 0, s>>>(*g, dx, dt, ind, f, in, F, ph, hp,
+                                                                                hpp));
+  }
+  return check_launch();
+}
+
+int fm_nabla_u_w(const fm_grid* g, int dtype, int order, double dx, const void* ux, const void* uy, const void* uz,
+                 const void* wx, const void* wy, const void* wz, void* rx, void* ry, void* rz, void* stream) {
+  int st = validate_grid(g, dtype);
+  if (st) return st;
+  if ((order != 2 && order != 3 && order != 4) || !mac_ok(*g, ux, uy, uz) || !mac_ok(*g, wx, wy, wz) ||
+      !mac_ok(*g, rx, ry, rz))
+    return FM_ERR_ARG;
+  dim3 grid = grid_for(max_face(*g), g->dim);
+  cudaStream_t s = FM_STREAM(stream);
+#define FM_NUW(T_)                                                                                          \
+  {                                                                                                         \
+    auto u = mac<T_>(ux, uy, uz);                                                                           \
+    auto w = mac<T_>(wx, wy, wz);                                                                           \
+    auto r = macw<T_>(rx, ry, rz);                                                                          \
+    FM_DISPATCH_D(*g, if (order == 2) k_nabla_u_w<T_, D, 2><<<grid, kThreads, 0, s>>>(*g, (T_)dx, u, w, r); \
+                  else if (order == 3) k_nabla_u_w<T_, D, 3><<<grid, kThreads, 0, s>>>(*g, (T_)dx, u, w, r);  \
+                  else k_nabla_u_w<T_, D, 4><<<grid, kThreads, 0, s>>>(*g, (T_)dx, u, w, r));               \
+  }
+  if (dtype == FM_F32) FM_NUW(float) else FM_NUW(double)
+#undef FM_NUW
+  return check_launch();
+}
+
+int fm_nabla_scalar_adjoint(const fm_grid* g, int dtype, double dx, const void* sc, const void* adj, void* rx,
+                            void* ry, void* rz, void* stream) {
+  int st = validate_grid(g, dtype);
+  if (st) return st;
+  if (!sc || !adj || !mac_ok(*g, rx, ry, rz)) return FM_ERR_ARG;
+  dim3 grid = grid_for(max_face(*g), g->dim);
+  cudaStream_t s = FM_STREAM(stream);
+  if (dtype == FM_F32) {
+    FM_DISPATCH_D(*g, k_nabla_scalar_adj<float, D><<<grid, kThreads, 0, s>>>(*g, (float)dx, (const float*)sc,
+                                                                            (const float*)adj, macw<float>(rx, ry, rz)));
+  } else {
+    FM_DISPATCH_D(*g, k_nabla_scalar_adj<double, D><<<grid, kThreads, 0, s>>>(
+                          *g, dx, (const double*)sc, (const double*)adj, macw<double>(rx, ry, rz)));
+  }
+  return check_launch();
+}
+
+int fm_reset_to_identity(const fm_grid* g, int dtype, double dx, void* psi_c, void* psi_x, void* psi_y, void* psi_z,
+                         void* T_x, void* T_y, void* T_z, void* stream) {
+  int st = validate_grid(g, dtype);
+  if (st) return st;
+  void* ps[3] = {psi_x, psi_y, psi_z};
+  void* ts[3] = {T_x, T_y, T_z};
+  long n = cell_shape(*g).size();
+  for (int c = 0; c < g->dim; ++c) n = face_shape(*g, c).size() > n ? face_shape(*g, c).size() : n;
+  dim3 grid = grid_for(n, g->dim + 1);
+  cudaStream_t s = FM_STREAM(stream);
+  if (dtype == FM_F32) {
+    MarchJobs<float> jobs{};
+    for (int c = 0; c < g->dim; ++c) jobs.j[c] = MarchJob<float>{(float*)ps[c], (float*)ts[c], c};
+    jobs.j[g->dim] = MarchJob<float>{(float*)psi_c, nullptr, -1};
+    FM_DISPATCH_D(*g, k_reset_identity<float, D><<<grid, kThreads, 0, s>>>(*g, (float)dx, jobs));
+  } else {
+    MarchJobs<double> jobs{};
+    for (int c = 0; c < g->dim; ++c) jobs.j[c] = MarchJob<double>{(double*)ps[c], (double*)ts[c], c};
+    jobs.j[g->dim] = MarchJob<double>{(double*)psi_c, nullptr, -1};
+    FM_DISPATCH_D(*g, k_reset_identity<double, D><<<grid, kThreads, 0, s>>>(*g, dx, jobs));
+  }
+  return check_launch();
+}
+
+int fm_add_fields(int dtype, long n, const void* f1, const void* f2, void* dest, double m, void* stream) {
+  if (dtype != FM_F32 && dtype != FM_F64) return FM_ERR_DTYPE;
+  if (n < 0 || (n > 0 && (!f1 || !f2 || !dest))) return FM_ERR_ARG;
+  if (n == 0) return FM_OK;
+  long blocks = (n + kThreads - 1) / kThreads;
+  if (blocks > 148 * 16) blocks = 148 * 16;
+  cudaStream_t s = FM_STREAM(stream);
+  if (dtype == FM_F32)
+    k_add_fields<float><<<(unsigned)blocks, kThreads, 0, s>>>(n, (const float*)f1, (const float*)f2, (float*)dest,
+                                                              (float)m);
+  else
+    k_add_fields<double><<<(unsigned)blocks, kThreads, 0, s>>>(n, (const double*)f1, (const double*)f2,
+                                                               (double*)dest, m);
+  return check_launch();
+}
+
+}  // extern "C"

@@ -1,0 +1,29 @@
+// fm_internal.h -- argument validation and error mapping shared by the C ABI.
+#pragma once
+#include <cuda_runtime.h>
+
+#include "../../include/flowmap_sm100.h"
+
+namespace fm {
+
+inline int validate_grid(const fm_grid* g, int dtype) {
+  if (dtype != FM_F32 && dtype != FM_F64) return FM_ERR_DTYPE;
+  if (!g) return FM_ERR_ARG;
+  if (g->dim != 2 && g->dim != 3) return FM_ERR_SHAPE;
+  for (int a = 0; a < 3; ++a)
+    if (g->n[a] < 1) return FM_ERR_SHAPE;
+  if (g->dim == 2 && g->n[2] != 1) return FM_ERR_SHAPE;
+  // the B-spline stencils clamp to [1, n-2]: at least 4 cells per axis
+  for (int a = 0; a < g->dim; ++a)
+    if (g->n[a] < 4) return FM_ERR_SHAPE;
+  // flat indices are 64-bit but per-axis extents fit int comfortably
+  if ((long long)(g->n[0] + 1) * (g->n[1] + 1) * (g->n[2] + 1) > (1LL << 34)) return FM_ERR_SHAPE;
+  return FM_OK;
+}
+
+inline int check_launch() {
+  cudaError_t e = cudaGetLastError();
+  return e == cudaSuccess ? FM_OK : FM_ERR_CUDA;
+}
+
+}  // namespace fm

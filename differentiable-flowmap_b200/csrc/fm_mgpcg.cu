@@ -1,0 +1,718 @@
+// fm_mgpcg.cu -- MGPCG pressure projection for sm_100a.
+//
+// Restates the reference solver (3D/mgpcg.py:12-439; 2D/vortex/mgpcg_solid.py
+// with an empty obstacle mask): all-Neumann 5/7-point Laplacian, red-black
+// Gauss-Seidel V-cycle (2 pre + 2 post sweeps, piecewise-constant prolongation,
+// restriction summing fine residuals into I//2 scaled 1/(dim-1), bottom RBGS),
+// recentring of r, PCG with absolute (and optional relative) rTr tolerance.
+//
+// B200 design:
+//  * alpha/beta/convergence live on the device (FP64), so an iteration issues
+//    no host read; the host only polls the `done` word every check_every
+//    iterations (the reference syncs three times per iteration).
+//  * inner products use fixed-grid block partials reduced in a fixed order
+//    (deterministic, FP64 accumulation).
+//  * restriction is a gather over the 2^dim children (no atomics, no zero-fill);
+//    the first red sweep of every level fuses the zero-fill of z (and, on the
+//    fine level, the recentring of r); the last fine sweep fuses z.r.
+//  * the coarsest level is smoothed by one CTA in shared memory (the reference
+//    issues 2*bottom launches there).
+//  * one PCG iteration (~40 launches) is captured once into a CUDA graph.
+#include <cuda_bf16.h>
+#include <math.h>
+#include <stdlib.h>
+#include <string.h>
+
+#include "fm_common.cuh"
+#include "fm_internal.h"
+
+namespace fm {
+
+constexpr int kRedBlocks = 148 * 4;  // fixed reduction grid: 4 CTAs per SM
+constexpr int kRedThreads = 256;
+constexpr int kMaxLevels = 16;
+
+struct DevState {
+  double zTr_old, tol, rTr, alpha, beta, mean, pAp;
+  int it;        // completed PCG iterations (reference `it`)
+  int done;      // converged, max_iters reached or non-finite
+  int conv;
+  int nonfinite;
+  int result_it;
+};
+
+// ---------------------------------------------------------------------------
+// helpers
+// ---------------------------------------------------------------------------
+template <int D>
+__device__ __forceinline__ int parity(int i, int j, int k) {
+  return (i + j + (D == 3 ? k : 0)) & 1;
+}
+
+// neighbor_sum / num_fluid_neighbors (3D/mgpcg.py:97-120), all-Neumann walls.
+template <typename T, int D>
+__device__ __forceinline__ T nb_sum(const T* __restrict__ x, const Shape& s, int i, int j, int k, T& diag) {
+  T acc = 0;
+  int nd = 2 * D;
+  const long q = s.idx(i, j, k);
+  if (i < s.s0 - 1) acc += x[q + (long)s.s1 * s.s2]; else --nd;
+  if (i > 0) acc += x[q - (long)s.s1 * s.s2]; else --nd;
+  if (j < s.s1 - 1) acc += x[q + s.s2]; else --nd;
+  if (j > 0) acc += x[q - s.s2]; else --nd;
+  if (D == 3) {
+    if (k < s.s2 - 1) acc += x[q + 1]; else --nd;
+    if (k > 0) acc += x[q - 1]; else --nd;
+  }
+  diag = (T)nd;
+  return acc;
+}
+
+template <int D>
+__device__ __forceinline__ int diag_of(const Shape& s, int i, int j, int k) {
+  int nd = 2 * D;
+  nd -= (i == 0) + (i == s.s0 - 1) + (j == 0) + (j == s.s1 - 1);
+  if (D == 3) nd -= (k == 0) + (k == s.s2 - 1);
+  return nd;
+}
+
+__device__ __forceinline__ void block_reduce2(double a, double b, double* out2) {
+  __shared__ double sa[32], sb[32];
+#pragma unroll
+  for (int o = 16; o > 0; o >>= 1) {
+    a += __shfl_down_sync(0xffffffffu, a, o);
+    b += __shfl_down_sync(0xffffffffu, b, o);
+  }
+  const int lane = threadIdx.x & 31, w = threadIdx.x >> 5, nw = (blockDim.x + 31) >> 5;
+  if (lane == 0) { sa[w] = a; sb[w] = b; }
+  __syncthreads();
+  if (w == 0) {
+    a = lane < nw ? sa[lane] : 0.0;
+    b = lane < nw ? sb[lane] : 0.0;
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) {
+      a += __shfl_down_sync(0xffffffffu, a, o);
+      b += __shfl_down_sync(0xffffffffu, b, o);
+    }
+    if (lane == 0) { out2[0] = a; out2[1] = b; }
+  }
+}
+
+// Sum the fixed-grid partials in a fixed order (one CTA of 256 threads).
+__device__ __forceinline__ void sum_partials(const double* __restrict__ part, double& a, double& b) {
+  double x = 0, y = 0;
+  for (int i = threadIdx.x; i < kRedBlocks; i += blockDim.x) { x += part[2 * i]; y += part[2 * i + 1]; }
+  __shared__ double res[2];
+  block_reduce2(x, y, res);
+  __syncthreads();
+  a = res[0];
+  b = res[1];
+}
+
+#define FM_GRID_STRIDE(q, n) for (long q = (long)blockIdx.x * blockDim.x + threadIdx.x; q < (n); q += (long)gridDim.x * blockDim.x)
+
+// ---------------------------------------------------------------------------
+// projection front/back end
+// ---------------------------------------------------------------------------
+// apply_bc + divergence + init(r = -div) + x = 0, with partial sums of r for
+// the recentring (3D/mgpcg.py:368-399, :76-84, :179-185).
+template <typename T, int D>
+__global__ void __launch_bounds__(kRedThreads) k_div_bc(fm_grid g, MacW<T> u, T* __restrict__ r, T* __restrict__ x,
+                                                        double* __restrict__ part) {
+  const Shape cs = cell_shape(g);
+  double sum = 0;
+  FM_GRID_STRIDE(q, cs.size()) {
+    int I[3];
+    unflatten(cs, q, I[0], I[1], I[2]);
+    T acc = 0;
+#pragma unroll
+    for (int c = 0; c < D; ++c) {
+      const Shape fs = face_shape(g, c);
+      const long ql = fs.idx(I[0], I[1], I[2]);
+      const long step = c == 0 ? (long)fs.s1 * fs.s2 : (c == 1 ? fs.s2 : 1);
+      const long qr = ql + step;
+      T vl = u.c[c][ql], vr = u.c[c][qr];
+      if (I[c] == 0) { vl = 0; u.c[c][ql] = 0; }
+      if (I[c] == axis_len(cs, c) - 1) { vr = 0; u.c[c][qr] = 0; }
+      if (c == 0) acc = vr - vl;
+      else { acc = acc + vr; acc = acc - vl; }
+    }
+    const T b = acc * (T)-1;
+    r[q] = b;
+    x[q] = 0;
+    sum += (double)b;
+  }
+  block_reduce2(sum, 0.0, part + 2 * blockIdx.x);
+}
+
+// rhs given directly (fm_mgpcg_solve)
+template <typename T>
+__global__ void __launch_bounds__(kRedThreads) k_load_rhs(long n, const T* __restrict__ b, T* __restrict__ r,
+                                                          T* __restrict__ x, double* __restrict__ part) {
+  double sum = 0;
+  FM_GRID_STRIDE(q, n) {
+    const T v = b[q];
+    r[q] = v;
+    x[q] = 0;
+    sum += (double)v;
+  }
+  block_reduce2(sum, 0.0, part + 2 * blockIdx.x);
+}
+
+// subtract_grad_p + apply_bc (3D/mgpcg.py:401-427)
+template <typename T, int D>
+__global__ void k_subgrad_bc(fm_grid g, const T* __restrict__ p, MacW<T> u) {
+  const int c = blockIdx.y;
+  const Shape fs = face_shape(g, c);
+  const Shape cs = cell_shape(g);
+  const long q = (long)blockIdx.x * blockDim.x + threadIdx.x;
+  if (q >= fs.size()) return;
+  int I[3];
+  unflatten(fs, q, I[0], I[1], I[2]);
+  if (I[c] == 0 || I[c] == axis_len(cs, c)) { u.c[c][q] = 0; return; }
+  const long pc = cs.idx(I[0], I[1], I[2]);
+  const long step = c == 0 ? (long)cs.s1 * cs.s2 : (c == 1 ? cs.s2 : 1);
+  u.c[c][q] -= p[pc] - p[pc - step];
+}
+
+// ---------------------------------------------------------------------------
+// scalar finalizers (one CTA)
+// ---------------------------------------------------------------------------
+__global__ void k_fin_mean(DevState* st, const double* part, double n) {
+  double a, b;
+  sum_partials(part, a, b);
+  if (threadIdx.x == 0) {
+    st->mean = a / n;
+    st->done = 0; st->conv = 0; st->nonfinite = 0; st->it = 0; st->result_it = 0;
+    st->beta = 0; st->alpha = 0;
+  }
+}
+
+__global__ void k_fin_alpha(DevState* st, const double* part, double eps) {
+  if (st->done) return;
+  double a, b;
+  sum_partials(part, a, b);
+  if (threadIdx.x == 0) {
+    st->pAp = a;
+    st->alpha = st->zTr_old / (a + eps);
+  }
+}
+
+__global__ void k_fin_conv(DevState* st, const double* part, double n) {
+  if (st->done) return;
+  double a, b;
+  sum_partials(part, a, b);
+  if (threadIdx.x == 0) {
+    st->rTr = a;
+    st->mean = b / n;
+    if (!isfinite(a)) { st->nonfinite = 1; st->done = 1; st->result_it = st->it; }
+    else if (a < st->tol) { st->conv = 1; st->done = 1; st->result_it = st->it; }
+  }
+}
+
+__global__ void k_fin_beta(DevState* st, const double* part, double eps, double abs_tol, double rel_tol,
+                           int max_iters, int first) {
+  if (st->done) return;
+  double a, b;
+  sum_partials(part, a, b);
+  if (threadIdx.x == 0) {
+    if (first) {
+      st->zTr_old = a;
+      double tol = abs_tol;
+      if (rel_tol > 0 && a * rel_tol > tol) tol = a * rel_tol;
+      st->tol = tol;
+      st->beta = 0;
+      if (!isfinite(a)) { st->nonfinite = 1; st->done = 1; }
+    } else {
+      st->beta = a / (st->zTr_old + eps);
+      st->zTr_old = a;
+      st->it += 1;
+      if (st->it >= max_iters) { st->done = 1; st->result_it = st->it; }
+    }
+  }
+}
+
+// ---------------------------------------------------------------------------
+// PCG vector kernels
+// ---------------------------------------------------------------------------
+template <typename T, int D>
+__global__ void __launch_bounds__(kRedThreads) k_Ap_dot(Shape s, const T* __restrict__ p, T* __restrict__ Ap,
+                                                        double* __restrict__ part, const DevState* st) {
+  if (st->done) return;
+  double acc = 0;
+  FM_GRID_STRIDE(q, s.size()) {
+    int i, j, k;
+    unflatten(s, q, i, j, k);
+    T diag;
+    const T nb = nb_sum<T, D>(p, s, i, j, k, diag);
+    const T pv = p[q];
+    const T a = diag * pv - nb;
+    Ap[q] = a;
+    acc += (double)pv * (double)a;
+  }
+  block_reduce2(acc, 0.0, part + 2 * blockIdx.x);
+}
+
+template <typename T>
+__global__ void __launch_bounds__(kRedThreads) k_update_xr(long n, T* __restrict__ x, T* __restrict__ r,
+                                                           const T* __restrict__ p, const T* __restrict__ Ap,
+                                                           double* __restrict__ part, const DevState* st) {
+  if (st->done) return;
+  const T alpha = (T)st->alpha;
+  double rr = 0, rs = 0;
+  FM_GRID_STRIDE(q, n) {
+    x[q] += alpha * p[q];
+    const T rv = r[q] - alpha * Ap[q];
+    r[q] = rv;
+    rr += (double)rv * (double)rv;
+    rs += (double)rv;
+  }
+  block_reduce2(rr, rs, part + 2 * blockIdx.x);
+}
+
+template <typename T>
+__global__ void k_update_p(long n, T* __restrict__ p, const T* __restrict__ z, const DevState* st, int first) {
+  if (st->done) return;
+  const T beta = (T)st->beta;
+  FM_GRID_STRIDE(q, n) p[q] = first ? z[q] : z[q] + beta * p[q];
+}
+
+// ---------------------------------------------------------------------------
+// V-cycle kernels
+// ---------------------------------------------------------------------------
+// First red sweep from z == 0 (fuses z.fill(0)); optionally recentres r.
+template <typename T, int D>
+__global__ void k_smooth_first(Shape s, T* __restrict__ r, T* __restrict__ z, const DevState* st, int recenter) {
+  if (st->done) return;
+  const T mean = recenter ? (T)st->mean : (T)0;
+  FM_GRID_STRIDE(q, s.size()) {
+    int i, j, k;
+    unflatten(s, q, i, j, k);
+    T rv = r[q];
+    if (recenter) { rv = rv - mean; r[q] = rv; }
+    const T diag = (T)diag_of<D>(s, i, j, k);
+    z[q] = parity<D>(i, j, k) == 0 ? rv / diag : (T)0;
+  }
+}
+
+// smooth(l, phase) (3D/mgpcg.py:170-177); with part != nullptr also z.r over all cells.
+template <typename T, int D, bool DOT>
+__global__ void __launch_bounds__(kRedThreads) k_smooth(Shape s, const T* __restrict__ r, T* z, int phase,
+                                                        double* __restrict__ part, const DevState* st) {
+  if (st->done) return;
+  double acc = 0;
+  FM_GRID_STRIDE(q, s.size()) {
+    int i, j, k;
+    unflatten(s, q, i, j, k);
+    T zv;
+    if (parity<D>(i, j, k) == phase) {
+      T diag;
+      const T nb = nb_sum<T, D>(z, s, i, j, k, diag);
+      zv = (r[q] + nb) / diag;
+      z[q] = zv;
+    } else {
+      zv = z[q];
+    }
+    if (DOT) acc += (double)zv * (double)r[q];
+  }
+  if (DOT) block_reduce2(acc, 0.0, part + 2 * blockIdx.x);
+}
+
+// restrict(l) (3D/mgpcg.py:157-163) as a gather over the 2^D children.
+template <typename T, int D>
+__global__ void k_restrict(Shape sf, Shape sc, const T* __restrict__ rf, const T* __restrict__ zf,
+                           T* __restrict__ rc, const DevState* st) {
+  if (st->done) return;
+  const T scale = (T)1.0 / (T)(D - 1.0);
+  FM_GRID_STRIDE(q, sc.size()) {
+    int I, J, K;
+    unflatten(sc, q, I, J, K);
+    T acc = 0;
+#pragma unroll
+    for (int di = 0; di < 2; ++di)
+#pragma unroll
+      for (int dj = 0; dj < 2; ++dj)
+#pragma unroll
+        for (int dk = 0; dk < (D == 3 ? 2 : 1); ++dk) {
+          const int i = 2 * I + di, j = 2 * J + dj, k = D == 3 ? 2 * K + dk : 0;
+          const long f = sf.idx(i, j, k);
+          T diag;
+          const T nb = nb_sum<T, D>(zf, sf, i, j, k, diag);
+          const T res = rf[f] - (diag * zf[f] - nb);
+          acc += res * scale;
+        }
+    rc[q] = acc;
+  }
+}
+
+// prolongate(l) (3D/mgpcg.py:165-168)
+template <typename T, int D>
+__global__ void k_prolong(Shape sf, Shape sc, T* __restrict__ zf, const T* __restrict__ zc, const DevState* st) {
+  if (st->done) return;
+  FM_GRID_STRIDE(q, sf.size()) {
+    int i, j, k;
+    unflatten(sf, q, i, j, k);
+    zf[q] += zc[sc.idx(i >> 1, j >> 1, D == 3 ? (k >> 1) : 0)];
+  }
+}
+
+// Bottom smoothing on the coarsest level by one CTA in shared memory.
+// z starts at zero (the reference zero-fills before restricting).
+template <typename T, int D>
+__global__ void k_bottom(Shape s, const T* __restrict__ r, T* __restrict__ z, int bottom, int mode,
+                         const DevState* st) {
+  if (st->done) return;
+  extern __shared__ unsigned char smem_raw[];
+  T* zs = reinterpret_cast<T*>(smem_raw);
+  T* rs = zs + s.size();
+  const long n = s.size();
+  for (long q = threadIdx.x; q < n; q += blockDim.x) { zs[q] = 0; rs[q] = r[q]; }
+  __syncthreads();
+  auto sweep = [&](int phase) {
+    for (long q = threadIdx.x; q < n; q += blockDim.x) {
+      int i, j, k;
+      unflatten(s, q, i, j, k);
+      if (parity<D>(i, j, k) == phase) {
+        T diag;
+        const T nb = nb_sum<T, D>(zs, s, i, j, k, diag);
+        zs[q] = (rs[q] + nb) / diag;
+      }
+    }
+    __syncthreads();
+  };
+  if (mode == 0) {
+    for (int it = 0; it < bottom; ++it) { sweep(0); sweep(1); }
+  } else {
+    for (int it = 0; it < bottom / 2; ++it) { sweep(0); sweep(1); }
+    for (int it = 0; it < bottom / 2; ++it) { sweep(1); sweep(0); }
+  }
+  for (long q = threadIdx.x; q < n; q += blockDim.x) z[q] = zs[q];
+}
+
+template <typename T, int D>
+__global__ void k_laplacian(Shape s, const T* __restrict__ p, T* __restrict__ Ap) {
+  FM_GRID_STRIDE(q, s.size()) {
+    int i, j, k;
+    unflatten(s, q, i, j, k);
+    T diag;
+    const T nb = nb_sum<T, D>(p, s, i, j, k, diag);
+    Ap[q] = diag * p[q] - nb;
+  }
+}
+
+}  // namespace fm
+
+using namespace fm;
+
+struct fm_mgpcg {
+  fm_grid g;
+  int dtype;
+  fm_mg_params P;
+  int L;
+  Shape lv[kMaxLevels];
+  void* r[kMaxLevels];
+  void* z[kMaxLevels];
+  void* x;
+  void* p;
+  void* Ap;
+  double* part;
+  DevState* st;
+  DevState* h_st;  // pinned
+  cudaStream_t cap;
+  cudaGraphExec_t chunk;
+  size_t bottom_smem;
+};
+
+namespace fm {
+
+static inline unsigned blocks_for(long n, int threads, long cap) {
+  long b = (n + threads - 1) / threads;
+  if (b > cap) b = cap;
+  if (b < 1) b = 1;
+  return (unsigned)b;
+}
+
+template <typename T, int D>
+static void launch_vcycle(fm_mgpcg* S, cudaStream_t s, bool dot_last) {
+  const int L = S->L;
+  const fm_mg_params& P = S->P;
+  T** r = (T**)S->r;
+  T** z = (T**)S->z;
+  const long cap = 148L * 16;
+  for (int l = 0; l < L - 1; ++l) {
+    const Shape sh = S->lv[l];
+    const unsigned nb = blocks_for(sh.size(), 256, cap);
+    for (int it = 0; it < P.pre_post; ++it) {
+      if (it == 0) k_smooth_first<T, D><<<nb, 256, 0, s>>>(sh, r[l], z[l], S->st, l == 0 ? 1 : 0);
+      else k_smooth<T, D, false><<<nb, 256, 0, s>>>(sh, r[l], z[l], 0, nullptr, S->st);
+      k_smooth<T, D, false><<<nb, 256, 0, s>>>(sh, r[l], z[l], 1, nullptr, S->st);
+    }
+    const Shape sc = S->lv[l + 1];
+    k_restrict<T, D><<<blocks_for(sc.size(), 256, cap), 256, 0, s>>>(sh, sc, r[l], z[l], r[l + 1], S->st);
+  }
+  const Shape sb = S->lv[L - 1];
+  if (S->bottom_smem) {
+    k_bottom<T, D><<<1, 512, S->bottom_smem, s>>>(sb, r[L - 1], z[L - 1], P.bottom, P.bottom_mode, S->st);
+  } else {
+    // large coarsest level: per-sweep launches (z zero-filled by the first sweep)
+    const unsigned nb = blocks_for(sb.size(), 256, cap);
+    int first = 1;
+    auto pair = [&](int a, int b) {
+      if (first && a == 0) k_smooth_first<T, D><<<nb, 256, 0, s>>>(sb, r[L - 1], z[L - 1], S->st, L == 1 ? 1 : 0);
+      else {
+        if (first) cudaMemsetAsync(z[L - 1], 0, sizeof(T) * sb.size(), s);
+        k_smooth<T, D, false><<<nb, 256, 0, s>>>(sb, r[L - 1], z[L - 1], a, nullptr, S->st);
+      }
+      first = 0;
+      k_smooth<T, D, false><<<nb, 256, 0, s>>>(sb, r[L - 1], z[L - 1], b, nullptr, S->st);
+    };
+    if (P.bottom_mode == 0) for (int i = 0; i < P.bottom; ++i) pair(0, 1);
+    else {
+      for (int i = 0; i < P.bottom / 2; ++i) pair(0, 1);
+      for (int i = 0; i < P.bottom / 2; ++i) pair(1, 0);
+    }
+  }
+  for (int l = L - 2; l >= 0; --l) {
+    const Shape sh = S->lv[l];
+    const Shape sc = S->lv[l + 1];
+    const unsigned nb = blocks_for(sh.size(), 256, cap);
+    k_prolong<T, D><<<nb, 256, 0, s>>>(sh, sc, z[l], z[l + 1], S->st);
+    for (int it = 0; it < P.pre_post; ++it) {
+      k_smooth<T, D, false><<<nb, 256, 0, s>>>(sh, r[l], z[l], 1, nullptr, S->st);
+      const bool last = dot_last && l == 0 && it == P.pre_post - 1;
+      if (last) k_smooth<T, D, true><<<kRedBlocks, kRedThreads, 0, s>>>(sh, r[l], z[l], 0, S->part, S->st);
+      else k_smooth<T, D, false><<<nb, 256, 0, s>>>(sh, r[l], z[l], 0, nullptr, S->st);
+    }
+  }
+  if (dot_last && L == 1) {
+    // single-level: z.r over the bottom result
+    k_smooth<T, D, true><<<kRedBlocks, kRedThreads, 0, s>>>(sb, r[0], z[0], 2 /* no update */, S->part, S->st);
+  }
+}
+
+// One PCG iteration (3D/mgpcg.py:240-284) as a fixed launch sequence.
+template <typename T, int D>
+static void launch_iteration(fm_mgpcg* S, cudaStream_t s) {
+  const Shape s0 = S->lv[0];
+  const long n = s0.size();
+  T* x = (T*)S->x;
+  T* p = (T*)S->p;
+  T* Ap = (T*)S->Ap;
+  T* r0 = (T*)S->r[0];
+  T* z0 = (T*)S->z[0];
+  k_Ap_dot<T, D><<<kRedBlocks, kRedThreads, 0, s>>>(s0, p, Ap, S->part, S->st);
+  k_fin_alpha<<<1, 256, 0, s>>>(S->st, S->part, S->P.eps);
+  k_update_xr<T><<<kRedBlocks, kRedThreads, 0, s>>>(n, x, r0, p, Ap, S->part, S->st);
+  k_fin_conv<<<1, 256, 0, s>>>(S->st, S->part, (double)n);
+  launch_vcycle<T, D>(S, s, true);
+  k_fin_beta<<<1, 256, 0, s>>>(S->st, S->part, S->P.eps, S->P.abs_tol, S->P.rel_tol, S->P.max_iters, 0);
+  k_update_p<T><<<blocks_for(n, 256, 148L * 16), 256, 0, s>>>(n, p, z0, S->st, 0);
+}
+
+// Prologue after r0 = b and partial sums of b: recentre, V-cycle, p = z, zTr.
+template <typename T, int D>
+static void launch_prologue(fm_mgpcg* S, cudaStream_t s) {
+  const long n = S->lv[0].size();
+  k_fin_mean<<<1, 256, 0, s>>>(S->st, S->part, (double)n);
+  launch_vcycle<T, D>(S, s, true);
+  k_fin_beta<<<1, 256, 0, s>>>(S->st, S->part, S->P.eps, S->P.abs_tol, S->P.rel_tol, S->P.max_iters, 1);
+  k_update_p<T><<<blocks_for(n, 256, 148L * 16), 256, 0, s>>>(n, (T*)S->p, (T*)S->z[0], S->st, 1);
+}
+
+template <typename T>
+static int run_solve(fm_mgpcg* S, cudaStream_t s, int* iters, double* rtr) {
+  const int D = S->g.dim;
+  if (D == 3) launch_prologue<T, 3>(S, s); else launch_prologue<T, 2>(S, s);
+  if (check_launch()) return FM_ERR_CUDA;
+  if (!S->chunk) {
+    cudaGraph_t graph;
+    if (cudaStreamBeginCapture(S->cap, cudaStreamCaptureModeThreadLocal) != cudaSuccess) return FM_ERR_CUDA;
+    for (int i = 0; i < S->P.check_every; ++i) {
+      if (D == 3) launch_iteration<T, 3>(S, S->cap); else launch_iteration<T, 2>(S, S->cap);
+    }
+    if (cudaStreamEndCapture(S->cap, &graph) != cudaSuccess) return FM_ERR_CUDA;
+    cudaError_t e = cudaGraphInstantiate(&S->chunk, graph, 0);
+    cudaGraphDestroy(graph);
+    if (e != cudaSuccess) { S->chunk = nullptr; return FM_ERR_CUDA; }
+  }
+  long launched = 0;
+  const long limit = (long)S->P.max_iters + S->P.check_every;
+  for (;;) {
+    if (cudaGraphLaunch(S->chunk, s) != cudaSuccess) return FM_ERR_CUDA;
+    launched += S->P.check_every;
+    if (cudaMemcpyAsync(S->h_st, S->st, sizeof(DevState), cudaMemcpyDeviceToHost, s) != cudaSuccess) return FM_ERR_CUDA;
+    if (cudaStreamSynchronize(s) != cudaSuccess) return FM_ERR_CUDA;
+    if (S->h_st->done || launched >= limit) break;
+  }
+  if (iters) *iters = S->h_st->result_it;
+  if (rtr) *rtr = S->h_st->rTr;
+  if (S->h_st->nonfinite) return FM_ERR_NONFINITE;
+  if (!S->h_st->conv) return FM_ERR_NOT_CONVERGED;
+  return FM_OK;
+}
+
+}  // namespace fm
+
+extern "C" {
+
+int fm_mgpcg_create(const fm_grid* g, int dtype, const fm_mg_params* params, fm_mgpcg** out) {
+  if (!out || !params) return FM_ERR_ARG;
+  *out = nullptr;
+  int st = validate_grid(g, dtype);
+  if (st) return st;
+  const fm_mg_params& P = *params;
+  if (P.levels < 2 || P.levels > kMaxLevels || P.pre_post < 1 || P.bottom < 0 || P.max_iters < 1 ||
+      P.check_every < 1 || (P.bottom_mode != 0 && P.bottom_mode != 1))
+    return FM_ERR_ARG;
+  if (P.coarse_bf16) return FM_ERR_ARG;  // not in this build
+  for (int a = 0; a < g->dim; ++a)
+    if (g->n[a] % (1 << (P.levels - 1)) != 0 || (g->n[a] >> (P.levels - 1)) < 1) return FM_ERR_SHAPE;
+  fm_mgpcg* S = (fm_mgpcg*)calloc(1, sizeof(fm_mgpcg));
+  if (!S) return FM_ERR_ARG;
+  S->g = *g;
+  S->dtype = dtype;
+  S->P = P;
+  S->L = P.levels;
+  const size_t es = dtype == FM_F32 ? sizeof(float) : sizeof(double);
+  bool ok = true;
+  for (int l = 0; l < S->L; ++l) {
+    Shape sh{1, 1, 1};
+    sh.s0 = g->n[0] >> l;
+    sh.s1 = g->n[1] >> l;
+    sh.s2 = g->dim == 3 ? (g->n[2] >> l) : 1;
+    S->lv[l] = sh;
+    ok = ok && cudaMalloc(&S->r[l], es * sh.size()) == cudaSuccess;
+    ok = ok && cudaMalloc(&S->z[l], es * sh.size()) == cudaSuccess;
+  }
+  const long n0 = S->lv[0].size();
+  ok = ok && cudaMalloc(&S->x, es * n0) == cudaSuccess;
+  ok = ok && cudaMalloc(&S->p, es * n0) == cudaSuccess;
+  ok = ok && cudaMalloc(&S->Ap, es * n0) == cudaSuccess;
+  ok = ok && cudaMalloc(&S->part, sizeof(double) * 2 * kRedBlocks) == cudaSuccess;
+  ok = ok && cudaMalloc(&S->st, sizeof(DevState)) == cudaSuccess;
+  ok = ok && cudaMallocHost(&S->h_st, sizeof(DevState)) == cudaSuccess;
+  ok = ok && cudaStreamCreateWithFlags(&S->cap, cudaStreamNonBlocking) == cudaSuccess;
+  if (ok) ok = cudaMemset(S->st, 0, sizeof(DevState)) == cudaSuccess;
+  const long nb = S->lv[S->L - 1].size();
+  const size_t smem = 2 * es * nb;
+  if (ok && smem <= 200 * 1024) {
+    S->bottom_smem = smem;
+    if (smem > 48 * 1024) {
+      cudaError_t e;
+      if (dtype == FM_F32)
+        e = g->dim == 3 ? cudaFuncSetAttribute(k_bottom<float, 3>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem)
+                        : cudaFuncSetAttribute(k_bottom<float, 2>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+      else
+        e = g->dim == 3 ? cudaFuncSetAttribute(k_bottom<double, 3>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem)
+                        : cudaFuncSetAttribute(k_bottom<double, 2>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+      if (e != cudaSuccess) S->bottom_smem = 0;
+    }
+  }
+  if (!ok) {
+    fm_mgpcg_destroy(S);
+    return FM_ERR_CUDA;
+  }
+  *out = S;
+  return FM_OK;
+}
+
+int fm_mgpcg_destroy(fm_mgpcg* S) {
+  if (!S) return FM_OK;
+  for (int l = 0; l < kMaxLevels; ++l) {
+    if (S->r[l]) cudaFree(S->r[l]);
+    if (S->z[l]) cudaFree(S->z[l]);
+  }
+  if (S->x) cudaFree(S->x);
+  if (S->p) cudaFree(S->p);
+  if (S->Ap) cudaFree(S->Ap);
+  if (S->part) cudaFree(S->part);
+  if (S->st) cudaFree(S->st);
+  if (S->h_st) cudaFreeHost(S->h_st);
+  if (S->chunk) cudaGraphExecDestroy(S->chunk);
+  if (S->cap) cudaStreamDestroy(S->cap);
+  free(S);
+  return FM_OK;
+}
+
+int fm_project(fm_mgpcg* S, void* ux, void* uy, void* uz, void* p_out, void* stream, int* iters, double* rtr) {
+  if (!S || !ux || !uy || (S->g.dim == 3 && !uz)) return FM_ERR_ARG;
+  cudaStream_t s = (cudaStream_t)stream;
+  const fm_grid g = S->g;
+  const long n = S->lv[0].size();
+  int status;
+  long maxf = 0;
+  for (int c = 0; c < g.dim; ++c) maxf = face_shape(g, c).size() > maxf ? face_shape(g, c).size() : maxf;
+  dim3 fgrid((unsigned)((maxf + 255) / 256), (unsigned)g.dim, 1);
+  if (S->dtype == FM_F32) {
+    MacW<float> u{{(float*)ux, (float*)uy, (float*)uz}};
+    if (g.dim == 3) k_div_bc<float, 3><<<kRedBlocks, kRedThreads, 0, s>>>(g, u, (float*)S->r[0], (float*)S->x, S->part);
+    else k_div_bc<float, 2><<<kRedBlocks, kRedThreads, 0, s>>>(g, u, (float*)S->r[0], (float*)S->x, S->part);
+    status = run_solve<float>(S, s, iters, rtr);
+    if (status == FM_ERR_CUDA) return status;
+    if (g.dim == 3) k_subgrad_bc<float, 3><<<fgrid, 256, 0, s>>>(g, (const float*)S->x, u);
+    else k_subgrad_bc<float, 2><<<fgrid, 256, 0, s>>>(g, (const float*)S->x, u);
+  } else {
+    MacW<double> u{{(double*)ux, (double*)uy, (double*)uz}};
+    if (g.dim == 3) k_div_bc<double, 3><<<kRedBlocks, kRedThreads, 0, s>>>(g, u, (double*)S->r[0], (double*)S->x, S->part);
+    else k_div_bc<double, 2><<<kRedBlocks, kRedThreads, 0, s>>>(g, u, (double*)S->r[0], (double*)S->x, S->part);
+    status = run_solve<double>(S, s, iters, rtr);
+    if (status == FM_ERR_CUDA) return status;
+    if (g.dim == 3) k_subgrad_bc<double, 3><<<fgrid, 256, 0, s>>>(g, (const double*)S->x, u);
+    else k_subgrad_bc<double, 2><<<fgrid, 256, 0, s>>>(g, (const double*)S->x, u);
+  }
+  if (p_out) cudaMemcpyAsync(p_out, S->x, (S->dtype == FM_F32 ? 4 : 8) * n, cudaMemcpyDeviceToDevice, s);
+  if (check_launch()) return FM_ERR_CUDA;
+  return status;
+}
+
+int fm_mgpcg_solve(fm_mgpcg* S, const void* b, void* x, void* stream, int* iters, double* rtr) {
+  if (!S || !b || !x) return FM_ERR_ARG;
+  cudaStream_t s = (cudaStream_t)stream;
+  const long n = S->lv[0].size();
+  int status;
+  if (S->dtype == FM_F32) {
+    k_load_rhs<float><<<kRedBlocks, kRedThreads, 0, s>>>(n, (const float*)b, (float*)S->r[0], (float*)S->x, S->part);
+    status = run_solve<float>(S, s, iters, rtr);
+  } else {
+    k_load_rhs<double><<<kRedBlocks, kRedThreads, 0, s>>>(n, (const double*)b, (double*)S->r[0], (double*)S->x, S->part);
+    status = run_solve<double>(S, s, iters, rtr);
+  }
+  if (status == FM_ERR_CUDA) return status;
+  cudaMemcpyAsync(x, S->x, (S->dtype == FM_F32 ? 4 : 8) * n, cudaMemcpyDeviceToDevice, s);
+  if (check_launch()) return FM_ERR_CUDA;
+  return status;
+}
+
+int fm_laplacian(const fm_grid* g, int dtype, const void* p, void* Ap, void* stream) {
+  int st = validate_grid(g, dtype);
+  if (st) return st;
+  if (!p || !Ap) return FM_ERR_ARG;
+  Shape s = cell_shape(*g);
+  cudaStream_t cs = (cudaStream_t)stream;
+  unsigned nb = blocks_for(s.size(), 256, 148L * 16);
+  if (dtype == FM_F32) {
+    if (g->dim == 3) k_laplacian<float, 3><<<nb, 256, 0, cs>>>(s, (const float*)p, (float*)Ap);
+    else k_laplacian<float, 2><<<nb, 256, 0, cs>>>(s, (const float*)p, (float*)Ap);
+  } else {
+    if (g->dim == 3) k_laplacian<double, 3><<<nb, 256, 0, cs>>>(s, (const double*)p, (double*)Ap);
+    else k_laplacian<double, 2><<<nb, 256, 0, cs>>>(s, (const double*)p, (double*)Ap);
+  }
+  return check_launch();
+}
+
+int fm_abi_version(void) { return 1; }
+
+const char* fm_status_string(int status) {
+  switch (status) {
+    case FM_OK: return "ok";
+    case FM_ERR_SHAPE: return "unsupported grid shape";
+    case FM_ERR_ARG: return "invalid argument";
+    case FM_ERR_NOT_CONVERGED: return "MGPCG did not converge within max_iters";
+    case FM_ERR_NONFINITE: return "non-finite residual in MGPCG";
+    case FM_ERR_TIMEOUT: return "bounded device wait timed out";
+    case FM_ERR_CUDA: return "CUDA runtime error";
+    case FM_ERR_DTYPE: return "unsupported dtype";
+    default: return "unknown status";
+  }
+}
+
+}  // extern "C"

@@ -1,0 +1,166 @@
+"""Thin, typed wrappers over the C ABI (one function per entry point).
+
+Fields are torch CUDA tensors.  A MAC velocity is a tuple of ``dim`` face
+tensors; vector fields on a grid (psi, T, phi, F) are ``(dim, *grid)``
+tensors (SoA planes), matching include/flowmap_sm100.h.
+"""
+from __future__ import annotations
+
+import ctypes as C
+from dataclasses import dataclass
+from typing import Optional, Sequence, Tuple
+
+import torch
+
+from . import _lib
+from ._lib import check, dtype_code, ptr, stream_ptr
+
+
+@dataclass(frozen=True)
+class GridSpec:
+    """Cell counts of a 2D (nz == 1) or 3D grid."""
+
+    shape: Tuple[int, ...]
+
+    @property
+    def dim(self) -> int:
+        return len(self.shape)
+
+    def c_grid(self) -> _lib.Grid:
+        n = list(self.shape) + [1] * (3 - self.dim)
+        return _lib.Grid(self.dim, (C.c_int * 3)(*n))
+
+    def face_shape(self, c: int) -> Tuple[int, ...]:
+        s = list(self.shape)
+        s[c] += 1
+        return tuple(s)
+
+    @property
+    def ncell(self) -> int:
+        n = 1
+        for v in self.shape:
+            n *= v
+        return n
+
+    @staticmethod
+    def from_mac(u: Sequence[torch.Tensor]) -> "GridSpec":
+        dim = len(u)
+        s = list(u[0].shape[-dim:])
+        s[0] -= 1
+        return GridSpec(tuple(s))
+
+    def which_grid(self, t: torch.Tensor) -> int:
+        """Face index (0..dim-1) of a field, or -1 for the cell grid."""
+        sh = tuple(t.shape[-self.dim:])
+        if sh == tuple(self.shape):
+            return -1
+        for c in range(self.dim):
+            if sh == self.face_shape(c):
+                return c
+        raise _lib.FlowmapError(1, f"field shape {tuple(t.shape)} does not match grid {self.shape}")
+
+
+def _mac3(u):
+    u = list(u) if u is not None else []
+    return [ptr(x) for x in u] + [None] * (3 - len(u))
+
+
+def _dt(t: torch.Tensor) -> int:
+    return dtype_code(t.dtype)
+
+
+def _chk_mac(g: GridSpec, u, name):
+    if len(u) != g.dim:
+        raise _lib.FlowmapError(2, f"{name}: expected {g.dim} components")
+    for c, x in enumerate(u):
+        if tuple(x.shape) != g.face_shape(c):
+            raise _lib.FlowmapError(1, f"{name}[{c}] has shape {tuple(x.shape)}, expected {g.face_shape(c)}")
+
+
+def _chk_vec(g: GridSpec, t, face, name):
+    want = (g.dim,) + (g.face_shape(face) if face >= 0 else tuple(g.shape))
+    if tuple(t.shape) != want:
+        raise _lib.FlowmapError(1, f"{name} has shape {tuple(t.shape)}, expected {want}")
+
+
+def advect_u_grid(g: GridSpec, rk: int, dx: float, dt: float, u0, u1, u2, stream=None):
+    for n, u in (("u0", u0), ("u1", u1), ("u2", u2)):
+        _chk_mac(g, u, n)
+    check(_lib.lib().fm_advect_u_grid(C.byref(g.c_grid()), _dt(u0[0]), rk, dx, dt, *_mac3(u0), *_mac3(u1),
+                                      *_mac3(u2), stream_ptr(stream)), "fm_advect_u_grid")
+
+
+def advect_scalar_grid(g: GridSpec, rk: int, dx: float, dt: float, u0, s1, s2, stream=None):
+    _chk_mac(g, u0, "u0")
+    check(_lib.lib().fm_advect_scalar_grid(C.byref(g.c_grid()), _dt(u0[0]), rk, dx, dt, *_mac3(u0), ptr(s1), ptr(s2),
+                                           stream_ptr(stream)), "fm_advect_scalar_grid")
+
+
+def rk_grid(g: GridSpec, rk: int, dx: float, dt: float, face: int, psi, T, u, stream=None):
+    _chk_mac(g, u, "u")
+    _chk_vec(g, psi, face, "psi")
+    if T is not None:
+        _chk_vec(g, T, face, "T")
+    check(_lib.lib().fm_rk_grid(C.byref(g.c_grid()), _dt(psi), rk, dx, dt, face, ptr(psi), ptr(T), *_mac3(u),
+                                stream_ptr(stream)), "fm_rk_grid")
+
+
+def march_map(g: GridSpec, rk: int, dx: float, dt: float, psi_c, psi_f, T_f, u, stream=None):
+    _chk_mac(g, u, "u")
+    ps = list(psi_f) + [None] * (3 - g.dim)
+    ts = list(T_f) + [None] * (3 - g.dim)
+    check(_lib.lib().fm_march_map(C.byref(g.c_grid()), _dt(u[0]), rk, dx, dt, ptr(psi_c), ptr(ps[0]), ptr(ts[0]),
+                                  ptr(ps[1]), ptr(ts[1]), ptr(ps[2]), ptr(ts[2]), *_mac3(u), stream_ptr(stream)),
+          "fm_march_map")
+
+
+def pullback_u(g: GridSpec, dx: float, u0, out, T_f, psi_f, alpha=1.0, beta=0.0, base=None, stream=None):
+    _chk_mac(g, u0, "u0")
+    _chk_mac(g, out, "out")
+    check(_lib.lib().fm_pullback_u(C.byref(g.c_grid()), _dt(u0[0]), dx, *_mac3(u0), *_mac3(out), *_mac3(T_f),
+                                   *_mac3(psi_f), alpha, beta, *_mac3(base), stream_ptr(stream)), "fm_pullback_u")
+
+
+def pullback_scalar(g: GridSpec, dx: float, s0, out, psi, alpha=1.0, beta=0.0, base=None, stream=None):
+    check(_lib.lib().fm_pullback_scalar(C.byref(g.c_grid()), _dt(s0), dx, ptr(s0), ptr(out), ptr(psi), alpha, beta,
+                                        ptr(base), stream_ptr(stream)), "fm_pullback_scalar")
+
+
+def accumulate_init(g: GridSpec, dx: float, dt: float, f, init, F_f, phi_f, Hp=None, Hpp=None, ind=0, stream=None):
+    ab3 = Hp is not None
+    hs = []
+    for c in range(3):
+        hs += [ptr(Hp[c]) if ab3 and c < g.dim else None, ptr(Hpp[c]) if ab3 and c < g.dim else None]
+    check(_lib.lib().fm_accumulate_init(C.byref(g.c_grid()), _dt(f[0]), dx, dt, int(ab3), ind, *_mac3(f),
+                                        *_mac3(init), *_mac3(F_f), *_mac3(phi_f), *hs, stream_ptr(stream)),
+          "fm_accumulate_init")
+
+
+def nabla_u_w(g: GridSpec, dx: float, u, w, r, order: Optional[int] = None, stream=None):
+    if order is None:
+        order = 3 if g.dim == 3 else 4
+    check(_lib.lib().fm_nabla_u_w(C.byref(g.c_grid()), _dt(u[0]), order, dx, *_mac3(u), *_mac3(w), *_mac3(r),
+                                  stream_ptr(stream)), "fm_nabla_u_w")
+
+
+def nabla_scalar_adjoint(g: GridSpec, dx: float, s, adj, r, stream=None):
+    check(_lib.lib().fm_nabla_scalar_adjoint(C.byref(g.c_grid()), _dt(s), dx, ptr(s), ptr(adj), *_mac3(r),
+                                             stream_ptr(stream)), "fm_nabla_scalar_adjoint")
+
+
+def reset_to_identity(g: GridSpec, dx: float, psi_c, psi_f, T_f, stream=None):
+    t = psi_c if psi_c is not None else (psi_f[0] if psi_f else T_f[0])
+    check(_lib.lib().fm_reset_to_identity(C.byref(g.c_grid()), _dt(t), dx, ptr(psi_c), *_mac3(psi_f), *_mac3(T_f),
+                                          stream_ptr(stream)), "fm_reset_to_identity")
+
+
+def add_fields(f1, f2, dest, m: float, stream=None):
+    """dest = f1 + m * f2 (elementwise, same shapes)."""
+    if f1.shape != f2.shape or f1.shape != dest.shape:
+        raise _lib.FlowmapError(1, "add_fields shape mismatch")
+    check(_lib.lib().fm_add_fields(_dt(dest), dest.numel(), ptr(f1), ptr(f2), ptr(dest), m, stream_ptr(stream)),
+          "fm_add_fields")
+
+
+def laplacian(g: GridSpec, p, Ap, stream=None):
+    check(_lib.lib().fm_laplacian(C.byref(g.c_grid()), _dt(p), ptr(p), ptr(Ap), stream_ptr(stream)), "fm_laplacian")

@@ -1,0 +1,135 @@
+"""MGPCG pressure projection with the reference's solver interface.
+
+``MGPCG_3`` / ``MGPCG_2`` mirror 3D/mgpcg.py:359-439 and 2D/shape/mgpcg.py:292-368
+(plain all-Neumann solver, base_level 3, bottom smoothing 50, absolute
+tolerance rTr < 1e-12, max 400 iterations).  ``MGPCG_2_solid`` mirrors
+2D/vortex/mgpcg_solid.py:370-458 with an empty obstacle mask (base_level 4,
+20 bottom sweeps as 10 x (R,B) + 10 x (B,R), tol = max(1e-14, 1e-16 zTr0)).
+``Poisson(u_x, u_y[, u_z])`` projects in place; ``Poisson_adj`` is the same
+operation (3D/fast_mgpcg.py:283-323 differs from Poisson only in name).
+
+Every solve runs on the device (libflowmap_sm100.so); there is no CPU path.
+"""
+from __future__ import annotations
+
+import ctypes as C
+import math
+import warnings
+from typing import Optional, Sequence
+
+import torch
+
+from . import _lib
+from .kernels import GridSpec
+
+
+class MGPCG:
+    """Owns the device MG hierarchy for one grid shape and dtype."""
+
+    def __init__(self, N: Sequence[int], dtype=torch.float32, *, base_level: int = 3, levels: Optional[int] = None,
+                 pre_post: int = 2, bottom: int = 50, bottom_mode: int = 0, max_iters: int = 400,
+                 abs_tol: float = 1e-12, rel_tol: float = 0.0, eps: float = 1e-12, check_every: int = 4,
+                 raise_on_nonconvergence: bool = False):
+        self.N = tuple(int(n) for n in N)
+        self.grid = GridSpec(self.N)
+        self.dtype = dtype
+        if levels is None:
+            levels = int(math.log2(min(self.N))) - base_level + 1
+        self.params = _lib.MGParams(levels, pre_post, bottom, bottom_mode, max_iters, abs_tol, rel_tol, eps,
+                                    check_every, 0)
+        self.raise_on_nonconvergence = raise_on_nonconvergence
+        self._h = C.c_void_p()
+        _lib.check(_lib.lib().fm_mgpcg_create(C.byref(self.grid.c_grid()), _lib.dtype_code(dtype),
+                                              C.byref(self.params), C.byref(self._h)), "fm_mgpcg_create")
+        self.last_iters = 0
+        self.last_rtr = 0.0
+        self.last_converged = True
+        self.history = []
+
+    @property
+    def n_mg_levels(self) -> int:
+        return self.params.levels
+
+    def close(self):
+        if self._h:
+            _lib.lib().fm_mgpcg_destroy(self._h)
+            self._h = C.c_void_p()
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def _status(self, st: int, where: str, it: C.c_int, rtr: C.c_double):
+        self.last_iters = it.value
+        self.last_rtr = rtr.value
+        self.last_converged = st == 0
+        self.history.append((it.value, rtr.value))
+        if st == 3:  # FM_ERR_NOT_CONVERGED: the reference continues silently
+            if self.raise_on_nonconvergence:
+                _lib.check(st, where)
+            return
+        _lib.check(st, where)
+
+    def project(self, u: Sequence[torch.Tensor], p_out: Optional[torch.Tensor] = None, stream=None):
+        """In-place pressure projection of the MAC velocity ``u``."""
+        if len(u) != self.grid.dim:
+            raise _lib.FlowmapError(2, "project: wrong number of components")
+        for c, x in enumerate(u):
+            if tuple(x.shape) != self.grid.face_shape(c) or x.dtype != self.dtype:
+                raise _lib.FlowmapError(1, f"project: component {c} shape/dtype mismatch")
+        ps = [_lib.ptr(x) for x in u] + [None] * (3 - len(u))
+        it, rtr = C.c_int(0), C.c_double(0)
+        st = _lib.lib().fm_project(self._h, ps[0], ps[1], ps[2], _lib.ptr(p_out), _lib.stream_ptr(stream),
+                                   C.byref(it), C.byref(rtr))
+        self._status(st, "fm_project", it, rtr)
+
+    def solve(self, b: torch.Tensor, x: torch.Tensor, stream=None):
+        it, rtr = C.c_int(0), C.c_double(0)
+        st = _lib.lib().fm_mgpcg_solve(self._h, _lib.ptr(b), _lib.ptr(x), _lib.stream_ptr(stream), C.byref(it),
+                                       C.byref(rtr))
+        self._status(st, "fm_mgpcg_solve", it, rtr)
+        return it.value, rtr.value
+
+    # reference names -------------------------------------------------------
+    def Poisson(self, *u, verbose: bool = False):
+        self.project(u)
+        if verbose:
+            print(f"[MGPCG] iters={self.last_iters} |r|={math.sqrt(max(self.last_rtr, 0.0)):.3e} "
+                  f"converged={self.last_converged}")
+
+    def Poisson_adj(self, *u, verbose: bool = False):
+        self.Poisson(*u, verbose=verbose)
+
+
+class MGPCG_3(MGPCG):
+    """3D/mgpcg.py:359 MGPCG_3(boundary_types, N, base_level=3)."""
+
+    def __init__(self, boundary_types=None, N=(128, 128, 128), base_level=3, real=None, dtype=torch.float32, **kw):
+        kw.setdefault("bottom", 50)
+        kw.setdefault("abs_tol", 1e-12)
+        super().__init__(N, dtype, base_level=base_level, **kw)
+
+
+class MGPCG_2(MGPCG):
+    """2D/shape/mgpcg.py:292 MGPCG_2(boundary_types, N, base_level=3)."""
+
+    def __init__(self, boundary_types=None, N=(256, 256), base_level=3, real=None, dtype=torch.float32, **kw):
+        kw.setdefault("bottom", 50)
+        kw.setdefault("abs_tol", 1e-12)
+        super().__init__(N, dtype, base_level=base_level, **kw)
+
+
+class MGPCG_2_solid(MGPCG):
+    """2D/vortex/mgpcg_solid.py:370 with an empty obstacle mask."""
+
+    def __init__(self, boundary_types=None, boundary_mask=None, boundary_vel=None, N=(256, 256), base_level=4,
+                 real=None, dtype=torch.float32, **kw):
+        if boundary_mask is not None and bool((boundary_mask > 0).any()):
+            raise _lib.FlowmapError(2, "MGPCG_2_solid: obstacle masks are not supported by this build")
+        kw.setdefault("bottom", 20)
+        kw.setdefault("bottom_mode", 1)
+        kw.setdefault("abs_tol", 1e-14)
+        kw.setdefault("rel_tol", 1e-16)
+        super().__init__(N, dtype, base_level=4, **kw)

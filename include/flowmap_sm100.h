@@ -1,0 +1,180 @@
+/*
+ * flowmap_sm100.h -- C ABI of libflowmap_sm100.so, the B200 (sm_100a) kernels
+ * for the leapfrog flow-map fluid step, its adjoint and the MGPCG pressure
+ * projection of pearseven/differentiable-flowmap.
+ *
+ * Every entry point takes raw device pointers, an explicit grid descriptor, a
+ * dtype selector (FM_F32: the reference's ti.f32 arithmetic; FM_F64: the FP64
+ * run used to state errors) and a cudaStream_t passed as `void *`.  Work is
+ * stream-ordered; nothing synchronises the host except fm_project /
+ * fm_mgpcg_solve in host-checked mode (see fm_mg_params.check_every).
+ * No entry point allocates memory except fm_mgpcg_create.
+ *
+ * Layout: scalar fields are C-order [i][j][k], k fastest.  2D grids use
+ * dim = 2 and n[2] = 1.  MAC face grid c has extent n[c]+1 on axis c.
+ * Vector fields on a grid (psi, T, phi, F) are SoA: dim consecutive planes of
+ * that grid's size.  For 2D calls the *_z pointers must be NULL.
+ *
+ * Return value: FM_OK or one of the FM_ERR_* codes below.
+ */
+#ifndef FLOWMAP_SM100_H
+#define FLOWMAP_SM100_H
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+typedef struct {
+    int dim;   /* 2 or 3 */
+    int n[3];  /* cell counts; n[2] == 1 when dim == 2 */
+} fm_grid;
+
+enum { FM_F32 = 0, FM_F64 = 1 };
+
+enum {
+    FM_OK = 0,
+    FM_ERR_SHAPE = 1,          /* bad grid / unsupported size */
+    FM_ERR_ARG = 2,            /* NULL pointer, bad rk/order/flag */
+    FM_ERR_NOT_CONVERGED = 3,  /* MGPCG hit max_iters without meeting the tolerance */
+    FM_ERR_NONFINITE = 4,      /* NaN/Inf residual in MGPCG */
+    FM_ERR_TIMEOUT = 5,        /* a bounded device wait gave up */
+    FM_ERR_CUDA = 6,           /* CUDA runtime error (launch/alloc) */
+    FM_ERR_DTYPE = 7           /* dtype not FM_F32/FM_F64 */
+};
+
+int fm_abi_version(void);
+const char *fm_status_string(int status);
+
+/* advect_u_grid: semi-Lagrangian advection, RK2 (midpoint) or RK4 backtrace
+ * of the face nodes through u0, then u2_c = (u1 sampled at the foot)_c.
+ * Replaces RK2_advect_u_grid / RK4_advect_u_grid (3D/flowmap.py:202-282,
+ * dispatch 3D/flowmap.py:27-37; 2D/vortex/flowmap.py:233-291).
+ * u2 must not alias u0 or u1. */
+int fm_advect_u_grid(const fm_grid *g, int dtype, int rk, double dx, double dt,
+                     const void *u0x, const void *u0y, const void *u0z,
+                     const void *u1x, const void *u1y, const void *u1z,
+                     void *u2x, void *u2y, void *u2z, void *stream);
+
+/* advect_scalar_grid: the same backtrace from cell centres, quadratic sample
+ * of s1.  Replaces RK2/RK4_advect_scalar_grid (3D/flowmap.py:284-320,
+ * dispatch :39-49).  s2 must not alias s1. */
+int fm_advect_scalar_grid(const fm_grid *g, int dtype, int rk, double dx, double dt,
+                          const void *u0x, const void *u0y, const void *u0z,
+                          const void *s1, void *s2, void *stream);
+
+/* RK_grid / RK_grid_only_psi: in-place march of a flow map (psi, dim planes)
+ * and, when T != NULL, its Jacobian rows (T, dim planes) with neg_dt = -dt.
+ * face = 0..dim-1 selects face grid c, face = -1 the cell-centre grid
+ * (T must then be NULL).  Replaces RK2_grid/RK4_grid (3D/flowmap.py:85-137)
+ * and RK*_grid_only_psi (3D/flowmap.py:139-179), dispatch :6-25. */
+int fm_rk_grid(const fm_grid *g, int dtype, int rk, double dx, double dt, int face,
+               void *psi, void *T, const void *ux, const void *uy, const void *uz, void *stream);
+
+/* March the centre map and all face maps with their Jacobians in one launch:
+ * march_phi_grid / march_psi_grid / march_no_neural
+ * (3D/lfm_midpoint_simulator.py:357-381, 3D/lfm_midpoint_diff_simulator.py:384-388).
+ * psi_c may be NULL (no centre map). */
+int fm_march_map(const fm_grid *g, int dtype, int rk, double dx, double dt,
+                 void *psi_c, void *psi_x, void *T_x, void *psi_y, void *T_y, void *psi_z, void *T_z,
+                 const void *ux, const void *uy, const void *uz, void *stream);
+
+/* advect_u (impulse pullback) with a fused epilogue:
+ *   out_c = alpha * (T_c . u0(psi_c) + beta * base_c)
+ * alpha=1, beta=0 is the reference's advect_u (3D/flowmap.py:51-69); the two
+ * other BFECC passes (3D/flowmap.py:405-434) are alpha=0.5, beta=-1,
+ * base=init and alpha=-1, beta=-1, base=u (in place).  base may be NULL when
+ * beta == 0 and may alias out; out must not alias u0. */
+int fm_pullback_u(const fm_grid *g, int dtype, double dx,
+                  const void *u0x, const void *u0y, const void *u0z,
+                  void *outx, void *outy, void *outz,
+                  const void *Tx, const void *Ty, const void *Tz,
+                  const void *psix, const void *psiy, const void *psiz,
+                  double alpha, double beta,
+                  const void *basex, const void *basey, const void *basez, void *stream);
+
+/* advect_scalar with the same epilogue: out = alpha*(s0(psi) + beta*base).
+ * Replaces advect_scalar (3D/flowmap.py:71-79) and the BFECC_scalar passes
+ * (3D/flowmap.py:436-452). */
+int fm_pullback_scalar(const fm_grid *g, int dtype, double dx, const void *s0, void *out,
+                       const void *psi, double alpha, double beta, const void *base, void *stream);
+
+/* accumulate_init (ab3 = 0) / accumulate_init_new (ab3 = 1): pull a face
+ * force back to the reinit frame, init_c += F_c . f(phi_c) * dt, with the
+ * reference's Adams-Bashforth-3 history (including its ind == 1 formula).
+ * Replaces 3D/flowmap.py:485-545 / 2D/vortex/flowmap.py:508-553.
+ * Hp/Hpp (3 pointers each) are read and updated when ab3 = 1. */
+int fm_accumulate_init(const fm_grid *g, int dtype, double dx, double dt, int ab3, int ind,
+                       const void *fx, const void *fy, const void *fz,
+                       void *initx, void *inity, void *initz,
+                       const void *Fx, const void *Fy, const void *Fz,
+                       const void *phix, const void *phiy, const void *phiz,
+                       void *Hpx, void *Hppx, void *Hpy, void *Hppy, void *Hpz, void *Hppz,
+                       void *stream);
+
+/* calculate_nabla_u_w: r_c = ((grad u)^T w)_c at face nodes, B-spline of
+ * `order` (3 = cubic, as 3D/flowmap.py:359-380; 4 = quartic, as
+ * 2D/vortex/flowmap.py:361-377). */
+int fm_nabla_u_w(const fm_grid *g, int dtype, int order, double dx,
+                 const void *ux, const void *uy, const void *uz,
+                 const void *wx, const void *wy, const void *wz,
+                 void *rx, void *ry, void *rz, void *stream);
+
+/* calculate_nabla_scalar_adjoint: r_c = (d_c s) * adj_s at face nodes, cubic.
+ * Replaces 3D/flowmap.py:382-403. */
+int fm_nabla_scalar_adjoint(const fm_grid *g, int dtype, double dx, const void *s, const void *adj,
+                            void *rx, void *ry, void *rz, void *stream);
+
+/* reset_to_identity (3D/flowmap.py:336-356).  Any pointer may be NULL. */
+int fm_reset_to_identity(const fm_grid *g, int dtype, double dx, void *psi_c,
+                         void *psi_x, void *psi_y, void *psi_z, void *T_x, void *T_y, void *T_z,
+                         void *stream);
+
+/* add_fields: dest = f1 + m * f2 over n elements (3D/taichi_utils.py:86-89).
+ * dest may alias f1 or f2. */
+int fm_add_fields(int dtype, long n, const void *f1, const void *f2, void *dest, double m, void *stream);
+
+/* ------------------------------------------------------------------------
+ * MGPCG pressure projection.  Replaces MGPCG_3 / MGPCG_2 / MGPCG_2_solid
+ * (3D/mgpcg.py:12-439, 2D/shape/mgpcg.py, 2D/vortex/mgpcg_solid.py) and the
+ * 3D fast_mgpcg wrapper (3D/fast_mgpcg.py:241-323), empty obstacle mask.
+ * ------------------------------------------------------------------------ */
+typedef struct {
+    int levels;        /* MG levels (reference: log2(min n) - base_level + 1) */
+    int pre_post;      /* RBGS sweeps per level down and up (reference: 2) */
+    int bottom;        /* bottom smoothing count */
+    int bottom_mode;   /* 0: bottom x (R,B) [3D/mgpcg.py:197-199];
+                          1: bottom/2 x (R,B) + bottom/2 x (B,R) [mgpcg_solid.py:263-268] */
+    int max_iters;     /* reference: 400 */
+    double abs_tol;    /* converged when rTr < max(abs_tol, rel_tol * zTr0) */
+    double rel_tol;
+    double eps;        /* added to alpha/beta denominators (reference: 1e-12) */
+    int check_every;   /* iterations per host convergence check (>= 1) */
+    int coarse_bf16;   /* 1: store levels >= 1 in BF16 (FM_F32 only) */
+} fm_mg_params;
+
+typedef struct fm_mgpcg fm_mgpcg;
+
+/* Allocates the MG hierarchy for one grid shape.  The only allocating call. */
+int fm_mgpcg_create(const fm_grid *g, int dtype, const fm_mg_params *params, fm_mgpcg **out);
+int fm_mgpcg_destroy(fm_mgpcg *solver);
+
+/* Poisson(u): apply_bc, divergence, solve A p = -div, u -= grad p, apply_bc,
+ * in place on the MAC velocity (3D/mgpcg.py:434-439).  Used for both
+ * Poisson and Poisson_adj (3D/fast_mgpcg.py:241-323, which differ only in
+ * name).  iters (reference `it`) and rtr (last r.r) may be NULL.
+ * p_out (cell grid) receives the pressure when not NULL.
+ * Returns FM_ERR_NOT_CONVERGED when max_iters was reached (the reference
+ * continues silently; the host decides). */
+int fm_project(fm_mgpcg *solver, void *ux, void *uy, void *uz, void *p_out, void *stream,
+               int *iters, double *rtr);
+
+/* Solve A x = b (b cell grid, recentred internally as the reference does). */
+int fm_mgpcg_solve(fm_mgpcg *solver, const void *b, void *x, void *stream, int *iters, double *rtr);
+
+/* Apply the Neumann Laplacian: Ap = A p (for tests and defect correction). */
+int fm_laplacian(const fm_grid *g, int dtype, const void *p, void *Ap, void *stream);
+
+#ifdef __cplusplus
+}
+#endif
+#endif /* FLOWMAP_SM100_H */

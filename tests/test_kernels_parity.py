@@ -1,0 +1,313 @@
+"""Kernel-level parity: every CUDA entry point vs the CPU oracle on the same
+seeded inputs (FP64 CUDA vs FP64 oracle, FP32 CUDA vs FP32 oracle).
+
+Tolerances: FP64 agree to 1e-10 relative to the field scale (only summation
+order differs); FP32 to 2e-5.
+"""
+import numpy as np
+import pytest
+import torch
+
+from oracle import MGParams, Oracle
+
+pytestmark = pytest.mark.gpu
+
+GRIDS = [(16, 16, 16), (12, 16, 20), (32, 32), (24, 40)]
+PRECS = [("f64", torch.float64, 1e-10), ("f32", torch.float32, 2e-5)]
+
+
+def _rand_mac(rng, shape, scale):
+    dim = len(shape)
+    out = []
+    for c in range(dim):
+        s = list(shape)
+        s[c] += 1
+        out.append(rng.uniform(-scale, scale, size=s))
+    return out
+
+
+def _rand_pos(rng, shape, grid_shape, dx, spread=2.5):
+    """Positions near the nodes of `grid_shape` plus a few outside the box."""
+    dim = len(shape)
+    base = np.stack(np.meshgrid(*[(np.arange(n) + 0.5) * dx for n in grid_shape], indexing="ij"))
+    p = base + rng.uniform(-spread * dx, spread * dx, size=base.shape)
+    p.reshape(dim, -1)[:, ::7] = rng.uniform(-0.1, 1.1, size=(dim, p.reshape(dim, -1)[:, ::7].shape[1]))
+    return p
+
+
+def _t(a, dtype, dev):
+    return torch.tensor(np.ascontiguousarray(a), dtype=dtype, device=dev)
+
+
+def _np(t):
+    return t.detach().cpu().numpy().astype(np.float64)
+
+
+def _rel(a, b):
+    a = np.asarray(a, np.float64)
+    b = np.asarray(b, np.float64)
+    return np.abs(a - b).max() / max(np.abs(b).max(), 1e-30)
+
+
+@pytest.fixture(params=GRIDS, ids=lambda s: "x".join(map(str, s)))
+def shape(request):
+    return request.param
+
+
+@pytest.fixture(params=PRECS, ids=lambda p: p[0])
+def prec(request):
+    return request.param
+
+
+def setup(shape, prec, seed=0):
+    rng = np.random.default_rng(seed)
+    name, dtype, tol = prec
+    o = Oracle(shape, name)
+    dx = 1.0 / shape[1]
+    return rng, o, dtype, tol, dx
+
+
+@pytest.mark.parametrize("rk", [2, 4])
+def test_advect_u_grid(fm, cuda, shape, prec, rk):
+    rng, o, dtype, tol, dx = setup(shape, prec)
+    g = fm.GridSpec(shape)
+    u0 = _rand_mac(rng, shape, 1.0)
+    u1 = _rand_mac(rng, shape, 1.0)
+    dt = 0.7 * dx
+    ref = [np.zeros_like(x, dtype=o.dtype) for x in u0]
+    o.advect_u_grid(rk, [x.astype(o.dtype) for x in u0], [x.astype(o.dtype) for x in u1], ref, dx, dt)
+    out = [torch.zeros(x.shape, dtype=dtype, device=cuda) for x in u0]
+    fm.kernels.advect_u_grid(g, rk, dx, dt, [_t(x, dtype, cuda) for x in u0], [_t(x, dtype, cuda) for x in u1], out)
+    torch.cuda.synchronize()
+    for c in range(len(shape)):
+        assert _rel(_np(out[c]), ref[c]) < tol
+
+
+@pytest.mark.parametrize("rk", [2, 4])
+def test_advect_scalar_grid(fm, cuda, shape, prec, rk):
+    rng, o, dtype, tol, dx = setup(shape, prec, 1)
+    g = fm.GridSpec(shape)
+    u0 = _rand_mac(rng, shape, 1.0)
+    s1 = rng.uniform(0, 1, size=shape)
+    dt = 0.7 * dx
+    ref = np.zeros(shape, o.dtype)
+    o.advect_scalar_grid(rk, [x.astype(o.dtype) for x in u0], s1.astype(o.dtype), ref, dx, dt)
+    out = torch.zeros(shape, dtype=dtype, device=cuda)
+    fm.kernels.advect_scalar_grid(g, rk, dx, dt, [_t(x, dtype, cuda) for x in u0], _t(s1, dtype, cuda), out)
+    torch.cuda.synchronize()
+    assert _rel(_np(out), ref) < tol
+
+
+@pytest.mark.parametrize("rk", [2, 4])
+@pytest.mark.parametrize("face", [-1, 0, 1])
+def test_rk_grid(fm, cuda, shape, prec, rk, face):
+    rng, o, dtype, tol, dx = setup(shape, prec, 2)
+    g = fm.GridSpec(shape)
+    dim = len(shape)
+    u = _rand_mac(rng, shape, 1.0)
+    gshape = shape if face < 0 else g.face_shape(face)
+    psi = _rand_pos(rng, shape, gshape, dx)
+    T = None if face < 0 else rng.uniform(-1, 1, size=(dim,) + tuple(gshape))
+    for dt in (0.6 * dx, -0.6 * dx):
+        p_ref = psi.astype(o.dtype).copy()
+        T_ref = None if T is None else T.astype(o.dtype).copy()
+        o.RK_grid(rk, face, p_ref, T_ref, [x.astype(o.dtype) for x in u], dx, dt)
+        p_d = _t(psi, dtype, cuda)
+        T_d = None if T is None else _t(T, dtype, cuda)
+        fm.kernels.rk_grid(g, rk, dx, dt, face, p_d, T_d, [_t(x, dtype, cuda) for x in u])
+        torch.cuda.synchronize()
+        assert _rel(_np(p_d), p_ref) < tol
+        if T is not None:
+            assert _rel(_np(T_d), T_ref) < tol * 10
+
+
+def test_march_map_matches_per_grid(fm, cuda, shape, prec):
+    rng, o, dtype, tol, dx = setup(shape, prec, 3)
+    g = fm.GridSpec(shape)
+    dim = len(shape)
+    u = [_t(x, dtype, cuda) for x in _rand_mac(rng, shape, 1.0)]
+    psi_c = _t(_rand_pos(rng, shape, shape, dx), dtype, cuda)
+    psi_f = [_t(_rand_pos(rng, shape, g.face_shape(c), dx), dtype, cuda) for c in range(dim)]
+    T_f = [_t(rng.uniform(-1, 1, size=(dim,) + g.face_shape(c)), dtype, cuda) for c in range(dim)]
+    a = [x.clone() for x in [psi_c] + psi_f + T_f]
+    for rk in (2, 4):
+        fm.kernels.march_map(g, rk, dx, 0.5 * dx, a[0], a[1:1 + dim], a[1 + dim:], u)
+        b = [x.clone() for x in [psi_c] + psi_f + T_f]
+        fm.kernels.rk_grid(g, rk, dx, 0.5 * dx, -1, b[0], None, u)
+        for c in range(dim):
+            fm.kernels.rk_grid(g, rk, dx, 0.5 * dx, c, b[1 + c], b[1 + dim + c], u)
+        for x, y in zip(a, b):
+            assert torch.equal(x, y)
+        a = [x.clone() for x in [psi_c] + psi_f + T_f]
+
+
+def test_pullback_u_and_bfecc_epilogues(fm, cuda, shape, prec):
+    rng, o, dtype, tol, dx = setup(shape, prec, 4)
+    g = fm.GridSpec(shape)
+    dim = len(shape)
+    u0 = _rand_mac(rng, shape, 1.0)
+    psi = [_rand_pos(rng, shape, g.face_shape(c), dx) for c in range(dim)]
+    T = [rng.uniform(-1, 1, size=(dim,) + g.face_shape(c)) for c in range(dim)]
+    base = _rand_mac(rng, shape, 1.0)
+    ref = [np.zeros(g.face_shape(c), o.dtype) for c in range(dim)]
+    o.advect_u([x.astype(o.dtype) for x in u0], ref, [x.astype(o.dtype) for x in T], [x.astype(o.dtype) for x in psi],
+               dx)
+    out = [torch.zeros(g.face_shape(c), dtype=dtype, device=cuda) for c in range(dim)]
+    U0 = [_t(x, dtype, cuda) for x in u0]
+    Td = [_t(x, dtype, cuda) for x in T]
+    Pd = [_t(x, dtype, cuda) for x in psi]
+    fm.kernels.pullback_u(g, dx, U0, out, Td, Pd)
+    torch.cuda.synchronize()
+    for c in range(dim):
+        assert _rel(_np(out[c]), ref[c]) < tol
+    # err = 0.5 * (pull - base) ; final = base - pull
+    B = [_t(x, dtype, cuda) for x in base]
+    fm.kernels.pullback_u(g, dx, U0, out, Td, Pd, alpha=0.5, beta=-1.0, base=B)
+    for c in range(dim):
+        assert _rel(_np(out[c]), 0.5 * (ref[c] - base[c])) < tol
+    Bc = [x.clone() for x in B]
+    fm.kernels.pullback_u(g, dx, U0, Bc, Td, Pd, alpha=-1.0, beta=-1.0, base=Bc)
+    for c in range(dim):
+        assert _rel(_np(Bc[c]), base[c] - ref[c]) < tol
+
+
+def test_pullback_scalar(fm, cuda, shape, prec):
+    rng, o, dtype, tol, dx = setup(shape, prec, 5)
+    g = fm.GridSpec(shape)
+    s0 = rng.uniform(0, 1, size=shape)
+    psi = _rand_pos(rng, shape, shape, dx)
+    ref = np.zeros(shape, o.dtype)
+    o.advect_scalar(s0.astype(o.dtype), ref, psi.astype(o.dtype), dx)
+    out = torch.zeros(shape, dtype=dtype, device=cuda)
+    fm.kernels.pullback_scalar(g, dx, _t(s0, dtype, cuda), out, _t(psi, dtype, cuda))
+    torch.cuda.synchronize()
+    assert _rel(_np(out), ref) < tol
+
+
+@pytest.mark.parametrize("ab3,ind", [(0, 0), (1, 0), (1, 1), (1, 2), (1, 5)])
+def test_accumulate_init(fm, cuda, shape, prec, ab3, ind):
+    rng, o, dtype, tol, dx = setup(shape, prec, 6)
+    g = fm.GridSpec(shape)
+    dim = len(shape)
+    f = _rand_mac(rng, shape, 1.0)
+    init = _rand_mac(rng, shape, 1.0)
+    F = [rng.uniform(-1, 1, size=(dim,) + g.face_shape(c)) for c in range(dim)]
+    phi = [_rand_pos(rng, shape, g.face_shape(c), dx) for c in range(dim)]
+    Hp = _rand_mac(rng, shape, 1.0)
+    Hpp = _rand_mac(rng, shape, 1.0)
+    dt = -2 * 0.3 * dx
+    cv = lambda L: [np.ascontiguousarray(x, o.dtype) for x in L]
+    init_r, Hp_r, Hpp_r = cv(init), cv(Hp), cv(Hpp)
+    if ab3:
+        o.accumulate_init_new(cv(f), init_r, cv(F), cv(phi), Hp_r, Hpp_r, ind, dx, dt)
+    else:
+        o.accumulate_init(cv(f), init_r, cv(F), cv(phi), dx, dt)
+    T_ = lambda L: [_t(x, dtype, cuda) for x in L]
+    init_d, Hp_d, Hpp_d = T_(init), T_(Hp), T_(Hpp)
+    if ab3:
+        fm.kernels.accumulate_init(g, dx, dt, T_(f), init_d, T_(F), T_(phi), Hp_d, Hpp_d, ind)
+    else:
+        fm.kernels.accumulate_init(g, dx, dt, T_(f), init_d, T_(F), T_(phi))
+    torch.cuda.synchronize()
+    for c in range(dim):
+        assert _rel(_np(init_d[c]), init_r[c]) < tol
+        if ab3:
+            assert _rel(_np(Hp_d[c]), Hp_r[c]) < tol
+            assert _rel(_np(Hpp_d[c]), Hpp_r[c]) < tol
+
+
+@pytest.mark.parametrize("order", [3, 4])
+def test_nabla_u_w(fm, cuda, shape, prec, order):
+    rng, o, dtype, tol, dx = setup(shape, prec, 7)
+    g = fm.GridSpec(shape)
+    dim = len(shape)
+    u = _rand_mac(rng, shape, 1.0)
+    w = _rand_mac(rng, shape, 1.0)
+    ref = [np.zeros(g.face_shape(c), o.dtype) for c in range(dim)]
+    cv = lambda L: [np.ascontiguousarray(x, o.dtype) for x in L]
+    o.calculate_nabla_u_w(cv(u), cv(w), ref, dx, order)
+    out = [torch.zeros(g.face_shape(c), dtype=dtype, device=cuda) for c in range(dim)]
+    fm.kernels.nabla_u_w(g, dx, [_t(x, dtype, cuda) for x in u], [_t(x, dtype, cuda) for x in w], out, order)
+    torch.cuda.synchronize()
+    for c in range(dim):
+        assert _rel(_np(out[c]), ref[c]) < tol
+
+
+def test_nabla_scalar_adjoint(fm, cuda, shape, prec):
+    rng, o, dtype, tol, dx = setup(shape, prec, 8)
+    g = fm.GridSpec(shape)
+    dim = len(shape)
+    s = rng.uniform(0, 1, size=shape)
+    a = rng.uniform(-1, 1, size=shape)
+    ref = [np.zeros(g.face_shape(c), o.dtype) for c in range(dim)]
+    o.calculate_nabla_scalar_adjoint(s.astype(o.dtype), a.astype(o.dtype), ref, dx)
+    out = [torch.zeros(g.face_shape(c), dtype=dtype, device=cuda) for c in range(dim)]
+    fm.kernels.nabla_scalar_adjoint(g, dx, _t(s, dtype, cuda), _t(a, dtype, cuda), out)
+    torch.cuda.synchronize()
+    for c in range(dim):
+        assert _rel(_np(out[c]), ref[c]) < tol
+
+
+def test_reset_to_identity(fm, cuda, shape, prec):
+    rng, o, dtype, tol, dx = setup(shape, prec, 9)
+    g = fm.GridSpec(shape)
+    dim = len(shape)
+    psi_r = np.zeros((dim,) + tuple(shape), o.dtype)
+    pf_r = [np.zeros((dim,) + g.face_shape(c), o.dtype) for c in range(dim)]
+    Tf_r = [np.zeros((dim,) + g.face_shape(c), o.dtype) for c in range(dim)]
+    o.reset_to_identity(psi_r, pf_r, Tf_r, dx)
+    psi = torch.full((dim,) + tuple(shape), 7.0, dtype=dtype, device=cuda)
+    pf = [torch.full((dim,) + g.face_shape(c), 7.0, dtype=dtype, device=cuda) for c in range(dim)]
+    Tf = [torch.full((dim,) + g.face_shape(c), 7.0, dtype=dtype, device=cuda) for c in range(dim)]
+    fm.kernels.reset_to_identity(g, dx, psi, pf, Tf)
+    torch.cuda.synchronize()
+    assert np.array_equal(_np(psi), psi_r)
+    for c in range(dim):
+        assert np.array_equal(_np(pf[c]), pf_r[c])
+        assert np.array_equal(_np(Tf[c]), Tf_r[c])
+
+
+def test_project_matches_oracle(fm, cuda, shape, prec):
+    """Poisson(u): projected velocity vs the oracle solved to high accuracy."""
+    rng, o, dtype, tol, dx = setup(shape, prec, 10)
+    g = fm.GridSpec(shape)
+    dim = len(shape)
+    u = _rand_mac(rng, shape, 1.0)
+    levels = max(2, int(np.log2(min(shape))) - 3 + 1)
+    abs_tol = 1e-24 if prec[0] == "f64" else 0.0
+    rel_tol = 1e-26 if prec[0] == "f64" else 1e-12
+    eps = 0.0 if prec[0] == "f64" else 1e-12
+    P = MGParams(levels, 2, 50, 0, 60, abs_tol, rel_tol, eps)
+    ref = [x.astype(o.dtype).copy() for x in u]
+    o.Poisson(P, ref)
+    sol = fm.MGPCG(shape, dtype, levels=levels, bottom=50, max_iters=60, abs_tol=abs_tol, rel_tol=rel_tol, eps=eps)
+    ud = [_t(x, dtype, cuda) for x in u]
+    sol.project(ud)
+    torch.cuda.synchronize()
+    ptol = 1e-9 if prec[0] == "f64" else 5e-4
+    for c in range(dim):
+        assert _rel(_np(ud[c]), ref[c]) < ptol
+    # projected field is discretely divergence-free
+    div = np.zeros(shape, o.dtype)
+    o.divergence([np.ascontiguousarray(_np(x), o.dtype) for x in ud], div)
+    scale = max(np.abs(x).max() for x in u)
+    assert np.abs(div).max() < (1e-9 if prec[0] == "f64" else 2e-3) * scale
+
+
+def test_vcycle_iterations_match_oracle(fm, cuda):
+    """Same preconditioner => same PCG convergence history length (FP64)."""
+    shape = (32, 32, 32)
+    rng = np.random.default_rng(11)
+    o = Oracle(shape, "f64")
+    b = rng.standard_normal(shape)
+    b -= b.mean()
+    P = MGParams(3, 2, 50, 0, 200, 0.0, 1e-20, 0.0)
+    x_ref = np.zeros(shape)
+    it_ref, rtr_ref, conv_ref = o.mgpcg_solve(P, b, x_ref)
+    sol = fm.MGPCG(shape, torch.float64, levels=3, bottom=50, max_iters=200, abs_tol=0.0, rel_tol=1e-20,
+                   eps=0.0, check_every=1)
+    x = torch.zeros(shape, dtype=torch.float64, device=cuda)
+    it, rtr = sol.solve(torch.tensor(b, device=cuda), x)
+    assert conv_ref and sol.last_converged
+    assert abs(it - it_ref) <= 1
+    assert _rel(x.cpu().numpy(), x_ref) < 1e-8
