@@ -1,0 +1,329 @@
+#!/usr/bin/env python
+"""Benchmark: forward+adjoint gradient evaluations per second, 3D 128^3.
+
+Workload (one bench "step" = one gradient evaluation): 3D smoke shape
+transition on a 128^3 MAC grid, 150 leapfrog flow-map steps, reinit every 8,
+RK4, dt = 0.0085, passive density; forward simulation + adjoint backtrack,
+dL/du0 of L = sum (rho(T) - rho*)^2.  Synthetic seeded inputs
+(configs.shape3d_inputs): sphere -> union of two spheres, u0 ~ N(0, 0.01^2).
+
+  python bench.py [--gpus N] [--steps K] [--warmup W] [--form plain|mixed]
+  python bench.py --impl reference ...   # the reference algorithm on the host CPU
+
+N > 1 runs N independent replicas (one per GPU, no data-path collective; the
+problem does not shard), launched by torchrun; value = N*K / max-over-ranks time.
+"""
+from __future__ import annotations
+
+import argparse
+import importlib
+import json
+import os
+import statistics
+import subprocess
+import sys
+import threading
+import time
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+METRIC = "fwd+adjoint grads/s, 3D 128³: mixed vs plain FP32 on B200 @ rel err ≤1e-4"
+UNIT = "grads/s"
+
+
+def parse():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=3)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
+    ap.add_argument("--form", default="plain", choices=["plain", "mixed"])
+    ap.add_argument("--res", type=int, default=128)
+    ap.add_argument("--sim-steps", type=int, default=150)
+    ap.add_argument("--reinit", type=int, default=8)
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--no-e2e", action="store_true")
+    return ap.parse_args()
+
+
+def workload_name(a):
+    return f"3D smoke shape transition {a.res}^3, {a.sim_steps} steps, reinit {a.reinit}, RK4, fwd+adjoint"
+
+
+# ---------------------------------------------------------------------------
+# clocks sampled during the timed region
+# ---------------------------------------------------------------------------
+class ClockSampler:
+    FIELDS = ("clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,clocks_event_reasons.hw_slowdown,"
+              "clocks_event_reasons.hw_thermal_slowdown,clocks_event_reasons.sw_thermal_slowdown,"
+              "clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, dev_uuid):
+        self.proc = None
+        self.lines = []
+        self.uuid = dev_uuid
+
+    def start(self):
+        try:
+            cmd = ["nvidia-smi", f"--query-gpu={self.FIELDS}", "--format=csv,noheader,nounits", "-lms", "200"]
+            if self.uuid:
+                cmd += ["-i", self.uuid]
+            self.proc = subprocess.Popen(cmd, stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+            self.t = threading.Thread(target=self._read, daemon=True)
+            self.t.start()
+        except Exception:
+            self.proc = None
+
+    def _read(self):
+        for line in self.proc.stdout:
+            self.lines.append(line.strip())
+
+    def stop(self):
+        if self.proc is None:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["unsampled"]}
+        self.proc.terminate()
+        try:
+            self.proc.wait(timeout=5)
+        except Exception:
+            self.proc.kill()
+        sm, mx, reasons = [], None, set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for ln in self.lines:
+            p = [x.strip() for x in ln.split(",")]
+            if len(p) < 8:
+                continue
+            try:
+                sm.append(float(p[0]))
+                mx = float(p[1])
+            except ValueError:
+                continue
+            for nm, v in zip(names, p[4:8]):
+                if v.lower().startswith("active"):
+                    reasons.add(nm)
+        return {"sm_mhz": statistics.median(sm) if sm else None, "sm_max_mhz": mx, "reasons": sorted(reasons),
+                "samples": len(sm)}
+
+
+# ---------------------------------------------------------------------------
+# CPU: the reference algorithm (oracle restatement, FP32) on the host cores
+# ---------------------------------------------------------------------------
+def cpu_sample(a, threads=None):
+    """One-step gradient (1 forward + 1 adjoint step incl. the adjoint's reinit
+    BFECC) at the bench resolution with the FP32 oracle; returns seconds."""
+    threads = threads or len(os.sched_getaffinity(0))
+    os.environ["OMP_NUM_THREADS"] = str(threads)
+    sys.path.insert(0, os.path.join(ROOT, "oracle"))
+    from oracle import MGParams  # noqa: E402  (checker only: CPU baseline leg)
+    from sim_oracle import OracleSim  # noqa: E402
+    C = importlib.import_module("differentiable-flowmap_b200.configs")
+    u0, rho0, rho_t = C.shape3d_inputs(a.res)
+    levels = int(__import__("math").log2(a.res)) - 3 + 1
+    mg = MGParams(levels, 2, 50, 0, 400, 0.0, 1e-6, 1e-12)
+    o = OracleSim((a.res,) * 3, 1.0 / a.res, 0.0085, a.reinit, 1, rk=4, backward_u=True, prec="f32", mg=mg)
+    f32 = lambda x: x.astype("float32")
+    t0 = time.perf_counter()
+    o.gradient([f32(x) for x in u0], f32(rho0), f32(rho_t))
+    return time.perf_counter() - t0, threads
+
+
+def run_reference(a):
+    rank = int(os.environ.get("RANK", "0"))
+    if rank != 0:
+        return 0
+    times = []
+    threads = len(os.sched_getaffinity(0))
+    for i in range(a.warmup + a.steps):
+        dt, threads = cpu_sample(a, threads)
+        if i >= a.warmup:
+            times.append(dt)
+    per_grad = statistics.mean(times) * a.sim_steps
+    v = 1.0 / per_grad
+    sample = (f"one-step gradient (1 forward + 1 adjoint step, incl. the adjoint reinit BFECC) at {a.res}^3, "
+              f"scaled x{a.sim_steps} steps; FP32 CPU restatement of the reference algorithm (Taichi CPU backend "
+              f"not installable here), OpenMP")
+    line = {"metric": METRIC, "value": v, "unit": UNIT, "impl": "reference", "n_gpus": a.gpus, "steps": a.steps,
+            "warmup": a.warmup, "ms_per_step": per_grad * 1e3, "higher_is_better": True, "scaling": "weak",
+            "vs_baseline": None, "dtype": "f32", "data": "synthetic",
+            "config": {"workload": workload_name(a), "form": "reference (CPU)", "parallelism": "host threads"},
+            "cpu_baseline": {"value": v, "unit": UNIT, "cores": threads, "kind": "port", "sample": sample},
+            "e2e": {"value": v, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
+    print(json.dumps(line), flush=True)
+    return 0
+
+
+# ---------------------------------------------------------------------------
+# GPU arm
+# ---------------------------------------------------------------------------
+def main():
+    a = parse()
+    if a.impl == "reference":
+        return run_reference(a)
+
+    import torch
+    import torch.distributed as dist
+
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    torch.cuda.set_device(local)
+    dev = torch.device("cuda", local)
+    if world > 1:
+        from datetime import timedelta
+        dist.init_process_group("nccl", timeout=timedelta(seconds=600), device_id=dev)
+
+    fm = importlib.import_module("differentiable-flowmap_b200")
+    C = importlib.import_module("differentiable-flowmap_b200.configs")
+    S = importlib.import_module("differentiable-flowmap_b200.simulator")
+    lib = fm._lib
+
+    store = torch.bfloat16 if a.form == "mixed" else None
+    backward_u = a.form != "mixed"
+    cfg = C.shape3d_config(res=a.res, steps=a.sim_steps, reinit_every=a.reinit, rk=4, store_dtype=store,
+                           backward_u=backward_u)
+    sim = S.LFM_Diff_Simulator(config=cfg, device=dev)
+    u0, rho0, rho_t = C.shape3d_inputs(a.res)
+    f32 = torch.float32
+    d_u0 = [torch.tensor(x, dtype=f32, device=dev) for x in u0]
+    d_r0 = torch.tensor(rho0, dtype=f32, device=dev)
+    d_rt = torch.tensor(rho_t, dtype=f32, device=dev)
+    h_u0 = [torch.tensor(x, dtype=f32).pin_memory() for x in u0]
+    h_r0 = torch.tensor(rho0, dtype=f32).pin_memory()
+    h_rt = torch.tensor(rho_t, dtype=f32).pin_memory()
+    h_grad = [torch.empty(x.shape, dtype=f32).pin_memory() for x in u0]
+    stream = torch.cuda.current_stream(dev)
+
+    def barrier():
+        if world > 1:
+            dist.barrier()
+
+    for _ in range(a.warmup):
+        sim.gradient(d_u0, d_r0, d_rt)
+    torch.cuda.synchronize(dev)
+    barrier()
+
+    uuid = None
+    try:
+        uuid = "GPU-" + str(torch.cuda.get_device_properties(dev).uuid)
+    except Exception:
+        pass
+    clocks = ClockSampler(uuid)
+    clocks.start()
+    iters = []
+    lib.launch_count(reset=True)
+    torch.cuda.synchronize(dev)
+    barrier()
+    ev0, ev1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    ev0.record(stream)
+    for _ in range(a.steps):
+        loss, grad = sim.gradient(d_u0, d_r0, d_rt)
+        iters.append(list(sim.solver.history))
+        sim.solver.history.clear()
+    ev1.record(stream)
+    torch.cuda.synchronize(dev)
+    barrier()
+    launches = lib.launch_count(reset=True)
+    clk = clocks.stop()
+    ms = ev0.elapsed_time(ev1)
+    t = torch.tensor([ms], dtype=torch.float64, device=dev)
+    if world > 1:
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    ms_max = float(t.item())
+    value = world * a.steps / (ms_max / 1e3)
+
+    # end-to-end through the public API with host buffers
+    e2e = None
+    if not a.no_e2e:
+        h2d = sum(x.numel() * 4 for x in h_u0) + h_r0.numel() * 4 + h_rt.numel() * 4
+        d2h = sum(x.numel() * 4 for x in h_grad) + 8
+        torch.cuda.synchronize(dev)
+        barrier()
+        ev0.record(stream)
+        for _ in range(a.steps):
+            loss, grad = sim.gradient(h_u0, h_r0, h_rt)
+            for hg, g in zip(h_grad, grad):
+                hg.copy_(g, non_blocking=True)
+            _ = float(loss)
+        ev1.record(stream)
+        torch.cuda.synchronize(dev)
+        barrier()
+        te = torch.tensor([ev0.elapsed_time(ev1)], dtype=torch.float64, device=dev)
+        if world > 1:
+            dist.all_reduce(te, op=dist.ReduceOp.MAX)
+        e2e = {"value": world * a.steps / (float(te.item()) / 1e3), "unit": UNIT, "h2d_bytes_per_step": h2d,
+               "d2h_bytes_per_step": d2h}
+
+    # roofline of the dominant kernel, timed live on the launching stream
+    roof = None
+    if rank == 0:
+        roof = dominant_kernel_roofline(fm, sim, dev, stream)
+
+    flat_iters = [it for run in iters for (it, _) in run]
+    line = None
+    if rank == 0:
+        line = {"metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": a.steps,
+                "warmup": a.warmup, "ms_per_step": ms_max / a.steps, "higher_is_better": True, "scaling": "weak",
+                "vs_baseline": None, "dtype": "f32", "data": "synthetic",
+                "config": {"workload": workload_name(a), "form": a.form, "res": a.res, "sim_steps": a.sim_steps,
+                           "reinit_every": a.reinit, "rk": 4, "backward_u": backward_u,
+                           "store_dtype": "bf16" if store is not None else "f32",
+                           "solver": {"levels": sim.solver.n_mg_levels, "rel_tol": cfg.solver.rel_tol,
+                                      "mean_pcg_iters": statistics.mean(flat_iters) if flat_iters else None,
+                                      "solves_per_grad": len(flat_iters) // max(a.steps, 1)},
+                           "parallelism": f"replicas x{world}" if world > 1 else "single GPU",
+                           "l2": "working set and trajectory stores exceed the 126 MB L2; no flush needed"},
+                "e2e": e2e, "gpu_launches": launches, "clocks": clk, "roofline": roof}
+        if world == 1 and not a.no_cpu_baseline:
+            secs, threads = cpu_sample(a)
+            line["cpu_baseline"] = {
+                "value": 1.0 / (secs * a.sim_steps), "unit": UNIT, "cores": threads, "kind": "port",
+                "sample": (f"one-step gradient (1 forward + 1 adjoint step incl. the adjoint reinit) at {a.res}^3 "
+                           f"with the FP32 CPU restatement, {secs:.1f} s, scaled x{a.sim_steps} steps")}
+        print(json.dumps(line), flush=True)
+    if world > 1:
+        dist.barrier()
+        dist.destroy_process_group()
+    return 0
+
+
+def dominant_kernel_roofline(fm, sim, dev, stream):
+    """Times fm_march_map (RK4 flow map + Jacobian on the three face grids and
+    the centre map) on the simulator's live state with CUDA events."""
+    import json as _j
+
+    import torch
+
+    peaks = {}
+    try:
+        peaks = _j.load(open(os.path.join(ROOT, "MEASURED_PEAKS.json")))
+    except Exception:
+        pass
+    hbm = peaks.get("hbm_gbs", 6650.0)
+    src = "measured" if "hbm_gbs" in peaks else "fallback"
+    g, K = sim.grid, fm.kernels
+    psi, psi_f, T_f = sim.psi.clone(), [x.clone() for x in sim.psi_f], [x.clone() for x in sim.T_f]
+    u = sim.u
+    reps = 5
+    K.march_map(g, 4, sim.dx, sim.dt, psi, psi_f, T_f, u)
+    torch.cuda.synchronize(dev)
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    e0.record(stream)
+    for _ in range(reps):
+        K.march_map(g, 4, sim.dx, sim.dt, psi, psi_f, T_f, u)
+    e1.record(stream)
+    torch.cuda.synchronize(dev)
+    ms = e0.elapsed_time(e1) / reps
+    ncell = g.ncell
+    nface = sum(int(torch.tensor(g.face_shape(c)).prod()) for c in range(g.dim))
+    # compulsory bytes: psi, T on 3 face grids r+w (2*6 floats per face node),
+    # centre psi r+w (6 floats per cell), u read once (3 floats per cell)
+    algo = 4 * (12 * nface + 6 * ncell + nface)
+    achieved = algo / (ms / 1e3) / 1e9
+    return {"kernel": "k_march<float,3,4> (fm_march_map)", "bound": "hbm", "achieved": achieved, "peak": hbm,
+            "unit": "GB/s", "frac": achieved / hbm, "traffic": None, "ms_per_launch": ms,
+            "algorithmic_bytes_per_launch": algo, "peak_source": f"{src} (MEASURED_PEAKS.json hbm_gbs)",
+            "note": "gather kernel: FP32-issue bound, HBM fraction is low by construction"}
+
+
+if __name__ == "__main__":
+    sys.exit(main())

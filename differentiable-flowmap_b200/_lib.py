@@ -57,6 +57,18 @@ class MGParams(C.Structure):
     ]
 
 
+class MGStats(C.Structure):
+    _fields_ = [
+        ("solves", C.c_longlong),
+        ("iterations", C.c_longlong),
+        ("not_converged", C.c_longlong),
+        ("nonfinite", C.c_longlong),
+        ("last_iters", C.c_int),
+        ("max_iters_seen", C.c_int),
+        ("last_rtr", C.c_double),
+    ]
+
+
 P, D, I, L = C.c_void_p, C.c_double, C.c_int, C.c_long
 GP = C.POINTER(Grid)
 
@@ -79,7 +91,10 @@ SIGNATURES = {
     "fm_project": [P, P, P, P, P, P, C.POINTER(I), C.POINTER(D)],
     "fm_mgpcg_solve": [P, P, P, P, C.POINTER(I), C.POINTER(D)],
     "fm_laplacian": [GP, I, P, P, P],
+    "fm_mgpcg_stats": [P, P, I, C.POINTER(MGStats)],
 }
+RESTYPES = {"fm_launch_count": C.c_longlong}
+SIGNATURES["fm_launch_count"] = [I]
 
 _lib = None
 
@@ -96,11 +111,16 @@ def lib() -> C.CDLL:
         for name, args in SIGNATURES.items():
             f = getattr(l, name)
             f.argtypes = args
-            f.restype = C.c_int
+            f.restype = RESTYPES.get(name, C.c_int)
         l.fm_status_string.argtypes = [C.c_int]
         l.fm_status_string.restype = C.c_char_p
         _lib = l
     return _lib
+
+
+def launch_count(reset: bool = False) -> int:
+    """Kernels launched by libflowmap_sm100.so so far (graph launches included)."""
+    return int(lib().fm_launch_count(1 if reset else 0))
 
 
 def check(status: int, where: str):

@@ -44,13 +44,18 @@ def build(force: bool = False, ptxas_verbose: bool = False) -> str:
     flags = ["-O3", "-std=c++17", "-lineinfo", "-Xcompiler", "-fPIC", "--expt-relaxed-constexpr", *ARCH]
     if ptxas_verbose:
         flags += ["-Xptxas", "-v"]
-    for src in SOURCES:
+    procs = []
+    for src in SOURCES:  # translation units compile in parallel
         obj = os.path.join(objdir, src.replace(".cu", ".o"))
-        cmd = [nvcc, *flags, "-c", os.path.join(CSRC, src), "-o", obj]
-        subprocess.run(cmd, check=True)
+        procs.append(subprocess.Popen([nvcc, *flags, "-c", os.path.join(CSRC, src), "-o", obj]))
         objs.append(obj)
+    for p in procs:
+        if p.wait() != 0:
+            raise subprocess.CalledProcessError(p.returncode, "nvcc")
     tmp = LIB + ".tmp"
-    subprocess.run([nvcc, *ARCH, "-shared", "-o", tmp, *objs, "-lcudart"], check=True)
+    # static CUDA runtime: the library does not depend on the version of
+    # libcudart that the host process (e.g. torch) happens to have loaded
+    subprocess.run([nvcc, *ARCH, "-shared", "-cudart", "static", "-o", tmp, *objs], check=True)
     os.replace(tmp, LIB)
     return LIB
 

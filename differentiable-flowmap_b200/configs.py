@@ -1,0 +1,99 @@
+"""Workload presets and seeded synthetic inputs.
+
+The reference optimises real experiments (Gaussian control forces, image
+masks); the benchmark configurations below use seeded synthetic inputs of the
+same shapes instead (numpy PCG64 generators, seeds fixed per config).
+"""
+from __future__ import annotations
+
+import math
+from dataclasses import replace
+
+import numpy as np
+import torch
+
+from .simulator import FlowmapConfig, SolverConfig
+
+
+def split_central_vector(vc: np.ndarray) -> list:
+    """Cell-centred vector (dim, *res) -> MAC faces, clamped sampling
+    (3D/taichi_utils.py:170-183, 2D/vortex/taichi_utils.py:158-167)."""
+    dim = vc.shape[0]
+    out = []
+    for c in range(dim):
+        v = vc[c]
+        lo = np.concatenate([v.take([0], axis=c), v], axis=c)      # index i-1 clamped
+        hi = np.concatenate([v, v.take([-1], axis=c)], axis=c)     # index i clamped
+        out.append(0.5 * (hi + lo))
+    return out
+
+
+def smooth_ball(res, center, radius, dx):
+    """Sphere/disc density with a one-cell tanh edge."""
+    axes = [(np.arange(n) + 0.5) * dx for n in res]
+    X = np.meshgrid(*axes, indexing="ij")
+    r = np.sqrt(sum((x - c) ** 2 for x, c in zip(X, center)))
+    return 0.5 * (1.0 - np.tanh((r - radius) / dx))
+
+
+def shape3d_config(res=128, steps=150, reinit_every=8, rk=4, dtype=torch.float32, store_dtype=None,
+                   backward_u=True, rel_tol=1e-6, abs_tol=0.0, max_iters=400, check_every=4):
+    """3D smoke shape transition, 128^3: 150 steps, reinit every 8, RK4,
+    dt = 0.0085 (3D/hyperparameters.py:268-295 with the stated overrides)."""
+    n = int(math.log2(res))
+    solver = SolverConfig(base_level=3, levels=n - 3 + 1, bottom=50, bottom_mode=0, max_iters=max_iters,
+                          abs_tol=abs_tol, rel_tol=rel_tol, eps=1e-12 if dtype == torch.float32 else 0.0,
+                          check_every=check_every)
+    return FlowmapConfig(res=(res, res, res), dx=1.0 / res, dt=0.0085, total_steps=steps,
+                         reinit_every=reinit_every, RK_number=rk, backward_u=backward_u, add_passive_scalar=True,
+                         dtype=dtype, store_dtype=store_dtype, solver=solver)
+
+
+def shape3d_inputs(res=128, seed_target=20, seed_u=21, u_std=0.01):
+    """rho0: sphere r=0.15 at the centre; rho*: union of two spheres with radii
+    U[0.08, 0.14], centres U[0.3, 0.7]^3; u0 cell-centred N(0, u_std^2) split to faces."""
+    dx = 1.0 / res
+    shape = (res, res, res)
+    rho0 = smooth_ball(shape, (0.5, 0.5, 0.5), 0.15, dx)
+    rng = np.random.default_rng(seed_target)
+    radii = rng.uniform(0.08, 0.14, size=2)
+    centers = rng.uniform(0.3, 0.7, size=(2, 3))
+    rho_t = np.maximum(smooth_ball(shape, centers[0], radii[0], dx), smooth_ball(shape, centers[1], radii[1], dx))
+    rng = np.random.default_rng(seed_u)
+    uc = rng.normal(0.0, u_std, size=(3,) + shape)
+    u0 = split_central_vector(uc)
+    return u0, rho0, rho_t
+
+
+def shape2d_config(res=256, steps=200, reinit_every=12, rk=2, dt=0.01, dtype=torch.float32, store_dtype=None,
+                   backward_u=True, rel_tol=1e-6, abs_tol=0.0, max_iters=400, check_every=4):
+    """2D smoke shape transition, 256^2, 200 steps, reinit every 12, RK2, MGPCG 5 levels."""
+    solver = SolverConfig(base_level=4, levels=int(math.log2(res)) - 4 + 1, bottom=20, bottom_mode=1,
+                          max_iters=max_iters, abs_tol=abs_tol, rel_tol=rel_tol,
+                          eps=1e-12 if dtype == torch.float32 else 0.0, check_every=check_every)
+    return FlowmapConfig(res=(res, res), dx=1.0 / res, dt=dt, total_steps=steps, reinit_every=reinit_every,
+                         RK_number=rk, backward_u=backward_u, add_passive_scalar=True, dtype=dtype,
+                         store_dtype=store_dtype, solver=solver)
+
+
+def shape2d_inputs(res=256, seed_rect=10, seed_disc=11, seed_u=12, u_std=0.01):
+    """rho0: union of 3 rectangles (sides U[0.1,0.3]); rho*: union of 3 discs
+    (radii U[0.05,0.15]); u0 cell-centred N(0, u_std^2) split to faces."""
+    dx = 1.0 / res
+    x = (np.arange(res) + 0.5) * dx
+    X, Y = np.meshgrid(x, x, indexing="ij")
+    rng = np.random.default_rng(seed_rect)
+    rho0 = np.zeros((res, res))
+    for _ in range(3):
+        sx, sy = rng.uniform(0.1, 0.3, size=2)
+        x0, y0 = rng.uniform(0.1, 0.9 - sx), rng.uniform(0.1, 0.9 - sy)
+        rho0 = np.maximum(rho0, ((X >= x0) & (X <= x0 + sx) & (Y >= y0) & (Y <= y0 + sy)).astype(np.float64))
+    rng = np.random.default_rng(seed_disc)
+    rho_t = np.zeros((res, res))
+    for _ in range(3):
+        r = rng.uniform(0.05, 0.15)
+        c = rng.uniform(0.2, 0.8, size=2)
+        rho_t = np.maximum(rho_t, smooth_ball((res, res), c, r, dx))
+    rng = np.random.default_rng(seed_u)
+    u0 = split_central_vector(rng.normal(0.0, u_std, size=(2, res, res)))
+    return u0, rho0, rho_t

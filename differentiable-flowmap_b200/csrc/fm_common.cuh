@@ -103,10 +103,16 @@ template <typename T> __device__ __forceinline__ T bs_dN4(T x) {
   return x < (T)0 ? -r : r;
 }
 
+// The reference loops over a window of n taps starting at iu+lo
+// (3D/taichi_utils.py:454, :489, :524).  A B-spline of degree ORDER is
+// non-zero on |x| < (ORDER+1)/2, so only nz = ORDER+1 consecutive taps of that
+// window can carry weight; the others have N = dN = 0 exactly (see
+// Axis::setup).  The kernels visit just those nz taps: 27 instead of 64 taps
+// per 3D quadratic sample, 64 instead of 216 cubic, 125 instead of 512 quartic.
 template <int ORDER> struct Taps;
-template <> struct Taps<2> { static constexpr int lo = -1, n = 4; };
-template <> struct Taps<3> { static constexpr int lo = -2, n = 6; };
-template <> struct Taps<4> { static constexpr int lo = -3, n = 8; };
+template <> struct Taps<2> { static constexpr int lo = -1, n = 4, nz = 3; };
+template <> struct Taps<3> { static constexpr int lo = -2, n = 6, nz = 4; };
+template <> struct Taps<4> { static constexpr int lo = -3, n = 8, nz = 5; };
 
 template <typename T, int ORDER>
 __device__ __forceinline__ void bs_eval(T x, T& w, T& dw) {
@@ -126,25 +132,37 @@ __device__ __forceinline__ T bs_val(T x) {
 // weight N(s - (iu+lo+t)); tap index clamped to [0, len-1] (sample()).
 // The upper bound is computed in double and rounded to T, as Taichi folds
 // the Python constant `u_dim - 2 - eps`.
+//
+// Non-zero window: with f = s - iu in [0,1) (exact in floating point), tap t of
+// the reference window sits at x_t = f - lo - t, which is exact as well, and is
+// non-zero iff |x_t| < (ORDER+1)/2.  Quadratic: taps 0..2 when f < 0.5, else
+// 1..3; cubic: taps 1..4; quartic: 1..5 when f < 0.5, else 2..6.
 template <typename T, int ORDER, bool GRAD>
 struct Axis {
-  T w[Taps<ORDER>::n];
-  T dw[GRAD ? Taps<ORDER>::n : 1];
-  int id[Taps<ORDER>::n];
+  static constexpr int NZ = Taps<ORDER>::nz;
+  T w[NZ];
+  T dw[GRAD ? NZ : 1];
+  int id[NZ];
   __device__ __forceinline__ void setup(T p, T dx, T bl, int len) {
     T u = p / dx;
     u = u - bl;
     const T hi = (T)((double)len - 2.0 - 1e-6);
     T s = u < hi ? u : hi;
     s = s > (T)1 ? s : (T)1;
-    T iu = floor(s);
-    int iiu = (int)iu;
+    const T iu = floor(s);
+    const int iiu = (int)iu;
+    const T f = s - iu;
+    int t0;
+    if (ORDER == 3) t0 = 1;
+    else if (ORDER == 2) t0 = f >= (T)0.5 ? 1 : 0;
+    else t0 = f >= (T)0.5 ? 2 : 1;
 #pragma unroll
-    for (int t = 0; t < Taps<ORDER>::n; ++t) {
-      T x = s - (iu + (T)(Taps<ORDER>::lo + t));
+    for (int t = 0; t < NZ; ++t) {
+      const int off = Taps<ORDER>::lo + t0 + t;
+      const T x = s - (iu + (T)off);
       if (GRAD) bs_eval<T, ORDER>(x, w[t], dw[t]);
       else w[t] = bs_val<T, ORDER>(x);
-      int ii = iiu + Taps<ORDER>::lo + t;
+      const int ii = iiu + off;
       id[t] = ii < 0 ? 0 : (ii > len - 1 ? len - 1 : ii);
     }
   }
@@ -158,7 +176,7 @@ __device__ __forceinline__ T ldg(const T* p) { return __ldg(p); }
 template <typename T, int D, int ORDER>
 __device__ __forceinline__ T interp_val(const T* __restrict__ f, const Shape& s, const T* p, T dx,
                                         T bl0, T bl1, T bl2) {
-  constexpr int NT = Taps<ORDER>::n;
+  constexpr int NT = Taps<ORDER>::nz;
   Axis<T, ORDER, false> ax, ay;
   ax.setup(p[0], dx, bl0, s.s0);
   ay.setup(p[1], dx, bl1, s.s1);
@@ -195,7 +213,7 @@ __device__ __forceinline__ T interp_val(const T* __restrict__ f, const Shape& s,
 template <typename T, int D, int ORDER>
 __device__ __forceinline__ void interp_grad(const T* __restrict__ f, const Shape& s, const T* p, T dx,
                                             T bl0, T bl1, T bl2, T& val, T* grad) {
-  constexpr int NT = Taps<ORDER>::n;
+  constexpr int NT = Taps<ORDER>::nz;
   const T inv_dx = (T)1 / dx;
   Axis<T, ORDER, true> ax, ay;
   ax.setup(p[0], dx, bl0, s.s0);
@@ -251,6 +269,73 @@ __device__ __forceinline__ void interp_grad(const T* __restrict__ f, const Shape
   }
 }
 
+// Gradient of f and value of h, two fields on the same staggered grid sampled
+// at the same position: one stencil setup, both fields gathered in one pass
+// (calculate_nabla_u_w interpolates u and w at the same node, 3D/flowmap.py:368-369).
+template <typename T, int D, int ORDER>
+__device__ __forceinline__ void interp_grad_val2(const T* __restrict__ f, const T* __restrict__ h, const Shape& s,
+                                                 const T* p, T dx, T bl0, T bl1, T bl2, T* grad, T& hval) {
+  constexpr int NT = Taps<ORDER>::nz;
+  const T inv_dx = (T)1 / dx;
+  Axis<T, ORDER, true> ax, ay;
+  ax.setup(p[0], dx, bl0, s.s0);
+  ay.setup(p[1], dx, bl1, s.s1);
+  if (D == 3) {
+    Axis<T, ORDER, true> az;
+    az.setup(p[2], dx, bl2, s.s2);
+    T gx = 0, gy = 0, gz = 0, hv = 0;
+#pragma unroll 1
+    for (int ti = 0; ti < NT; ++ti) {
+      T A = 0, B = 0, Cc = 0, H = 0;
+#pragma unroll
+      for (int tj = 0; tj < NT; ++tj) {
+        const long row = ((long)ax.id[ti] * s.s1 + ay.id[tj]) * s.s2;
+        T a = 0, b = 0, hh = 0;
+#pragma unroll
+        for (int tk = 0; tk < NT; ++tk) {
+          const T fv = ldg(f + row + az.id[tk]);
+          const T hv2 = ldg(h + row + az.id[tk]);
+          a += fv * az.w[tk];
+          b += fv * az.dw[tk];
+          hh += hv2 * az.w[tk];
+        }
+        A += a * ay.w[tj];
+        B += a * ay.dw[tj];
+        Cc += b * ay.w[tj];
+        H += hh * ay.w[tj];
+      }
+      gx += A * ax.dw[ti];
+      gy += B * ax.w[ti];
+      gz += Cc * ax.w[ti];
+      hv += H * ax.w[ti];
+    }
+    grad[0] = gx * inv_dx;
+    grad[1] = gy * inv_dx;
+    grad[2] = gz * inv_dx;
+    hval = hv;
+  } else {
+    T gx = 0, gy = 0, hv = 0;
+#pragma unroll
+    for (int ti = 0; ti < NT; ++ti) {
+      T a = 0, b = 0, hh = 0;
+#pragma unroll
+      for (int tj = 0; tj < NT; ++tj) {
+        const long idx = (long)ax.id[ti] * s.s1 + ay.id[tj];
+        const T fv = ldg(f + idx);
+        a += fv * ay.w[tj];
+        b += fv * ay.dw[tj];
+        hh += ldg(h + idx) * ay.w[tj];
+      }
+      gx += a * ax.dw[ti];
+      gy += b * ax.w[ti];
+      hv += hh * ax.w[ti];
+    }
+    grad[0] = gx * inv_dx;
+    grad[1] = gy * inv_dx;
+    hval = hv;
+  }
+}
+
 // MAC velocity (D component pointers) on grid g.
 template <typename T>
 struct Mac {
@@ -284,12 +369,42 @@ __device__ __forceinline__ void interp_mac_grad(const Mac<T>& u, const fm_grid& 
   }
 }
 
+// Select element c (a runtime value such as blockIdx.y) without indexing the
+// by-value kernel parameter dynamically (which would copy it to local memory).
+template <typename P>
+__device__ __forceinline__ P pick3(const P& a, const P& b, const P& c2, int c) {
+  return c == 0 ? a : (c == 1 ? b : c2);
+}
+template <typename T>
+__device__ __forceinline__ const T* pick(const Mac<T>& m, int c) { return pick3(m.c[0], m.c[1], m.c[2], c); }
+template <typename T>
+__device__ __forceinline__ T* pick(const MacW<T>& m, int c) { return pick3(m.c[0], m.c[1], m.c[2], c); }
+
 // One component c of the MAC velocity at p.
 template <typename T, int D>
 __device__ __forceinline__ T interp_mac_comp(const Mac<T>& u, const fm_grid& g, int c, const T* p, T dx) {
   Shape s = face_shape(g, c);
-  return interp_val<T, D, 2>(u.c[c], s, p, dx, c == 0 ? (T)0 : (T)0.5, c == 1 ? (T)0 : (T)0.5,
+  return interp_val<T, D, 2>(pick(u, c), s, p, dx, c == 0 ? (T)0 : (T)0.5, c == 1 ? (T)0 : (T)0.5,
                              c == 2 ? (T)0 : (T)0.5);
+}
+
+// Velocity v = u(p) and the Jacobian-row update d = (grad u)(p) . t, without
+// materialising the 3x3 gradient (RK_grid's dT/dt = grad_u @ T,
+// 3D/flowmap.py:95).
+template <typename T, int D>
+__device__ __forceinline__ void interp_mac_grad_dot(const Mac<T>& u, const fm_grid& g, const T* p, T dx,
+                                                    const T* t, T* v, T* d) {
+#pragma unroll
+  for (int c = 0; c < D; ++c) {
+    Shape s = face_shape(g, c);
+    T gr[3];
+    interp_grad<T, D, 2>(u.c[c], s, p, dx, c == 0 ? (T)0 : (T)0.5, c == 1 ? (T)0 : (T)0.5,
+                         c == 2 ? (T)0 : (T)0.5, v[c], gr);
+    T acc = 0;
+#pragma unroll
+    for (int b = 0; b < D; ++b) acc += gr[b] * t[b];
+    d[c] = acc;
+  }
 }
 
 }  // namespace fm

@@ -15,6 +15,11 @@ namespace fm {
 
 constexpr int kThreads = 256;
 
+// CTAs per SM the march kernel is compiled for (2 caps it at 128 registers).
+#ifndef FM_MARCH_MIN_BLOCKS
+#define FM_MARCH_MIN_BLOCKS 2
+#endif
+
 // Midpoint (RK2) / RK4 backtrace from X through u0 (3D/flowmap.py:210-219, :257-262).
 template <typename T, int D, int RK>
 __device__ __forceinline__ void backtrace(const Mac<T>& u0, const fm_grid& g, const T* X, T dx, T dt, T* p) {
@@ -23,20 +28,20 @@ __device__ __forceinline__ void backtrace(const Mac<T>& u0, const fm_grid& g, co
 #pragma unroll
   for (int a = 0; a < D; ++a) q[a] = X[a] - v1[a] * dt * (T)0.5;
   interp_mac_val<T, D>(u0, g, q, dx, v2);
-  if (RK == 2) {
+  if constexpr (RK == 2) {
 #pragma unroll
     for (int a = 0; a < D; ++a) p[a] = X[a] - v2[a] * dt;
-    return;
+  } else {
+    T v3[3], v4[3];
+#pragma unroll
+    for (int a = 0; a < D; ++a) q[a] = X[a] - v2[a] * dt * (T)0.5;
+    interp_mac_val<T, D>(u0, g, q, dx, v3);
+#pragma unroll
+    for (int a = 0; a < D; ++a) q[a] = X[a] - v3[a] * dt;
+    interp_mac_val<T, D>(u0, g, q, dx, v4);
+#pragma unroll
+    for (int a = 0; a < D; ++a) p[a] = X[a] - (v1[a] + (T)2 * v2[a] + (T)2 * v3[a] + v4[a]) / (T)6.0 * dt;
   }
-  T v3[3], v4[3];
-#pragma unroll
-  for (int a = 0; a < D; ++a) q[a] = X[a] - v2[a] * dt * (T)0.5;
-  interp_mac_val<T, D>(u0, g, q, dx, v3);
-#pragma unroll
-  for (int a = 0; a < D; ++a) q[a] = X[a] - v3[a] * dt;
-  interp_mac_val<T, D>(u0, g, q, dx, v4);
-#pragma unroll
-  for (int a = 0; a < D; ++a) p[a] = X[a] - (v1[a] + (T)2 * v2[a] + (T)2 * v3[a] + v4[a]) / (T)6.0 * dt;
 }
 
 template <typename T, int D, int RK>
@@ -51,7 +56,7 @@ __global__ void __launch_bounds__(kThreads) k_advect_u_grid(fm_grid g, T dx, T d
   T X[3] = {0, 0, 0}, p[3] = {0, 0, 0};
   node_pos<T, D>(c, i, j, k, dx, X);
   backtrace<T, D, RK>(u0, g, X, dx, dt, p);
-  u2.c[c][q] = interp_mac_comp<T, D>(u1, g, c, p, dx);
+  pick(u2, c)[q] = interp_mac_comp<T, D>(u1, g, c, p, dx);
 }
 
 template <typename T, int D, int RK>
@@ -81,66 +86,90 @@ struct MarchJobs {
   MarchJob<T> j[4];
 };
 
-template <typename T, int D>
-__device__ __forceinline__ void matvec(const T G[3][3], const T* v, T* out) {
+// One RK stage: velocity k = u(pos) and, with the Jacobian, d = (grad u)(pos) . t.
+template <typename T, int D, bool WT>
+__device__ __forceinline__ void march_eval(const Mac<T>& u, const fm_grid& g, const T* pos, const T* t, T dx, T* k,
+                                           T* d) {
+  if constexpr (WT) interp_mac_grad_dot<T, D>(u, g, pos, dx, t, k, d);
+  else interp_mac_val<T, D>(u, g, pos, dx, k);
+}
+
+// RK2_grid / RK4_grid (WT) and RK*_grid_only_psi (!WT) for one node, in place.
+// The RK4 sums (k1 + 2 k2 + 2 k3 + k4) are accumulated as the stages complete,
+// in the reference's left-to-right order.
+template <typename T, int D, int RK, bool WT>
+__device__ __forceinline__ void march_node(const Mac<T>& u, const fm_grid& g, T dx, T dt, T* psi, T* Tm, long N,
+                                           long q) {
+  T P[3] = {0, 0, 0}, Tv[3] = {0, 0, 0};
 #pragma unroll
   for (int a = 0; a < D; ++a) {
-    T acc = 0;
+    P[a] = psi[a * N + q];
+    if constexpr (WT) Tv[a] = Tm[a * N + q];
+  }
+  const T neg_dt = -dt;
+  const T h = (T)0.5 * neg_dt;
+  T k[3], d[3] = {0, 0, 0}, pos[3] = {0, 0, 0}, tt[3] = {0, 0, 0};
+  march_eval<T, D, WT>(u, g, P, Tv, dx, k, d);
+  if constexpr (RK == 2) {
 #pragma unroll
-    for (int b = 0; b < D; ++b) acc += G[a][b] * v[b];
-    out[a] = acc;
+    for (int a = 0; a < D; ++a) { pos[a] = P[a] + h * k[a]; tt[a] = Tv[a] + h * d[a]; }
+    march_eval<T, D, WT>(u, g, pos, tt, dx, k, d);
+#pragma unroll
+    for (int a = 0; a < D; ++a) {
+      psi[a * N + q] = P[a] + neg_dt * k[a];
+      if constexpr (WT) Tm[a * N + q] = Tv[a] + neg_dt * d[a];
+    }
+  } else {
+    T ks[3], ds[3] = {0, 0, 0};
+#pragma unroll
+    for (int a = 0; a < D; ++a) {
+      ks[a] = k[a];
+      ds[a] = d[a];
+      pos[a] = P[a] + h * k[a];
+      tt[a] = Tv[a] + h * d[a];
+    }
+    march_eval<T, D, WT>(u, g, pos, tt, dx, k, d);  // stage 2
+#pragma unroll
+    for (int a = 0; a < D; ++a) {
+      ks[a] = ks[a] + (T)2 * k[a];
+      ds[a] = ds[a] + (T)2 * d[a];
+      pos[a] = P[a] + h * k[a];
+      tt[a] = Tv[a] + h * d[a];
+    }
+    march_eval<T, D, WT>(u, g, pos, tt, dx, k, d);  // stage 3
+#pragma unroll
+    for (int a = 0; a < D; ++a) {
+      ks[a] = ks[a] + (T)2 * k[a];
+      ds[a] = ds[a] + (T)2 * d[a];
+      pos[a] = P[a] + (T)1.0 * neg_dt * k[a];
+      tt[a] = Tv[a] + (T)1.0 * neg_dt * d[a];
+    }
+    march_eval<T, D, WT>(u, g, pos, tt, dx, k, d);  // stage 4
+    const T c6 = neg_dt * (T)1 / (T)6;
+#pragma unroll
+    for (int a = 0; a < D; ++a) {
+      psi[a * N + q] = P[a] + c6 * (ks[a] + k[a]);
+      if constexpr (WT) Tm[a * N + q] = Tv[a] + c6 * (ds[a] + d[a]);
+    }
   }
 }
 
-// RK2_grid / RK4_grid (with T) and RK*_grid_only_psi (without).
+template <typename T>
+__device__ __forceinline__ MarchJob<T> pick_job(const MarchJobs<T>& jobs, int y) {
+  return y == 0 ? jobs.j[0] : (y == 1 ? jobs.j[1] : (y == 2 ? jobs.j[2] : jobs.j[3]));
+}
+
+// RK2_grid / RK4_grid (with T) and RK*_grid_only_psi (without); blockIdx.y
+// selects the job (face grids and/or the centre map of one march).
 template <typename T, int D, int RK>
-__global__ void __launch_bounds__(kThreads) k_march(fm_grid g, T dx, T dt, MarchJobs<T> jobs, Mac<T> u) {
-  const MarchJob<T> job = jobs.j[blockIdx.y];
+__global__ void __launch_bounds__(kThreads, FM_MARCH_MIN_BLOCKS) k_march(fm_grid g, T dx, T dt, MarchJobs<T> jobs, Mac<T> u) {
+  const MarchJob<T> job = pick_job(jobs, blockIdx.y);
   const Shape s = job.face >= 0 ? face_shape(g, job.face) : cell_shape(g);
   const long N = s.size();
   const long q = (long)blockIdx.x * blockDim.x + threadIdx.x;
   if (q >= N) return;
-  const bool wt = job.Tm != nullptr;
-  T P[3] = {0, 0, 0}, Tv[3] = {0, 0, 0};
-#pragma unroll
-  for (int a = 0; a < D; ++a) {
-    P[a] = job.psi[a * N + q];
-    if (wt) Tv[a] = job.Tm[a * N + q];
-  }
-  const T neg_dt = -dt;
-  const T h = (T)0.5 * neg_dt;
-  T G[3][3];
-  T k1[3], k2[3], q1[3] = {0, 0, 0}, t1[3] = {0, 0, 0}, d1[3] = {0, 0, 0}, d2[3] = {0, 0, 0};
-  if (wt) interp_mac_grad<T, D, 2>(u, g, P, dx, k1, G);
-  else interp_mac_val<T, D>(u, g, P, dx, k1);
-  if (wt) matvec<T, D>(G, Tv, d1);
-#pragma unroll
-  for (int a = 0; a < D; ++a) { q1[a] = P[a] + h * k1[a]; t1[a] = Tv[a] + h * d1[a]; }
-  if (wt) { interp_mac_grad<T, D, 2>(u, g, q1, dx, k2, G); matvec<T, D>(G, t1, d2); }
-  else interp_mac_val<T, D>(u, g, q1, dx, k2);
-  if (RK == 2) {
-#pragma unroll
-    for (int a = 0; a < D; ++a) {
-      job.psi[a * N + q] = P[a] + neg_dt * k2[a];
-      if (wt) job.Tm[a * N + q] = Tv[a] + neg_dt * d2[a];
-    }
-    return;
-  }
-  T k3[3], k4[3], d3[3] = {0, 0, 0}, d4[3] = {0, 0, 0};
-#pragma unroll
-  for (int a = 0; a < D; ++a) { q1[a] = P[a] + h * k2[a]; t1[a] = Tv[a] + h * d2[a]; }
-  if (wt) { interp_mac_grad<T, D, 2>(u, g, q1, dx, k3, G); matvec<T, D>(G, t1, d3); }
-  else interp_mac_val<T, D>(u, g, q1, dx, k3);
-#pragma unroll
-  for (int a = 0; a < D; ++a) { q1[a] = P[a] + neg_dt * k3[a]; t1[a] = Tv[a] + neg_dt * d3[a]; }
-  if (wt) { interp_mac_grad<T, D, 2>(u, g, q1, dx, k4, G); matvec<T, D>(G, t1, d4); }
-  else interp_mac_val<T, D>(u, g, q1, dx, k4);
-  const T c6 = neg_dt * (T)1 / (T)6;
-#pragma unroll
-  for (int a = 0; a < D; ++a) {
-    job.psi[a * N + q] = P[a] + c6 * (k1[a] + (T)2 * k2[a] + (T)2 * k3[a] + k4[a]);
-    if (wt) job.Tm[a * N + q] = Tv[a] + c6 * (d1[a] + (T)2 * d2[a] + (T)2 * d3[a] + d4[a]);
-  }
+  if (job.Tm != nullptr) march_node<T, D, RK, true>(u, g, dx, dt, job.psi, job.Tm, N, q);
+  else march_node<T, D, RK, false>(u, g, dx, dt, job.psi, nullptr, N, q);
 }
 
 // out_c = alpha * (T_c . u0(psi_c) + beta * base_c)
@@ -152,15 +181,17 @@ __global__ void __launch_bounds__(kThreads) k_pullback_u(fm_grid g, T dx, Mac<T>
   const long N = s.size();
   const long q = (long)blockIdx.x * blockDim.x + threadIdx.x;
   if (q >= N) return;
+  const T* psi_c = pick(psi, c);
+  const T* T_c = pick(Tm, c);
   T p[3] = {0, 0, 0}, v[3];
 #pragma unroll
-  for (int a = 0; a < D; ++a) p[a] = psi.c[c][a * N + q];
+  for (int a = 0; a < D; ++a) p[a] = psi_c[a * N + q];
   interp_mac_val<T, D>(u0, g, p, dx, v);
   T acc = 0;
 #pragma unroll
-  for (int a = 0; a < D; ++a) acc += Tm.c[c][a * N + q] * v[a];
-  if (beta != (T)0) acc = acc + beta * base.c[c][q];
-  out.c[c][q] = alpha * acc;
+  for (int a = 0; a < D; ++a) acc += T_c[a * N + q] * v[a];
+  if (beta != (T)0) acc = acc + beta * pick(base, c)[q];
+  pick(out, c)[q] = alpha * acc;
 }
 
 template <typename T, int D>
@@ -187,28 +218,34 @@ __global__ void __launch_bounds__(kThreads) k_accumulate(fm_grid g, T dx, T dt, 
   const long N = s.size();
   const long q = (long)blockIdx.x * blockDim.x + threadIdx.x;
   if (q >= N) return;
+  const T* phi_c = pick(phi, c);
+  const T* F_c = pick(F, c);
   T p[3] = {0, 0, 0}, v[3];
 #pragma unroll
-  for (int a = 0; a < D; ++a) p[a] = phi.c[c][a * N + q];
+  for (int a = 0; a < D; ++a) p[a] = phi_c[a * N + q];
   interp_mac_val<T, D>(f, g, p, dx, v);
   T Fv = 0, Fv23 = 0, Fv16 = 0;
 #pragma unroll
   for (int a = 0; a < D; ++a) {
-    const T Fa = F.c[c][a * N + q];
+    const T Fa = F_c[a * N + q];
     Fv += Fa * v[a];
     if (AB3) { Fv23 += ((T)23 * Fa) * v[a]; Fv16 += ((T)16 * Fa) * v[a]; }
   }
-  T acc = init.c[c][q];
+  T* init_c = pick(init, c);
+  T acc = init_c[q];
   if (!AB3 || ind == 0) {
     acc += Fv * dt;
   } else {
-    const T hp = Hp.c[c][q];
+    const T hp = pick(Hp, c)[q];
     if (ind == 1) acc += (Fv23 - Fv16 + (T)5 * hp) / (T)12 * dt;
-    else acc += (Fv23 - (T)16 * hp + (T)5 * Hpp.c[c][q]) / (T)12 * dt;
-    Hpp.c[c][q] = hp;
-    Hp.c[c][q] = Fv;
+    else acc += (Fv23 - (T)16 * hp + (T)5 * pick(Hpp, c)[q]) / (T)12 * dt;
   }
-  init.c[c][q] = acc;
+  if (AB3) {  // history shifts on every call, ind == 0 included
+    T* hp_c = pick(Hp, c);
+    pick(Hpp, c)[q] = hp_c[q];
+    hp_c[q] = Fv;
+  }
+  init_c[q] = acc;
 }
 
 template <typename T, int D, int ORDER>
@@ -226,12 +263,11 @@ __global__ void __launch_bounds__(kThreads) k_nabla_u_w(fm_grid g, T dx, Mac<T> 
   for (int a = 0; a < D; ++a) {
     const Shape sa = face_shape(g, a);
     const T b0 = a == 0 ? (T)0 : (T)0.5, b1 = a == 1 ? (T)0 : (T)0.5, b2 = a == 2 ? (T)0 : (T)0.5;
-    T uv, gr[3];
-    interp_grad<T, D, ORDER>(u.c[a], sa, X, dx, b0, b1, b2, uv, gr);
-    const T wv = interp_val<T, D, ORDER>(w.c[a], sa, X, dx, b0, b1, b2);
-    acc += gr[c] * wv;
+    T gr[3], wv;
+    interp_grad_val2<T, D, ORDER>(u.c[a], w.c[a], sa, X, dx, b0, b1, b2, gr, wv);
+    acc += pick3(gr[0], gr[1], gr[2], c) * wv;
   }
-  r.c[c][q] = acc;
+  pick(r, c)[q] = acc;
 }
 
 template <typename T, int D>
@@ -249,12 +285,12 @@ __global__ void __launch_bounds__(kThreads) k_nabla_scalar_adj(fm_grid g, T dx, 
   T v, gr[3];
   interp_grad<T, D, 3>(sc, cs, X, dx, (T)0.5, (T)0.5, (T)0.5, v, gr);
   const T av = interp_val<T, D, 3>(adj, cs, X, dx, (T)0.5, (T)0.5, (T)0.5);
-  r.c[c][q] = gr[c] * av;
+  pick(r, c)[q] = pick3(gr[0], gr[1], gr[2], c) * av;
 }
 
 template <typename T, int D>
 __global__ void k_reset_identity(fm_grid g, T dx, MarchJobs<T> jobs) {
-  const MarchJob<T> job = jobs.j[blockIdx.y];
+  const MarchJob<T> job = pick_job(jobs, blockIdx.y);
   if (!job.psi && !job.Tm) return;
   const Shape s = job.face >= 0 ? face_shape(g, job.face) : cell_shape(g);
   const long N = s.size();

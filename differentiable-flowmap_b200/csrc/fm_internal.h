@@ -2,6 +2,9 @@
 #pragma once
 #include <cuda_runtime.h>
 
+#include <atomic>
+#include <utility>
+
 #include "../../include/flowmap_sm100.h"
 
 namespace fm {
@@ -21,9 +24,27 @@ inline int validate_grid(const fm_grid* g, int dtype) {
   return FM_OK;
 }
 
-inline int check_launch() {
+// Host-side count of kernels this library has launched (graph launches add
+// the number of kernel nodes they contain); read by fm_launch_count().
+extern std::atomic<long long> g_launch_count;
+inline void count_launch(long long n = 1) { g_launch_count.fetch_add(n, std::memory_order_relaxed); }
+
+inline int check_cuda() {
   cudaError_t e = cudaGetLastError();
   return e == cudaSuccess ? FM_OK : FM_ERR_CUDA;
+}
+
+// After an entry point's single kernel launch.
+inline int check_launch() {
+  count_launch();
+  return check_cuda();
+}
+
+// Launch helper that counts the launch.
+template <typename... KArgs, typename... Args>
+inline void launch(void (*k)(KArgs...), dim3 grid, dim3 block, size_t smem, cudaStream_t s, Args&&... args) {
+  k<<<grid, block, smem, s>>>(std::forward<Args>(args)...);
+  count_launch();
 }
 
 }  // namespace fm

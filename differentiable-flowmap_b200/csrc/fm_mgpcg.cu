@@ -28,6 +28,8 @@
 
 namespace fm {
 
+std::atomic<long long> g_launch_count{0};
+
 constexpr int kRedBlocks = 148 * 4;  // fixed reduction grid: 4 CTAs per SM
 constexpr int kRedThreads = 256;
 constexpr int kMaxLevels = 16;
@@ -39,6 +41,10 @@ struct DevState {
   int conv;
   int nonfinite;
   int result_it;
+  int max_it_seen;
+  // cumulative over all solves since create / the last stats reset
+  long long solves, iters_total, not_converged, nonfinite_count;
+  long long bodies;  // while-loop bodies executed (device mode), for the launch count
 };
 
 // ---------------------------------------------------------------------------
@@ -197,6 +203,17 @@ __global__ void k_fin_alpha(DevState* st, const double* part, double eps) {
   }
 }
 
+// Called by thread 0 when a solve ends: fold it into the cumulative counters.
+__device__ __forceinline__ void finish_solve(DevState* st) {
+  st->done = 1;
+  st->result_it = st->it;
+  st->solves += 1;
+  st->iters_total += st->it;
+  if (st->it > st->max_it_seen) st->max_it_seen = st->it;
+  if (st->nonfinite) st->nonfinite_count += 1;
+  else if (!st->conv) st->not_converged += 1;
+}
+
 __global__ void k_fin_conv(DevState* st, const double* part, double n) {
   if (st->done) return;
   double a, b;
@@ -204,9 +221,15 @@ __global__ void k_fin_conv(DevState* st, const double* part, double n) {
   if (threadIdx.x == 0) {
     st->rTr = a;
     st->mean = b / n;
-    if (!isfinite(a)) { st->nonfinite = 1; st->done = 1; st->result_it = st->it; }
-    else if (a < st->tol) { st->conv = 1; st->done = 1; st->result_it = st->it; }
+    if (!isfinite(a)) { st->nonfinite = 1; finish_solve(st); }
+    else if (a < st->tol) { st->conv = 1; finish_solve(st); }
   }
+}
+
+// Last node of the while-loop body: keep iterating until the solve is done.
+__global__ void k_loop_cond(cudaGraphConditionalHandle h, DevState* st) {
+  st->bodies += 1;
+  cudaGraphSetConditional(h, st->done ? 0u : 1u);
 }
 
 __global__ void k_fin_beta(DevState* st, const double* part, double eps, double abs_tol, double rel_tol,
@@ -221,12 +244,12 @@ __global__ void k_fin_beta(DevState* st, const double* part, double eps, double 
       if (rel_tol > 0 && a * rel_tol > tol) tol = a * rel_tol;
       st->tol = tol;
       st->beta = 0;
-      if (!isfinite(a)) { st->nonfinite = 1; st->done = 1; }
+      if (!isfinite(a)) { st->nonfinite = 1; finish_solve(st); }
     } else {
       st->beta = a / (st->zTr_old + eps);
       st->zTr_old = a;
       st->it += 1;
-      if (st->it >= max_iters) { st->done = 1; st->result_it = st->it; }
+      if (st->it >= max_iters) finish_solve(st);
     }
   }
 }
@@ -418,7 +441,10 @@ struct fm_mgpcg {
   DevState* st;
   DevState* h_st;  // pinned
   cudaStream_t cap;
-  cudaGraphExec_t chunk;
+  cudaGraphExec_t chunk;       // host-checked mode: check_every iterations
+  long long chunk_kernels;
+  cudaGraphExec_t loop;        // device mode: conditional WHILE node around one iteration
+  long long loop_kernels;      // kernels per loop iteration
   size_t bottom_smem;
 };
 
@@ -442,28 +468,28 @@ static void launch_vcycle(fm_mgpcg* S, cudaStream_t s, bool dot_last) {
     const Shape sh = S->lv[l];
     const unsigned nb = blocks_for(sh.size(), 256, cap);
     for (int it = 0; it < P.pre_post; ++it) {
-      if (it == 0) k_smooth_first<T, D><<<nb, 256, 0, s>>>(sh, r[l], z[l], S->st, l == 0 ? 1 : 0);
-      else k_smooth<T, D, false><<<nb, 256, 0, s>>>(sh, r[l], z[l], 0, nullptr, S->st);
-      k_smooth<T, D, false><<<nb, 256, 0, s>>>(sh, r[l], z[l], 1, nullptr, S->st);
+      if (it == 0) launch(k_smooth_first<T, D>, nb, 256, 0, s, sh, r[l], z[l], S->st, l == 0 ? 1 : 0);
+      else launch(k_smooth<T, D, false>, nb, 256, 0, s, sh, r[l], z[l], 0, nullptr, S->st);
+      launch(k_smooth<T, D, false>, nb, 256, 0, s, sh, r[l], z[l], 1, nullptr, S->st);
     }
     const Shape sc = S->lv[l + 1];
-    k_restrict<T, D><<<blocks_for(sc.size(), 256, cap), 256, 0, s>>>(sh, sc, r[l], z[l], r[l + 1], S->st);
+    launch(k_restrict<T, D>, blocks_for(sc.size(), 256, cap), 256, 0, s, sh, sc, r[l], z[l], r[l + 1], S->st);
   }
   const Shape sb = S->lv[L - 1];
   if (S->bottom_smem) {
-    k_bottom<T, D><<<1, 512, S->bottom_smem, s>>>(sb, r[L - 1], z[L - 1], P.bottom, P.bottom_mode, S->st);
+    launch(k_bottom<T, D>, 1, 512, S->bottom_smem, s, sb, r[L - 1], z[L - 1], P.bottom, P.bottom_mode, S->st);
   } else {
     // large coarsest level: per-sweep launches (z zero-filled by the first sweep)
     const unsigned nb = blocks_for(sb.size(), 256, cap);
     int first = 1;
     auto pair = [&](int a, int b) {
-      if (first && a == 0) k_smooth_first<T, D><<<nb, 256, 0, s>>>(sb, r[L - 1], z[L - 1], S->st, L == 1 ? 1 : 0);
+      if (first && a == 0) launch(k_smooth_first<T, D>, nb, 256, 0, s, sb, r[L - 1], z[L - 1], S->st, L == 1 ? 1 : 0);
       else {
         if (first) cudaMemsetAsync(z[L - 1], 0, sizeof(T) * sb.size(), s);
-        k_smooth<T, D, false><<<nb, 256, 0, s>>>(sb, r[L - 1], z[L - 1], a, nullptr, S->st);
+        launch(k_smooth<T, D, false>, nb, 256, 0, s, sb, r[L - 1], z[L - 1], a, nullptr, S->st);
       }
       first = 0;
-      k_smooth<T, D, false><<<nb, 256, 0, s>>>(sb, r[L - 1], z[L - 1], b, nullptr, S->st);
+      launch(k_smooth<T, D, false>, nb, 256, 0, s, sb, r[L - 1], z[L - 1], b, nullptr, S->st);
     };
     if (P.bottom_mode == 0) for (int i = 0; i < P.bottom; ++i) pair(0, 1);
     else {
@@ -475,17 +501,17 @@ static void launch_vcycle(fm_mgpcg* S, cudaStream_t s, bool dot_last) {
     const Shape sh = S->lv[l];
     const Shape sc = S->lv[l + 1];
     const unsigned nb = blocks_for(sh.size(), 256, cap);
-    k_prolong<T, D><<<nb, 256, 0, s>>>(sh, sc, z[l], z[l + 1], S->st);
+    launch(k_prolong<T, D>, nb, 256, 0, s, sh, sc, z[l], z[l + 1], S->st);
     for (int it = 0; it < P.pre_post; ++it) {
-      k_smooth<T, D, false><<<nb, 256, 0, s>>>(sh, r[l], z[l], 1, nullptr, S->st);
+      launch(k_smooth<T, D, false>, nb, 256, 0, s, sh, r[l], z[l], 1, nullptr, S->st);
       const bool last = dot_last && l == 0 && it == P.pre_post - 1;
-      if (last) k_smooth<T, D, true><<<kRedBlocks, kRedThreads, 0, s>>>(sh, r[l], z[l], 0, S->part, S->st);
-      else k_smooth<T, D, false><<<nb, 256, 0, s>>>(sh, r[l], z[l], 0, nullptr, S->st);
+      if (last) launch(k_smooth<T, D, true>, kRedBlocks, kRedThreads, 0, s, sh, r[l], z[l], 0, S->part, S->st);
+      else launch(k_smooth<T, D, false>, nb, 256, 0, s, sh, r[l], z[l], 0, nullptr, S->st);
     }
   }
   if (dot_last && L == 1) {
     // single-level: z.r over the bottom result
-    k_smooth<T, D, true><<<kRedBlocks, kRedThreads, 0, s>>>(sb, r[0], z[0], 2 /* no update */, S->part, S->st);
+    launch(k_smooth<T, D, true>, kRedBlocks, kRedThreads, 0, s, sb, r[0], z[0], 2 /* no update */, S->part, S->st);
   }
 }
 
@@ -499,36 +525,91 @@ static void launch_iteration(fm_mgpcg* S, cudaStream_t s) {
   T* Ap = (T*)S->Ap;
   T* r0 = (T*)S->r[0];
   T* z0 = (T*)S->z[0];
-  k_Ap_dot<T, D><<<kRedBlocks, kRedThreads, 0, s>>>(s0, p, Ap, S->part, S->st);
-  k_fin_alpha<<<1, 256, 0, s>>>(S->st, S->part, S->P.eps);
-  k_update_xr<T><<<kRedBlocks, kRedThreads, 0, s>>>(n, x, r0, p, Ap, S->part, S->st);
-  k_fin_conv<<<1, 256, 0, s>>>(S->st, S->part, (double)n);
+  launch(k_Ap_dot<T, D>, kRedBlocks, kRedThreads, 0, s, s0, p, Ap, S->part, S->st);
+  launch(k_fin_alpha, 1, 256, 0, s, S->st, S->part, S->P.eps);
+  launch(k_update_xr<T>, kRedBlocks, kRedThreads, 0, s, n, x, r0, p, Ap, S->part, S->st);
+  launch(k_fin_conv, 1, 256, 0, s, S->st, S->part, (double)n);
   launch_vcycle<T, D>(S, s, true);
-  k_fin_beta<<<1, 256, 0, s>>>(S->st, S->part, S->P.eps, S->P.abs_tol, S->P.rel_tol, S->P.max_iters, 0);
-  k_update_p<T><<<blocks_for(n, 256, 148L * 16), 256, 0, s>>>(n, p, z0, S->st, 0);
+  launch(k_fin_beta, 1, 256, 0, s, S->st, S->part, S->P.eps, S->P.abs_tol, S->P.rel_tol, S->P.max_iters, 0);
+  launch(k_update_p<T>, blocks_for(n, 256, 148L * 16), 256, 0, s, n, p, z0, S->st, 0);
 }
 
 // Prologue after r0 = b and partial sums of b: recentre, V-cycle, p = z, zTr.
 template <typename T, int D>
 static void launch_prologue(fm_mgpcg* S, cudaStream_t s) {
   const long n = S->lv[0].size();
-  k_fin_mean<<<1, 256, 0, s>>>(S->st, S->part, (double)n);
+  launch(k_fin_mean, 1, 256, 0, s, S->st, S->part, (double)n);
   launch_vcycle<T, D>(S, s, true);
-  k_fin_beta<<<1, 256, 0, s>>>(S->st, S->part, S->P.eps, S->P.abs_tol, S->P.rel_tol, S->P.max_iters, 1);
-  k_update_p<T><<<blocks_for(n, 256, 148L * 16), 256, 0, s>>>(n, (T*)S->p, (T*)S->z[0], S->st, 1);
+  launch(k_fin_beta, 1, 256, 0, s, S->st, S->part, S->P.eps, S->P.abs_tol, S->P.rel_tol, S->P.max_iters, 1);
+  launch(k_update_p<T>, blocks_for(n, 256, 148L * 16), 256, 0, s, n, (T*)S->p, (T*)S->z[0], S->st, 1);
+}
+
+// Device mode: one graph holding a conditional WHILE node whose body is one PCG
+// iteration followed by k_loop_cond.  The solve then needs no host round trip.
+template <typename T>
+static int build_loop_graph(fm_mgpcg* S) {
+  const int D = S->g.dim;
+  cudaGraph_t graph = nullptr;
+  if (cudaGraphCreate(&graph, 0) != cudaSuccess) return FM_ERR_CUDA;
+  int status = FM_ERR_CUDA;
+  do {
+    cudaGraphConditionalHandle h;
+    if (cudaGraphConditionalHandleCreate(&h, graph, 1, cudaGraphCondAssignDefault) != cudaSuccess) break;
+    cudaGraphNodeParams cp = {cudaGraphNodeTypeConditional};
+    cp.conditional.handle = h;
+    cp.conditional.type = cudaGraphCondTypeWhile;
+    cp.conditional.size = 1;
+    cudaGraphNode_t node;
+    if (cudaGraphAddNode(&node, graph, nullptr, 0, &cp) != cudaSuccess) break;
+    cudaGraph_t body = cp.conditional.phGraph_out[0];
+    if (cudaStreamBeginCaptureToGraph(S->cap, body, nullptr, nullptr, 0, cudaStreamCaptureModeThreadLocal) !=
+        cudaSuccess)
+      break;
+    const long long before = g_launch_count.load();
+    if (D == 3) launch_iteration<T, 3>(S, S->cap); else launch_iteration<T, 2>(S, S->cap);
+    launch(k_loop_cond, 1, 1, 0, S->cap, h, S->st);
+    S->loop_kernels = g_launch_count.load() - before;
+    g_launch_count.fetch_sub(S->loop_kernels);
+    cudaGraph_t captured = nullptr;
+    if (cudaStreamEndCapture(S->cap, &captured) != cudaSuccess) break;
+    if (cudaGraphInstantiate(&S->loop, graph, 0) != cudaSuccess) { S->loop = nullptr; break; }
+    status = FM_OK;
+  } while (0);
+  cudaGraphDestroy(graph);
+  cudaGetLastError();
+  return status;
 }
 
 template <typename T>
 static int run_solve(fm_mgpcg* S, cudaStream_t s, int* iters, double* rtr) {
   const int D = S->g.dim;
   if (D == 3) launch_prologue<T, 3>(S, s); else launch_prologue<T, 2>(S, s);
-  if (check_launch()) return FM_ERR_CUDA;
+  if (check_cuda()) return FM_ERR_CUDA;
+  if (S->P.check_every == 0) {
+    if (!S->loop) {
+      int e = build_loop_graph<T>(S);
+      if (e) return e;
+    }
+    if (cudaGraphLaunch(S->loop, s) != cudaSuccess) return FM_ERR_CUDA;
+    if (!iters && !rtr) return FM_OK;  // asynchronous: outcome via fm_mgpcg_stats
+    if (cudaMemcpyAsync(S->h_st, S->st, sizeof(DevState), cudaMemcpyDeviceToHost, s) != cudaSuccess) return FM_ERR_CUDA;
+    if (cudaStreamSynchronize(s) != cudaSuccess) return FM_ERR_CUDA;
+    if (iters) *iters = S->h_st->result_it;
+    if (rtr) *rtr = S->h_st->rTr;
+    if (S->h_st->nonfinite) return FM_ERR_NONFINITE;
+    if (!S->h_st->conv) return FM_ERR_NOT_CONVERGED;
+    return FM_OK;
+  }
   if (!S->chunk) {
     cudaGraph_t graph;
     if (cudaStreamBeginCapture(S->cap, cudaStreamCaptureModeThreadLocal) != cudaSuccess) return FM_ERR_CUDA;
+    const long long before = g_launch_count.load();
     for (int i = 0; i < S->P.check_every; ++i) {
       if (D == 3) launch_iteration<T, 3>(S, S->cap); else launch_iteration<T, 2>(S, S->cap);
     }
+    // captured, not executed: count them per graph launch instead
+    S->chunk_kernels = g_launch_count.load() - before;
+    g_launch_count.fetch_sub(S->chunk_kernels);
     if (cudaStreamEndCapture(S->cap, &graph) != cudaSuccess) return FM_ERR_CUDA;
     cudaError_t e = cudaGraphInstantiate(&S->chunk, graph, 0);
     cudaGraphDestroy(graph);
@@ -538,6 +619,7 @@ static int run_solve(fm_mgpcg* S, cudaStream_t s, int* iters, double* rtr) {
   const long limit = (long)S->P.max_iters + S->P.check_every;
   for (;;) {
     if (cudaGraphLaunch(S->chunk, s) != cudaSuccess) return FM_ERR_CUDA;
+    count_launch(S->chunk_kernels);
     launched += S->P.check_every;
     if (cudaMemcpyAsync(S->h_st, S->st, sizeof(DevState), cudaMemcpyDeviceToHost, s) != cudaSuccess) return FM_ERR_CUDA;
     if (cudaStreamSynchronize(s) != cudaSuccess) return FM_ERR_CUDA;
@@ -561,7 +643,7 @@ int fm_mgpcg_create(const fm_grid* g, int dtype, const fm_mg_params* params, fm_
   if (st) return st;
   const fm_mg_params& P = *params;
   if (P.levels < 2 || P.levels > kMaxLevels || P.pre_post < 1 || P.bottom < 0 || P.max_iters < 1 ||
-      P.check_every < 1 || (P.bottom_mode != 0 && P.bottom_mode != 1))
+      P.check_every < 0 || (P.bottom_mode != 0 && P.bottom_mode != 1))
     return FM_ERR_ARG;
   if (P.coarse_bf16) return FM_ERR_ARG;  // not in this build
   for (int a = 0; a < g->dim; ++a)
@@ -628,6 +710,7 @@ int fm_mgpcg_destroy(fm_mgpcg* S) {
   if (S->st) cudaFree(S->st);
   if (S->h_st) cudaFreeHost(S->h_st);
   if (S->chunk) cudaGraphExecDestroy(S->chunk);
+  if (S->loop) cudaGraphExecDestroy(S->loop);
   if (S->cap) cudaStreamDestroy(S->cap);
   free(S);
   return FM_OK;
@@ -644,23 +727,23 @@ int fm_project(fm_mgpcg* S, void* ux, void* uy, void* uz, void* p_out, void* str
   dim3 fgrid((unsigned)((maxf + 255) / 256), (unsigned)g.dim, 1);
   if (S->dtype == FM_F32) {
     MacW<float> u{{(float*)ux, (float*)uy, (float*)uz}};
-    if (g.dim == 3) k_div_bc<float, 3><<<kRedBlocks, kRedThreads, 0, s>>>(g, u, (float*)S->r[0], (float*)S->x, S->part);
-    else k_div_bc<float, 2><<<kRedBlocks, kRedThreads, 0, s>>>(g, u, (float*)S->r[0], (float*)S->x, S->part);
+    if (g.dim == 3) launch(k_div_bc<float, 3>, kRedBlocks, kRedThreads, 0, s, g, u, (float*)S->r[0], (float*)S->x, S->part);
+    else launch(k_div_bc<float, 2>, kRedBlocks, kRedThreads, 0, s, g, u, (float*)S->r[0], (float*)S->x, S->part);
     status = run_solve<float>(S, s, iters, rtr);
     if (status == FM_ERR_CUDA) return status;
-    if (g.dim == 3) k_subgrad_bc<float, 3><<<fgrid, 256, 0, s>>>(g, (const float*)S->x, u);
-    else k_subgrad_bc<float, 2><<<fgrid, 256, 0, s>>>(g, (const float*)S->x, u);
+    if (g.dim == 3) launch(k_subgrad_bc<float, 3>, fgrid, 256, 0, s, g, (const float*)S->x, u);
+    else launch(k_subgrad_bc<float, 2>, fgrid, 256, 0, s, g, (const float*)S->x, u);
   } else {
     MacW<double> u{{(double*)ux, (double*)uy, (double*)uz}};
-    if (g.dim == 3) k_div_bc<double, 3><<<kRedBlocks, kRedThreads, 0, s>>>(g, u, (double*)S->r[0], (double*)S->x, S->part);
-    else k_div_bc<double, 2><<<kRedBlocks, kRedThreads, 0, s>>>(g, u, (double*)S->r[0], (double*)S->x, S->part);
+    if (g.dim == 3) launch(k_div_bc<double, 3>, kRedBlocks, kRedThreads, 0, s, g, u, (double*)S->r[0], (double*)S->x, S->part);
+    else launch(k_div_bc<double, 2>, kRedBlocks, kRedThreads, 0, s, g, u, (double*)S->r[0], (double*)S->x, S->part);
     status = run_solve<double>(S, s, iters, rtr);
     if (status == FM_ERR_CUDA) return status;
-    if (g.dim == 3) k_subgrad_bc<double, 3><<<fgrid, 256, 0, s>>>(g, (const double*)S->x, u);
-    else k_subgrad_bc<double, 2><<<fgrid, 256, 0, s>>>(g, (const double*)S->x, u);
+    if (g.dim == 3) launch(k_subgrad_bc<double, 3>, fgrid, 256, 0, s, g, (const double*)S->x, u);
+    else launch(k_subgrad_bc<double, 2>, fgrid, 256, 0, s, g, (const double*)S->x, u);
   }
   if (p_out) cudaMemcpyAsync(p_out, S->x, (S->dtype == FM_F32 ? 4 : 8) * n, cudaMemcpyDeviceToDevice, s);
-  if (check_launch()) return FM_ERR_CUDA;
+  if (check_cuda()) return FM_ERR_CUDA;
   return status;
 }
 
@@ -670,16 +753,45 @@ int fm_mgpcg_solve(fm_mgpcg* S, const void* b, void* x, void* stream, int* iters
   const long n = S->lv[0].size();
   int status;
   if (S->dtype == FM_F32) {
-    k_load_rhs<float><<<kRedBlocks, kRedThreads, 0, s>>>(n, (const float*)b, (float*)S->r[0], (float*)S->x, S->part);
+    launch(k_load_rhs<float>, kRedBlocks, kRedThreads, 0, s, n, (const float*)b, (float*)S->r[0], (float*)S->x, S->part);
     status = run_solve<float>(S, s, iters, rtr);
   } else {
-    k_load_rhs<double><<<kRedBlocks, kRedThreads, 0, s>>>(n, (const double*)b, (double*)S->r[0], (double*)S->x, S->part);
+    launch(k_load_rhs<double>, kRedBlocks, kRedThreads, 0, s, n, (const double*)b, (double*)S->r[0], (double*)S->x, S->part);
     status = run_solve<double>(S, s, iters, rtr);
   }
   if (status == FM_ERR_CUDA) return status;
   cudaMemcpyAsync(x, S->x, (S->dtype == FM_F32 ? 4 : 8) * n, cudaMemcpyDeviceToDevice, s);
-  if (check_launch()) return FM_ERR_CUDA;
+  if (check_cuda()) return FM_ERR_CUDA;
   return status;
+}
+
+int fm_mgpcg_stats(fm_mgpcg* S, void* stream, int reset, fm_mg_stats* out) {
+  if (!S || !out) return FM_ERR_ARG;
+  cudaStream_t s = (cudaStream_t)stream;
+  if (cudaMemcpyAsync(S->h_st, S->st, sizeof(DevState), cudaMemcpyDeviceToHost, s) != cudaSuccess) return FM_ERR_CUDA;
+  if (cudaStreamSynchronize(s) != cudaSuccess) return FM_ERR_CUDA;
+  const DevState& h = *S->h_st;
+  out->solves = h.solves;
+  out->iterations = h.iters_total;
+  out->not_converged = h.not_converged;
+  out->nonfinite = h.nonfinite_count;
+  out->last_iters = h.result_it;
+  out->max_iters_seen = h.max_it_seen;
+  out->last_rtr = h.rTr;
+  // kernels run inside device-mode while loops since the last call
+  count_launch(h.bodies * S->loop_kernels);
+  long long zero_bodies = 0;
+  if (cudaMemcpyAsync(&S->st->bodies, &zero_bodies, sizeof(long long), cudaMemcpyHostToDevice, s) != cudaSuccess)
+    return FM_ERR_CUDA;
+  if (reset) {
+    DevState z = h;
+    z.solves = z.iters_total = z.not_converged = z.nonfinite_count = 0;
+    z.max_it_seen = 0;
+    z.bodies = 0;
+    if (cudaMemcpyAsync(S->st, &z, sizeof(DevState), cudaMemcpyHostToDevice, s) != cudaSuccess) return FM_ERR_CUDA;
+  }
+  if (cudaStreamSynchronize(s) != cudaSuccess) return FM_ERR_CUDA;
+  return FM_OK;
 }
 
 int fm_laplacian(const fm_grid* g, int dtype, const void* p, void* Ap, void* stream) {
@@ -690,16 +802,21 @@ int fm_laplacian(const fm_grid* g, int dtype, const void* p, void* Ap, void* str
   cudaStream_t cs = (cudaStream_t)stream;
   unsigned nb = blocks_for(s.size(), 256, 148L * 16);
   if (dtype == FM_F32) {
-    if (g->dim == 3) k_laplacian<float, 3><<<nb, 256, 0, cs>>>(s, (const float*)p, (float*)Ap);
-    else k_laplacian<float, 2><<<nb, 256, 0, cs>>>(s, (const float*)p, (float*)Ap);
+    if (g->dim == 3) launch(k_laplacian<float, 3>, nb, 256, 0, cs, s, (const float*)p, (float*)Ap);
+    else launch(k_laplacian<float, 2>, nb, 256, 0, cs, s, (const float*)p, (float*)Ap);
   } else {
-    if (g->dim == 3) k_laplacian<double, 3><<<nb, 256, 0, cs>>>(s, (const double*)p, (double*)Ap);
-    else k_laplacian<double, 2><<<nb, 256, 0, cs>>>(s, (const double*)p, (double*)Ap);
+    if (g->dim == 3) launch(k_laplacian<double, 3>, nb, 256, 0, cs, s, (const double*)p, (double*)Ap);
+    else launch(k_laplacian<double, 2>, nb, 256, 0, cs, s, (const double*)p, (double*)Ap);
   }
-  return check_launch();
+  return check_cuda();
 }
 
 int fm_abi_version(void) { return 1; }
+
+long long fm_launch_count(int reset) {
+  if (reset) return g_launch_count.exchange(0);
+  return g_launch_count.load();
+}
 
 const char* fm_status_string(int status) {
   switch (status) {

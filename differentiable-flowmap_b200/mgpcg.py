@@ -80,10 +80,29 @@ class MGPCG:
             if tuple(x.shape) != self.grid.face_shape(c) or x.dtype != self.dtype:
                 raise _lib.FlowmapError(1, f"project: component {c} shape/dtype mismatch")
         ps = [_lib.ptr(x) for x in u] + [None] * (3 - len(u))
+        if self.device_mode:
+            # asynchronous: the outcome is folded into stats()
+            st = _lib.lib().fm_project(self._h, ps[0], ps[1], ps[2], _lib.ptr(p_out), _lib.stream_ptr(stream),
+                                       None, None)
+            _lib.check(st, "fm_project")
+            return
         it, rtr = C.c_int(0), C.c_double(0)
         st = _lib.lib().fm_project(self._h, ps[0], ps[1], ps[2], _lib.ptr(p_out), _lib.stream_ptr(stream),
                                    C.byref(it), C.byref(rtr))
         self._status(st, "fm_project", it, rtr)
+
+    @property
+    def device_mode(self) -> bool:
+        return self.params.check_every == 0
+
+    def stats(self, reset: bool = False, stream=None) -> dict:
+        """Cumulative solver outcome (synchronises the stream)."""
+        s = _lib.MGStats()
+        _lib.check(_lib.lib().fm_mgpcg_stats(self._h, _lib.stream_ptr(stream), int(reset), C.byref(s)),
+                   "fm_mgpcg_stats")
+        return {"solves": s.solves, "iterations": s.iterations, "not_converged": s.not_converged,
+                "nonfinite": s.nonfinite, "last_iters": s.last_iters, "max_iters_seen": s.max_iters_seen,
+                "last_rtr": s.last_rtr}
 
     def solve(self, b: torch.Tensor, x: torch.Tensor, stream=None):
         it, rtr = C.c_int(0), C.c_double(0)

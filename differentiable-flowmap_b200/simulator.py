@@ -1,0 +1,495 @@
+"""Leapfrog flow-map simulator and its adjoint, driving libflowmap_sm100.so.
+
+``LFM_Simulator`` mirrors 3D/lfm_midpoint_simulator.py:167-807 (and the 2D
+copies, 2D/vortex/lfm_midpoint_simulator.py:186-661): ``init``,
+``step_midpoint`` -> ``step_flow_map``, ``backtrack_psi_grid``,
+``march_phi_grid``.  ``LFM_Diff_Simulator`` mirrors
+3D/lfm_midpoint_diff_simulator.py:15-594: ``forward_step_midpoint``,
+``init_gradient``, ``backtrack_step_midpoint`` -> ``backtrack_flow_map``.
+
+Differences from the reference, all on the plumbing side:
+  * the trajectory the adjoint needs (every step's midpoint velocity, the
+    flow maps phi/F at every reinit, optionally every step's passive scalar)
+    stays resident in HBM instead of being written to .npy files by RW_Cache;
+    the in-interval midpoint velocities that backtrack_psi_grid replays are the
+    same device buffers (the reference copies them through a host dict);
+  * copy_to/add_fields/scale_field chains are fused into the kernels'
+    epilogues (BFECC is three launches) and result buffers are rotated instead
+    of copied;
+  * calc_max_speed only feeds a print in the reference and is not computed.
+
+Control flow and arithmetic follow the reference step for step; the flags of
+3D/hyperparameters.py are fields of ``FlowmapConfig``.
+"""
+from __future__ import annotations
+
+import math
+from dataclasses import dataclass, field, replace
+from typing import Dict, List, Optional, Sequence
+
+import numpy as np
+import torch
+
+from . import kernels as K
+from ._lib import FlowmapError
+from .kernels import GridSpec
+from .mgpcg import MGPCG
+
+
+@dataclass
+class SolverConfig:
+    """MGPCG parameters (3D/mgpcg.py:22-35, :429-431)."""
+
+    base_level: int = 3
+    levels: Optional[int] = None
+    pre_post: int = 2
+    bottom: int = 50
+    bottom_mode: int = 0
+    max_iters: int = 400
+    abs_tol: float = 1e-12
+    rel_tol: float = 0.0
+    eps: float = 1e-12
+    check_every: int = 4
+
+
+@dataclass
+class FlowmapConfig:
+    """Simulation flags (names follow 3D/hyperparameters.py)."""
+
+    res: tuple = (128, 128, 128)
+    dx: float = 1.0 / 128
+    dt: float = 0.0085            # act_dt
+    total_steps: int = 150
+    reinit_every: int = 8
+    RK_number: int = 4
+    backward_u: bool = True       # adjoint re-advects u backwards (reference default)
+    add_passive_scalar: bool = True
+    BFECC_clamp: bool = False
+    use_short_BFECC: bool = False
+    trajectory_loss: bool = False  # reference's no-force branch: loss over reinit frames
+    dtype: torch.dtype = torch.float32
+    store_dtype: Optional[torch.dtype] = None  # checkpoint storage dtype (None: dtype)
+    solver: SolverConfig = field(default_factory=SolverConfig)
+
+    @property
+    def dim(self) -> int:
+        return len(self.res)
+
+
+class _Scalar:
+    """0-d holder supporting the reference's ``field[None]`` indexing."""
+
+    def __init__(self, v=0):
+        self.v = v
+
+    def __getitem__(self, k):
+        return self.v
+
+    def __setitem__(self, k, v):
+        self.v = v
+
+
+def _mac(grid: GridSpec, dtype, device, fill=0.0):
+    return [torch.full(grid.face_shape(c), fill, dtype=dtype, device=device) for c in range(grid.dim)]
+
+
+def _vec_face(grid: GridSpec, dtype, device):
+    return [torch.zeros((grid.dim,) + grid.face_shape(c), dtype=dtype, device=device) for c in range(grid.dim)]
+
+
+def _copy_mac(dst, src):
+    for d, s in zip(dst, src):
+        d.copy_(s)
+
+
+def _as_tensor(x):
+    """numpy array or (pinned host / device) tensor -> tensor for copy_()."""
+    return x if isinstance(x, torch.Tensor) else torch.from_numpy(np.ascontiguousarray(x))
+
+
+class LFM_Simulator:
+    """Forward leapfrog flow-map simulator (3D/lfm_midpoint_simulator.py:167)."""
+
+    def __init__(self, res_x=None, res_y=None, res_z=None, dx=None, dt=None, reinit_every=None, log_dir=None,
+                 log_target_dir=None, *, config: Optional[FlowmapConfig] = None, device="cuda"):
+        cfg = config if config is not None else FlowmapConfig()
+        if res_x is not None:
+            res = (res_x, res_y) if res_z is None else (res_x, res_y, res_z)
+            cfg = replace(cfg, res=tuple(res))
+        if dx is not None:
+            cfg = replace(cfg, dx=dx)
+        if dt is not None:
+            cfg = replace(cfg, dt=dt)
+        if reinit_every is not None:
+            cfg = replace(cfg, reinit_every=reinit_every)
+        if cfg.BFECC_clamp or cfg.use_short_BFECC:
+            raise FlowmapError(2, "BFECC_clamp / use_short_BFECC are not supported by this build")
+        if not torch.cuda.is_available():
+            raise FlowmapError(6, "LFM_Simulator needs a CUDA device (no CPU fallback)")
+        self.cfg = cfg
+        self.device = torch.device(device)
+        self.grid = GridSpec(tuple(cfg.res))
+        self.dim = self.grid.dim
+        self.dx = cfg.dx
+        self.dt = cfg.dt
+        self.reinit_every = cfg.reinit_every
+        self.res_x, self.res_y = cfg.res[0], cfg.res[1]
+        self.res_z = cfg.res[2] if self.dim == 3 else 1
+        self.log_dir = log_dir
+        self.log_target_dir = log_target_dir
+        dt_, dev, g = cfg.dtype, self.device, self.grid
+        self.store_dtype = cfg.store_dtype or cfg.dtype
+
+        sc = cfg.solver
+        self.solver = MGPCG(g.shape, dt_, base_level=sc.base_level, levels=sc.levels, pre_post=sc.pre_post,
+                            bottom=sc.bottom, bottom_mode=sc.bottom_mode, max_iters=sc.max_iters,
+                            abs_tol=sc.abs_tol, rel_tol=sc.rel_tol, eps=sc.eps, check_every=sc.check_every)
+
+        # flow maps: backward (psi, T) and forward (phi, F); centre maps for scalars
+        self.psi = torch.zeros((self.dim,) + g.shape, dtype=dt_, device=dev)
+        self.phi = torch.zeros((self.dim,) + g.shape, dtype=dt_, device=dev)
+        self.psi_f = _vec_face(g, dt_, dev)
+        self.T_f = _vec_face(g, dt_, dev)
+        self.phi_f = _vec_face(g, dt_, dev)
+        self.F_f = _vec_face(g, dt_, dev)
+
+        self.u = _mac(g, dt_, dev)
+        self.ad_u = _mac(g, dt_, dev)
+        self.final_u = _mac(g, dt_, dev)
+        self.init_u = _mac(g, dt_, dev)
+        self.err_u = _mac(g, dt_, dev)
+
+        self.passive = torch.zeros(g.shape, dtype=dt_, device=dev)
+        self.final_passive = torch.zeros_like(self.passive)
+        self.init_passive = torch.zeros_like(self.passive)
+        self.err_passive = torch.zeros_like(self.passive)
+
+        self.step_num = _Scalar(-1)
+        self.frame_idx = _Scalar(0)
+        self.total_steps = cfg.total_steps
+        self._alloc_stores()
+        self.reset_to_identity(self.phi, self.phi_f, self.F_f)
+
+    # ------------------------------------------------------------ stores
+    def _alloc_stores(self):
+        """Device-resident trajectory for the adjoint (replaces RW_Cache disk I/O)."""
+        g, steps, dev = self.grid, self.total_steps, self.device
+        n_int = (steps + self.reinit_every - 1) // self.reinit_every
+        sd, wd = self.store_dtype, self.cfg.dtype
+        self.store_mid = [torch.zeros((steps,) + g.face_shape(c), dtype=sd, device=dev) for c in range(self.dim)]
+        # flow maps (positions and Jacobians) stay in the working dtype: a BF16
+        # position would be ~0.5 cells off at 128^3
+        self.store_phi = torch.zeros((n_int, self.dim) + g.shape, dtype=wd, device=dev)
+        self.store_phi_f = [torch.zeros((n_int, self.dim) + g.face_shape(c), dtype=wd, device=dev)
+                            for c in range(self.dim)]
+        self.store_F_f = [torch.zeros((n_int, self.dim) + g.face_shape(c), dtype=wd, device=dev)
+                          for c in range(self.dim)]
+        need_passive = self.cfg.add_passive_scalar and (not self.cfg.backward_u or self.cfg.trajectory_loss)
+        self.store_passive = (torch.zeros((steps + 1,) + g.shape, dtype=sd, device=dev) if need_passive else None)
+        # in-interval midpoint velocities replayed by backtrack_psi_grid, in the working dtype
+        if sd == self.cfg.dtype:
+            self._ring = None
+        else:
+            self._ring = [[torch.zeros(g.face_shape(c), dtype=self.cfg.dtype, device=dev) for c in range(self.dim)]
+                          for _ in range(self.reinit_every)]
+
+    # ------------------------------------------------------------ kernels
+    def reset_to_identity(self, psi, psi_f, T_f):
+        K.reset_to_identity(self.grid, self.dx, psi, psi_f, T_f)
+
+    def _advect_u_grid(self, u0, u1, u2, dt):
+        K.advect_u_grid(self.grid, self.cfg.RK_number, self.dx, dt, u0, u1, u2)
+
+    def _advect_scalar_grid(self, u0, s1, s2, dt):
+        K.advect_scalar_grid(self.grid, self.cfg.RK_number, self.dx, dt, u0, s1, s2)
+
+    def _march(self, psi_c, psi_f, T_f, u, dt):
+        K.march_map(self.grid, self.cfg.RK_number, self.dx, dt, psi_c, psi_f, T_f, u)
+
+    def BFECC(self, init_u, u, err_u, T_f, psi_f, F_f, phi_f):
+        """BFECC (3D/flowmap.py:405-434, BFECC_clamp=False) in three fused launches:
+        u = T.init(psi); err = 0.5*(F.u(phi) - init); u = u - T.err(psi)."""
+        g, dx = self.grid, self.dx
+        K.pullback_u(g, dx, init_u, u, T_f, psi_f)
+        K.pullback_u(g, dx, u, err_u, F_f, phi_f, alpha=0.5, beta=-1.0, base=init_u)
+        K.pullback_u(g, dx, err_u, u, T_f, psi_f, alpha=-1.0, beta=-1.0, base=u)
+
+    def BFECC_scalar(self, init_s, s, err_s, psi, phi):
+        """BFECC_scalar (3D/flowmap.py:436-452, BFECC_clamp=False)."""
+        g, dx = self.grid, self.dx
+        K.pullback_scalar(g, dx, init_s, s, psi)
+        K.pullback_scalar(g, dx, s, err_s, phi, alpha=0.5, beta=-1.0, base=init_s)
+        K.pullback_scalar(g, dx, err_s, s, psi, alpha=-1.0, beta=-1.0, base=s)
+
+    def project(self, u):
+        self.solver.project(u)
+
+    # ------------------------------------------------------------ API
+    @property
+    def u_x(self):
+        return self.u[0]
+
+    @property
+    def u_y(self):
+        return self.u[1]
+
+    @property
+    def u_z(self):
+        return self.u[2] if self.dim == 3 else None
+
+    def init(self, theta=None, forward=True, target=False, init_passive_np=None):
+        """Case-11 initialisation (3D/lfm_midpoint_simulator.py:592-615): u from
+        ``theta`` (dict with u_x/u_y[/u_z] or a sequence of face arrays; zeros if
+        None), projected; passive from ``init_passive_np``; phi, F reset."""
+        if not forward:
+            return
+        for c in range(self.dim):
+            self.u[c].zero_()
+        if theta is not None:
+            comps = ([theta[k] for k in ("u_x", "u_y", "u_z")[: self.dim]] if isinstance(theta, dict) else list(theta))
+            for c in range(self.dim):
+                self.u[c].copy_(_as_tensor(comps[c]), non_blocking=True)
+        self.project(self.u)
+        if self.cfg.add_passive_scalar and init_passive_np is not None:
+            self.passive.copy_(_as_tensor(init_passive_np), non_blocking=True)
+            self.init_passive.copy_(self.passive)
+        self.step_num[None] = -1
+        self.frame_idx[None] = 0
+        self.reset_to_identity(self.phi, self.phi_f, self.F_f)
+        _copy_mac(self.init_u, self.u)
+
+    def final_condition(self):
+        return self.step_num[None] == self.total_steps - 1
+
+    def step_midpoint(self, write_flow_map=True, write_passive=True, control_force_para=None):
+        """One leapfrog step (3D/lfm_midpoint_simulator.py:648-682)."""
+        if control_force_para is not None:
+            raise FlowmapError(2, "control forces are not supported by this build")
+        self.step_num[None] += 1
+        n = self.step_num[None]
+        if n >= self.total_steps:
+            raise FlowmapError(2, f"step {n} beyond total_steps={self.total_steps}")
+        j = n % self.reinit_every
+        if self.store_passive is not None:
+            self.store_passive[n].copy_(self.passive)
+        self.step_flow_map(j, self.dt)
+        if self.final_condition() and self.store_passive is not None:
+            self.store_passive[n + 1].copy_(self.passive)
+        return False, self.final_condition()
+
+    def march_phi_grid(self, u):
+        """3D/lfm_midpoint_simulator.py:377-381 (one launch for centre + faces)."""
+        self._march(self.phi, self.phi_f, self.F_f, u, -self.dt)
+
+    def backtrack_psi_grid(self, curr_step: int, interval_start: int):
+        """3D/lfm_midpoint_simulator.py:357-375: rebuild psi, T over the
+        interval, the last sub-step with the current u (as the reference does)."""
+        self.reset_to_identity(self.psi, self.psi_f, self.T_f)
+        self._march(self.psi, self.psi_f, self.T_f, self.u, self.dt)
+        for s in reversed(range(curr_step)):
+            if self._ring is not None:
+                um = self._ring[s]
+            else:
+                um = [m[interval_start + s] for m in self.store_mid]
+            self._march(self.psi, self.psi_f, self.T_f, um, self.dt)
+
+    def step_flow_map(self, j: int, curr_dt: float):
+        """3D/lfm_midpoint_simulator.py:684-807 with add_control_force=False,
+        use_short_BFECC=False, viscosity=0."""
+        cfg = self.cfg
+        n = self.step_num[None]
+        _copy_mac(self.ad_u, self.u)
+        self._advect_u_grid(self.ad_u, self.ad_u, self.u, 0.5 * curr_dt)
+        self.project(self.u)
+        # write_velocity + RW_Cache("u"): the midpoint velocity of step n
+        for c in range(self.dim):
+            self.store_mid[c][n].copy_(self.u[c])
+            if self._ring is not None:
+                self._ring[j][c].copy_(self.u[c])
+        self.march_phi_grid(self.u)
+        if cfg.add_passive_scalar:
+            self._advect_scalar_grid(self.u, self.passive, self.final_passive, curr_dt)
+            self.passive, self.final_passive = self.final_passive, self.passive
+        self._advect_u_grid(self.u, self.ad_u, self.final_u, curr_dt)
+        self.u, self.final_u = self.final_u, self.u
+        self.project(self.u)
+
+        if j == self.reinit_every - 1:
+            self.backtrack_psi_grid(self.reinit_every - 1, n - j)
+            self.BFECC(self.init_u, self.u, self.err_u, self.T_f, self.psi_f, self.F_f, self.phi_f)
+            self.project(self.u)
+            if cfg.add_passive_scalar:
+                self.BFECC_scalar(self.init_passive, self.passive, self.err_passive, self.psi, self.phi)
+                self.init_passive.copy_(self.passive)
+            k = n // self.reinit_every
+            self.store_phi[k].copy_(self.phi)
+            for c in range(self.dim):
+                self.store_phi_f[c][k].copy_(self.phi_f[c])
+                self.store_F_f[c][k].copy_(self.F_f[c])
+            self.reset_to_identity(self.phi, self.phi_f, self.F_f)
+            _copy_mac(self.init_u, self.u)
+        elif n == self.total_steps - 1:
+            # a final partial interval: keep its forward map for the adjoint
+            k = n // self.reinit_every
+            self.store_phi[k].copy_(self.phi)
+            for c in range(self.dim):
+                self.store_phi_f[c][k].copy_(self.phi_f[c])
+                self.store_F_f[c][k].copy_(self.F_f[c])
+
+
+class LFM_Diff_Simulator(LFM_Simulator):
+    """Adjoint simulator (3D/lfm_midpoint_diff_simulator.py:15-594)."""
+
+    def __init__(self, *a, **kw):
+        super().__init__(*a, **kw)
+        g, dt_, dev = self.grid, self.cfg.dtype, self.device
+        self.adj_u = _mac(g, dt_, dev)
+        self.init_adj_u = _mac(g, dt_, dev)
+        self.src = _mac(g, dt_, dev)            # ajd_uw_source
+        self.H_prev = _mac(g, dt_, dev)         # adj_u_*_AB_tem
+        self.H_prev_prev = _mac(g, dt_, dev)    # adj_u_*_AB_tem2
+        self.adj_passive = torch.zeros(g.shape, dtype=dt_, device=dev)
+        self.init_adj_passive = torch.zeros_like(self.adj_passive)
+        self.adj_passive_f = _mac(g, dt_, dev)
+        self.mid_u = _mac(g, dt_, dev)
+        self.target_passive = None
+        self.target_trajectory = None
+        self.loss = 0.0
+        self.final_ind = None
+
+    @property
+    def adj_u_x(self):
+        return self.adj_u[0]
+
+    @property
+    def adj_u_y(self):
+        return self.adj_u[1]
+
+    @property
+    def adj_u_z(self):
+        return self.adj_u[2] if self.dim == 3 else None
+
+    def forward_step_midpoint(self, write_flow_map=True, write_passive=True, control_force_para=None):
+        return self.step_midpoint(write_flow_map, write_passive, control_force_para)
+
+    def init_gradient(self, theta=None, target_passive=None):
+        """Loss and adjoint seed (3D/lfm_midpoint_diff_simulator.py:336-376, case 11):
+        L = sum (s - s*)^2, adj_passive = 2 (s - s*), adj_u = 0; psi, T reset."""
+        if target_passive is not None:
+            self.target_passive = torch.empty(self.grid.shape, dtype=self.cfg.dtype, device=self.device)
+            self.target_passive.copy_(_as_tensor(target_passive), non_blocking=True)
+        if self.target_passive is None:
+            raise FlowmapError(2, "init_gradient needs target_passive")
+        self.final_ind = self.step_num[None] + 1
+        for c in range(self.dim):
+            self.adj_u[c].zero_()
+            self.H_prev[c].zero_()
+            self.H_prev_prev[c].zero_()
+        diff = self.passive - self.target_passive
+        self.adj_passive.copy_(2 * diff)
+        self.loss = float(torch.sum(diff.double() ** 2))
+        self.step_num[None] = self.final_ind
+        _copy_mac(self.init_adj_u, self.adj_u)
+        self.init_adj_passive.copy_(self.adj_passive)
+        if self.cfg.backward_u:
+            _copy_mac(self.init_u, self.u)
+            self.init_passive.copy_(self.passive)
+        self.reset_to_identity(self.psi, self.psi_f, self.T_f)
+
+    def march_psi_grid(self, dt):
+        self._march(self.psi, self.psi_f, self.T_f, self.mid_u, dt)
+
+    def backtrack_step_midpoint(self, write_gradient=False, write_passive=False, control_force_para=None):
+        """3D/lfm_midpoint_diff_simulator.py:390-419."""
+        if control_force_para is not None:
+            raise FlowmapError(2, "control forces are not supported by this build")
+        self.step_num[None] -= 1
+        n = self.step_num[None]
+        j = n % self.reinit_every
+        if self.cfg.add_passive_scalar and not self.cfg.backward_u:
+            self.passive.copy_(self.store_passive[n + 1])
+        self.backtrack_flow_map(j, self.dt)
+        return False, n == 0
+
+    def backtrack_flow_map(self, j: int, curr_dt: float):
+        """3D/lfm_midpoint_diff_simulator.py:421-594 with add_control_force=False,
+        use_short_BFECC=False."""
+        cfg, g, dx = self.cfg, self.grid, self.dx
+        n = self.step_num[None]
+        for c in range(self.dim):
+            self.mid_u[c].copy_(self.store_mid[c][n])
+        K.nabla_u_w(g, dx, self.u if cfg.backward_u else self.mid_u, self.adj_u, self.src)
+        if cfg.add_passive_scalar:
+            K.nabla_scalar_adjoint(g, dx, self.passive, self.adj_passive, self.adj_passive_f)
+
+        self._advect_u_grid(self.mid_u, self.adj_u, self.final_u, -curr_dt)
+        self.adj_u, self.final_u = self.final_u, self.adj_u
+        if cfg.backward_u:
+            if cfg.add_passive_scalar:
+                self._advect_scalar_grid(self.mid_u, self.passive, self.final_passive, -curr_dt)
+                self.passive, self.final_passive = self.final_passive, self.passive
+            self._advect_u_grid(self.mid_u, self.u, self.final_u, -curr_dt)
+            self.u, self.final_u = self.final_u, self.u
+        for c in range(self.dim):
+            K.add_fields(self.adj_u[c], self.src[c], self.adj_u[c], -curr_dt)
+        if cfg.add_passive_scalar:
+            self._advect_scalar_grid(self.mid_u, self.adj_passive, self.final_passive, -curr_dt)
+            self.adj_passive, self.final_passive = self.final_passive, self.adj_passive
+            for c in range(self.dim):
+                K.add_fields(self.adj_u[c], self.adj_passive_f[c], self.adj_u[c], -curr_dt)
+
+        self.march_psi_grid(curr_dt)
+        # Adams-Bashforth index: adjoint steps already taken in this interval
+        # (= reinit_every-1-j for a full interval, as the reference computes it)
+        interval_last = min((n // self.reinit_every) * self.reinit_every + self.reinit_every - 1,
+                            self.total_steps - 1)
+        K.accumulate_init(g, dx, -2 * curr_dt, self.src, self.init_adj_u, self.T_f, self.psi_f, self.H_prev,
+                          self.H_prev_prev, interval_last - n)
+        if cfg.add_passive_scalar:
+            K.accumulate_init(g, dx, -curr_dt, self.adj_passive_f, self.init_adj_u, self.T_f, self.psi_f)
+        self.project(self.adj_u)  # Poisson_adj
+        if cfg.backward_u:
+            self.project(self.u)
+
+        if j == 0:
+            k = n // self.reinit_every
+            self.phi.copy_(self.store_phi[k])
+            for c in range(self.dim):
+                self.phi_f[c].copy_(self.store_phi_f[c][k])
+                self.F_f[c].copy_(self.store_F_f[c][k])
+            self.BFECC(self.init_adj_u, self.adj_u, self.err_u, self.F_f, self.phi_f, self.T_f, self.psi_f)
+            self.project(self.adj_u)
+            _copy_mac(self.init_adj_u, self.adj_u)
+            if cfg.backward_u:
+                self.BFECC(self.init_u, self.u, self.err_u, self.F_f, self.phi_f, self.T_f, self.psi_f)
+                self.project(self.u)
+                _copy_mac(self.init_u, self.u)
+            if cfg.add_passive_scalar:
+                if cfg.trajectory_loss or not cfg.backward_u:
+                    self.passive.copy_(self.store_passive[n])
+                else:
+                    self.BFECC_scalar(self.init_passive, self.passive, self.err_passive, self.phi, self.psi)
+                self.init_passive.copy_(self.passive)
+                self.BFECC_scalar(self.init_adj_passive, self.adj_passive, self.err_passive, self.phi, self.psi)
+                if cfg.trajectory_loss:
+                    tgt = self.target_trajectory[n]
+                    d = self.passive - tgt
+                    self.adj_passive.add_(d)
+                    self.loss += float(torch.sum(d.double() ** 2))
+                self.init_adj_passive.copy_(self.adj_passive)
+            self.reset_to_identity(self.psi, self.psi_f, self.T_f)
+
+    # --------------------------------------------------------- driver
+    def gradient(self, u0, passive0, target_passive):
+        """Full forward + adjoint: returns (loss, dL/du0 as a list of face tensors)."""
+        self.init(theta=u0, init_passive_np=passive0)
+        while True:
+            _, final = self.forward_step_midpoint()
+            if final:
+                break
+        self.init_gradient(target_passive=target_passive)
+        while True:
+            _, done = self.backtrack_step_midpoint()
+            if done:
+                break
+        return self.loss, [x.clone() for x in self.adj_u]

@@ -45,6 +45,12 @@ enum {
 int fm_abi_version(void);
 const char *fm_status_string(int status);
 
+/* Number of kernels this library has launched on any stream since load (or
+ * the last reset); a CUDA-graph launch adds the kernels it contains.  Used by
+ * the benchmark to report its launch count.  reset != 0 returns the count and
+ * zeroes it. */
+long long fm_launch_count(int reset);
+
 /* advect_u_grid: semi-Lagrangian advection, RK2 (midpoint) or RK4 backtrace
  * of the face nodes through u0, then u2_c = (u1 sampled at the foot)_c.
  * Replaces RK2_advect_u_grid / RK4_advect_u_grid (3D/flowmap.py:202-282,
@@ -148,7 +154,11 @@ typedef struct {
     double abs_tol;    /* converged when rTr < max(abs_tol, rel_tol * zTr0) */
     double rel_tol;
     double eps;        /* added to alpha/beta denominators (reference: 1e-12) */
-    int check_every;   /* iterations per host convergence check (>= 1) */
+    int check_every;   /* 0: device mode -- the PCG loop is a CUDA-graph conditional
+                          WHILE node, the solve never synchronises the host, and
+                          its outcome is read with fm_mgpcg_stats;
+                          k >= 1: host-checked mode, the host polls convergence
+                          every k iterations */
     int coarse_bf16;   /* 1: store levels >= 1 in BF16 (FM_F32 only) */
 } fm_mg_params;
 
@@ -168,8 +178,25 @@ int fm_mgpcg_destroy(fm_mgpcg *solver);
 int fm_project(fm_mgpcg *solver, void *ux, void *uy, void *uz, void *p_out, void *stream,
                int *iters, double *rtr);
 
-/* Solve A x = b (b cell grid, recentred internally as the reference does). */
+/* Solve A x = b (b cell grid, recentred internally as the reference does).
+ * In device mode (check_every = 0) fm_project and fm_mgpcg_solve return as
+ * soon as the work is enqueued when iters and rtr are both NULL; passing
+ * either synchronises the stream and reports the outcome. */
 int fm_mgpcg_solve(fm_mgpcg *solver, const void *b, void *x, void *stream, int *iters, double *rtr);
+
+/* Cumulative solver outcome (synchronises `stream`).  reset != 0 zeroes the
+ * counters afterwards.  The reference reports non-convergence only with a
+ * print (3D/mgpcg.py:286-289); here it is counted. */
+typedef struct {
+    long long solves;         /* completed solves */
+    long long iterations;     /* sum of PCG iterations */
+    long long not_converged;  /* solves that hit max_iters */
+    long long nonfinite;      /* solves stopped by a NaN/Inf residual */
+    int last_iters;           /* iterations of the last solve */
+    int max_iters_seen;       /* largest iteration count */
+    double last_rtr;          /* last r.r */
+} fm_mg_stats;
+int fm_mgpcg_stats(fm_mgpcg *solver, void *stream, int reset, fm_mg_stats *out);
 
 /* Apply the Neumann Laplacian: Ap = A p (for tests and defect correction). */
 int fm_laplacian(const fm_grid *g, int dtype, const void *p, void *Ap, void *stream);

@@ -1,0 +1,276 @@
+"""CPU restatement of the reference simulator's control flow (forward leapfrog
+step with reinitialisation, adjoint backtrack).  TEST INFRASTRUCTURE ONLY:
+the end-to-end parity checker for the CUDA simulator; never used by the product.
+
+Follows, statement by statement (including copy_to / add_fields / scale_field
+sequences, which the product fuses):
+  forward  3D/lfm_midpoint_simulator.py:648-807   (step_midpoint, step_flow_map,
+           backtrack_psi_grid :368-375, march_phi_grid :377-381)
+  adjoint  3D/lfm_midpoint_diff_simulator.py:336-594 (init_gradient case 11,
+           backtrack_step_midpoint, backtrack_flow_map)
+  BFECC    3D/flowmap.py:405-452
+with add_control_force=False, use_short_BFECC=False, BFECC_clamp=False,
+viscosity=0 and empty obstacle masks.  The trajectory the reference writes to
+.npy files is kept in Python lists.  Two documented extensions match the
+product: a run whose last reinit interval is partial stores that interval's
+forward map at the last step, and the Adams-Bashforth index counts adjoint
+steps from the end of the interval actually simulated (identical to the
+reference's reinit_every-1-j for full intervals).
+"""
+from __future__ import annotations
+
+import numpy as np
+
+from oracle import MGParams, Oracle
+
+
+class OracleSim:
+    def __init__(self, res, dx, dt, reinit_every, total_steps, rk=4, backward_u=True, passive=True,
+                 trajectory_loss=False, prec="f64", mg=None):
+        self.o = Oracle(tuple(res), prec)
+        self.dim = len(res)
+        self.res = tuple(res)
+        self.dx, self.dt, self.R, self.total_steps = dx, dt, reinit_every, total_steps
+        self.rk, self.backward_u, self.passive_on, self.trajectory_loss = rk, backward_u, passive, trajectory_loss
+        self.mg = mg if mg is not None else MGParams(max(2, int(np.log2(min(res))) - 2), 2, 50, 0, 400, 1e-12, 0.0,
+                                                    1e-12)
+        o = self.o
+        mac = o.zeros_mac
+        self.u, self.ad_u, self.final_u, self.init_u = mac(), mac(), mac(), mac()
+        self.err_u, self.tmp_u = mac(), mac()
+        self.psi, self.phi = o.zeros_cell(self.dim), o.zeros_cell(self.dim)
+        self.psi_f = [o.zeros_face(c, self.dim) for c in range(self.dim)]
+        self.T_f = [o.zeros_face(c, self.dim) for c in range(self.dim)]
+        self.phi_f = [o.zeros_face(c, self.dim) for c in range(self.dim)]
+        self.F_f = [o.zeros_face(c, self.dim) for c in range(self.dim)]
+        self.passive = o.zeros_cell()
+        self.final_passive, self.init_passive = o.zeros_cell(), o.zeros_cell()
+        self.err_passive, self.tmp_passive = o.zeros_cell(), o.zeros_cell()
+        self.velocity_storage = {}
+        self.store_mid, self.store_passive, self.store_maps = {}, {}, {}
+        self.step_num = -1
+        self.iters = []
+
+    # -------------------------------------------------------------- helpers
+    def Poisson(self, u):
+        it, rtr, conv = self.o.Poisson(self.mg, u)
+        self.iters.append(it)
+
+    def reset_to_identity(self, psi, psi_f, T_f):
+        self.o.reset_to_identity(psi, psi_f, T_f, self.dx)
+
+    def RK_grid_only_psi(self, psi, u, dt):
+        self.o.RK_grid(self.rk, -1, psi, None, u, self.dx, dt)
+
+    def RK_grid(self, face, psi, T, u, dt):
+        self.o.RK_grid(self.rk, face, psi, T, u, self.dx, dt)
+
+    def BFECC(self, init_u, u, err_u, tmp_u, T_f, psi_f, F_f, phi_f):
+        o = self.o
+        o.advect_u(init_u, u, T_f, psi_f, self.dx)
+        o.advect_u(u, err_u, F_f, phi_f, self.dx)
+        for c in range(self.dim):
+            err_u[c][...] = err_u[c] + (-1.0) * init_u[c]   # add_fields(err, init, err, -1)
+        for c in range(self.dim):
+            err_u[c][...] = 0.5 * err_u[c]                  # scale_field(err, 0.5, err)
+        o.advect_u(err_u, tmp_u, T_f, psi_f, self.dx)
+        for c in range(self.dim):
+            err_u[c][...] = u[c] + (-1.0) * tmp_u[c]        # add_fields(u, tmp, err, -1)
+        for c in range(self.dim):
+            u[c][...] = err_u[c]                            # copy_to(err, u)
+
+    def BFECC_scalar(self, init_s, s, err_s, tmp_s, psi, phi):
+        o = self.o
+        o.advect_scalar(init_s, s, psi, self.dx)
+        o.advect_scalar(s, err_s, phi, self.dx)
+        err_s[...] = err_s + (-1.0) * init_s
+        err_s[...] = 0.5 * err_s
+        o.advect_scalar(err_s, tmp_s, psi, self.dx)
+        err_s[...] = s + (-1.0) * tmp_s
+        s[...] = err_s
+
+    # -------------------------------------------------------------- forward
+    def init(self, u0, passive0):
+        for c in range(self.dim):
+            self.u[c][...] = u0[c]
+        self.Poisson(self.u)
+        if self.passive_on:
+            self.passive[...] = passive0
+            self.init_passive[...] = self.passive
+        self.step_num = -1
+        self.reset_to_identity(self.phi, self.phi_f, self.F_f)
+        for c in range(self.dim):
+            self.init_u[c][...] = self.u[c]
+
+    def march_phi_grid(self):
+        self.RK_grid_only_psi(self.phi, self.u, -1 * self.dt)
+        for c in range(self.dim):
+            self.RK_grid(c, self.phi_f[c], self.F_f[c], self.u, -1 * self.dt)
+
+    def march_no_neural(self, step):
+        tmp = [np.array(x) for x in self.velocity_storage[step]]
+        for c in range(self.dim):
+            self.RK_grid(c, self.psi_f[c], self.T_f[c], tmp, self.dt)
+        self.RK_grid_only_psi(self.psi, tmp, self.dt)
+
+    def backtrack_psi_grid(self, curr_step):
+        self.reset_to_identity(self.psi, self.psi_f, self.T_f)
+        self.RK_grid_only_psi(self.psi, self.u, self.dt)
+        for c in range(self.dim):
+            self.RK_grid(c, self.psi_f[c], self.T_f[c], self.u, self.dt)
+        for step in reversed(range(curr_step)):
+            self.march_no_neural(step)
+
+    def step_midpoint(self):
+        self.step_num += 1
+        n = self.step_num
+        j = n % self.R
+        if self.passive_on:
+            self.store_passive[n] = self.passive.copy()
+        self.step_flow_map(j, self.dt)
+        final = n == self.total_steps - 1
+        if final and self.passive_on:
+            self.store_passive[n + 1] = self.passive.copy()
+        return final
+
+    def step_flow_map(self, j, dt):
+        o, d = self.o, self.dim
+        for c in range(d):
+            self.ad_u[c][...] = self.u[c]
+        o.advect_u_grid(self.rk, self.ad_u, self.ad_u, self.u, self.dx, 0.5 * dt)
+        self.Poisson(self.u)
+        self.velocity_storage[j] = [x.copy() for x in self.u]
+        self.march_phi_grid()
+        self.store_mid[self.step_num] = [x.copy() for x in self.u]
+        if self.passive_on:
+            o.advect_scalar_grid(self.rk, self.u, self.passive, self.final_passive, self.dx, dt)
+            self.passive[...] = self.final_passive
+        o.advect_u_grid(self.rk, self.u, self.ad_u, self.final_u, self.dx, dt)
+        for c in range(d):
+            self.u[c][...] = self.final_u[c]
+        self.Poisson(self.u)
+        n = self.step_num
+        if j == self.R - 1:
+            self.backtrack_psi_grid(self.R - 1)
+            self.BFECC(self.init_u, self.u, self.err_u, self.tmp_u, self.T_f, self.psi_f, self.F_f, self.phi_f)
+            self.Poisson(self.u)
+            if self.passive_on:
+                self.BFECC_scalar(self.init_passive, self.passive, self.err_passive, self.tmp_passive, self.psi,
+                                  self.phi)
+                self.init_passive[...] = self.passive
+            self.store_maps[n // self.R] = (self.phi.copy(), [x.copy() for x in self.phi_f],
+                                            [x.copy() for x in self.F_f])
+            self.reset_to_identity(self.phi, self.phi_f, self.F_f)
+            for c in range(d):
+                self.init_u[c][...] = self.u[c]
+            self.velocity_storage = {}
+        elif n == self.total_steps - 1:
+            self.store_maps[n // self.R] = (self.phi.copy(), [x.copy() for x in self.phi_f],
+                                            [x.copy() for x in self.F_f])
+
+    # -------------------------------------------------------------- adjoint
+    def init_gradient(self, target):
+        o, d = self.o, self.dim
+        self.final_ind = self.step_num + 1
+        self.adj_u = o.zeros_mac()
+        self.init_adj_u = o.zeros_mac()
+        self.src = o.zeros_mac()
+        self.H_prev, self.H_prev_prev = o.zeros_mac(), o.zeros_mac()
+        self.mid_u = o.zeros_mac()
+        self.adj_passive_f = o.zeros_mac()
+        diff = self.passive - target
+        self.adj_passive = (2 * diff).astype(o.dtype)
+        self.loss = float(np.sum(diff.astype(np.float64) ** 2))
+        self.init_adj_passive = self.adj_passive.copy()
+        self.step_num = self.final_ind
+        if self.backward_u:
+            for c in range(d):
+                self.init_u[c][...] = self.u[c]
+            self.init_passive[...] = self.passive
+        self.reset_to_identity(self.psi, self.psi_f, self.T_f)
+
+    def march_psi_grid(self, dt):
+        self.RK_grid_only_psi(self.psi, self.mid_u, dt)
+        for c in range(self.dim):
+            self.RK_grid(c, self.psi_f[c], self.T_f[c], self.mid_u, dt)
+
+    def backtrack_step_midpoint(self):
+        self.step_num -= 1
+        n = self.step_num
+        j = n % self.R
+        if self.passive_on and not self.backward_u:
+            self.passive[...] = self.store_passive[n + 1]
+        self.backtrack_flow_map(j, self.dt)
+        return n == 0
+
+    def backtrack_flow_map(self, j, dt):
+        o, d, dx = self.o, self.dim, self.dx
+        n = self.step_num
+        for c in range(d):
+            self.mid_u[c][...] = self.store_mid[n][c]
+        o.calculate_nabla_u_w(self.u if self.backward_u else self.mid_u, self.adj_u, self.src, dx)
+        if self.passive_on:
+            o.calculate_nabla_scalar_adjoint(self.passive, self.adj_passive, self.adj_passive_f, dx)
+        o.advect_u_grid(self.rk, self.mid_u, self.adj_u, self.final_u, dx, -dt)
+        for c in range(d):
+            self.adj_u[c][...] = self.final_u[c]
+        if self.backward_u:
+            if self.passive_on:
+                o.advect_scalar_grid(self.rk, self.mid_u, self.passive, self.final_passive, dx, -dt)
+                self.passive[...] = self.final_passive
+            o.advect_u_grid(self.rk, self.mid_u, self.u, self.final_u, dx, -dt)
+            for c in range(d):
+                self.u[c][...] = self.final_u[c]
+        for c in range(d):
+            self.adj_u[c][...] = self.adj_u[c] + (-dt) * self.src[c]
+        if self.passive_on:
+            o.advect_scalar_grid(self.rk, self.mid_u, self.adj_passive, self.final_passive, dx, -dt)
+            self.adj_passive[...] = self.final_passive
+            for c in range(d):
+                self.adj_u[c][...] = self.adj_u[c] + (-dt) * self.adj_passive_f[c]
+        self.march_psi_grid(dt)
+        interval_last = min((n // self.R) * self.R + self.R - 1, self.total_steps - 1)
+        ind = interval_last - n
+        o.accumulate_init_new(self.src, self.init_adj_u, self.T_f, self.psi_f, self.H_prev, self.H_prev_prev, ind,
+                              dx, -2 * dt)
+        if self.passive_on:
+            o.accumulate_init(self.adj_passive_f, self.init_adj_u, self.T_f, self.psi_f, dx, -dt)
+        self.Poisson(self.adj_u)
+        if self.backward_u:
+            self.Poisson(self.u)
+        if j == 0:
+            phi, phi_f, F_f = self.store_maps[n // self.R]
+            self.phi[...] = phi
+            for c in range(d):
+                self.phi_f[c][...] = phi_f[c]
+                self.F_f[c][...] = F_f[c]
+            self.BFECC(self.init_adj_u, self.adj_u, self.err_u, self.tmp_u, self.F_f, self.phi_f, self.T_f,
+                       self.psi_f)
+            self.Poisson(self.adj_u)
+            for c in range(d):
+                self.init_adj_u[c][...] = self.adj_u[c]
+            if self.backward_u:
+                self.BFECC(self.init_u, self.u, self.err_u, self.tmp_u, self.F_f, self.phi_f, self.T_f, self.psi_f)
+                self.Poisson(self.u)
+                for c in range(d):
+                    self.init_u[c][...] = self.u[c]
+            if self.passive_on:
+                if self.trajectory_loss or not self.backward_u:
+                    self.passive[...] = self.store_passive[n]
+                else:
+                    self.BFECC_scalar(self.init_passive, self.passive, self.err_passive, self.tmp_passive, self.phi,
+                                      self.psi)
+                self.init_passive[...] = self.passive
+                self.BFECC_scalar(self.init_adj_passive, self.adj_passive, self.err_passive, self.tmp_passive,
+                                  self.phi, self.psi)
+                self.init_adj_passive[...] = self.adj_passive
+            self.reset_to_identity(self.psi, self.psi_f, self.T_f)
+
+    def gradient(self, u0, passive0, target):
+        self.init(u0, passive0)
+        while not self.step_midpoint():
+            pass
+        self.init_gradient(target)
+        while not self.backtrack_step_midpoint():
+            pass
+        return self.loss, [x.copy() for x in self.adj_u]

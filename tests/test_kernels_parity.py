@@ -196,7 +196,7 @@ def test_accumulate_init(fm, cuda, shape, prec, ab3, ind):
     Hp = _rand_mac(rng, shape, 1.0)
     Hpp = _rand_mac(rng, shape, 1.0)
     dt = -2 * 0.3 * dx
-    cv = lambda L: [np.ascontiguousarray(x, o.dtype) for x in L]
+    cv = lambda L: [np.array(x, dtype=o.dtype, copy=True) for x in L]
     init_r, Hp_r, Hpp_r = cv(init), cv(Hp), cv(Hpp)
     if ab3:
         o.accumulate_init_new(cv(f), init_r, cv(F), cv(phi), Hp_r, Hpp_r, ind, dx, dt)
@@ -224,7 +224,7 @@ def test_nabla_u_w(fm, cuda, shape, prec, order):
     u = _rand_mac(rng, shape, 1.0)
     w = _rand_mac(rng, shape, 1.0)
     ref = [np.zeros(g.face_shape(c), o.dtype) for c in range(dim)]
-    cv = lambda L: [np.ascontiguousarray(x, o.dtype) for x in L]
+    cv = lambda L: [np.array(x, dtype=o.dtype, copy=True) for x in L]
     o.calculate_nabla_u_w(cv(u), cv(w), ref, dx, order)
     out = [torch.zeros(g.face_shape(c), dtype=dtype, device=cuda) for c in range(dim)]
     fm.kernels.nabla_u_w(g, dx, [_t(x, dtype, cuda) for x in u], [_t(x, dtype, cuda) for x in w], out, order)
@@ -311,3 +311,29 @@ def test_vcycle_iterations_match_oracle(fm, cuda):
     assert conv_ref and sol.last_converged
     assert abs(it - it_ref) <= 1
     assert _rel(x.cpu().numpy(), x_ref) < 1e-8
+
+
+@pytest.mark.parametrize("shape", [(32, 32, 32), (64, 64)])
+def test_project_device_mode_matches_host_mode(fm, cuda, shape):
+    """check_every=0 (conditional WHILE graph, no host sync) gives the same
+    projection and iteration count as the host-checked loop; stats count solves."""
+    rng = np.random.default_rng(12)
+    g = fm.GridSpec(shape)
+    levels = int(np.log2(min(shape))) - 3 + 1
+    u = [torch.tensor(rng.uniform(-1, 1, size=g.face_shape(c)), dtype=torch.float64, device=cuda)
+         for c in range(len(shape))]
+    a = [x.clone() for x in u]
+    b = [x.clone() for x in u]
+    host = fm.MGPCG(shape, torch.float64, levels=levels, rel_tol=1e-10, abs_tol=0.0, eps=0.0, check_every=1)
+    dev = fm.MGPCG(shape, torch.float64, levels=levels, rel_tol=1e-10, abs_tol=0.0, eps=0.0, check_every=0)
+    host.project(a)
+    dev.project(b)
+    st = dev.stats(reset=True)
+    assert st["solves"] == 1 and st["not_converged"] == 0 and st["nonfinite"] == 0
+    assert st["last_iters"] == host.last_iters
+    for x, y in zip(a, b):
+        assert torch.equal(x, y)
+    for _ in range(3):
+        dev.project([x.clone() for x in u])
+    st = dev.stats()
+    assert st["solves"] == 3 and st["iterations"] == 3 * host.last_iters
