@@ -25,6 +25,7 @@ STATUS = {
     5: "FM_ERR_TIMEOUT",
     6: "FM_ERR_CUDA",
     7: "FM_ERR_DTYPE",
+    8: "FM_ERR_CAPACITY",
 }
 
 
@@ -92,6 +93,7 @@ SIGNATURES = {
     "fm_mgpcg_solve": [P, P, P, P, C.POINTER(I), C.POINTER(D)],
     "fm_laplacian": [GP, I, P, P, P],
     "fm_mgpcg_stats": [P, P, I, C.POINTER(MGStats)],
+    "fm_project_noalloc": [GP, I, C.POINTER(MGParams), P, P, P, P, C.POINTER(I), C.POINTER(D)],
 }
 RESTYPES = {"fm_launch_count": C.c_longlong}
 SIGNATURES["fm_launch_count"] = [I]

@@ -23,6 +23,8 @@
 #include <stdlib.h>
 #include <string.h>
 
+#include <mutex>
+
 #include "fm_common.cuh"
 #include "fm_internal.h"
 
@@ -828,8 +830,149 @@ const char* fm_status_string(int status) {
     case FM_ERR_TIMEOUT: return "bounded device wait timed out";
     case FM_ERR_CUDA: return "CUDA runtime error";
     case FM_ERR_DTYPE: return "unsupported dtype";
+    case FM_ERR_CAPACITY: return "grid too large for the static scratch of fm_project_noalloc";
     default: return "unknown status";
   }
 }
 
 }  // extern "C"
+
+// ---------------------------------------------------------------------------
+// fm_project_noalloc: the projection without any allocation.
+//
+// Its MG hierarchy, PCG vectors, reduction partials and solver state are carved
+// out of one file-scope __device__ array (kNoAllocScratchBytes), which every
+// GPU that loads this library holds until the process exits.  Host code cannot
+// use the array's name as a device address (it names a host-side shadow), so
+// the address is fetched with cudaGetSymbolAddress once per device, with that
+// device current, on the first call made on it; that first call should
+// therefore come before any stream capture.  Kernels are launched directly (no
+// CUDA graph, whose instantiation may allocate) and convergence is polled
+// through a host stack variable (no pinned buffer).
+// ---------------------------------------------------------------------------
+namespace fm {
+
+constexpr size_t kNoAllocScratchBytes = size_t(48) << 20;  // 48 MiB
+static __device__ __align__(256) unsigned char g_noalloc_scratch[kNoAllocScratchBytes];
+
+constexpr int kMaxDevices = 64;
+static void* g_noalloc_base[kMaxDevices];
+static std::mutex g_noalloc_mu;
+
+static int noalloc_scratch(void** out) {
+  int dev = 0;
+  if (cudaGetDevice(&dev) != cudaSuccess || dev < 0 || dev >= kMaxDevices) return FM_ERR_CUDA;
+  std::lock_guard<std::mutex> lock(g_noalloc_mu);
+  if (!g_noalloc_base[dev]) {
+    void* p = nullptr;
+    if (cudaGetSymbolAddress(&p, g_noalloc_scratch) != cudaSuccess || !p) return FM_ERR_CUDA;
+    g_noalloc_base[dev] = p;
+  }
+  *out = g_noalloc_base[dev];
+  return FM_OK;
+}
+
+// Lays the solver's buffers out from `base` (nullptr: size only); returns bytes.
+static size_t noalloc_layout(const fm_grid& g, int dtype, int levels, fm_mgpcg* S, unsigned char* base) {
+  size_t off = 0;
+  auto take = [&](size_t bytes) -> void* {
+    off = (off + 255) & ~size_t(255);
+    void* p = base ? (void*)(base + off) : nullptr;
+    off += bytes;
+    return p;
+  };
+  const size_t es = dtype == FM_F32 ? sizeof(float) : sizeof(double);
+  for (int l = 0; l < levels; ++l) {
+    Shape sh{g.n[0] >> l, g.n[1] >> l, g.dim == 3 ? (g.n[2] >> l) : 1};
+    S->lv[l] = sh;
+    S->r[l] = take(es * sh.size());
+    S->z[l] = take(es * sh.size());
+  }
+  const long n0 = S->lv[0].size();
+  S->x = take(es * n0);
+  S->p = take(es * n0);
+  S->Ap = take(es * n0);
+  S->part = (double*)take(sizeof(double) * 2 * kRedBlocks);
+  S->st = (DevState*)take(sizeof(DevState));
+  return off;
+}
+
+// Host-checked solve with direct launches (no graph).
+template <typename T>
+static int run_solve_direct(fm_mgpcg* S, cudaStream_t s, int* iters, double* rtr) {
+  const int D = S->g.dim;
+  const int every = S->P.check_every > 0 ? S->P.check_every : 4;
+  if (D == 3) launch_prologue<T, 3>(S, s); else launch_prologue<T, 2>(S, s);
+  DevState h;
+  long launched = 0;
+  const long limit = (long)S->P.max_iters + every;
+  for (;;) {
+    for (int i = 0; i < every; ++i) {
+      if (D == 3) launch_iteration<T, 3>(S, s); else launch_iteration<T, 2>(S, s);
+    }
+    launched += every;
+    if (cudaMemcpyAsync(&h, S->st, sizeof(DevState), cudaMemcpyDeviceToHost, s) != cudaSuccess) return FM_ERR_CUDA;
+    if (cudaStreamSynchronize(s) != cudaSuccess) return FM_ERR_CUDA;
+    if (h.done || launched >= limit) break;
+  }
+  if (iters) *iters = h.result_it;
+  if (rtr) *rtr = h.rTr;
+  if (h.nonfinite) return FM_ERR_NONFINITE;
+  if (!h.conv) return FM_ERR_NOT_CONVERGED;
+  return FM_OK;
+}
+
+}  // namespace fm
+
+extern "C" int fm_project_noalloc(const fm_grid* g, int dtype, const fm_mg_params* params, void* ux, void* uy,
+                                  void* uz, void* stream, int* iters, double* rtr) {
+  int st = validate_grid(g, dtype);
+  if (st) return st;
+  if (!params || !ux || !uy || (g->dim == 3 && !uz)) return FM_ERR_ARG;
+  const fm_mg_params& P = *params;
+  if (P.levels < 2 || P.levels > kMaxLevels || P.pre_post < 1 || P.bottom < 0 || P.max_iters < 1 ||
+      P.check_every < 0 || (P.bottom_mode != 0 && P.bottom_mode != 1) || P.coarse_bf16)
+    return FM_ERR_ARG;
+  for (int a = 0; a < g->dim; ++a)
+    if (g->n[a] % (1 << (P.levels - 1)) != 0) return FM_ERR_SHAPE;
+  fm_mgpcg S;
+  memset(&S, 0, sizeof(S));
+  S.g = *g;
+  S.dtype = dtype;
+  S.P = P;
+  S.L = P.levels;
+  if (noalloc_layout(*g, dtype, P.levels, &S, nullptr) > kNoAllocScratchBytes) return FM_ERR_CAPACITY;
+  void* base = nullptr;
+  if ((st = noalloc_scratch(&base))) return st;
+  noalloc_layout(*g, dtype, P.levels, &S, (unsigned char*)base);
+  const size_t es = dtype == FM_F32 ? sizeof(float) : sizeof(double);
+  const size_t smem = 2 * es * S.lv[S.L - 1].size();
+  S.bottom_smem = smem <= 48 * 1024 ? smem : 0;  // larger coarsest levels: per-sweep launches
+  cudaStream_t s = (cudaStream_t)stream;
+  // the scratch keeps the previous call's contents: the solver state must start at zero
+  if (cudaMemsetAsync(S.st, 0, sizeof(DevState), s) != cudaSuccess) return FM_ERR_CUDA;
+  long maxf = 0;
+  for (int c = 0; c < g->dim; ++c) maxf = face_shape(*g, c).size() > maxf ? face_shape(*g, c).size() : maxf;
+  dim3 fgrid((unsigned)((maxf + 255) / 256), (unsigned)g->dim, 1);
+  const fm_grid gg = *g;
+  int status;
+  if (dtype == FM_F32) {
+    MacW<float> u{{(float*)ux, (float*)uy, (float*)uz}};
+    if (gg.dim == 3) launch(k_div_bc<float, 3>, kRedBlocks, kRedThreads, 0, s, gg, u, (float*)S.r[0], (float*)S.x, S.part);
+    else launch(k_div_bc<float, 2>, kRedBlocks, kRedThreads, 0, s, gg, u, (float*)S.r[0], (float*)S.x, S.part);
+    status = run_solve_direct<float>(&S, s, iters, rtr);
+    if (status == FM_ERR_CUDA) return status;
+    if (gg.dim == 3) launch(k_subgrad_bc<float, 3>, fgrid, 256, 0, s, gg, (const float*)S.x, u);
+    else launch(k_subgrad_bc<float, 2>, fgrid, 256, 0, s, gg, (const float*)S.x, u);
+  } else {
+    MacW<double> u{{(double*)ux, (double*)uy, (double*)uz}};
+    if (gg.dim == 3) launch(k_div_bc<double, 3>, kRedBlocks, kRedThreads, 0, s, gg, u, (double*)S.r[0], (double*)S.x, S.part);
+    else launch(k_div_bc<double, 2>, kRedBlocks, kRedThreads, 0, s, gg, u, (double*)S.r[0], (double*)S.x, S.part);
+    status = run_solve_direct<double>(&S, s, iters, rtr);
+    if (status == FM_ERR_CUDA) return status;
+    if (gg.dim == 3) launch(k_subgrad_bc<double, 3>, fgrid, 256, 0, s, gg, (const double*)S.x, u);
+    else launch(k_subgrad_bc<double, 2>, fgrid, 256, 0, s, gg, (const double*)S.x, u);
+  }
+  if (check_cuda()) return FM_ERR_CUDA;
+  return status;
+}

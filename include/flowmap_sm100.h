@@ -39,7 +39,8 @@ enum {
     FM_ERR_NONFINITE = 4,      /* NaN/Inf residual in MGPCG */
     FM_ERR_TIMEOUT = 5,        /* a bounded device wait gave up */
     FM_ERR_CUDA = 6,           /* CUDA runtime error (launch/alloc) */
-    FM_ERR_DTYPE = 7           /* dtype not FM_F32/FM_F64 */
+    FM_ERR_DTYPE = 7,          /* dtype not FM_F32/FM_F64 */
+    FM_ERR_CAPACITY = 8        /* grid too large for fm_project_noalloc's static scratch */
 };
 
 int fm_abi_version(void);
@@ -197,6 +198,24 @@ typedef struct {
     double last_rtr;          /* last r.r */
 } fm_mg_stats;
 int fm_mgpcg_stats(fm_mgpcg *solver, void *stream, int reset, fm_mg_stats *out);
+
+/* Allocation-free Poisson(u).  This entry point has no counterpart in the
+ * reference.  It is for callers that cannot allocate device memory: code
+ * running inside another runtime's preallocated pool (Taichi claims its device
+ * memory at ti.init), under a fixed memory budget, or where a cudaMalloc would
+ * synchronise the device at a bad moment.  It does what fm_mgpcg_create +
+ * fm_project + fm_mgpcg_destroy do, with every scratch buffer carved out of
+ * one static 48 MiB array inside the library: FP32 grids up to about 2.4 M
+ * cells (128^3, 1024^2), FP64 up to about 1.2 M.  Larger grids return
+ * FM_ERR_CAPACITY.  It calls no cudaMalloc, cudaFree or allocating library
+ * routine.  The array is one per GPU and shared by all calls: calls that
+ * overlap on the GPU (other streams, other host threads) race and must be
+ * serialised by the caller.  The first call on a device looks the array's
+ * address up (cudaGetSymbolAddress) and should come before any stream capture.
+ * Every call synchronises `stream` to poll convergence (params->check_every
+ * iterations per poll; 0 means 4).  Result and status as fm_project. */
+int fm_project_noalloc(const fm_grid *g, int dtype, const fm_mg_params *params, void *ux, void *uy, void *uz,
+                       void *stream, int *iters, double *rtr);
 
 /* Apply the Neumann Laplacian: Ap = A p (for tests and defect correction). */
 int fm_laplacian(const fm_grid *g, int dtype, const void *p, void *Ap, void *stream);
