@@ -217,8 +217,7 @@ def main():
     ev0.record(stream)
     for _ in range(a.steps):
         loss, grad = sim.gradient(d_u0, d_r0, d_rt)
-        iters.append(list(sim.solver.history))
-        sim.solver.history.clear()
+        iters.append(dict(sim.solver_stats or {}))
     ev1.record(stream)
     torch.cuda.synchronize(dev)
     barrier()
@@ -258,7 +257,9 @@ def main():
     if rank == 0:
         roof = dominant_kernel_roofline(fm, sim, dev, stream)
 
-    flat_iters = [it for run in iters for (it, _) in run]
+    solves = sum(r.get("solves", 0) for r in iters)
+    pcg_iters = sum(r.get("iterations", 0) for r in iters)
+    not_conv = sum(r.get("not_converged", 0) for r in iters)
     line = None
     if rank == 0:
         line = {"metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": a.steps,
@@ -268,8 +269,9 @@ def main():
                            "reinit_every": a.reinit, "rk": 4, "backward_u": backward_u,
                            "store_dtype": "bf16" if store is not None else "f32",
                            "solver": {"levels": sim.solver.n_mg_levels, "rel_tol": cfg.solver.rel_tol,
-                                      "mean_pcg_iters": statistics.mean(flat_iters) if flat_iters else None,
-                                      "solves_per_grad": len(flat_iters) // max(a.steps, 1)},
+                                      "mean_pcg_iters": pcg_iters / solves if solves else None,
+                                      "solves_per_grad": solves // max(a.steps, 1),
+                                      "not_converged": not_conv, "mode": "device (graph WHILE loop)"},
                            "parallelism": f"replicas x{world}" if world > 1 else "single GPU",
                            "l2": "working set and trajectory stores exceed the 126 MB L2; no flush needed"},
                 "e2e": e2e, "gpu_launches": launches, "clocks": clk, "roofline": roof}

@@ -94,6 +94,7 @@ SIGNATURES = {
     "fm_laplacian": [GP, I, P, P, P],
     "fm_mgpcg_stats": [P, P, I, C.POINTER(MGStats)],
     "fm_project_noalloc": [GP, I, C.POINTER(MGParams), P, P, P, P, C.POINTER(I), C.POINTER(D)],
+    "fm_convert": [L, I, P, I, P, P],
 }
 RESTYPES = {"fm_launch_count": C.c_longlong}
 SIGNATURES["fm_launch_count"] = [I]
@@ -132,11 +133,17 @@ def check(status: int, where: str):
         raise FlowmapError(status, where)
 
 
-def dtype_code(t: torch.dtype) -> int:
+FM_BF16 = 2
+
+
+def dtype_code(t: torch.dtype, storage: bool = False) -> int:
+    """FM_F32/FM_F64 for compute entry points; FM_BF16 too for storage (fm_convert)."""
     if t == torch.float32:
         return FM_F32
     if t == torch.float64:
         return FM_F64
+    if storage and t == torch.bfloat16:
+        return FM_BF16
     raise FlowmapError(7, f"dtype {t}")
 
 

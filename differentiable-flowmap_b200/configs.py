@@ -37,7 +37,7 @@ def smooth_ball(res, center, radius, dx):
 
 
 def shape3d_config(res=128, steps=150, reinit_every=8, rk=4, dtype=torch.float32, store_dtype=None,
-                   backward_u=True, rel_tol=1e-6, abs_tol=0.0, max_iters=400, check_every=4):
+                   backward_u=True, rel_tol=1e-6, abs_tol=0.0, max_iters=400, check_every=0):
     """3D smoke shape transition, 128^3: 150 steps, reinit every 8, RK4,
     dt = 0.0085 (3D/hyperparameters.py:268-295 with the stated overrides)."""
     n = int(math.log2(res))
@@ -66,7 +66,7 @@ def shape3d_inputs(res=128, seed_target=20, seed_u=21, u_std=0.01):
 
 
 def shape2d_config(res=256, steps=200, reinit_every=12, rk=2, dt=0.01, dtype=torch.float32, store_dtype=None,
-                   backward_u=True, rel_tol=1e-6, abs_tol=0.0, max_iters=400, check_every=4):
+                   backward_u=True, rel_tol=1e-6, abs_tol=0.0, max_iters=400, check_every=0):
     """2D smoke shape transition, 256^2, 200 steps, reinit every 12, RK2, MGPCG 5 levels."""
     solver = SolverConfig(base_level=4, levels=int(math.log2(res)) - 4 + 1, bottom=20, bottom_mode=1,
                           max_iters=max_iters, abs_tol=abs_tol, rel_tol=rel_tol,

@@ -10,6 +10,7 @@
 //   reset_to_identity, add_fields
 #include "fm_common.cuh"
 #include "fm_internal.h"
+#include "fm_q2.cuh"
 
 namespace fm {
 
@@ -22,25 +23,28 @@ constexpr int kThreads = 256;
 
 // Midpoint (RK2) / RK4 backtrace from X through u0 (3D/flowmap.py:210-219, :257-262).
 template <typename T, int D, int RK>
-__device__ __forceinline__ void backtrace(const Mac<T>& u0, const fm_grid& g, const T* X, T dx, T dt, T* p) {
-  T v1[3], v2[3], q[3] = {0, 0, 0};
-  interp_mac_val<T, D>(u0, g, X, dx, v1);
+__device__ __forceinline__ void backtrace(const Mac<T>& u0, const fm_grid& g, const T* X, T inv_dx, T dt, T* p) {
+  T v[3], vs[3], q[3] = {0, 0, 0};
+  q2_mac_val<T, D>(u0, g, X, inv_dx, v);
 #pragma unroll
-  for (int a = 0; a < D; ++a) q[a] = X[a] - v1[a] * dt * (T)0.5;
-  interp_mac_val<T, D>(u0, g, q, dx, v2);
+  for (int a = 0; a < D; ++a) q[a] = X[a] - v[a] * dt * (T)0.5;
   if constexpr (RK == 2) {
+    q2_mac_val<T, D>(u0, g, q, inv_dx, v);
 #pragma unroll
-    for (int a = 0; a < D; ++a) p[a] = X[a] - v2[a] * dt;
+    for (int a = 0; a < D; ++a) p[a] = X[a] - v[a] * dt;
   } else {
-    T v3[3], v4[3];
+    // v1 + 2 v2 + 2 v3 + v4 accumulated left to right as the stages complete
 #pragma unroll
-    for (int a = 0; a < D; ++a) q[a] = X[a] - v2[a] * dt * (T)0.5;
-    interp_mac_val<T, D>(u0, g, q, dx, v3);
+    for (int a = 0; a < D; ++a) vs[a] = v[a];
+    q2_mac_val<T, D>(u0, g, q, inv_dx, v);
 #pragma unroll
-    for (int a = 0; a < D; ++a) q[a] = X[a] - v3[a] * dt;
-    interp_mac_val<T, D>(u0, g, q, dx, v4);
+    for (int a = 0; a < D; ++a) { vs[a] = vs[a] + (T)2 * v[a]; q[a] = X[a] - v[a] * dt * (T)0.5; }
+    q2_mac_val<T, D>(u0, g, q, inv_dx, v);
 #pragma unroll
-    for (int a = 0; a < D; ++a) p[a] = X[a] - (v1[a] + (T)2 * v2[a] + (T)2 * v3[a] + v4[a]) / (T)6.0 * dt;
+    for (int a = 0; a < D; ++a) { vs[a] = vs[a] + (T)2 * v[a]; q[a] = X[a] - v[a] * dt; }
+    q2_mac_val<T, D>(u0, g, q, inv_dx, v);
+#pragma unroll
+    for (int a = 0; a < D; ++a) p[a] = X[a] - (vs[a] + v[a]) / (T)6.0 * dt;
   }
 }
 
@@ -55,8 +59,9 @@ __global__ void __launch_bounds__(kThreads) k_advect_u_grid(fm_grid g, T dx, T d
   unflatten(s, q, i, j, k);
   T X[3] = {0, 0, 0}, p[3] = {0, 0, 0};
   node_pos<T, D>(c, i, j, k, dx, X);
-  backtrace<T, D, RK>(u0, g, X, dx, dt, p);
-  pick(u2, c)[q] = interp_mac_comp<T, D>(u1, g, c, p, dx);
+  const T inv_dx = (T)1 / dx;
+  backtrace<T, D, RK>(u0, g, X, inv_dx, dt, p);
+  pick(u2, c)[q] = q2_mac_comp<T, D>(u1, g, c, p, inv_dx);
 }
 
 template <typename T, int D, int RK>
@@ -69,8 +74,9 @@ __global__ void __launch_bounds__(kThreads) k_advect_scalar_grid(fm_grid g, T dx
   unflatten(s, q, i, j, k);
   T X[3] = {0, 0, 0}, p[3] = {0, 0, 0};
   node_pos<T, D>(-1, i, j, k, dx, X);
-  backtrace<T, D, RK>(u0, g, X, dx, dt, p);
-  s2[q] = interp_val<T, D, 2>(s1, s, p, dx, (T)0.5, (T)0.5, (T)0.5);
+  const T inv_dx = (T)1 / dx;
+  backtrace<T, D, RK>(u0, g, X, inv_dx, dt, p);
+  s2[q] = q2_scalar<T, D>(s1, g, p, inv_dx);
 }
 
 // One march job: a flow map psi (D planes) on grid `face` (-1 = centre),
@@ -88,10 +94,10 @@ struct MarchJobs {
 
 // One RK stage: velocity k = u(pos) and, with the Jacobian, d = (grad u)(pos) . t.
 template <typename T, int D, bool WT>
-__device__ __forceinline__ void march_eval(const Mac<T>& u, const fm_grid& g, const T* pos, const T* t, T dx, T* k,
-                                           T* d) {
-  if constexpr (WT) interp_mac_grad_dot<T, D>(u, g, pos, dx, t, k, d);
-  else interp_mac_val<T, D>(u, g, pos, dx, k);
+__device__ __forceinline__ void march_eval(const Mac<T>& u, const fm_grid& g, const T* pos, const T* t, T inv_dx,
+                                           T* k, T* d) {
+  if constexpr (WT) q2_mac_grad_dot<T, D>(u, g, pos, inv_dx, t, k, d);
+  else q2_mac_val<T, D>(u, g, pos, inv_dx, k);
 }
 
 // RK2_grid / RK4_grid (WT) and RK*_grid_only_psi (!WT) for one node, in place.
@@ -108,12 +114,13 @@ __device__ __forceinline__ void march_node(const Mac<T>& u, const fm_grid& g, T 
   }
   const T neg_dt = -dt;
   const T h = (T)0.5 * neg_dt;
+  const T inv_dx = (T)1 / dx;
   T k[3], d[3] = {0, 0, 0}, pos[3] = {0, 0, 0}, tt[3] = {0, 0, 0};
-  march_eval<T, D, WT>(u, g, P, Tv, dx, k, d);
+  march_eval<T, D, WT>(u, g, P, Tv, inv_dx, k, d);
   if constexpr (RK == 2) {
 #pragma unroll
     for (int a = 0; a < D; ++a) { pos[a] = P[a] + h * k[a]; tt[a] = Tv[a] + h * d[a]; }
-    march_eval<T, D, WT>(u, g, pos, tt, dx, k, d);
+    march_eval<T, D, WT>(u, g, pos, tt, inv_dx, k, d);
 #pragma unroll
     for (int a = 0; a < D; ++a) {
       psi[a * N + q] = P[a] + neg_dt * k[a];
@@ -128,7 +135,7 @@ __device__ __forceinline__ void march_node(const Mac<T>& u, const fm_grid& g, T 
       pos[a] = P[a] + h * k[a];
       tt[a] = Tv[a] + h * d[a];
     }
-    march_eval<T, D, WT>(u, g, pos, tt, dx, k, d);  // stage 2
+    march_eval<T, D, WT>(u, g, pos, tt, inv_dx, k, d);  // stage 2
 #pragma unroll
     for (int a = 0; a < D; ++a) {
       ks[a] = ks[a] + (T)2 * k[a];
@@ -136,7 +143,7 @@ __device__ __forceinline__ void march_node(const Mac<T>& u, const fm_grid& g, T 
       pos[a] = P[a] + h * k[a];
       tt[a] = Tv[a] + h * d[a];
     }
-    march_eval<T, D, WT>(u, g, pos, tt, dx, k, d);  // stage 3
+    march_eval<T, D, WT>(u, g, pos, tt, inv_dx, k, d);  // stage 3
 #pragma unroll
     for (int a = 0; a < D; ++a) {
       ks[a] = ks[a] + (T)2 * k[a];
@@ -144,7 +151,7 @@ __device__ __forceinline__ void march_node(const Mac<T>& u, const fm_grid& g, T 
       pos[a] = P[a] + (T)1.0 * neg_dt * k[a];
       tt[a] = Tv[a] + (T)1.0 * neg_dt * d[a];
     }
-    march_eval<T, D, WT>(u, g, pos, tt, dx, k, d);  // stage 4
+    march_eval<T, D, WT>(u, g, pos, tt, inv_dx, k, d);  // stage 4
     const T c6 = neg_dt * (T)1 / (T)6;
 #pragma unroll
     for (int a = 0; a < D; ++a) {
@@ -186,7 +193,7 @@ __global__ void __launch_bounds__(kThreads) k_pullback_u(fm_grid g, T dx, Mac<T>
   T p[3] = {0, 0, 0}, v[3];
 #pragma unroll
   for (int a = 0; a < D; ++a) p[a] = psi_c[a * N + q];
-  interp_mac_val<T, D>(u0, g, p, dx, v);
+  q2_mac_val<T, D>(u0, g, p, (T)1 / dx, v);
   T acc = 0;
 #pragma unroll
   for (int a = 0; a < D; ++a) acc += T_c[a * N + q] * v[a];
@@ -205,7 +212,7 @@ __global__ void __launch_bounds__(kThreads) k_pullback_scalar(fm_grid g, T dx, c
   T p[3] = {0, 0, 0};
 #pragma unroll
   for (int a = 0; a < D; ++a) p[a] = psi[a * N + q];
-  T acc = interp_val<T, D, 2>(s0, s, p, dx, (T)0.5, (T)0.5, (T)0.5);
+  T acc = q2_scalar<T, D>(s0, g, p, (T)1 / dx);
   if (beta != (T)0) acc = acc + beta * base[q];
   out[q] = alpha * acc;
 }
@@ -223,7 +230,7 @@ __global__ void __launch_bounds__(kThreads) k_accumulate(fm_grid g, T dx, T dt, 
   T p[3] = {0, 0, 0}, v[3];
 #pragma unroll
   for (int a = 0; a < D; ++a) p[a] = phi_c[a * N + q];
-  interp_mac_val<T, D>(f, g, p, dx, v);
+  q2_mac_val<T, D>(f, g, p, (T)1 / dx, v);
   T Fv = 0, Fv23 = 0, Fv16 = 0;
 #pragma unroll
   for (int a = 0; a < D; ++a) {

@@ -162,5 +162,21 @@ def add_fields(f1, f2, dest, m: float, stream=None):
           "fm_add_fields")
 
 
+def convert(src, dst, stream=None):
+    """dst = src with a dtype change (FP32/FP64/BF16), elementwise."""
+    if src.numel() != dst.numel():
+        raise _lib.FlowmapError(1, "convert size mismatch")
+    check(_lib.lib().fm_convert(src.numel(), dtype_code(src.dtype, True), ptr(src), dtype_code(dst.dtype, True),
+                                ptr(dst), stream_ptr(stream)), "fm_convert")
+
+
+def store(src, dst, stream=None):
+    """Copy into a trajectory store slot: device memcpy when dtypes match, else fm_convert."""
+    if src.dtype == dst.dtype:
+        dst.copy_(src)
+    else:
+        convert(src, dst, stream)
+
+
 def laplacian(g: GridSpec, p, Ap, stream=None):
     check(_lib.lib().fm_laplacian(C.byref(g.c_grid()), _dt(p), ptr(p), ptr(Ap), stream_ptr(stream)), "fm_laplacian")

@@ -185,7 +185,9 @@ class LFM_Simulator:
         self.store_F_f = [torch.zeros((n_int, self.dim) + g.face_shape(c), dtype=wd, device=dev)
                           for c in range(self.dim)]
         need_passive = self.cfg.add_passive_scalar and (not self.cfg.backward_u or self.cfg.trajectory_loss)
-        self.store_passive = (torch.zeros((steps + 1,) + g.shape, dtype=sd, device=dev) if need_passive else None)
+        # the passive scalar feeds the adjoint source (nabla_scalar_adjoint) directly: stored in BF16 it
+        # raised the 64^3 gradient error from 4e-5 to 1.8e-4, so it stays in the working dtype
+        self.store_passive = (torch.zeros((steps + 1,) + g.shape, dtype=wd, device=dev) if need_passive else None)
         # in-interval midpoint velocities replayed by backtrack_psi_grid, in the working dtype
         if sd == self.cfg.dtype:
             self._ring = None
@@ -271,10 +273,10 @@ class LFM_Simulator:
             raise FlowmapError(2, f"step {n} beyond total_steps={self.total_steps}")
         j = n % self.reinit_every
         if self.store_passive is not None:
-            self.store_passive[n].copy_(self.passive)
+            K.store(self.passive, self.store_passive[n])
         self.step_flow_map(j, self.dt)
         if self.final_condition() and self.store_passive is not None:
-            self.store_passive[n + 1].copy_(self.passive)
+            K.store(self.passive, self.store_passive[n + 1])
         return False, self.final_condition()
 
     def march_phi_grid(self, u):
@@ -303,7 +305,7 @@ class LFM_Simulator:
         self.project(self.u)
         # write_velocity + RW_Cache("u"): the midpoint velocity of step n
         for c in range(self.dim):
-            self.store_mid[c][n].copy_(self.u[c])
+            K.store(self.u[c], self.store_mid[c][n])
             if self._ring is not None:
                 self._ring[j][c].copy_(self.u[c])
         self.march_phi_grid(self.u)
@@ -407,7 +409,7 @@ class LFM_Diff_Simulator(LFM_Simulator):
         n = self.step_num[None]
         j = n % self.reinit_every
         if self.cfg.add_passive_scalar and not self.cfg.backward_u:
-            self.passive.copy_(self.store_passive[n + 1])
+            K.store(self.store_passive[n + 1], self.passive)
         self.backtrack_flow_map(j, self.dt)
         return False, n == 0
 
@@ -417,7 +419,7 @@ class LFM_Diff_Simulator(LFM_Simulator):
         cfg, g, dx = self.cfg, self.grid, self.dx
         n = self.step_num[None]
         for c in range(self.dim):
-            self.mid_u[c].copy_(self.store_mid[c][n])
+            K.store(self.store_mid[c][n], self.mid_u[c])
         K.nabla_u_w(g, dx, self.u if cfg.backward_u else self.mid_u, self.adj_u, self.src)
         if cfg.add_passive_scalar:
             K.nabla_scalar_adjoint(g, dx, self.passive, self.adj_passive, self.adj_passive_f)
@@ -466,7 +468,7 @@ class LFM_Diff_Simulator(LFM_Simulator):
                 _copy_mac(self.init_u, self.u)
             if cfg.add_passive_scalar:
                 if cfg.trajectory_loss or not cfg.backward_u:
-                    self.passive.copy_(self.store_passive[n])
+                    K.store(self.store_passive[n], self.passive)
                 else:
                     self.BFECC_scalar(self.init_passive, self.passive, self.err_passive, self.phi, self.psi)
                 self.init_passive.copy_(self.passive)
@@ -492,4 +494,8 @@ class LFM_Diff_Simulator(LFM_Simulator):
             _, done = self.backtrack_step_midpoint()
             if done:
                 break
+        # device-mode solves report once per gradient (one stream sync)
+        self.solver_stats = self.solver.stats(reset=True) if self.solver.device_mode else None
+        if self.solver_stats and self.solver_stats["nonfinite"]:
+            raise FlowmapError(4, f"{self.solver_stats['nonfinite']} projection(s) hit a non-finite residual")
         return self.loss, [x.clone() for x in self.adj_u]

@@ -29,7 +29,7 @@ typedef struct {
     int n[3];  /* cell counts; n[2] == 1 when dim == 2 */
 } fm_grid;
 
-enum { FM_F32 = 0, FM_F64 = 1 };
+enum { FM_F32 = 0, FM_F64 = 1, FM_BF16 = 2 /* storage only: fm_convert */ };
 
 enum {
     FM_OK = 0,
@@ -139,6 +139,13 @@ int fm_reset_to_identity(const fm_grid *g, int dtype, double dx, void *psi_c,
 /* add_fields: dest = f1 + m * f2 over n elements (3D/taichi_utils.py:86-89).
  * dest may alias f1 or f2. */
 int fm_add_fields(int dtype, long n, const void *f1, const void *f2, void *dest, double m, void *stream);
+
+/* Elementwise conversion between FM_F32 / FM_F64 / FM_BF16 (round to nearest
+ * even) for the trajectory stores that replace RW_Cache
+ * (3D/lfm_midpoint_simulator.py:46-165): the mixed-precision form stores each
+ * step's midpoint velocity and passive scalar in BF16.  src and dst must not
+ * overlap. */
+int fm_convert(long n, int src_dtype, const void *src, int dst_dtype, void *dst, void *stream);
 
 /* ------------------------------------------------------------------------
  * MGPCG pressure projection.  Replaces MGPCG_3 / MGPCG_2 / MGPCG_2_solid
