@@ -38,13 +38,30 @@ def parse():
     ap.add_argument("--steps", type=int, default=3)
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
-    ap.add_argument("--form", default="plain", choices=["plain", "mixed"])
+    ap.add_argument("--form", default="both", choices=["plain", "mixed", "both"])
+    ap.add_argument("--no-error", action="store_true", help="skip the FP64 reference runs")
+    ap.add_argument("--solver-check-every", type=int, default=0,
+                    help="0: device-side PCG loop (CUDA-graph WHILE node); k: host polls every k iterations "
+                         "(kernel-level profilers cannot see inside the WHILE node)")
     ap.add_argument("--res", type=int, default=128)
     ap.add_argument("--sim-steps", type=int, default=150)
     ap.add_argument("--reinit", type=int, default=8)
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-e2e", action="store_true")
     return ap.parse_args()
+
+
+def form_config(C, a, form, dtype):
+    """plain: the reference's FP32 drop-in (backward_u=True: the adjoint re-advects
+    u backwards and re-projects it); mixed: the checkpointed form (backward_u=False:
+    the adjoint reads the stored trajectory; midpoint velocities in BF16, passive
+    in FP32), FP64 reductions."""
+    import torch
+
+    mixed = form == "mixed"
+    store = torch.bfloat16 if (mixed and dtype == torch.float32) else None
+    return C.shape3d_config(res=a.res, steps=a.sim_steps, reinit_every=a.reinit, rk=4, dtype=dtype,
+                            store_dtype=store, backward_u=not mixed, check_every=a.solver_check_every)
 
 
 def workload_name(a):
@@ -177,11 +194,15 @@ def main():
     S = importlib.import_module("differentiable-flowmap_b200.simulator")
     lib = fm._lib
 
-    store = torch.bfloat16 if a.form == "mixed" else None
-    backward_u = a.form != "mixed"
-    cfg = C.shape3d_config(res=a.res, steps=a.sim_steps, reinit_every=a.reinit, rk=4, store_dtype=store,
-                           backward_u=backward_u)
-    sim = S.LFM_Diff_Simulator(config=cfg, device=dev)
+    forms = ["plain", "mixed"] if a.form == "both" else [a.form]
+    head = forms[-1]
+    sims, cfgs = {}, {}
+    for f in forms:
+        cfgs[f] = form_config(C, a, f, torch.float32)
+        sims[f] = S.LFM_Diff_Simulator(config=cfgs[f], device=dev)
+    sim, cfg = sims[head], cfgs[head]
+    store = cfg.store_dtype
+    backward_u = cfg.backward_u
     u0, rho0, rho_t = C.shape3d_inputs(a.res)
     f32 = torch.float32
     d_u0 = [torch.tensor(x, dtype=f32, device=dev) for x in u0]
@@ -197,38 +218,45 @@ def main():
         if world > 1:
             dist.barrier()
 
-    for _ in range(a.warmup):
-        sim.gradient(d_u0, d_r0, d_rt)
-    torch.cuda.synchronize(dev)
-    barrier()
-
     uuid = None
     try:
         uuid = "GPU-" + str(torch.cuda.get_device_properties(dev).uuid)
     except Exception:
         pass
     clocks = ClockSampler(uuid)
-    clocks.start()
-    iters = []
-    lib.launch_count(reset=True)
-    torch.cuda.synchronize(dev)
-    barrier()
     ev0, ev1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
-    ev0.record(stream)
-    for _ in range(a.steps):
-        loss, grad = sim.gradient(d_u0, d_r0, d_rt)
-        iters.append(dict(sim.solver_stats or {}))
-    ev1.record(stream)
-    torch.cuda.synchronize(dev)
-    barrier()
-    launches = lib.launch_count(reset=True)
+    results = {}
+    for f in forms:  # the headline form last
+        s_ = sims[f]
+        for _ in range(a.warmup):
+            s_.gradient(d_u0, d_r0, d_rt)
+        torch.cuda.synchronize(dev)
+        barrier()
+        if f == forms[0]:
+            clocks.start()
+        iters = []
+        lib.launch_count(reset=True)
+        torch.cuda.synchronize(dev)
+        barrier()
+        ev0.record(stream)
+        for _ in range(a.steps):
+            loss, grad = s_.gradient(d_u0, d_r0, d_rt)
+            iters.append(dict(s_.solver_stats or {}))
+        ev1.record(stream)
+        torch.cuda.synchronize(dev)
+        barrier()
+        launches = lib.launch_count(reset=True)
+        t = torch.tensor([ev0.elapsed_time(ev1)], dtype=torch.float64, device=dev)
+        if world > 1:
+            dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        ms_max = float(t.item())
+        results[f] = {"value": world * a.steps / (ms_max / 1e3), "ms_per_step": ms_max / a.steps,
+                      "launches": launches, "iters": iters, "loss": float(loss), "grad": grad}
     clk = clocks.stop()
-    ms = ev0.elapsed_time(ev1)
-    t = torch.tensor([ms], dtype=torch.float64, device=dev)
-    if world > 1:
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-    ms_max = float(t.item())
-    value = world * a.steps / (ms_max / 1e3)
+    value = results[head]["value"]
+    ms_max = results[head]["ms_per_step"] * a.steps
+    launches = results[head]["launches"]
+    iters = results[head]["iters"]
 
     # end-to-end through the public API with host buffers
     e2e = None
@@ -257,6 +285,19 @@ def main():
     if rank == 0:
         roof = dominant_kernel_roofline(fm, sim, dev, stream)
 
+    # gradient error of each form against an FP64 run of the same algorithm
+    errors = {}
+    if rank == 0 and not a.no_error:
+        for f in forms:
+            s64 = S.LFM_Diff_Simulator(config=form_config(C, a, f, torch.float64), device=dev)
+            l64, g64 = s64.gradient([x.double() for x in d_u0], d_r0.double(), d_rt.double())
+            g32 = results[f]["grad"]
+            num = sum(float(((x.double() - y) ** 2).sum()) for x, y in zip(g32, g64))
+            den = sum(float((y ** 2).sum()) for y in g64)
+            errors[f] = {"grad_rel_l2": (num / den) ** 0.5, "loss_rel": abs(results[f]["loss"] - l64) / abs(l64)}
+            del s64, g64
+            torch.cuda.empty_cache()
+
     solves = sum(r.get("solves", 0) for r in iters)
     pcg_iters = sum(r.get("iterations", 0) for r in iters)
     not_conv = sum(r.get("not_converged", 0) for r in iters)
@@ -265,7 +306,8 @@ def main():
         line = {"metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": a.steps,
                 "warmup": a.warmup, "ms_per_step": ms_max / a.steps, "higher_is_better": True, "scaling": "weak",
                 "vs_baseline": None, "dtype": "f32", "data": "synthetic",
-                "config": {"workload": workload_name(a), "form": a.form, "res": a.res, "sim_steps": a.sim_steps,
+                "config": {"workload": workload_name(a), "form": head, "value_form": head,
+                           "res": a.res, "sim_steps": a.sim_steps,
                            "reinit_every": a.reinit, "rk": 4, "backward_u": backward_u,
                            "store_dtype": "bf16" if store is not None else "f32",
                            "solver": {"levels": sim.solver.n_mg_levels, "rel_tol": cfg.solver.rel_tol,
@@ -274,7 +316,13 @@ def main():
                                       "not_converged": not_conv, "mode": "device (graph WHILE loop)"},
                            "parallelism": f"replicas x{world}" if world > 1 else "single GPU",
                            "l2": "working set and trajectory stores exceed the 126 MB L2; no flush needed"},
-                "e2e": e2e, "gpu_launches": launches, "clocks": clk, "roofline": roof}
+                "e2e": e2e, "gpu_launches": launches, "clocks": clk, "roofline": roof,
+                "forms": {f: {"value": r["value"], "ms_per_step": r["ms_per_step"], "gpu_launches": r["launches"],
+                              "backward_u": cfgs[f].backward_u,
+                              "velocity_store": "bf16" if cfgs[f].store_dtype == torch.bfloat16 else "f32",
+                              "grad_error_vs_fp64": errors.get(f)} for f, r in results.items()}}
+        if "plain" in results and "mixed" in results:
+            line["mixed_over_plain"] = results["mixed"]["value"] / results["plain"]["value"]
         if world == 1 and not a.no_cpu_baseline:
             secs, threads = cpu_sample(a)
             line["cpu_baseline"] = {

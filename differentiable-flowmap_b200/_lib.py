@@ -95,6 +95,8 @@ SIGNATURES = {
     "fm_mgpcg_stats": [P, P, I, C.POINTER(MGStats)],
     "fm_project_noalloc": [GP, I, C.POINTER(MGParams), P, P, P, P, C.POINTER(I), C.POINTER(D)],
     "fm_convert": [L, I, P, I, P, P],
+    "fm_advect_u_grid_pair": [GP, I, I, D, D] + [P] * 15 + [P],
+    "fm_advect_scalar_grid_pair": [GP, I, I, D, D] + [P] * 7 + [P],
 }
 RESTYPES = {"fm_launch_count": C.c_longlong}
 SIGNATURES["fm_launch_count"] = [I]

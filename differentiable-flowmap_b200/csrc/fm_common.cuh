@@ -37,11 +37,15 @@ __host__ __device__ __forceinline__ int axis_len(const Shape& s, int a) {
   return a == 0 ? s.s0 : (a == 1 ? s.s1 : s.s2);
 }
 
+// Flat index -> (i, j, k).  Grids stay below 2^32 entries (validate_grid), so
+// 32-bit unsigned division suffices; 64-bit division would cost ~5x more.
 __device__ __forceinline__ void unflatten(const Shape& s, long q, int& i, int& j, int& k) {
-  k = (int)(q % s.s2);
-  long r = q / s.s2;
-  j = (int)(r % s.s1);
-  i = (int)(r / s.s1);
+  const unsigned uq = (unsigned)q;
+  const unsigned r = uq / (unsigned)s.s2;
+  k = (int)(uq - r * (unsigned)s.s2);
+  const unsigned ii = r / (unsigned)s.s1;
+  j = (int)(r - ii * (unsigned)s.s1);
+  i = (int)ii;
 }
 
 // Node coordinates: center (I+0.5)*dx; face c: axis c at i*dx, others

@@ -48,9 +48,12 @@ __device__ __forceinline__ void backtrace(const Mac<T>& u0, const fm_grid& g, co
   }
 }
 
+// u2 = u1 sampled at the foot of the backtrace through u0; with u1b/u2b set,
+// a second field is sampled at the same foot (the adjoint advects adj_u and u
+// along the same midpoint velocity, 3D/lfm_midpoint_diff_simulator.py:488-499).
 template <typename T, int D, int RK>
 __global__ void __launch_bounds__(kThreads) k_advect_u_grid(fm_grid g, T dx, T dt, Mac<T> u0, Mac<T> u1,
-                                                            MacW<T> u2) {
+                                                            MacW<T> u2, Mac<T> u1b, MacW<T> u2b) {
   const int c = blockIdx.y;
   const Shape s = face_shape(g, c);
   const long q = (long)blockIdx.x * blockDim.x + threadIdx.x;
@@ -61,12 +64,16 @@ __global__ void __launch_bounds__(kThreads) k_advect_u_grid(fm_grid g, T dx, T d
   node_pos<T, D>(c, i, j, k, dx, X);
   const T inv_dx = (T)1 / dx;
   backtrace<T, D, RK>(u0, g, X, inv_dx, dt, p);
-  pick(u2, c)[q] = q2_mac_comp<T, D>(u1, g, c, p, inv_dx);
+  CompStencil<T, D> st;
+  st.setup(g, c, p, inv_dx);
+  pick(u2, c)[q] = st.eval(pick(u1, c), s);
+  if (u1b.c[0] != nullptr) pick(u2b, c)[q] = st.eval(pick(u1b, c), s);
 }
 
 template <typename T, int D, int RK>
 __global__ void __launch_bounds__(kThreads) k_advect_scalar_grid(fm_grid g, T dx, T dt, Mac<T> u0,
-                                                                 const T* __restrict__ s1, T* __restrict__ s2) {
+                                                                 const T* __restrict__ s1, T* __restrict__ s2,
+                                                                 const T* __restrict__ s1b, T* __restrict__ s2b) {
   const Shape s = cell_shape(g);
   const long q = (long)blockIdx.x * blockDim.x + threadIdx.x;
   if (q >= s.size()) return;
@@ -76,7 +83,12 @@ __global__ void __launch_bounds__(kThreads) k_advect_scalar_grid(fm_grid g, T dx
   node_pos<T, D>(-1, i, j, k, dx, X);
   const T inv_dx = (T)1 / dx;
   backtrace<T, D, RK>(u0, g, X, inv_dx, dt, p);
-  s2[q] = q2_scalar<T, D>(s1, g, p, inv_dx);
+  Q2<T, false> ax, ay, az;
+  ax.setup(p[0] * inv_dx, (T)0.5, g.n[0]);
+  ay.setup(p[1] * inv_dx, (T)0.5, g.n[1]);
+  if (D == 3) az.setup(p[2] * inv_dx, (T)0.5, g.n[2]);
+  s2[q] = q2_val<T, D, false>(s1, s, ax, ay, az);
+  if (s1b != nullptr) s2b[q] = q2_val<T, D, false>(s1b, s, ax, ay, az);
 }
 
 // One march job: a flow map psi (D planes) on grid `face` (-1 = centre),
@@ -255,46 +267,6 @@ __global__ void __launch_bounds__(kThreads) k_accumulate(fm_grid g, T dx, T dt, 
   init_c[q] = acc;
 }
 
-template <typename T, int D, int ORDER>
-__global__ void __launch_bounds__(kThreads) k_nabla_u_w(fm_grid g, T dx, Mac<T> u, Mac<T> w, MacW<T> r) {
-  const int c = blockIdx.y;
-  const Shape s = face_shape(g, c);
-  const long q = (long)blockIdx.x * blockDim.x + threadIdx.x;
-  if (q >= s.size()) return;
-  int i, j, k;
-  unflatten(s, q, i, j, k);
-  T X[3] = {0, 0, 0};
-  node_pos<T, D>(c, i, j, k, dx, X);
-  T acc = 0;
-#pragma unroll
-  for (int a = 0; a < D; ++a) {
-    const Shape sa = face_shape(g, a);
-    const T b0 = a == 0 ? (T)0 : (T)0.5, b1 = a == 1 ? (T)0 : (T)0.5, b2 = a == 2 ? (T)0 : (T)0.5;
-    T gr[3], wv;
-    interp_grad_val2<T, D, ORDER>(u.c[a], w.c[a], sa, X, dx, b0, b1, b2, gr, wv);
-    acc += pick3(gr[0], gr[1], gr[2], c) * wv;
-  }
-  pick(r, c)[q] = acc;
-}
-
-template <typename T, int D>
-__global__ void __launch_bounds__(kThreads) k_nabla_scalar_adj(fm_grid g, T dx, const T* __restrict__ sc,
-                                                               const T* __restrict__ adj, MacW<T> r) {
-  const int c = blockIdx.y;
-  const Shape s = face_shape(g, c);
-  const long q = (long)blockIdx.x * blockDim.x + threadIdx.x;
-  if (q >= s.size()) return;
-  int i, j, k;
-  unflatten(s, q, i, j, k);
-  T X[3] = {0, 0, 0};
-  node_pos<T, D>(c, i, j, k, dx, X);
-  const Shape cs = cell_shape(g);
-  T v, gr[3];
-  interp_grad<T, D, 3>(sc, cs, X, dx, (T)0.5, (T)0.5, (T)0.5, v, gr);
-  const T av = interp_val<T, D, 3>(adj, cs, X, dx, (T)0.5, (T)0.5, (T)0.5);
-  pick(r, c)[q] = pick3(gr[0], gr[1], gr[2], c) * av;
-}
-
 template <typename T, int D>
 __global__ void k_reset_identity(fm_grid g, T dx, MarchJobs<T> jobs) {
   const MarchJob<T> job = pick_job(jobs, blockIdx.y);
@@ -356,19 +328,22 @@ static inline bool mac_ok(const fm_grid& g, const void* x, const void* y, const 
 
 template <typename T>
 static int advect_u_grid_t(const fm_grid& g, int rk, double dx, double dt, Mac<T> u0, Mac<T> u1, MacW<T> u2,
-                           cudaStream_t st) {
+                           Mac<T> u1b, MacW<T> u2b, cudaStream_t st) {
   dim3 grid = grid_for(max_face(g), g.dim);
-  FM_DISPATCH_D(g, if (rk == 2) k_advect_u_grid<T, D, 2><<<grid, kThreads, 0, st>>>(g, (T)dx, (T)dt, u0, u1, u2);
-                else k_advect_u_grid<T, D, 4><<<grid, kThreads, 0, st>>>(g, (T)dx, (T)dt, u0, u1, u2));
+  FM_DISPATCH_D(g, if (rk == 2) k_advect_u_grid<T, D, 2><<<grid, kThreads, 0, st>>>(g, (T)dx, (T)dt, u0, u1, u2,
+                                                                                     u1b, u2b);
+                else k_advect_u_grid<T, D, 4><<<grid, kThreads, 0, st>>>(g, (T)dx, (T)dt, u0, u1, u2, u1b, u2b));
   return check_launch();
 }
 
 template <typename T>
 static int advect_scalar_grid_t(const fm_grid& g, int rk, double dx, double dt, Mac<T> u0, const T* s1, T* s2,
-                                cudaStream_t st) {
+                                const T* s1b, T* s2b, cudaStream_t st) {
   dim3 grid = grid_for(cell_shape(g).size(), 1);
-  FM_DISPATCH_D(g, if (rk == 2) k_advect_scalar_grid<T, D, 2><<<grid, kThreads, 0, st>>>(g, (T)dx, (T)dt, u0, s1, s2);
-                else k_advect_scalar_grid<T, D, 4><<<grid, kThreads, 0, st>>>(g, (T)dx, (T)dt, u0, s1, s2));
+  FM_DISPATCH_D(g, if (rk == 2) k_advect_scalar_grid<T, D, 2><<<grid, kThreads, 0, st>>>(g, (T)dx, (T)dt, u0, s1,
+                                                                                         s2, s1b, s2b);
+                else k_advect_scalar_grid<T, D, 4><<<grid, kThreads, 0, st>>>(g, (T)dx, (T)dt, u0, s1, s2, s1b,
+                                                                              s2b));
   return check_launch();
 }
 
@@ -404,21 +379,47 @@ int fm_advect_u_grid(const fm_grid* g, int dtype, int rk, double dx, double dt, 
     return FM_ERR_ARG;
   if (dtype == FM_F32)
     return advect_u_grid_t<float>(*g, rk, dx, dt, mac<float>(u0x, u0y, u0z), mac<float>(u1x, u1y, u1z),
-                                  macw<float>(u2x, u2y, u2z), FM_STREAM(stream));
+                                  macw<float>(u2x, u2y, u2z), mac<float>(nullptr, nullptr, nullptr),
+                                  macw<float>(nullptr, nullptr, nullptr), FM_STREAM(stream));
   return advect_u_grid_t<double>(*g, rk, dx, dt, mac<double>(u0x, u0y, u0z), mac<double>(u1x, u1y, u1z),
-                                 macw<double>(u2x, u2y, u2z), FM_STREAM(stream));
+                                 macw<double>(u2x, u2y, u2z), mac<double>(nullptr, nullptr, nullptr),
+                                 macw<double>(nullptr, nullptr, nullptr), FM_STREAM(stream));
+}
+
+int fm_advect_u_grid_pair(const fm_grid* g, int dtype, int rk, double dx, double dt, const void* u0x,
+                          const void* u0y, const void* u0z, const void* u1x, const void* u1y, const void* u1z,
+                          void* u2x, void* u2y, void* u2z, const void* v1x, const void* v1y, const void* v1z,
+                          void* v2x, void* v2y, void* v2z, void* stream) {
+  int st = validate_grid(g, dtype);
+  if (st) return st;
+  if ((rk != 2 && rk != 4) || !mac_ok(*g, u0x, u0y, u0z) || !mac_ok(*g, u1x, u1y, u1z) ||
+      !mac_ok(*g, u2x, u2y, u2z) || !mac_ok(*g, v1x, v1y, v1z) || !mac_ok(*g, v2x, v2y, v2z))
+    return FM_ERR_ARG;
+  if (dtype == FM_F32)
+    return advect_u_grid_t<float>(*g, rk, dx, dt, mac<float>(u0x, u0y, u0z), mac<float>(u1x, u1y, u1z),
+                                  macw<float>(u2x, u2y, u2z), mac<float>(v1x, v1y, v1z),
+                                  macw<float>(v2x, v2y, v2z), FM_STREAM(stream));
+  return advect_u_grid_t<double>(*g, rk, dx, dt, mac<double>(u0x, u0y, u0z), mac<double>(u1x, u1y, u1z),
+                                 macw<double>(u2x, u2y, u2z), mac<double>(v1x, v1y, v1z),
+                                 macw<double>(v2x, v2y, v2z), FM_STREAM(stream));
 }
 
 int fm_advect_scalar_grid(const fm_grid* g, int dtype, int rk, double dx, double dt, const void* u0x,
                           const void* u0y, const void* u0z, const void* s1, void* s2, void* stream) {
+  return fm_advect_scalar_grid_pair(g, dtype, rk, dx, dt, u0x, u0y, u0z, s1, s2, nullptr, nullptr, stream);
+}
+
+int fm_advect_scalar_grid_pair(const fm_grid* g, int dtype, int rk, double dx, double dt, const void* u0x,
+                               const void* u0y, const void* u0z, const void* s1, void* s2, const void* t1, void* t2,
+                               void* stream) {
   int st = validate_grid(g, dtype);
   if (st) return st;
-  if ((rk != 2 && rk != 4) || !mac_ok(*g, u0x, u0y, u0z) || !s1 || !s2) return FM_ERR_ARG;
+  if ((rk != 2 && rk != 4) || !mac_ok(*g, u0x, u0y, u0z) || !s1 || !s2 || (!t1 != !t2)) return FM_ERR_ARG;
   if (dtype == FM_F32)
     return advect_scalar_grid_t<float>(*g, rk, dx, dt, mac<float>(u0x, u0y, u0z), (const float*)s1, (float*)s2,
-                                       FM_STREAM(stream));
+                                       (const float*)t1, (float*)t2, FM_STREAM(stream));
   return advect_scalar_grid_t<double>(*g, rk, dx, dt, mac<double>(u0x, u0y, u0z), (const double*)s1, (double*)s2,
-                                      FM_STREAM(stream));
+                                      (const double*)t1, (double*)t2, FM_STREAM(stream));
 }
 
 int fm_rk_grid(const fm_grid* g, int dtype, int rk, double dx, double dt, int face, void* psi, void* T,
@@ -539,46 +540,6 @@ int fm_accumulate_init(const fm_grid* g, int dtype, double dx, double dt, int ab
                                                                                         ph, hp, hpp);
                   else k_accumulate<double, D, false><<<grid, kThreads, 0, s>>>(*g, dx, dt, ind, f, in, F, ph, hp,
                                                                                 hpp));
-  }
-  return check_launch();
-}
-
-int fm_nabla_u_w(const fm_grid* g, int dtype, int order, double dx, const void* ux, const void* uy, const void* uz,
-                 const void* wx, const void* wy, const void* wz, void* rx, void* ry, void* rz, void* stream) {
-  int st = validate_grid(g, dtype);
-  if (st) return st;
-  if ((order != 2 && order != 3 && order != 4) || !mac_ok(*g, ux, uy, uz) || !mac_ok(*g, wx, wy, wz) ||
-      !mac_ok(*g, rx, ry, rz))
-    return FM_ERR_ARG;
-  dim3 grid = grid_for(max_face(*g), g->dim);
-  cudaStream_t s = FM_STREAM(stream);
-#define FM_NUW(T_)                                                                                          \
-  {                                                                                                         \
-    auto u = mac<T_>(ux, uy, uz);                                                                           \
-    auto w = mac<T_>(wx, wy, wz);                                                                           \
-    auto r = macw<T_>(rx, ry, rz);                                                                          \
-    FM_DISPATCH_D(*g, if (order == 2) k_nabla_u_w<T_, D, 2><<<grid, kThreads, 0, s>>>(*g, (T_)dx, u, w, r); \
-                  else if (order == 3) k_nabla_u_w<T_, D, 3><<<grid, kThreads, 0, s>>>(*g, (T_)dx, u, w, r);  \
-                  else k_nabla_u_w<T_, D, 4><<<grid, kThreads, 0, s>>>(*g, (T_)dx, u, w, r));               \
-  }
-  if (dtype == FM_F32) FM_NUW(float) else FM_NUW(double)
-#undef FM_NUW
-  return check_launch();
-}
-
-int fm_nabla_scalar_adjoint(const fm_grid* g, int dtype, double dx, const void* sc, const void* adj, void* rx,
-                            void* ry, void* rz, void* stream) {
-  int st = validate_grid(g, dtype);
-  if (st) return st;
-  if (!sc || !adj || !mac_ok(*g, rx, ry, rz)) return FM_ERR_ARG;
-  dim3 grid = grid_for(max_face(*g), g->dim);
-  cudaStream_t s = FM_STREAM(stream);
-  if (dtype == FM_F32) {
-    FM_DISPATCH_D(*g, k_nabla_scalar_adj<float, D><<<grid, kThreads, 0, s>>>(*g, (float)dx, (const float*)sc,
-                                                                            (const float*)adj, macw<float>(rx, ry, rz)));
-  } else {
-    FM_DISPATCH_D(*g, k_nabla_scalar_adj<double, D><<<grid, kThreads, 0, s>>>(
-                          *g, dx, (const double*)sc, (const double*)adj, macw<double>(rx, ry, rz)));
   }
   return check_launch();
 }

@@ -19,8 +19,9 @@ inline int validate_grid(const fm_grid* g, int dtype) {
   // the B-spline stencils clamp to [1, n-2]: at least 4 cells per axis
   for (int a = 0; a < g->dim; ++a)
     if (g->n[a] < 4) return FM_ERR_SHAPE;
-  // flat indices are 64-bit but per-axis extents fit int comfortably
-  if ((long long)(g->n[0] + 1) * (g->n[1] + 1) * (g->n[2] + 1) > (1LL << 34)) return FM_ERR_SHAPE;
+  // kernels decompose flat indices with 32-bit arithmetic: every grid (faces
+  // included) must hold fewer than 2^32 entries
+  if ((long long)(g->n[0] + 1) * (g->n[1] + 1) * (g->n[2] + 1) >= (1LL << 32)) return FM_ERR_SHAPE;
   return FM_OK;
 }
 

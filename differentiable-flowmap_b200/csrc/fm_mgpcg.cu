@@ -35,6 +35,10 @@ std::atomic<long long> g_launch_count{0};
 constexpr int kRedBlocks = 148 * 4;  // fixed reduction grid: 4 CTAs per SM
 constexpr int kRedThreads = 256;
 constexpr int kMaxLevels = 16;
+// single-CTA bottom solve: 512 threads x up to 8 cells each
+constexpr int kBottomThreads = 512;
+constexpr int kBottomCellsPerThread = 8;
+constexpr int kBottomMaxCells = kBottomThreads * kBottomCellsPerThread;
 
 struct DevState {
   double zTr_old, tol, rTr, alpha, beta, mean, pAp;
@@ -389,17 +393,49 @@ __global__ void k_bottom(Shape s, const T* __restrict__ r, T* __restrict__ z, in
   extern __shared__ unsigned char smem_raw[];
   T* zs = reinterpret_cast<T*>(smem_raw);
   T* rs = zs + s.size();
-  const long n = s.size();
-  for (long q = threadIdx.x; q < n; q += blockDim.x) { zs[q] = 0; rs[q] = r[q]; }
-  __syncthreads();
-  auto sweep = [&](int phase) {
-    for (long q = threadIdx.x; q < n; q += blockDim.x) {
+  const int n = (int)s.size();
+  for (int q = threadIdx.x; q < n; q += blockDim.x) { zs[q] = 0; rs[q] = r[q]; }
+  // per-thread cells (n <= kBottomMaxCells = 8 * blockDim): index, parity,
+  // in-domain neighbour mask and diagonal computed once, outside the sweeps
+  int cq[kBottomCellsPerThread], cinfo[kBottomCellsPerThread];
+  T cdiag[kBottomCellsPerThread];
+  const int si = s.s1 * s.s2, sj = s.s2;
+#pragma unroll
+  for (int m = 0; m < kBottomCellsPerThread; ++m) {
+    const int q = threadIdx.x + m * blockDim.x;
+    cq[m] = q;
+    cinfo[m] = -1;
+    cdiag[m] = 1;
+    if (q < n) {
       int i, j, k;
       unflatten(s, q, i, j, k);
-      if (parity<D>(i, j, k) == phase) {
-        T diag;
-        const T nb = nb_sum<T, D>(zs, s, i, j, k, diag);
-        zs[q] = (rs[q] + nb) / diag;
+      int mask = 0;
+      mask |= (i < s.s0 - 1) << 0;
+      mask |= (i > 0) << 1;
+      mask |= (j < s.s1 - 1) << 2;
+      mask |= (j > 0) << 3;
+      if (D == 3) { mask |= (k < s.s2 - 1) << 4; mask |= (k > 0) << 5; }
+      cinfo[m] = mask | (parity<D>(i, j, k) << 6);
+      cdiag[m] = (T)__popc(mask);
+    }
+  }
+  __syncthreads();
+  auto sweep = [&](int phase) {
+#pragma unroll
+    for (int m = 0; m < kBottomCellsPerThread; ++m) {
+      const int info = cinfo[m];
+      if (info >= 0 && (info >> 6) == phase) {
+        const int q = cq[m];
+        T nb = 0;
+        if (info & 1) nb += zs[q + si];
+        if (info & 2) nb += zs[q - si];
+        if (info & 4) nb += zs[q + sj];
+        if (info & 8) nb += zs[q - sj];
+        if (D == 3) {
+          if (info & 16) nb += zs[q + 1];
+          if (info & 32) nb += zs[q - 1];
+        }
+        zs[q] = (rs[q] + nb) / cdiag[m];
       }
     }
     __syncthreads();
@@ -479,7 +515,8 @@ static void launch_vcycle(fm_mgpcg* S, cudaStream_t s, bool dot_last) {
   }
   const Shape sb = S->lv[L - 1];
   if (S->bottom_smem) {
-    launch(k_bottom<T, D>, 1, 512, S->bottom_smem, s, sb, r[L - 1], z[L - 1], P.bottom, P.bottom_mode, S->st);
+    launch(k_bottom<T, D>, 1, kBottomThreads, S->bottom_smem, s, sb, r[L - 1], z[L - 1], P.bottom, P.bottom_mode,
+           S->st);
   } else {
     // large coarsest level: per-sweep launches (z zero-filled by the first sweep)
     const unsigned nb = blocks_for(sb.size(), 256, cap);
@@ -678,7 +715,7 @@ int fm_mgpcg_create(const fm_grid* g, int dtype, const fm_mg_params* params, fm_
   if (ok) ok = cudaMemset(S->st, 0, sizeof(DevState)) == cudaSuccess;
   const long nb = S->lv[S->L - 1].size();
   const size_t smem = 2 * es * nb;
-  if (ok && smem <= 200 * 1024) {
+  if (ok && smem <= 200 * 1024 && nb <= kBottomMaxCells) {
     S->bottom_smem = smem;
     if (smem > 48 * 1024) {
       cudaError_t e;
@@ -947,7 +984,8 @@ extern "C" int fm_project_noalloc(const fm_grid* g, int dtype, const fm_mg_param
   noalloc_layout(*g, dtype, P.levels, &S, (unsigned char*)base);
   const size_t es = dtype == FM_F32 ? sizeof(float) : sizeof(double);
   const size_t smem = 2 * es * S.lv[S.L - 1].size();
-  S.bottom_smem = smem <= 48 * 1024 ? smem : 0;  // larger coarsest levels: per-sweep launches
+  // larger coarsest levels: per-sweep launches
+  S.bottom_smem = (smem <= 48 * 1024 && S.lv[S.L - 1].size() <= kBottomMaxCells) ? smem : 0;
   cudaStream_t s = (cudaStream_t)stream;
   // the scratch keeps the previous call's contents: the solver state must start at zero
   if (cudaMemsetAsync(S.st, 0, sizeof(DevState), s) != cudaSuccess) return FM_ERR_CUDA;

@@ -164,14 +164,24 @@ __device__ __forceinline__ void q2_mac_val(const Mac<T>& u, const fm_grid& g, co
   for (int c = 0; c < D; ++c) v[c] = q2_val<T, D, false>(u.c[c], face_shape(g, c), st.ax(c, 0), st.ax(c, 1), st.ax(c, 2 % D));
 }
 
+// Stencil of face component c (runtime) at p.
+template <typename T, int D>
+struct CompStencil {
+  Q2<T, false> ax, ay, az;
+  __device__ __forceinline__ void setup(const fm_grid& g, int c, const T* p, T inv_dx) {
+    ax.setup(p[0] * inv_dx, c == 0 ? (T)0 : (T)0.5, g.n[0] + (c == 0));
+    ay.setup(p[1] * inv_dx, c == 1 ? (T)0 : (T)0.5, g.n[1] + (c == 1));
+    if (D == 3) az.setup(p[2] * inv_dx, c == 2 ? (T)0 : (T)0.5, g.n[2] + (c == 2));
+  }
+  __device__ __forceinline__ T eval(const T* f, const Shape& s) const { return q2_val<T, D, false>(f, s, ax, ay, az); }
+};
+
 // one component c (runtime) of the MAC velocity
 template <typename T, int D>
 __device__ __forceinline__ T q2_mac_comp(const Mac<T>& u, const fm_grid& g, int c, const T* p, T inv_dx) {
-  Q2<T, false> ax, ay, az;
-  ax.setup(p[0] * inv_dx, c == 0 ? (T)0 : (T)0.5, g.n[0] + (c == 0));
-  ay.setup(p[1] * inv_dx, c == 1 ? (T)0 : (T)0.5, g.n[1] + (c == 1));
-  if (D == 3) az.setup(p[2] * inv_dx, c == 2 ? (T)0 : (T)0.5, g.n[2] + (c == 2));
-  return q2_val<T, D, false>(pick(u, c), face_shape(g, c), ax, ay, az);
+  CompStencil<T, D> st;
+  st.setup(g, c, p, inv_dx);
+  return st.eval(pick(u, c), face_shape(g, c));
 }
 
 // value v = u(p) and d = (grad u)(p) . t (RK_grid's Jacobian update)

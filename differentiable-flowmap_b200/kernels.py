@@ -96,6 +96,23 @@ def advect_scalar_grid(g: GridSpec, rk: int, dx: float, dt: float, u0, s1, s2, s
                                            stream_ptr(stream)), "fm_advect_scalar_grid")
 
 
+def advect_u_grid_pair(g: GridSpec, rk: int, dx: float, dt: float, u0, u1, u2, v1, v2, stream=None):
+    """Two advect_u_grid calls sharing u0/rk/dt, with one backtrace per node."""
+    for n, u in (("u0", u0), ("u1", u1), ("u2", u2), ("v1", v1), ("v2", v2)):
+        _chk_mac(g, u, n)
+    check(_lib.lib().fm_advect_u_grid_pair(C.byref(g.c_grid()), _dt(u0[0]), rk, dx, dt, *_mac3(u0), *_mac3(u1),
+                                           *_mac3(u2), *_mac3(v1), *_mac3(v2), stream_ptr(stream)),
+          "fm_advect_u_grid_pair")
+
+
+def advect_scalar_grid_pair(g: GridSpec, rk: int, dx: float, dt: float, u0, s1, s2, t1, t2, stream=None):
+    """Two advect_scalar_grid calls sharing u0/rk/dt, with one backtrace per cell."""
+    _chk_mac(g, u0, "u0")
+    check(_lib.lib().fm_advect_scalar_grid_pair(C.byref(g.c_grid()), _dt(u0[0]), rk, dx, dt, *_mac3(u0), ptr(s1),
+                                                ptr(s2), ptr(t1), ptr(t2), stream_ptr(stream)),
+          "fm_advect_scalar_grid_pair")
+
+
 def rk_grid(g: GridSpec, rk: int, dx: float, dt: float, face: int, psi, T, u, stream=None):
     _chk_mac(g, u, "u")
     _chk_vec(g, psi, face, "psi")

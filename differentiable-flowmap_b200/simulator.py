@@ -424,19 +424,26 @@ class LFM_Diff_Simulator(LFM_Simulator):
         if cfg.add_passive_scalar:
             K.nabla_scalar_adjoint(g, dx, self.passive, self.adj_passive, self.adj_passive_f)
 
-        self._advect_u_grid(self.mid_u, self.adj_u, self.final_u, -curr_dt)
-        self.adj_u, self.final_u = self.final_u, self.adj_u
+        rk = cfg.RK_number
         if cfg.backward_u:
-            if cfg.add_passive_scalar:
-                self._advect_scalar_grid(self.mid_u, self.passive, self.final_passive, -curr_dt)
-                self.passive, self.final_passive = self.final_passive, self.passive
-            self._advect_u_grid(self.mid_u, self.u, self.final_u, -curr_dt)
-            self.u, self.final_u = self.final_u, self.u
+            # adj_u and u go back along the same midpoint velocity: one backtrace
+            K.advect_u_grid_pair(g, rk, dx, -curr_dt, self.mid_u, self.adj_u, self.final_u, self.u, self.err_u)
+            self.adj_u, self.final_u = self.final_u, self.adj_u
+            self.u, self.err_u = self.err_u, self.u
+        else:
+            self._advect_u_grid(self.mid_u, self.adj_u, self.final_u, -curr_dt)
+            self.adj_u, self.final_u = self.final_u, self.adj_u
         for c in range(self.dim):
             K.add_fields(self.adj_u[c], self.src[c], self.adj_u[c], -curr_dt)
         if cfg.add_passive_scalar:
-            self._advect_scalar_grid(self.mid_u, self.adj_passive, self.final_passive, -curr_dt)
-            self.adj_passive, self.final_passive = self.final_passive, self.adj_passive
+            if cfg.backward_u:  # passive and adj_passive along the same backtrace
+                K.advect_scalar_grid_pair(g, rk, dx, -curr_dt, self.mid_u, self.passive, self.final_passive,
+                                          self.adj_passive, self.err_passive)
+                self.passive, self.final_passive = self.final_passive, self.passive
+                self.adj_passive, self.err_passive = self.err_passive, self.adj_passive
+            else:
+                self._advect_scalar_grid(self.mid_u, self.adj_passive, self.final_passive, -curr_dt)
+                self.adj_passive, self.final_passive = self.final_passive, self.adj_passive
             for c in range(self.dim):
                 K.add_fields(self.adj_u[c], self.adj_passive_f[c], self.adj_u[c], -curr_dt)
 
@@ -494,8 +501,8 @@ class LFM_Diff_Simulator(LFM_Simulator):
             _, done = self.backtrack_step_midpoint()
             if done:
                 break
-        # device-mode solves report once per gradient (one stream sync)
-        self.solver_stats = self.solver.stats(reset=True) if self.solver.device_mode else None
+        # the solver's device-side counters, read once per gradient (one stream sync)
+        self.solver_stats = self.solver.stats(reset=True)
         if self.solver_stats and self.solver_stats["nonfinite"]:
             raise FlowmapError(4, f"{self.solver_stats['nonfinite']} projection(s) hit a non-finite residual")
         return self.loss, [x.clone() for x in self.adj_u]

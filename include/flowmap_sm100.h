@@ -62,12 +62,31 @@ int fm_advect_u_grid(const fm_grid *g, int dtype, int rk, double dx, double dt,
                      const void *u1x, const void *u1y, const void *u1z,
                      void *u2x, void *u2y, void *u2z, void *stream);
 
+/* Two advect_u_grid calls that share u0, rk and dt, in one pass: the foot of
+ * each face node's backtrace is computed once and both u1 (-> u2) and v1
+ * (-> v2) are sampled there.  The adjoint advects adj_u and u backwards along
+ * the same midpoint velocity (3D/lfm_midpoint_diff_simulator.py:488-499);
+ * results equal two fm_advect_u_grid calls. */
+int fm_advect_u_grid_pair(const fm_grid *g, int dtype, int rk, double dx, double dt,
+                          const void *u0x, const void *u0y, const void *u0z,
+                          const void *u1x, const void *u1y, const void *u1z,
+                          void *u2x, void *u2y, void *u2z,
+                          const void *v1x, const void *v1y, const void *v1z,
+                          void *v2x, void *v2y, void *v2z, void *stream);
+
 /* advect_scalar_grid: the same backtrace from cell centres, quadratic sample
  * of s1.  Replaces RK2/RK4_advect_scalar_grid (3D/flowmap.py:284-320,
  * dispatch :39-49).  s2 must not alias s1. */
 int fm_advect_scalar_grid(const fm_grid *g, int dtype, int rk, double dx, double dt,
                           const void *u0x, const void *u0y, const void *u0z,
                           const void *s1, void *s2, void *stream);
+
+/* Two scalars along the same backtrace (passive and adj_passive in the
+ * adjoint, 3D/lfm_midpoint_diff_simulator.py:494, :506).  t1/t2 may both be
+ * NULL (then equal to fm_advect_scalar_grid). */
+int fm_advect_scalar_grid_pair(const fm_grid *g, int dtype, int rk, double dx, double dt,
+                               const void *u0x, const void *u0y, const void *u0z,
+                               const void *s1, void *s2, const void *t1, void *t2, void *stream);
 
 /* RK_grid / RK_grid_only_psi: in-place march of a flow map (psi, dim planes)
  * and, when T != NULL, its Jacobian rows (T, dim planes) with neg_dt = -dt.

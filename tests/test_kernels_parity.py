@@ -337,3 +337,27 @@ def test_project_device_mode_matches_host_mode(fm, cuda, shape):
         dev.project([x.clone() for x in u])
     st = dev.stats()
     assert st["solves"] == 3 and st["iterations"] == 3 * host.last_iters
+
+
+@pytest.mark.parametrize("rk", [2, 4])
+def test_paired_advection_equals_two_calls(fm, cuda, shape, rk):
+    """fm_advect_u_grid_pair / fm_advect_scalar_grid_pair share one backtrace and
+    reproduce two single calls bit for bit."""
+    rng = np.random.default_rng(21)
+    g = fm.GridSpec(shape)
+    dx = 1.0 / shape[1]
+    T_ = lambda L: [_t(x, torch.float32, cuda) for x in L]
+    u0, u1, v1 = T_(_rand_mac(rng, shape, 1.0)), T_(_rand_mac(rng, shape, 1.0)), T_(_rand_mac(rng, shape, 1.0))
+    a2, b2 = [torch.empty_like(x) for x in u0], [torch.empty_like(x) for x in u0]
+    c2, d2 = [torch.empty_like(x) for x in u0], [torch.empty_like(x) for x in u0]
+    fm.kernels.advect_u_grid_pair(g, rk, dx, -0.6 * dx, u0, u1, a2, v1, b2)
+    fm.kernels.advect_u_grid(g, rk, dx, -0.6 * dx, u0, u1, c2)
+    fm.kernels.advect_u_grid(g, rk, dx, -0.6 * dx, u0, v1, d2)
+    for x, y in zip(a2 + b2, c2 + d2):
+        assert torch.equal(x, y)
+    s, t = _t(rng.uniform(size=shape), torch.float32, cuda), _t(rng.uniform(size=shape), torch.float32, cuda)
+    s2, t2, s3, t3 = [torch.empty_like(s) for _ in range(4)]
+    fm.kernels.advect_scalar_grid_pair(g, rk, dx, -0.6 * dx, u0, s, s2, t, t2)
+    fm.kernels.advect_scalar_grid(g, rk, dx, -0.6 * dx, u0, s, s3)
+    fm.kernels.advect_scalar_grid(g, rk, dx, -0.6 * dx, u0, t, t3)
+    assert torch.equal(s2, s3) and torch.equal(t2, t3)
