@@ -97,6 +97,7 @@ SIGNATURES = {
     "fm_convert": [L, I, P, I, P, P],
     "fm_advect_u_grid_pair": [GP, I, I, D, D] + [P] * 15 + [P],
     "fm_advect_scalar_grid_pair": [GP, I, I, D, D] + [P] * 7 + [P],
+    "fm_mg_vcycle": [P, P, P, P],
 }
 RESTYPES = {"fm_launch_count": C.c_longlong}
 SIGNATURES["fm_launch_count"] = [I]

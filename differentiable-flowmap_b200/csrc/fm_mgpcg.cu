@@ -56,6 +56,39 @@ struct DevState {
 // ---------------------------------------------------------------------------
 // helpers
 // ---------------------------------------------------------------------------
+// Round-to-nearest arithmetic that the compiler may not fuse into FMAs: the
+// MG operators then round exactly as the reference's separate multiply and
+// subtract do.
+__device__ __forceinline__ float rn_add(float a, float b) { return __fadd_rn(a, b); }
+__device__ __forceinline__ double rn_add(double a, double b) { return __dadd_rn(a, b); }
+__device__ __forceinline__ float rn_sub(float a, float b) { return __fsub_rn(a, b); }
+__device__ __forceinline__ double rn_sub(double a, double b) { return __dsub_rn(a, b); }
+__device__ __forceinline__ float rn_mul(float a, float b) { return __fmul_rn(a, b); }
+__device__ __forceinline__ double rn_mul(double a, double b) { return __dmul_rn(a, b); }
+
+// x / nd for the RBGS update, nd = number of in-domain neighbours (0..6),
+// rounded exactly as the IEEE division.  FP32: nd = s * d with s a power of
+// two (exact scaling) and d in {1, 3, 5}; q0 = y * RN(1/d), e = y - q0 * d
+// (exact by FMA), q = q0 + e * RN(1/d).  Checked against the IEEE quotient for
+// all 2^32 float inputs and every nd: equal bit for bit whenever
+// 2^-100 <= |x| <= 2^100; outside that range (zeros, tiny, huge, non-finite)
+// and for nd = 0 the IEEE division is used.  It replaces a division whose
+// latency doubled the time of a coarse-level half-sweep.
+__device__ __forceinline__ float div_nd(float x, int nd) {
+  const float ax = fabsf(x);
+  if (ax >= 0x1p-100f && ax <= 0x1p100f && nd > 0) {
+    const float s = (nd == 2 || nd == 6) ? 0.5f : (nd == 4 ? 0.25f : 1.0f);
+    const float d = (nd == 3 || nd == 6) ? 3.0f : (nd == 5 ? 5.0f : 1.0f);
+    const float rd = (nd == 3 || nd == 6) ? (1.0f / 3.0f) : (nd == 5 ? (1.0f / 5.0f) : 1.0f);
+    const float y = __fmul_rn(x, s);
+    const float q0 = __fmul_rn(y, rd);
+    const float e = __fmaf_rn(-q0, d, y);
+    return __fmaf_rn(e, rd, q0);
+  }
+  return x / (float)nd;
+}
+__device__ __forceinline__ double div_nd(double x, int nd) { return x / (double)nd; }
+
 template <int D>
 __device__ __forceinline__ int parity(int i, int j, int k) {
   return (i + j + (D == 3 ? k : 0)) & 1;
@@ -274,7 +307,7 @@ __global__ void __launch_bounds__(kRedThreads) k_Ap_dot(Shape s, const T* __rest
     T diag;
     const T nb = nb_sum<T, D>(p, s, i, j, k, diag);
     const T pv = p[q];
-    const T a = diag * pv - nb;
+    const T a = rn_sub(rn_mul(diag, pv), nb);
     Ap[q] = a;
     acc += (double)pv * (double)a;
   }
@@ -289,8 +322,8 @@ __global__ void __launch_bounds__(kRedThreads) k_update_xr(long n, T* __restrict
   const T alpha = (T)st->alpha;
   double rr = 0, rs = 0;
   FM_GRID_STRIDE(q, n) {
-    x[q] += alpha * p[q];
-    const T rv = r[q] - alpha * Ap[q];
+    x[q] = rn_add(x[q], rn_mul(alpha, p[q]));
+    const T rv = rn_sub(r[q], rn_mul(alpha, Ap[q]));
     r[q] = rv;
     rr += (double)rv * (double)rv;
     rs += (double)rv;
@@ -302,7 +335,7 @@ template <typename T>
 __global__ void k_update_p(long n, T* __restrict__ p, const T* __restrict__ z, const DevState* st, int first) {
   if (st->done) return;
   const T beta = (T)st->beta;
-  FM_GRID_STRIDE(q, n) p[q] = first ? z[q] : z[q] + beta * p[q];
+  FM_GRID_STRIDE(q, n) p[q] = first ? z[q] : rn_add(z[q], rn_mul(beta, p[q]));
 }
 
 // ---------------------------------------------------------------------------
@@ -318,8 +351,7 @@ __global__ void k_smooth_first(Shape s, T* __restrict__ r, T* __restrict__ z, co
     unflatten(s, q, i, j, k);
     T rv = r[q];
     if (recenter) { rv = rv - mean; r[q] = rv; }
-    const T diag = (T)diag_of<D>(s, i, j, k);
-    z[q] = parity<D>(i, j, k) == 0 ? rv / diag : (T)0;
+    z[q] = parity<D>(i, j, k) == 0 ? div_nd(rv, diag_of<D>(s, i, j, k)) : (T)0;
   }
 }
 
@@ -336,7 +368,7 @@ __global__ void __launch_bounds__(kRedThreads) k_smooth(Shape s, const T* __rest
     if (parity<D>(i, j, k) == phase) {
       T diag;
       const T nb = nb_sum<T, D>(z, s, i, j, k, diag);
-      zv = (r[q] + nb) / diag;
+      zv = div_nd(r[q] + nb, diag_of<D>(s, i, j, k));
       z[q] = zv;
     } else {
       zv = z[q];
@@ -366,8 +398,8 @@ __global__ void k_restrict(Shape sf, Shape sc, const T* __restrict__ rf, const T
           const long f = sf.idx(i, j, k);
           T diag;
           const T nb = nb_sum<T, D>(zf, sf, i, j, k, diag);
-          const T res = rf[f] - (diag * zf[f] - nb);
-          acc += res * scale;
+          const T res = rn_sub(rf[f], rn_sub(rn_mul(diag, zf[f]), nb));
+          acc = rn_add(acc, rn_mul(res, scale));
         }
     rc[q] = acc;
   }
@@ -398,14 +430,12 @@ __global__ void k_bottom(Shape s, const T* __restrict__ r, T* __restrict__ z, in
   // per-thread cells (n <= kBottomMaxCells = 8 * blockDim): index, parity,
   // in-domain neighbour mask and diagonal computed once, outside the sweeps
   int cq[kBottomCellsPerThread], cinfo[kBottomCellsPerThread];
-  T cdiag[kBottomCellsPerThread];
   const int si = s.s1 * s.s2, sj = s.s2;
 #pragma unroll
   for (int m = 0; m < kBottomCellsPerThread; ++m) {
     const int q = threadIdx.x + m * blockDim.x;
     cq[m] = q;
     cinfo[m] = -1;
-    cdiag[m] = 1;
     if (q < n) {
       int i, j, k;
       unflatten(s, q, i, j, k);
@@ -416,7 +446,6 @@ __global__ void k_bottom(Shape s, const T* __restrict__ r, T* __restrict__ z, in
       mask |= (j > 0) << 3;
       if (D == 3) { mask |= (k < s.s2 - 1) << 4; mask |= (k > 0) << 5; }
       cinfo[m] = mask | (parity<D>(i, j, k) << 6);
-      cdiag[m] = (T)__popc(mask);
     }
   }
   __syncthreads();
@@ -435,7 +464,7 @@ __global__ void k_bottom(Shape s, const T* __restrict__ r, T* __restrict__ z, in
           if (info & 16) nb += zs[q + 1];
           if (info & 32) nb += zs[q - 1];
         }
-        zs[q] = (rs[q] + nb) / cdiag[m];
+        zs[q] = div_nd(rs[q] + nb, __popc(info & 63));
       }
     }
     __syncthreads();
@@ -456,11 +485,13 @@ __global__ void k_laplacian(Shape s, const T* __restrict__ p, T* __restrict__ Ap
     unflatten(s, q, i, j, k);
     T diag;
     const T nb = nb_sum<T, D>(p, s, i, j, k, diag);
-    Ap[q] = diag * p[q] - nb;
+    Ap[q] = rn_sub(rn_mul(diag, p[q]), nb);
   }
 }
 
 }  // namespace fm
+
+#include "fm_mg_cluster.cuh"
 
 using namespace fm;
 
@@ -484,9 +515,61 @@ struct fm_mgpcg {
   cudaGraphExec_t loop;        // device mode: conditional WHILE node around one iteration
   long long loop_kernels;      // kernels per loop iteration
   size_t bottom_smem;
+  int lc;                      // levels lc .. L-1 run as one cluster launch (<= 0: per-level launches)
+  int nc;                      // CTAs in that cluster
+  size_t coarse_smem;
 };
 
 namespace fm {
+
+// (red, black) cell pairs along the innermost axis of `planes` planes of level s.
+static long coarse_pairs(const Shape& s, int dim, int planes) {
+  const long nin = dim == 3 ? s.s2 : s.s1;
+  return (long)planes * (dim == 3 ? s.s1 : 1) * ((nin + 1) / 2);
+}
+static long coarse_ring(const Shape& s, int dim, int planes) {
+  return (long)planes * (s.s1 + 2) * (dim == 3 ? s.s2 + 2 : 1);
+}
+
+// Picks the finest level lc >= 1 from which the rest of the V-cycle fits one
+// cluster launch: level lc split into nc <= 8 slabs of an even number of
+// planes, every slab and every deeper level at most kCoarsePPT cell pairs per
+// thread, all of it (zero-ringed z, compact r) within 200 KB of shared memory
+// per CTA.  lc = -1 when no level qualifies (the V-cycle launches per level).
+static void plan_coarse(fm_mgpcg* S, size_t es) {
+  S->lc = -1;
+  S->nc = 0;
+  S->coarse_smem = 0;
+  const int dim = S->g.dim;
+  const long max_pairs = (long)kCoarsePPT * kCoarseThreads;
+  for (int l = 1; l < S->L - 1; ++l) {
+    const Shape t = S->lv[l];
+    int nc = kCoarseMaxNC;
+    while (nc > 1 && t.s0 % (2 * nc) != 0) nc >>= 1;
+    if (t.s0 % (2 * nc) != 0) continue;
+    const int P = t.s0 / nc;
+    if (coarse_pairs(t, dim, P) > max_pairs) continue;
+    long cells = coarse_ring(t, dim, P + 2) + (long)P * t.s1 * t.s2;
+    bool fits = true;
+    for (int m = l + 1; m < S->L; ++m) {
+      const Shape d = S->lv[m];
+      fits = fits && coarse_pairs(d, dim, d.s0) <= max_pairs;
+      cells += d.size() + coarse_ring(d, dim, d.s0 + 2);
+    }
+    const size_t smem = es * (size_t)cells;
+    if (!fits || smem > 200 * 1024) continue;
+    S->lc = l;
+    S->nc = nc;
+    S->coarse_smem = smem;
+    return;
+  }
+}
+
+template <typename T, int D>
+static bool enable_coarse_kernel(size_t smem) {
+  return cudaFuncSetAttribute(k_mg_coarse<T, D>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem) ==
+         cudaSuccess;
+}
 
 static inline unsigned blocks_for(long n, int threads, long cap) {
   long b = (n + threads - 1) / threads;
@@ -495,18 +578,59 @@ static inline unsigned blocks_for(long n, int threads, long cap) {
   return (unsigned)b;
 }
 
+// Levels lc .. L-1 of the V-cycle as one cluster launch (fm_mg_cluster.cuh).
 template <typename T, int D>
-static void launch_vcycle(fm_mgpcg* S, cudaStream_t s, bool dot_last) {
+static void launch_coarse(fm_mgpcg* S, cudaStream_t s) {
+  CoarseArgs a;
+  int off = 0;  // deep levels in CTA 0: compact r, then zero-ringed z
+  for (int l = 0; l < kMaxLevels; ++l) {
+    a.lv[l] = S->lv[l];
+    a.roff[l] = a.zoff[l] = off;
+    if (l > S->lc && l < S->L) {
+      a.zoff[l] = off + (int)S->lv[l].size();
+      off = a.zoff[l] + (int)coarse_ring(S->lv[l], S->g.dim, S->lv[l].s0 + 2);
+    }
+  }
+  a.lc = S->lc;
+  a.L = S->L;
+  a.pre_post = S->P.pre_post;
+  a.bottom = S->P.bottom;
+  a.bottom_mode = S->P.bottom_mode;
+  a.r_top = S->r[S->lc];
+  a.z_top = S->z[S->lc];
+  cudaLaunchConfig_t cfg = {};
+  cfg.gridDim = dim3((unsigned)S->nc, 1, 1);
+  cfg.blockDim = dim3(kCoarseThreads, 1, 1);
+  cfg.dynamicSmemBytes = S->coarse_smem;
+  cfg.stream = s;
+  cudaLaunchAttribute attr[1];
+  attr[0].id = cudaLaunchAttributeClusterDimension;
+  attr[0].val.clusterDim.x = (unsigned)S->nc;
+  attr[0].val.clusterDim.y = 1;
+  attr[0].val.clusterDim.z = 1;
+  cfg.attrs = attr;
+  cfg.numAttrs = 1;
+  const DevState* st = S->st;
+  cudaLaunchKernelEx(&cfg, k_mg_coarse<T, D>, a, st);
+  count_launch(1);
+}
+
+// One V-cycle (apply_preconditioner, 3D/mgpcg.py:187-205) on r[0] -> z[0].
+// recenter: subtract st->mean from r[0] first (fused into the first sweep);
+// dot_last: the last fine sweep also writes z.r block partials.
+template <typename T, int D>
+static void launch_vcycle(fm_mgpcg* S, cudaStream_t s, bool dot_last, bool recenter = true) {
   const int L = S->L;
   const fm_mg_params& P = S->P;
   T** r = (T**)S->r;
   T** z = (T**)S->z;
   const long cap = 148L * 16;
-  for (int l = 0; l < L - 1; ++l) {
+  const int lc = S->lc > 0 ? S->lc : L - 1;  // first level not smoothed by per-level launches
+  for (int l = 0; l < lc; ++l) {
     const Shape sh = S->lv[l];
     const unsigned nb = blocks_for(sh.size(), 256, cap);
     for (int it = 0; it < P.pre_post; ++it) {
-      if (it == 0) launch(k_smooth_first<T, D>, nb, 256, 0, s, sh, r[l], z[l], S->st, l == 0 ? 1 : 0);
+      if (it == 0) launch(k_smooth_first<T, D>, nb, 256, 0, s, sh, r[l], z[l], S->st, l == 0 && recenter ? 1 : 0);
       else launch(k_smooth<T, D, false>, nb, 256, 0, s, sh, r[l], z[l], 0, nullptr, S->st);
       launch(k_smooth<T, D, false>, nb, 256, 0, s, sh, r[l], z[l], 1, nullptr, S->st);
     }
@@ -514,7 +638,9 @@ static void launch_vcycle(fm_mgpcg* S, cudaStream_t s, bool dot_last) {
     launch(k_restrict<T, D>, blocks_for(sc.size(), 256, cap), 256, 0, s, sh, sc, r[l], z[l], r[l + 1], S->st);
   }
   const Shape sb = S->lv[L - 1];
-  if (S->bottom_smem) {
+  if (S->lc > 0) {
+    launch_coarse<T, D>(S, s);
+  } else if (S->bottom_smem) {
     launch(k_bottom<T, D>, 1, kBottomThreads, S->bottom_smem, s, sb, r[L - 1], z[L - 1], P.bottom, P.bottom_mode,
            S->st);
   } else {
@@ -535,8 +661,9 @@ static void launch_vcycle(fm_mgpcg* S, cudaStream_t s, bool dot_last) {
       for (int i = 0; i < P.bottom / 2; ++i) pair(0, 1);
       for (int i = 0; i < P.bottom / 2; ++i) pair(1, 0);
     }
+    if (first) cudaMemsetAsync(z[L - 1], 0, sizeof(T) * sb.size(), s);  // no bottom sweeps
   }
-  for (int l = L - 2; l >= 0; --l) {
+  for (int l = lc - 1; l >= 0; --l) {
     const Shape sh = S->lv[l];
     const Shape sc = S->lv[l + 1];
     const unsigned nb = blocks_for(sh.size(), 256, cap);
@@ -728,6 +855,19 @@ int fm_mgpcg_create(const fm_grid* g, int dtype, const fm_mg_params* params, fm_
       if (e != cudaSuccess) S->bottom_smem = 0;
     }
   }
+  if (ok) {
+    plan_coarse(S, es);
+    if (S->lc > 0) {
+      const bool en = dtype == FM_F32 ? (g->dim == 3 ? enable_coarse_kernel<float, 3>(S->coarse_smem)
+                                                     : enable_coarse_kernel<float, 2>(S->coarse_smem))
+                                      : (g->dim == 3 ? enable_coarse_kernel<double, 3>(S->coarse_smem)
+                                                     : enable_coarse_kernel<double, 2>(S->coarse_smem));
+      if (!en) {
+        cudaGetLastError();
+        S->lc = -1;
+      }
+    }
+  }
   if (!ok) {
     fm_mgpcg_destroy(S);
     return FM_ERR_CUDA;
@@ -802,6 +942,24 @@ int fm_mgpcg_solve(fm_mgpcg* S, const void* b, void* x, void* stream, int* iters
   cudaMemcpyAsync(x, S->x, (S->dtype == FM_F32 ? 4 : 8) * n, cudaMemcpyDeviceToDevice, s);
   if (check_cuda()) return FM_ERR_CUDA;
   return status;
+}
+
+int fm_mg_vcycle(fm_mgpcg* S, const void* r, void* z, void* stream) {
+  if (!S || !r || !z) return FM_ERR_ARG;
+  cudaStream_t s = (cudaStream_t)stream;
+  const size_t bytes = (S->dtype == FM_F32 ? 4 : 8) * (size_t)S->lv[0].size();
+  if (cudaMemcpyAsync(S->r[0], r, bytes, cudaMemcpyDeviceToDevice, s) != cudaSuccess) return FM_ERR_CUDA;
+  // every V-cycle kernel is gated on the solver's `done` word
+  if (cudaMemsetAsync(&S->st->done, 0, sizeof(int), s) != cudaSuccess) return FM_ERR_CUDA;
+  if (S->dtype == FM_F32) {
+    if (S->g.dim == 3) launch_vcycle<float, 3>(S, s, false, false);
+    else launch_vcycle<float, 2>(S, s, false, false);
+  } else {
+    if (S->g.dim == 3) launch_vcycle<double, 3>(S, s, false, false);
+    else launch_vcycle<double, 2>(S, s, false, false);
+  }
+  if (cudaMemcpyAsync(z, S->z[0], bytes, cudaMemcpyDeviceToDevice, s) != cudaSuccess) return FM_ERR_CUDA;
+  return check_cuda();
 }
 
 int fm_mgpcg_stats(fm_mgpcg* S, void* stream, int reset, fm_mg_stats* out) {

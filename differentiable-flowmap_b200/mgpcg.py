@@ -111,6 +111,16 @@ class MGPCG:
         self._status(st, "fm_mgpcg_solve", it, rtr)
         return it.value, rtr.value
 
+    def apply_preconditioner(self, r: torch.Tensor, z: Optional[torch.Tensor] = None, stream=None) -> torch.Tensor:
+        """One V-cycle z = M^-1 r (3D/mgpcg.py:187-205), r not recentred."""
+        if tuple(r.shape) != self.N or r.dtype != self.dtype:
+            raise _lib.FlowmapError(1, "apply_preconditioner: r shape/dtype mismatch")
+        if z is None:
+            z = torch.empty_like(r)
+        _lib.check(_lib.lib().fm_mg_vcycle(self._h, _lib.ptr(r), _lib.ptr(z), _lib.stream_ptr(stream)),
+                   "fm_mg_vcycle")
+        return z
+
     # reference names -------------------------------------------------------
     def Poisson(self, *u, verbose: bool = False):
         self.project(u)

@@ -211,6 +211,13 @@ int fm_project(fm_mgpcg *solver, void *ux, void *uy, void *uz, void *p_out, void
  * either synchronises the stream and reports the outcome. */
 int fm_mgpcg_solve(fm_mgpcg *solver, const void *b, void *x, void *stream, int *iters, double *rtr);
 
+/* One application of the MG preconditioner, z = M^-1 r (apply_preconditioner,
+ * 3D/mgpcg.py:187-205): z = 0, per level pre_post x (red, black) sweeps and a
+ * restriction, bottom smoothing, then per level prolongation and pre_post x
+ * (black, red) sweeps.  r is not recentred.  r and z are cell-grid arrays of
+ * the solver's dtype; the solver's level-0 buffers are overwritten. */
+int fm_mg_vcycle(fm_mgpcg *solver, const void *r, void *z, void *stream);
+
 /* Cumulative solver outcome (synchronises `stream`).  reset != 0 zeroes the
  * counters afterwards.  The reference reports non-convergence only with a
  * print (3D/mgpcg.py:286-289); here it is counted. */

@@ -37,6 +37,7 @@ def test_invalid_arguments_rejected_without_device(fm):
     p = fm._lib.MGParams(5, 2, 50, 0, 400, 1e-12, 0.0, 1e-12, 4, 0)  # 8 not divisible by 2^4
     assert lib.fm_mgpcg_create(C.byref(g), 0, C.byref(p), C.byref(h)) == 1
     assert lib.fm_project(None, None, None, None, None, None, None, None) == 2
+    assert lib.fm_mg_vcycle(None, None, None, None) == 2
 
 
 def test_no_cpu_fallback(fm):

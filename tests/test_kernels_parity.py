@@ -313,6 +313,47 @@ def test_vcycle_iterations_match_oracle(fm, cuda):
     assert _rel(x.cpu().numpy(), x_ref) < 1e-8
 
 
+# (shape, levels, pre_post, bottom, bottom_mode): the first cases run the coarse
+# levels as one cluster launch (slabs of 2..8 planes, 2..8 CTAs; 128^3 after two
+# per-level launches), (16,16,16)/2 and (48,48)/2 the single-CTA bottom kernel,
+# (160,160)/2 per-sweep bottom launches.
+VCYCLE_CASES = [
+    ((128, 128, 128), 5, 2, 50, 0),
+    ((32, 32, 32), 3, 2, 50, 0),
+    ((64, 64, 64), 4, 2, 50, 0),
+    ((24, 16, 32), 3, 2, 50, 0),
+    ((64, 64), 4, 2, 50, 0),
+    ((128, 96), 3, 1, 20, 1),
+    ((32, 48, 16), 3, 3, 7, 1),
+    ((64, 32), 5, 2, 0, 0),
+    ((16, 16, 16), 2, 2, 50, 0),
+    ((48, 48), 2, 2, 10, 1),
+    ((160, 160), 2, 1, 3, 0),
+]
+
+
+@pytest.mark.parametrize("case", VCYCLE_CASES, ids=lambda c: "x".join(map(str, c[0])) + f"-L{c[1]}-pp{c[2]}-b{c[3]}m{c[4]}")
+@pytest.mark.parametrize("pname", ["f64", "f32"])
+def test_vcycle_bitwise_matches_oracle(fm, cuda, case, pname):
+    """One preconditioner application (apply_preconditioner, 3D/mgpcg.py:187-205)
+    equals the oracle's sequential V-cycle bit for bit: same operations, same
+    order, no FMA contraction, on every launch path of the coarse levels."""
+    shape, levels, pre_post, bottom, mode = case
+    dtype = torch.float64 if pname == "f64" else torch.float32
+    o = Oracle(shape, pname)
+    rng = np.random.default_rng(sum(shape) + levels)
+    r = rng.standard_normal(shape).astype(o.dtype)
+    P = MGParams(levels, pre_post, bottom, mode, 1, 0.0, 0.0, 0.0)
+    z_ref = np.zeros(shape, o.dtype)
+    o.mg_vcycle(P, r.copy(), z_ref)
+    sol = fm.MGPCG(shape, dtype, levels=levels, pre_post=pre_post, bottom=bottom, bottom_mode=mode)
+    z = sol.apply_preconditioner(torch.tensor(r, device=cuda))
+    z2 = sol.apply_preconditioner(torch.tensor(r, device=cuda))  # the solver's buffers start dirty now
+    zn = z.cpu().numpy()
+    assert np.array_equal(zn, z_ref), np.abs(zn - z_ref).max()
+    assert torch.equal(z, z2)
+
+
 @pytest.mark.parametrize("shape", [(32, 32, 32), (64, 64)])
 def test_project_device_mode_matches_host_mode(fm, cuda, shape):
     """check_every=0 (conditional WHILE graph, no host sync) gives the same
