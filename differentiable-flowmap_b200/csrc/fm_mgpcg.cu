@@ -355,6 +355,90 @@ __global__ void k_smooth_first(Shape s, T* __restrict__ r, T* __restrict__ z, co
   }
 }
 
+// Pair-per-thread RBGS sweeps for the levels above the cluster kernel.  A
+// thread owns cells (.., 2m) and (.., 2m+1) along the innermost axis (k in 3D,
+// j in 2D), one red and one black, so every lane updates a cell in every
+// half-sweep.  Launch: block (32, 8); 3D grid (pairs/32, n1/8, n0) over
+// (pair, j, i), 2D grid (pairs/32, n0/8) over (pair, i).
+constexpr int kPairBX = 32, kPairBY = 8;
+
+template <int D>
+__device__ __forceinline__ bool pair_coords(const Shape& s, int& i, int& j, int& k0) {
+  const int m = blockIdx.x * kPairBX + threadIdx.x;
+  if (D == 3) {
+    i = blockIdx.z;
+    j = blockIdx.y * kPairBY + threadIdx.y;
+    k0 = 2 * m;
+    return j < s.s1 && k0 < s.s2;
+  }
+  i = blockIdx.y * kPairBY + threadIdx.y;
+  j = 2 * m;
+  k0 = 0;
+  return i < s.s0 && j < s.s1;
+}
+
+// Neighbour sum (reference order +i, -i, +j, -j, +k, -k) and neighbour count
+// of cell (i, j, k) at 32-bit index q.
+template <typename T, int D>
+__device__ __forceinline__ T nb_sum32(const T* __restrict__ x, const Shape& s, unsigned q, int i, int j, int k,
+                                      int& nd) {
+  const unsigned si = (unsigned)s.s1 * s.s2, sj = s.s2;
+  T acc = 0;
+  nd = 0;
+  if (i < s.s0 - 1) { acc += x[q + si]; ++nd; }
+  if (i > 0) { acc += x[q - si]; ++nd; }
+  if (j < s.s1 - 1) { acc += x[q + sj]; ++nd; }
+  if (j > 0) { acc += x[q - sj]; ++nd; }
+  if (D == 3) {
+    if (k < s.s2 - 1) { acc += x[q + 1]; ++nd; }
+    if (k > 0) { acc += x[q - 1]; ++nd; }
+  }
+  return acc;
+}
+
+// smooth(l, phase) over pairs: only the cell of colour `phase` is updated.
+template <typename T, int D>
+__global__ void __launch_bounds__(kPairBX* kPairBY) k_smooth_pair(Shape s, const T* __restrict__ r, T* z, int phase,
+                                                                 const DevState* st) {
+  if (st->done) return;
+  int i, j, k;
+  if (!pair_coords<D>(s, i, j, k)) return;
+  // the colour-`phase` cell of the pair: parity(i, j, k0) is (i + j) & 1 in 3D, i & 1 in 2D
+  const int shift = ((D == 3 ? i + j : i) + phase) & 1;
+  if (D == 3) k += shift; else j += shift;
+  if ((D == 3 ? k : j) >= (D == 3 ? s.s2 : s.s1)) return;
+  const unsigned q = ((unsigned)i * s.s1 + j) * s.s2 + k;
+  int nd;
+  const T nb = nb_sum32<T, D>(z, s, q, i, j, k, nd);
+  z[q] = div_nd(r[q] + nb, nd);
+}
+
+// First red sweep from z == 0 over pairs (fuses z.fill(0)); optionally recentres r.
+template <typename T, int D>
+__global__ void __launch_bounds__(kPairBX* kPairBY) k_smooth_first_pair(Shape s, T* __restrict__ r, T* __restrict__ z,
+                                                                       const DevState* st, int recenter) {
+  if (st->done) return;
+  int i, j, k;
+  if (!pair_coords<D>(s, i, j, k)) return;
+  const T mean = recenter ? (T)st->mean : (T)0;
+  const int red_second = (D == 3 ? i + j : i) & 1;  // the pair's second cell is red
+  const unsigned q0 = ((unsigned)i * s.s1 + j) * s.s2 + k;
+  const bool has2 = (D == 3 ? k : j) + 1 < (D == 3 ? s.s2 : s.s1);
+#pragma unroll
+  for (int c = 0; c < 2; ++c) {
+    if (c == 1 && !has2) break;
+    const unsigned q = q0 + c;
+    T rv = r[q];
+    if (recenter) { rv = rv - mean; r[q] = rv; }
+    if (c == red_second) {
+      const int ci = i, cj = D == 3 ? j : j + c, ck = D == 3 ? k + c : 0;
+      z[q] = div_nd(rv, diag_of<D>(s, ci, cj, ck));
+    } else {
+      z[q] = 0;
+    }
+  }
+}
+
 // smooth(l, phase) (3D/mgpcg.py:170-177); with part != nullptr also z.r over all cells.
 template <typename T, int D, bool DOT>
 __global__ void __launch_bounds__(kRedThreads) k_smooth(Shape s, const T* __restrict__ r, T* z, int phase,
@@ -510,6 +594,8 @@ struct fm_mgpcg {
   DevState* st;
   DevState* h_st;  // pinned
   cudaStream_t cap;
+  cudaGraphExec_t prologue;    // recentring, first V-cycle, p = z, zTr
+  long long prologue_kernels;
   cudaGraphExec_t chunk;       // host-checked mode: check_every iterations
   long long chunk_kernels;
   cudaGraphExec_t loop;        // device mode: conditional WHILE node around one iteration
@@ -626,13 +712,20 @@ static void launch_vcycle(fm_mgpcg* S, cudaStream_t s, bool dot_last, bool recen
   T** z = (T**)S->z;
   const long cap = 148L * 16;
   const int lc = S->lc > 0 ? S->lc : L - 1;  // first level not smoothed by per-level launches
+  const dim3 pblk(kPairBX, kPairBY, 1);
+  auto pair_grid = [](const Shape& sh) {
+    if (D == 3)
+      return dim3((unsigned)((sh.s2 + 1) / 2 + kPairBX - 1) / kPairBX, (unsigned)(sh.s1 + kPairBY - 1) / kPairBY,
+                  (unsigned)sh.s0);
+    return dim3((unsigned)((sh.s1 + 1) / 2 + kPairBX - 1) / kPairBX, (unsigned)(sh.s0 + kPairBY - 1) / kPairBY, 1);
+  };
   for (int l = 0; l < lc; ++l) {
     const Shape sh = S->lv[l];
-    const unsigned nb = blocks_for(sh.size(), 256, cap);
+    const dim3 pg = pair_grid(sh);
     for (int it = 0; it < P.pre_post; ++it) {
-      if (it == 0) launch(k_smooth_first<T, D>, nb, 256, 0, s, sh, r[l], z[l], S->st, l == 0 && recenter ? 1 : 0);
-      else launch(k_smooth<T, D, false>, nb, 256, 0, s, sh, r[l], z[l], 0, nullptr, S->st);
-      launch(k_smooth<T, D, false>, nb, 256, 0, s, sh, r[l], z[l], 1, nullptr, S->st);
+      if (it == 0) launch(k_smooth_first_pair<T, D>, pg, pblk, 0, s, sh, r[l], z[l], S->st, l == 0 && recenter ? 1 : 0);
+      else launch(k_smooth_pair<T, D>, pg, pblk, 0, s, sh, (const T*)r[l], z[l], 0, S->st);
+      launch(k_smooth_pair<T, D>, pg, pblk, 0, s, sh, (const T*)r[l], z[l], 1, S->st);
     }
     const Shape sc = S->lv[l + 1];
     launch(k_restrict<T, D>, blocks_for(sc.size(), 256, cap), 256, 0, s, sh, sc, r[l], z[l], r[l + 1], S->st);
@@ -668,11 +761,12 @@ static void launch_vcycle(fm_mgpcg* S, cudaStream_t s, bool dot_last, bool recen
     const Shape sc = S->lv[l + 1];
     const unsigned nb = blocks_for(sh.size(), 256, cap);
     launch(k_prolong<T, D>, nb, 256, 0, s, sh, sc, z[l], z[l + 1], S->st);
+    const dim3 pg = pair_grid(sh);
     for (int it = 0; it < P.pre_post; ++it) {
-      launch(k_smooth<T, D, false>, nb, 256, 0, s, sh, r[l], z[l], 1, nullptr, S->st);
+      launch(k_smooth_pair<T, D>, pg, pblk, 0, s, sh, (const T*)r[l], z[l], 1, S->st);
       const bool last = dot_last && l == 0 && it == P.pre_post - 1;
       if (last) launch(k_smooth<T, D, true>, kRedBlocks, kRedThreads, 0, s, sh, r[l], z[l], 0, S->part, S->st);
-      else launch(k_smooth<T, D, false>, nb, 256, 0, s, sh, r[l], z[l], 0, nullptr, S->st);
+      else launch(k_smooth_pair<T, D>, pg, pblk, 0, s, sh, (const T*)r[l], z[l], 0, S->st);
     }
   }
   if (dot_last && L == 1) {
@@ -746,11 +840,31 @@ static int build_loop_graph(fm_mgpcg* S) {
   return status;
 }
 
+// The prologue (~45 kernels, internal buffers only) captured once into a graph.
+template <typename T>
+static int build_prologue_graph(fm_mgpcg* S) {
+  cudaGraph_t graph;
+  if (cudaStreamBeginCapture(S->cap, cudaStreamCaptureModeThreadLocal) != cudaSuccess) return FM_ERR_CUDA;
+  const long long before = g_launch_count.load();
+  if (S->g.dim == 3) launch_prologue<T, 3>(S, S->cap); else launch_prologue<T, 2>(S, S->cap);
+  S->prologue_kernels = g_launch_count.load() - before;
+  g_launch_count.fetch_sub(S->prologue_kernels);  // captured, not executed
+  if (cudaStreamEndCapture(S->cap, &graph) != cudaSuccess) return FM_ERR_CUDA;
+  const cudaError_t e = cudaGraphInstantiate(&S->prologue, graph, 0);
+  cudaGraphDestroy(graph);
+  if (e != cudaSuccess) { S->prologue = nullptr; return FM_ERR_CUDA; }
+  return FM_OK;
+}
+
 template <typename T>
 static int run_solve(fm_mgpcg* S, cudaStream_t s, int* iters, double* rtr) {
   const int D = S->g.dim;
-  if (D == 3) launch_prologue<T, 3>(S, s); else launch_prologue<T, 2>(S, s);
-  if (check_cuda()) return FM_ERR_CUDA;
+  if (!S->prologue) {
+    const int e = build_prologue_graph<T>(S);
+    if (e) return e;
+  }
+  if (cudaGraphLaunch(S->prologue, s) != cudaSuccess) return FM_ERR_CUDA;
+  count_launch(S->prologue_kernels);
   if (S->P.check_every == 0) {
     if (!S->loop) {
       int e = build_loop_graph<T>(S);
@@ -889,6 +1003,7 @@ int fm_mgpcg_destroy(fm_mgpcg* S) {
   if (S->st) cudaFree(S->st);
   if (S->h_st) cudaFreeHost(S->h_st);
   if (S->chunk) cudaGraphExecDestroy(S->chunk);
+  if (S->prologue) cudaGraphExecDestroy(S->prologue);
   if (S->loop) cudaGraphExecDestroy(S->loop);
   if (S->cap) cudaStreamDestroy(S->cap);
   free(S);
