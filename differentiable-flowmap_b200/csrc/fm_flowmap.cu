@@ -23,26 +23,27 @@ constexpr int kThreads = 256;
 
 // Midpoint (RK2) / RK4 backtrace from X through u0 (3D/flowmap.py:210-219, :257-262).
 template <typename T, int D, int RK>
-__device__ __forceinline__ void backtrace(const Mac<T>& u0, const fm_grid& g, const T* X, T inv_dx, T dt, T* p) {
+__device__ __forceinline__ void backtrace(const Mac<T>& u0, const fm_grid& g, const Q2Lim<T>& lim, const T* X,
+                                          T inv_dx, T dt, T* p) {
   T v[3], vs[3], q[3] = {0, 0, 0};
-  q2_mac_val<T, D>(u0, g, X, inv_dx, v);
+  q2_mac_val<T, D>(u0, g, lim, X, inv_dx, v);
 #pragma unroll
   for (int a = 0; a < D; ++a) q[a] = X[a] - v[a] * dt * (T)0.5;
   if constexpr (RK == 2) {
-    q2_mac_val<T, D>(u0, g, q, inv_dx, v);
+    q2_mac_val<T, D>(u0, g, lim, q, inv_dx, v);
 #pragma unroll
     for (int a = 0; a < D; ++a) p[a] = X[a] - v[a] * dt;
   } else {
     // v1 + 2 v2 + 2 v3 + v4 accumulated left to right as the stages complete
 #pragma unroll
     for (int a = 0; a < D; ++a) vs[a] = v[a];
-    q2_mac_val<T, D>(u0, g, q, inv_dx, v);
+    q2_mac_val<T, D>(u0, g, lim, q, inv_dx, v);
 #pragma unroll
     for (int a = 0; a < D; ++a) { vs[a] = vs[a] + (T)2 * v[a]; q[a] = X[a] - v[a] * dt * (T)0.5; }
-    q2_mac_val<T, D>(u0, g, q, inv_dx, v);
+    q2_mac_val<T, D>(u0, g, lim, q, inv_dx, v);
 #pragma unroll
     for (int a = 0; a < D; ++a) { vs[a] = vs[a] + (T)2 * v[a]; q[a] = X[a] - v[a] * dt; }
-    q2_mac_val<T, D>(u0, g, q, inv_dx, v);
+    q2_mac_val<T, D>(u0, g, lim, q, inv_dx, v);
 #pragma unroll
     for (int a = 0; a < D; ++a) p[a] = X[a] - (vs[a] + v[a]) / (T)6.0 * dt;
   }
@@ -63,9 +64,10 @@ __global__ void __launch_bounds__(kThreads) k_advect_u_grid(fm_grid g, T dx, T d
   T X[3] = {0, 0, 0}, p[3] = {0, 0, 0};
   node_pos<T, D>(c, i, j, k, dx, X);
   const T inv_dx = (T)1 / dx;
-  backtrace<T, D, RK>(u0, g, X, inv_dx, dt, p);
+  const Q2Lim<T> lim(g);
+  backtrace<T, D, RK>(u0, g, lim, X, inv_dx, dt, p);
   CompStencil<T, D> st;
-  st.setup(g, c, p, inv_dx);
+  st.setup(lim, c, p, inv_dx);
   pick(u2, c)[q] = st.eval(pick(u1, c), s);
   if (u1b.c[0] != nullptr) pick(u2b, c)[q] = st.eval(pick(u1b, c), s);
 }
@@ -82,11 +84,12 @@ __global__ void __launch_bounds__(kThreads) k_advect_scalar_grid(fm_grid g, T dx
   T X[3] = {0, 0, 0}, p[3] = {0, 0, 0};
   node_pos<T, D>(-1, i, j, k, dx, X);
   const T inv_dx = (T)1 / dx;
-  backtrace<T, D, RK>(u0, g, X, inv_dx, dt, p);
+  const Q2Lim<T> lim(g);
+  backtrace<T, D, RK>(u0, g, lim, X, inv_dx, dt, p);
   Q2<T, false> ax, ay, az;
-  ax.setup(p[0] * inv_dx, (T)0.5, g.n[0]);
-  ay.setup(p[1] * inv_dx, (T)0.5, g.n[1]);
-  if (D == 3) az.setup(p[2] * inv_dx, (T)0.5, g.n[2]);
+  ax.setup(p[0] * inv_dx, (T)0.5, lim.h5[0]);
+  ay.setup(p[1] * inv_dx, (T)0.5, lim.h5[1]);
+  if (D == 3) az.setup(p[2] * inv_dx, (T)0.5, lim.h5[2]);
   s2[q] = q2_val<T, D, false>(s1, s, ax, ay, az);
   if (s1b != nullptr) s2b[q] = q2_val<T, D, false>(s1b, s, ax, ay, az);
 }
@@ -106,10 +109,10 @@ struct MarchJobs {
 
 // One RK stage: velocity k = u(pos) and, with the Jacobian, d = (grad u)(pos) . t.
 template <typename T, int D, bool WT>
-__device__ __forceinline__ void march_eval(const Mac<T>& u, const fm_grid& g, const T* pos, const T* t, T inv_dx,
-                                           T* k, T* d) {
-  if constexpr (WT) q2_mac_grad_dot<T, D>(u, g, pos, inv_dx, t, k, d);
-  else q2_mac_val<T, D>(u, g, pos, inv_dx, k);
+__device__ __forceinline__ void march_eval(const Mac<T>& u, const fm_grid& g, const Q2Lim<T>& lim, const T* pos,
+                                           const T* t, T inv_dx, T* k, T* d) {
+  if constexpr (WT) q2_mac_grad_dot<T, D>(u, g, lim, pos, inv_dx, t, k, d);
+  else q2_mac_val<T, D>(u, g, lim, pos, inv_dx, k);
 }
 
 // RK2_grid / RK4_grid (WT) and RK*_grid_only_psi (!WT) for one node, in place.
@@ -127,12 +130,13 @@ __device__ __forceinline__ void march_node(const Mac<T>& u, const fm_grid& g, T 
   const T neg_dt = -dt;
   const T h = (T)0.5 * neg_dt;
   const T inv_dx = (T)1 / dx;
+  const Q2Lim<T> lim(g);
   T k[3], d[3] = {0, 0, 0}, pos[3] = {0, 0, 0}, tt[3] = {0, 0, 0};
-  march_eval<T, D, WT>(u, g, P, Tv, inv_dx, k, d);
+  march_eval<T, D, WT>(u, g, lim, P, Tv, inv_dx, k, d);
   if constexpr (RK == 2) {
 #pragma unroll
     for (int a = 0; a < D; ++a) { pos[a] = P[a] + h * k[a]; tt[a] = Tv[a] + h * d[a]; }
-    march_eval<T, D, WT>(u, g, pos, tt, inv_dx, k, d);
+    march_eval<T, D, WT>(u, g, lim, pos, tt, inv_dx, k, d);
 #pragma unroll
     for (int a = 0; a < D; ++a) {
       psi[a * N + q] = P[a] + neg_dt * k[a];
@@ -147,7 +151,7 @@ __device__ __forceinline__ void march_node(const Mac<T>& u, const fm_grid& g, T 
       pos[a] = P[a] + h * k[a];
       tt[a] = Tv[a] + h * d[a];
     }
-    march_eval<T, D, WT>(u, g, pos, tt, inv_dx, k, d);  // stage 2
+    march_eval<T, D, WT>(u, g, lim, pos, tt, inv_dx, k, d);  // stage 2
 #pragma unroll
     for (int a = 0; a < D; ++a) {
       ks[a] = ks[a] + (T)2 * k[a];
@@ -155,7 +159,7 @@ __device__ __forceinline__ void march_node(const Mac<T>& u, const fm_grid& g, T 
       pos[a] = P[a] + h * k[a];
       tt[a] = Tv[a] + h * d[a];
     }
-    march_eval<T, D, WT>(u, g, pos, tt, inv_dx, k, d);  // stage 3
+    march_eval<T, D, WT>(u, g, lim, pos, tt, inv_dx, k, d);  // stage 3
 #pragma unroll
     for (int a = 0; a < D; ++a) {
       ks[a] = ks[a] + (T)2 * k[a];
@@ -163,7 +167,7 @@ __device__ __forceinline__ void march_node(const Mac<T>& u, const fm_grid& g, T 
       pos[a] = P[a] + (T)1.0 * neg_dt * k[a];
       tt[a] = Tv[a] + (T)1.0 * neg_dt * d[a];
     }
-    march_eval<T, D, WT>(u, g, pos, tt, inv_dx, k, d);  // stage 4
+    march_eval<T, D, WT>(u, g, lim, pos, tt, inv_dx, k, d);  // stage 4
     const T c6 = neg_dt * (T)1 / (T)6;
 #pragma unroll
     for (int a = 0; a < D; ++a) {
@@ -205,7 +209,7 @@ __global__ void __launch_bounds__(kThreads) k_pullback_u(fm_grid g, T dx, Mac<T>
   T p[3] = {0, 0, 0}, v[3];
 #pragma unroll
   for (int a = 0; a < D; ++a) p[a] = psi_c[a * N + q];
-  q2_mac_val<T, D>(u0, g, p, (T)1 / dx, v);
+  q2_mac_val<T, D>(u0, g, Q2Lim<T>(g), p, (T)1 / dx, v);
   T acc = 0;
 #pragma unroll
   for (int a = 0; a < D; ++a) acc += T_c[a * N + q] * v[a];
@@ -224,7 +228,7 @@ __global__ void __launch_bounds__(kThreads) k_pullback_scalar(fm_grid g, T dx, c
   T p[3] = {0, 0, 0};
 #pragma unroll
   for (int a = 0; a < D; ++a) p[a] = psi[a * N + q];
-  T acc = q2_scalar<T, D>(s0, g, p, (T)1 / dx);
+  T acc = q2_scalar<T, D>(s0, g, Q2Lim<T>(g), p, (T)1 / dx);
   if (beta != (T)0) acc = acc + beta * base[q];
   out[q] = alpha * acc;
 }
@@ -242,7 +246,7 @@ __global__ void __launch_bounds__(kThreads) k_accumulate(fm_grid g, T dx, T dt, 
   T p[3] = {0, 0, 0}, v[3];
 #pragma unroll
   for (int a = 0; a < D; ++a) p[a] = phi_c[a * N + q];
-  q2_mac_val<T, D>(f, g, p, (T)1 / dx, v);
+  q2_mac_val<T, D>(f, g, Q2Lim<T>(g), p, (T)1 / dx, v);
   T Fv = 0, Fv23 = 0, Fv16 = 0;
 #pragma unroll
   for (int a = 0; a < D; ++a) {
