@@ -329,6 +329,9 @@ VCYCLE_CASES = [
     ((16, 16, 16), 2, 2, 50, 0),
     ((48, 48), 2, 2, 10, 1),
     ((160, 160), 2, 1, 3, 0),
+    # innermost extents 18 / 42 (not multiples of 4) and an odd bottom extent (9)
+    ((16, 16, 18), 2, 2, 50, 0),
+    ((32, 42), 2, 2, 20, 1),
 ]
 
 
