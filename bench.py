@@ -51,6 +51,12 @@ def parse():
     ap.add_argument("--no-roofline", action="store_true",
                     help="skip the dominant-kernel roofline timing (used for profiler runs, which need W >= 1 only; "
                          "a reported bench value needs W >= 3)")
+    ap.add_argument("--workload", default="gradient", choices=["gradient", "poisson"],
+                    help="gradient: the headline 3D gradient benchmark; poisson: the mixed-precision Poisson solve "
+                         "(seeded k^-5/3 divergence RHS, all-Neumann, --poisson-res^3)")
+    ap.add_argument("--poisson-res", type=int, default=256)
+    ap.add_argument("--poisson-inner-tol", type=float, default=1e-8,
+                    help="relative z.r tolerance of the FP32 inner solves of the mixed Poisson solve")
     return ap.parse_args()
 
 
@@ -175,10 +181,92 @@ def run_reference(a):
 # ---------------------------------------------------------------------------
 # GPU arm
 # ---------------------------------------------------------------------------
+def run_poisson(a):
+    """Mixed-precision Poisson benchmark: FP32 MGPCG inner solves (FP32
+    hierarchy), FP64 outer defect correction to |r|/|b| <= 1e-10, next to the
+    plain FP32 MGPCG to |r|/|b| <= 1e-6; both pressures compared with an FP64
+    MGPCG solve of the same system in the mean-zero gauge."""
+    import numpy as np
+    import torch
+
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    torch.cuda.set_device(local)
+    dev = torch.device("cuda", local)
+    fm = importlib.import_module("differentiable-flowmap_b200")
+    C = importlib.import_module("differentiable-flowmap_b200.configs")
+    n = a.poisson_res
+    shape = (n, n, n)
+    levels = int(np.log2(n)) - 3 + 1
+    b = C.poisson_spectrum_rhs(n, seed=30)
+    d_b = torch.tensor(b, device=dev)
+    b64 = d_b.double()
+    b64 -= b64.mean()
+    bnorm2 = float((b64 * b64).sum())
+
+    def gauge(x):
+        x = x.double()
+        return x - x.mean()
+
+    # FP64 reference solve
+    s64 = fm.MGPCG(shape, torch.float64, levels=levels, abs_tol=1e-26 * bnorm2, rel_tol=0.0, eps=0.0, max_iters=400,
+                   check_every=4)
+    x64 = torch.zeros(shape, dtype=torch.float64, device=dev)
+    it64, _ = s64.solve(b64, x64)
+    ref = gauge(x64)
+    refn = float(ref.norm())
+    del s64
+
+    def timed(fn):
+        for _ in range(a.warmup):
+            fn()
+        torch.cuda.synchronize(dev)
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record()
+        for _ in range(a.steps):
+            out = fn()
+        e1.record()
+        torch.cuda.synchronize(dev)
+        return e0.elapsed_time(e1) / a.steps, out
+
+    # plain FP32 MGPCG, |r| <= 1e-6 |b| (rTr <= 1e-12 |b|^2)
+    sp = fm.MGPCG(shape, torch.float32, levels=levels, abs_tol=1e-12 * bnorm2, rel_tol=0.0, max_iters=400,
+                  check_every=0)
+    xp = torch.zeros(shape, device=dev)
+    ms_plain, _ = timed(lambda: sp.solve(d_b, xp))
+    it_plain = sp.last_iters
+    err_plain = float((gauge(xp) - ref).norm()) / refn
+    del sp
+
+    # mixed: FP32 inner solves, FP64 defect correction to 1e-10
+    sm = fm.MGPCG(shape, torch.float32, levels=levels, abs_tol=0.0, rel_tol=a.poisson_inner_tol, max_iters=100,
+                  check_every=0)
+    xm = torch.empty(shape, dtype=torch.float64, device=dev)
+    work = torch.empty(shape, dtype=torch.float64, device=dev)
+    ms_mixed, (xm, outer, inner, rel) = timed(lambda: sm.solve_mixed(d_b, xm, rel_tol=1e-10, work=work))
+    err_mixed = float((gauge(xm) - ref).norm()) / refn
+    if rank == 0:
+        line = {"metric": f"mixed-precision Poisson solve time, {n}^3 all-Neumann, |r|/|b| <= 1e-10",
+                "value": ms_mixed, "unit": "ms", "n_gpus": 1, "steps": a.steps, "warmup": a.warmup,
+                "ms_per_step": ms_mixed, "higher_is_better": False, "scaling": "weak", "vs_baseline": None,
+                "dtype": "f32 (inner) / f64 (outer)", "data": "synthetic",
+                "config": {"workload": f"Poisson {n}^3, divergence of a seeded k^-5/3 velocity (seed 30)",
+                           "levels": levels, "inner_rel_tol_zr": a.poisson_inner_tol},
+                "mixed": {"ms": ms_mixed, "outer_corrections": outer, "inner_pcg_iters": inner,
+                          "rel_residual_fp64": rel, "pressure_rel_err_vs_fp64": err_mixed},
+                "plain_fp32": {"ms": ms_plain, "pcg_iters": it_plain, "target_rel_residual": 1e-6,
+                               "pressure_rel_err_vs_fp64": err_plain},
+                "fp64_reference": {"pcg_iters": it64, "abs_tol_rTr": 1e-26 * bnorm2}}
+        print(json.dumps(line), flush=True)
+    return 0
+
+
 def main():
     a = parse()
     if a.impl == "reference":
         return run_reference(a)
+    if a.workload == "poisson":
+        return run_poisson(a)
 
     import torch
     import torch.distributed as dist

@@ -98,6 +98,7 @@ SIGNATURES = {
     "fm_advect_u_grid_pair": [GP, I, I, D, D] + [P] * 15 + [P],
     "fm_advect_scalar_grid_pair": [GP, I, I, D, D] + [P] * 7 + [P],
     "fm_mg_vcycle": [P, P, P, P],
+    "fm_mgpcg_solve_dc": [P, I, P, P, P, D, I, P, C.POINTER(I), C.POINTER(I), C.POINTER(D)],
 }
 RESTYPES = {"fm_launch_count": C.c_longlong}
 SIGNATURES["fm_launch_count"] = [I]

@@ -97,3 +97,53 @@ def shape2d_inputs(res=256, seed_rect=10, seed_disc=11, seed_u=12, u_std=0.01):
     rng = np.random.default_rng(seed_u)
     u0 = split_central_vector(rng.normal(0.0, u_std, size=(2, res, res)))
     return u0, rho0, rho_t
+
+
+# ---------------------------------------------------------------------------
+# Mixed-precision Poisson benchmark (256^3 cell-centred, Neumann walls)
+# ---------------------------------------------------------------------------
+def spectrum_velocity(res, seed=30, dtype=np.float32):
+    """Random cell-centred velocity (dim, *res) with an isotropic E(k) ~ k^(-5/3)
+    spectrum: per-mode amplitude |k|^(-11/6), uniform random phases, |k| >= 1,
+    the mean and the Nyquist planes zeroed; built by inverse FFT, unit RMS."""
+    rng = np.random.default_rng(seed)
+    res = tuple(res)
+    dim = len(res)
+    ks = [np.fft.fftfreq(n, d=1.0 / n) for n in res[:-1]] + [np.fft.rfftfreq(res[-1], d=1.0 / res[-1])]
+    K = np.meshgrid(*ks, indexing="ij")
+    kmag = np.sqrt(sum(k.astype(np.float64) ** 2 for k in K))
+    amp = np.zeros_like(kmag)
+    amp[kmag >= 1] = kmag[kmag >= 1] ** (-11.0 / 6.0)
+    for k, n in zip(K, res):
+        amp[np.abs(k) == n // 2] = 0.0  # Nyquist planes
+    out = np.empty((dim,) + res, dtype=np.float64)
+    for c in range(dim):
+        phase = rng.uniform(0.0, 2.0 * np.pi, size=amp.shape)
+        out[c] = np.fft.irfftn(amp * np.exp(1j * phase), s=res, axes=tuple(range(dim)))
+    out /= np.sqrt(np.mean(out ** 2))
+    return out.astype(dtype)
+
+
+def divergence_rhs(u_faces, dtype=np.float32):
+    """Cell divergence of a MAC velocity with zero normal velocity on the walls
+    (apply_bc + divergence, 3D/mgpcg.py:368-399): sum over axes of u[i+1] - u[i]."""
+    dim = len(u_faces)
+    div = None
+    for c, f in enumerate(u_faces):
+        f = np.array(f, dtype=np.float64, copy=True)
+        idx0 = [slice(None)] * dim
+        idx1 = [slice(None)] * dim
+        idx0[c] = 0
+        idx1[c] = -1
+        f[tuple(idx0)] = 0.0
+        f[tuple(idx1)] = 0.0
+        d = np.diff(f, axis=c)
+        div = d if div is None else div + d
+    return div.astype(dtype)
+
+
+def poisson_spectrum_rhs(res=256, seed=30):
+    """RHS of the mixed-precision Poisson benchmark: the divergence of the
+    seeded k^(-5/3) velocity, cell-centred -> faces -> divergence (FP32)."""
+    vc = spectrum_velocity((res,) * 3 if np.isscalar(res) else res, seed=seed)
+    return divergence_rhs(split_central_vector(vc))

@@ -51,6 +51,8 @@ struct DevState {
   // cumulative over all solves since create / the last stats reset
   long long solves, iters_total, not_converged, nonfinite_count;
   long long bodies;  // while-loop bodies executed (device mode), for the launch count
+  // outer defect correction (fm_mgpcg_solve_dc): mean of b, |b - mean|^2, |r|^2
+  double dc_mean, dc_b2, dc_r2;
 };
 
 // ---------------------------------------------------------------------------
@@ -201,6 +203,71 @@ __global__ void __launch_bounds__(kRedThreads) k_load_rhs(long n, const T* __res
     sum += (double)v;
   }
   block_reduce2(sum, 0.0, part + 2 * blockIdx.x);
+}
+
+// ---------------------------------------------------------------------------
+// outer defect correction in FP64 around FP32 MGPCG solves (fm_mgpcg_solve_dc)
+// ---------------------------------------------------------------------------
+template <typename TB>
+__global__ void __launch_bounds__(kRedThreads) k_dc_sum(long n, const TB* __restrict__ b, double* __restrict__ part) {
+  double sum = 0;
+  FM_GRID_STRIDE(q, n) sum += (double)b[q];
+  block_reduce2(sum, 0.0, part + 2 * blockIdx.x);
+}
+
+// which = 0: dc_mean = sum / n;  1: dc_b2 = dc_r2 = sum of squares;  2: dc_r2 = sum of squares
+__global__ void k_dc_fin(DevState* st, const double* part, double n, int which) {
+  double a, b;
+  sum_partials(part, a, b);
+  if (threadIdx.x == 0) {
+    if (which == 0) st->dc_mean = a / n;
+    else {
+      st->dc_r2 = b;
+      if (which == 1) st->dc_b2 = b;
+    }
+  }
+}
+
+// work = (b - mean) - A x in FP64, partial sums of work^2 (second slot).
+template <typename TB, int D>
+__global__ void __launch_bounds__(kRedThreads) k_dc_residual(Shape s, const TB* __restrict__ b,
+                                                             const double* __restrict__ x, double* __restrict__ work,
+                                                             double* __restrict__ part, const DevState* st) {
+  const double mean = st->dc_mean;
+  double acc = 0;
+  FM_GRID_STRIDE(q, s.size()) {
+    int i, j, k;
+    unflatten(s, q, i, j, k);
+    double diag;
+    const double nb = nb_sum<double, D>(x, s, i, j, k, diag);
+    const double r = ((double)b[q] - mean) - (diag * x[q] - nb);
+    work[q] = r;
+    acc += r * r;
+  }
+  block_reduce2(0.0, acc, part + 2 * blockIdx.x);
+}
+
+// Inner right-hand side r32 = work / |work| (unit norm keeps FP32 away from
+// underflow as the residual shrinks), x32 = 0, partial sums of r32 for the
+// recentring of the inner solve.
+__global__ void __launch_bounds__(kRedThreads) k_dc_load(long n, const double* __restrict__ work,
+                                                         float* __restrict__ r, float* __restrict__ x,
+                                                         double* __restrict__ part, const DevState* st) {
+  const double inv = 1.0 / sqrt(st->dc_r2);
+  double sum = 0;
+  FM_GRID_STRIDE(q, n) {
+    const float v = (float)(work[q] * inv);
+    r[q] = v;
+    x[q] = 0.f;
+    sum += (double)v;
+  }
+  block_reduce2(sum, 0.0, part + 2 * blockIdx.x);
+}
+
+// x += |r| * e
+__global__ void k_dc_update(long n, double* __restrict__ x, const float* __restrict__ e, const DevState* st) {
+  const double s = sqrt(st->dc_r2);
+  FM_GRID_STRIDE(q, n) x[q] += s * (double)e[q];
 }
 
 // subtract_grad_p + apply_bc (3D/mgpcg.py:401-427)
@@ -1075,6 +1142,58 @@ int fm_mg_vcycle(fm_mgpcg* S, const void* r, void* z, void* stream) {
   }
   if (cudaMemcpyAsync(z, S->z[0], bytes, cudaMemcpyDeviceToDevice, s) != cudaSuccess) return FM_ERR_CUDA;
   return check_cuda();
+}
+
+int fm_mgpcg_solve_dc(fm_mgpcg* S, int b_dtype, const void* b, double* x, double* work, double rel_tol,
+                      int max_outer, void* stream, int* outer_iters, int* inner_iters, double* rel_res) {
+  if (!S || !b || !x || !work || max_outer < 0 || !(rel_tol >= 0.0)) return FM_ERR_ARG;
+  if (S->dtype != FM_F32 || (b_dtype != FM_F32 && b_dtype != FM_F64)) return FM_ERR_DTYPE;
+  cudaStream_t s = (cudaStream_t)stream;
+  const Shape s0 = S->lv[0];
+  const long n = s0.size();
+  const int D = S->g.dim;
+  const unsigned nb = blocks_for(n, 256, 148L * 16);
+  if (b_dtype == FM_F32) launch(k_dc_sum<float>, kRedBlocks, kRedThreads, 0, s, n, (const float*)b, S->part);
+  else launch(k_dc_sum<double>, kRedBlocks, kRedThreads, 0, s, n, (const double*)b, S->part);
+  launch(k_dc_fin, 1, 256, 0, s, S->st, S->part, (double)n, 0);
+  if (cudaMemsetAsync(x, 0, sizeof(double) * n, s) != cudaSuccess) return FM_ERR_CUDA;
+  auto residual = [&](int which) {
+    if (b_dtype == FM_F32) {
+      if (D == 3) launch(k_dc_residual<float, 3>, kRedBlocks, kRedThreads, 0, s, s0, (const float*)b, x, work, S->part, S->st);
+      else launch(k_dc_residual<float, 2>, kRedBlocks, kRedThreads, 0, s, s0, (const float*)b, x, work, S->part, S->st);
+    } else {
+      if (D == 3) launch(k_dc_residual<double, 3>, kRedBlocks, kRedThreads, 0, s, s0, (const double*)b, x, work, S->part, S->st);
+      else launch(k_dc_residual<double, 2>, kRedBlocks, kRedThreads, 0, s, s0, (const double*)b, x, work, S->part, S->st);
+    }
+    launch(k_dc_fin, 1, 256, 0, s, S->st, S->part, (double)n, which);
+  };
+  residual(1);
+  int outer = 0, inner = 0, status = FM_OK;
+  double rel = 0;
+  for (;;) {
+    if (cudaMemcpyAsync(S->h_st, S->st, sizeof(DevState), cudaMemcpyDeviceToHost, s) != cudaSuccess) return FM_ERR_CUDA;
+    if (cudaStreamSynchronize(s) != cudaSuccess) return FM_ERR_CUDA;
+    const double b2 = S->h_st->dc_b2, r2 = S->h_st->dc_r2;
+    rel = b2 > 0 ? sqrt(r2 / b2) : 0.0;
+    if (!isfinite(rel)) { status = FM_ERR_NONFINITE; break; }
+    if (rel <= rel_tol || r2 == 0.0) break;
+    if (outer >= max_outer) { status = FM_ERR_NOT_CONVERGED; break; }
+    launch(k_dc_load, kRedBlocks, kRedThreads, 0, s, n, (const double*)work, (float*)S->r[0], (float*)S->x, S->part,
+           (const DevState*)S->st);
+    int it = 0;
+    double rtr = 0;
+    const int st = run_solve<float>(S, s, &it, &rtr);  // reaching max_iters is fine: the outer loop corrects
+    inner += it;
+    if (st == FM_ERR_CUDA || st == FM_ERR_NONFINITE) { status = st; break; }
+    launch(k_dc_update, nb, 256, 0, s, n, x, (const float*)S->x, (const DevState*)S->st);
+    ++outer;
+    residual(2);
+  }
+  if (outer_iters) *outer_iters = outer;
+  if (inner_iters) *inner_iters = inner;
+  if (rel_res) *rel_res = rel;
+  if (check_cuda()) return FM_ERR_CUDA;
+  return status;
 }
 
 int fm_mgpcg_stats(fm_mgpcg* S, void* stream, int reset, fm_mg_stats* out) {

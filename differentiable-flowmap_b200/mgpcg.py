@@ -121,6 +121,28 @@ class MGPCG:
                    "fm_mg_vcycle")
         return z
 
+    def solve_mixed(self, b: torch.Tensor, x: Optional[torch.Tensor] = None, rel_tol: float = 1e-10,
+                    max_outer: int = 10, work: Optional[torch.Tensor] = None, stream=None):
+        """Mixed-precision solve: FP32 MGPCG inner solves (this FP32 solver) inside
+        an FP64 defect correction, until |b - A x| <= rel_tol |b| in FP64.
+        Returns (x FP64, outer corrections, inner PCG iterations, final relative residual)."""
+        if self.dtype != torch.float32:
+            raise _lib.FlowmapError(7, "solve_mixed needs an FP32 solver")
+        if tuple(b.shape) != self.N:
+            raise _lib.FlowmapError(1, "solve_mixed: b shape mismatch")
+        if x is None:
+            x = torch.empty(self.N, dtype=torch.float64, device=b.device)
+        if work is None:
+            work = torch.empty(self.N, dtype=torch.float64, device=b.device)
+        no, ni, rr = C.c_int(0), C.c_int(0), C.c_double(0)
+        st = _lib.lib().fm_mgpcg_solve_dc(self._h, _lib.dtype_code(b.dtype), _lib.ptr(b), _lib.ptr(x),
+                                          _lib.ptr(work), rel_tol, max_outer, _lib.stream_ptr(stream),
+                                          C.byref(no), C.byref(ni), C.byref(rr))
+        self.last_converged = st == 0
+        if st != 3 or self.raise_on_nonconvergence:
+            _lib.check(st, "fm_mgpcg_solve_dc")
+        return x, no.value, ni.value, rr.value
+
     # reference names -------------------------------------------------------
     def Poisson(self, *u, verbose: bool = False):
         self.project(u)

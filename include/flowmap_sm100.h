@@ -218,6 +218,22 @@ int fm_mgpcg_solve(fm_mgpcg *solver, const void *b, void *x, void *stream, int *
  * the solver's dtype; the solver's level-0 buffers are overwritten. */
 int fm_mg_vcycle(fm_mgpcg *solver, const void *r, void *z, void *stream);
 
+/* Mixed-precision solve of A x = b to a relative FP64 residual: FP32 MGPCG
+ * inner solves on `solver` (an FM_F32 handle; its tolerances set the inner
+ * accuracy) inside an FP64 outer defect correction.  The solver itself and its
+ * RBGS V-cycle are those of 3D/mgpcg.py:12-289; the outer loop has no
+ * reference counterpart (the reference solves in FP32 only).
+ *   b (b_dtype FM_F32 or FM_F64, cell grid) is recentred to mean zero in FP64;
+ *   x (FP64, cell grid) receives the solution, starting from 0;
+ *   work (FP64, cell grid) is caller-provided scratch.
+ * Loop: r = (b - mean b) - A x in FP64; stop when |r| <= rel_tol |b - mean b|;
+ * else solve A e = r/|r| in FP32 and x += |r| e.  At most max_outer
+ * corrections (FM_ERR_NOT_CONVERGED beyond).  outer_iters, inner_iters (total
+ * PCG iterations) and rel_res (final |r|/|b - mean b|) may be NULL.
+ * Synchronises `stream` once per correction. */
+int fm_mgpcg_solve_dc(fm_mgpcg *solver, int b_dtype, const void *b, double *x, double *work, double rel_tol,
+                      int max_outer, void *stream, int *outer_iters, int *inner_iters, double *rel_res);
+
 /* Cumulative solver outcome (synchronises `stream`).  reset != 0 zeroes the
  * counters afterwards.  The reference reports non-convergence only with a
  * print (3D/mgpcg.py:286-289); here it is counted. */

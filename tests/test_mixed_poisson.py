@@ -1,0 +1,99 @@
+"""Mixed-precision Poisson solve (fm_mgpcg_solve_dc): FP32 MGPCG inner solves
+inside an FP64 defect correction, on the seeded k^-5/3 divergence RHS.
+
+Checked against (1) an independent FP64 residual computed here with numpy,
+(2) an FP64 MGPCG solve of the same system on the GPU and (3) the FP64 oracle
+(the reference solver restated, 3D/mgpcg.py:207-289), pressures compared in the
+mean-zero gauge (the all-Neumann operator is singular).
+"""
+import numpy as np
+import pytest
+import torch
+
+from oracle import MGParams, Oracle
+
+pytestmark = pytest.mark.gpu
+
+
+def _laplacian64(x):
+    """A x for the all-Neumann 5/7-point operator (diag = in-domain neighbours)."""
+    out = np.zeros_like(x)
+    for a in range(x.ndim):
+        d = np.diff(x, axis=a)  # x[i+1] - x[i]
+        lo = [slice(None)] * x.ndim
+        hi = [slice(None)] * x.ndim
+        lo[a] = slice(0, -1)
+        hi[a] = slice(1, None)
+        out[tuple(lo)] -= d  # x[i] - x[i+1]
+        out[tuple(hi)] += d  # x[i+1] - x[i], i.e. x[j] - x[j-1] at j = i+1
+    return out
+
+
+def _gauge(x):
+    x = np.asarray(x, np.float64)
+    return x - x.mean()
+
+
+def _rhs(C, shape, seed=30):
+    return C.divergence_rhs(C.split_central_vector(C.spectrum_velocity(shape, seed=seed)))
+
+
+@pytest.mark.parametrize("shape", [(64, 64, 64), (128, 96), (48, 32, 40)])
+def test_mixed_solve_reaches_fp64_residual(fm, cuda, shape):
+    import importlib
+
+    C = importlib.import_module("differentiable-flowmap_b200.configs")
+    b = _rhs(C, shape)
+    levels = max(2, int(np.log2(min(shape))) - 3 + 1)
+    while any(n % (1 << (levels - 1)) for n in shape):
+        levels -= 1
+    sol = fm.MGPCG(shape, torch.float32, levels=levels, abs_tol=0.0, rel_tol=1e-8, max_iters=100, check_every=0)
+    x, outer, inner, rel = sol.solve_mixed(torch.tensor(b, device=cuda), rel_tol=1e-10, max_outer=12)
+    xh = x.cpu().numpy()
+    bh = b.astype(np.float64) - b.astype(np.float64).mean()
+    res = np.linalg.norm(bh - _laplacian64(xh)) / np.linalg.norm(bh)
+    assert rel <= 1e-10 and res <= 1.5e-10, (rel, res, outer, inner)
+    assert 1 <= outer <= 6
+    # FP64 MGPCG on the GPU, solved far past the mixed tolerance
+    s64 = fm.MGPCG(shape, torch.float64, levels=levels, abs_tol=0.0, rel_tol=1e-24, eps=0.0, max_iters=300,
+                   check_every=1)
+    x64 = torch.zeros(shape, dtype=torch.float64, device=cuda)
+    s64.solve(torch.tensor(bh, device=cuda), x64)
+    ref = _gauge(x64.cpu().numpy())
+    err = np.linalg.norm(_gauge(xh) - ref) / np.linalg.norm(ref)
+    assert err < 1e-8, err
+
+
+def test_mixed_solve_matches_oracle_fp64(fm, cuda):
+    import importlib
+
+    C = importlib.import_module("differentiable-flowmap_b200.configs")
+    shape = (32, 32, 32)
+    b = _rhs(C, shape, seed=31)
+    o = Oracle(shape, "f64")
+    bh = b.astype(np.float64)
+    x_ref = np.zeros(shape)
+    it, rtr, conv = o.mgpcg_solve(MGParams(3, 2, 50, 0, 200, 0.0, 1e-24, 0.0), bh, x_ref)
+    assert conv
+    sol = fm.MGPCG(shape, torch.float32, levels=3, abs_tol=0.0, rel_tol=1e-8, max_iters=100)
+    x, outer, inner, rel = sol.solve_mixed(torch.tensor(b, device=cuda), rel_tol=1e-11)
+    err = np.linalg.norm(_gauge(x.cpu().numpy()) - _gauge(x_ref)) / np.linalg.norm(_gauge(x_ref))
+    assert rel <= 1e-11 and err < 1e-9, (rel, err)
+
+
+def test_mixed_solve_fp64_rhs_and_limits(fm, cuda):
+    """FP64 right-hand side; max_outer = 0 reports the initial residual and
+    FM_ERR_NOT_CONVERGED; a zero right-hand side returns x = 0 at once."""
+    import importlib
+
+    C = importlib.import_module("differentiable-flowmap_b200.configs")
+    shape = (32, 32)
+    b = torch.tensor(_rhs(C, shape).astype(np.float64), device=cuda)
+    sol = fm.MGPCG(shape, torch.float32, levels=3, abs_tol=0.0, rel_tol=1e-8, max_iters=100)
+    x, outer, inner, rel = sol.solve_mixed(b, rel_tol=1e-10)
+    assert rel <= 1e-10 and outer >= 1
+    x0, outer0, inner0, rel0 = sol.solve_mixed(b, rel_tol=1e-10, max_outer=0)
+    assert outer0 == 0 and inner0 == 0 and abs(rel0 - 1.0) < 1e-12 and not sol.last_converged
+    assert float(x0.abs().max()) == 0.0
+    z, oz, iz, rz = sol.solve_mixed(torch.zeros_like(b), rel_tol=1e-10)
+    assert oz == 0 and float(z.abs().max()) == 0.0
