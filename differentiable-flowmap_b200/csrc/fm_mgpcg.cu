@@ -51,8 +51,9 @@ struct DevState {
   // cumulative over all solves since create / the last stats reset
   long long solves, iters_total, not_converged, nonfinite_count;
   long long bodies;  // while-loop bodies executed (device mode), for the launch count
-  // outer defect correction (fm_mgpcg_solve_dc): mean of b, |b - mean|^2, |r|^2
-  double dc_mean, dc_b2, dc_r2;
+  // outer defect correction (fm_mgpcg_solve_dc): mean of b, |b - mean|^2, |r|^2,
+  // and an rTr floor for the inner solves (0 outside a defect correction)
+  double dc_mean, dc_b2, dc_r2, dc_tol;
 };
 
 // ---------------------------------------------------------------------------
@@ -109,6 +110,35 @@ __device__ __forceinline__ T nb_sum(const T* __restrict__ x, const Shape& s, int
   if (D == 3) {
     if (k < s.s2 - 1) acc += x[q + 1]; else --nd;
     if (k > 0) acc += x[q - 1]; else --nd;
+  }
+  diag = (T)nd;
+  return acc;
+}
+
+// Storage of MG levels: the compute type T, or BF16 for the levels between the
+// finest and the cluster-resident ones when coarse_bf16 is set (FP32 solvers).
+__device__ __forceinline__ float to_c(float v) { return v; }
+__device__ __forceinline__ double to_c(double v) { return v; }
+__device__ __forceinline__ float to_c(__nv_bfloat16 v) { return __bfloat162float(v); }
+template <typename S, typename T>
+__device__ __forceinline__ S to_s(T v) {
+  if constexpr (std::is_same<S, __nv_bfloat16>::value) return __float2bfloat16_rn((float)v);
+  else return (S)v;
+}
+
+// nb_sum over a stored level (values converted to the compute type T)
+template <typename T, int D, typename S>
+__device__ __forceinline__ T nb_sum_s(const S* __restrict__ x, const Shape& s, int i, int j, int k, T& diag) {
+  T acc = 0;
+  int nd = 2 * D;
+  const long q = s.idx(i, j, k);
+  if (i < s.s0 - 1) acc += (T)to_c(x[q + (long)s.s1 * s.s2]); else --nd;
+  if (i > 0) acc += (T)to_c(x[q - (long)s.s1 * s.s2]); else --nd;
+  if (j < s.s1 - 1) acc += (T)to_c(x[q + s.s2]); else --nd;
+  if (j > 0) acc += (T)to_c(x[q - s.s2]); else --nd;
+  if (D == 3) {
+    if (k < s.s2 - 1) acc += (T)to_c(x[q + 1]); else --nd;
+    if (k > 0) acc += (T)to_c(x[q - 1]); else --nd;
   }
   diag = (T)nd;
   return acc;
@@ -264,6 +294,13 @@ __global__ void __launch_bounds__(kRedThreads) k_dc_load(long n, const double* _
   block_reduce2(sum, 0.0, part + 2 * blockIdx.x);
 }
 
+// rTr floor of the next inner solve (unit-norm right-hand side): a correction
+// only has to bring |r| down to rel_tol |b|, with a factor 2 margin; 0 clears it.
+__global__ void k_dc_set_tol(DevState* st, double rel_tol, int clear) {
+  const double t = clear ? 0.0 : 0.5 * rel_tol * sqrt(st->dc_b2 / st->dc_r2);
+  st->dc_tol = t * t;
+}
+
 // x += |r| * e
 __global__ void k_dc_update(long n, double* __restrict__ x, const float* __restrict__ e, const DevState* st) {
   const double s = sqrt(st->dc_r2);
@@ -348,6 +385,7 @@ __global__ void k_fin_beta(DevState* st, const double* part, double eps, double 
       st->zTr_old = a;
       double tol = abs_tol;
       if (rel_tol > 0 && a * rel_tol > tol) tol = a * rel_tol;
+      if (st->dc_tol > tol) tol = st->dc_tol;
       st->tol = tol;
       st->beta = 0;
       if (!isfinite(a)) { st->nonfinite = 1; finish_solve(st); }
@@ -446,26 +484,27 @@ __device__ __forceinline__ bool pair_coords(const Shape& s, int& i, int& j, int&
 
 // Neighbour sum (reference order +i, -i, +j, -j, +k, -k) and neighbour count
 // of cell (i, j, k) at 32-bit index q.
-template <typename T, int D>
-__device__ __forceinline__ T nb_sum32(const T* __restrict__ x, const Shape& s, unsigned q, int i, int j, int k,
+template <typename T, int D, typename S>
+__device__ __forceinline__ T nb_sum32(const S* __restrict__ x, const Shape& s, unsigned q, int i, int j, int k,
                                       int& nd) {
   const unsigned si = (unsigned)s.s1 * s.s2, sj = s.s2;
   T acc = 0;
   nd = 0;
-  if (i < s.s0 - 1) { acc += x[q + si]; ++nd; }
-  if (i > 0) { acc += x[q - si]; ++nd; }
-  if (j < s.s1 - 1) { acc += x[q + sj]; ++nd; }
-  if (j > 0) { acc += x[q - sj]; ++nd; }
+  if (i < s.s0 - 1) { acc += (T)to_c(x[q + si]); ++nd; }
+  if (i > 0) { acc += (T)to_c(x[q - si]); ++nd; }
+  if (j < s.s1 - 1) { acc += (T)to_c(x[q + sj]); ++nd; }
+  if (j > 0) { acc += (T)to_c(x[q - sj]); ++nd; }
   if (D == 3) {
-    if (k < s.s2 - 1) { acc += x[q + 1]; ++nd; }
-    if (k > 0) { acc += x[q - 1]; ++nd; }
+    if (k < s.s2 - 1) { acc += (T)to_c(x[q + 1]); ++nd; }
+    if (k > 0) { acc += (T)to_c(x[q - 1]); ++nd; }
   }
   return acc;
 }
 
 // smooth(l, phase) over pairs: only the cell of colour `phase` is updated.
-template <typename T, int D>
-__global__ void __launch_bounds__(kPairBX* kPairBY) k_smooth_pair(Shape s, const T* __restrict__ r, T* z, int phase,
+// S: storage type of the level (T, or BF16 with coarse_bf16).
+template <typename T, int D, typename S = T>
+__global__ void __launch_bounds__(kPairBX* kPairBY) k_smooth_pair(Shape s, const S* __restrict__ r, S* z, int phase,
                                                                  const DevState* st) {
   if (st->done) return;
   int i, j, k;
@@ -476,13 +515,13 @@ __global__ void __launch_bounds__(kPairBX* kPairBY) k_smooth_pair(Shape s, const
   if ((D == 3 ? k : j) >= (D == 3 ? s.s2 : s.s1)) return;
   const unsigned q = ((unsigned)i * s.s1 + j) * s.s2 + k;
   int nd;
-  const T nb = nb_sum32<T, D>(z, s, q, i, j, k, nd);
-  z[q] = div_nd(r[q] + nb, nd);
+  const T nb = nb_sum32<T, D, S>(z, s, q, i, j, k, nd);
+  z[q] = to_s<S>(div_nd((T)to_c(r[q]) + nb, nd));
 }
 
 // First red sweep from z == 0 over pairs (fuses z.fill(0)); optionally recentres r.
-template <typename T, int D>
-__global__ void __launch_bounds__(kPairBX* kPairBY) k_smooth_first_pair(Shape s, T* __restrict__ r, T* __restrict__ z,
+template <typename T, int D, typename S = T>
+__global__ void __launch_bounds__(kPairBX* kPairBY) k_smooth_first_pair(Shape s, S* __restrict__ r, S* __restrict__ z,
                                                                        const DevState* st, int recenter) {
   if (st->done) return;
   int i, j, k;
@@ -495,13 +534,13 @@ __global__ void __launch_bounds__(kPairBX* kPairBY) k_smooth_first_pair(Shape s,
   for (int c = 0; c < 2; ++c) {
     if (c == 1 && !has2) break;
     const unsigned q = q0 + c;
-    T rv = r[q];
-    if (recenter) { rv = rv - mean; r[q] = rv; }
+    T rv = (T)to_c(r[q]);
+    if (recenter) { rv = rv - mean; r[q] = to_s<S>(rv); }
     if (c == red_second) {
       const int ci = i, cj = D == 3 ? j : j + c, ck = D == 3 ? k + c : 0;
-      z[q] = div_nd(rv, diag_of<D>(s, ci, cj, ck));
+      z[q] = to_s<S>(div_nd(rv, diag_of<D>(s, ci, cj, ck)));
     } else {
-      z[q] = 0;
+      z[q] = to_s<S>((T)0);
     }
   }
 }
@@ -530,9 +569,10 @@ __global__ void __launch_bounds__(kRedThreads) k_smooth(Shape s, const T* __rest
 }
 
 // restrict(l) (3D/mgpcg.py:157-163) as a gather over the 2^D children.
-template <typename T, int D>
-__global__ void k_restrict(Shape sf, Shape sc, const T* __restrict__ rf, const T* __restrict__ zf,
-                           T* __restrict__ rc, const DevState* st) {
+// SF / SC: storage types of the fine and the coarse level.
+template <typename T, int D, typename SF = T, typename SC = T>
+__global__ void k_restrict(Shape sf, Shape sc, const SF* __restrict__ rf, const SF* __restrict__ zf,
+                           SC* __restrict__ rc, const DevState* st) {
   if (st->done) return;
   const T scale = (T)1.0 / (T)(D - 1.0);
   FM_GRID_STRIDE(q, sc.size()) {
@@ -548,22 +588,22 @@ __global__ void k_restrict(Shape sf, Shape sc, const T* __restrict__ rf, const T
           const int i = 2 * I + di, j = 2 * J + dj, k = D == 3 ? 2 * K + dk : 0;
           const long f = sf.idx(i, j, k);
           T diag;
-          const T nb = nb_sum<T, D>(zf, sf, i, j, k, diag);
-          const T res = rn_sub(rf[f], rn_sub(rn_mul(diag, zf[f]), nb));
+          const T nb = nb_sum_s<T, D, SF>(zf, sf, i, j, k, diag);
+          const T res = rn_sub((T)to_c(rf[f]), rn_sub(rn_mul(diag, (T)to_c(zf[f])), nb));
           acc = rn_add(acc, rn_mul(res, scale));
         }
-    rc[q] = acc;
+    rc[q] = to_s<SC>(acc);
   }
 }
 
 // prolongate(l) (3D/mgpcg.py:165-168)
-template <typename T, int D>
-__global__ void k_prolong(Shape sf, Shape sc, T* __restrict__ zf, const T* __restrict__ zc, const DevState* st) {
+template <typename T, int D, typename SF = T, typename SC = T>
+__global__ void k_prolong(Shape sf, Shape sc, SF* __restrict__ zf, const SC* __restrict__ zc, const DevState* st) {
   if (st->done) return;
   FM_GRID_STRIDE(q, sf.size()) {
     int i, j, k;
     unflatten(sf, q, i, j, k);
-    zf[q] += zc[sc.idx(i >> 1, j >> 1, D == 3 ? (k >> 1) : 0)];
+    zf[q] = to_s<SF>((T)to_c(zf[q]) + (T)to_c(zc[sc.idx(i >> 1, j >> 1, D == 3 ? (k >> 1) : 0)]));
   }
 }
 
@@ -671,6 +711,7 @@ struct fm_mgpcg {
   int lc;                      // levels lc .. L-1 run as one cluster launch (<= 0: per-level launches)
   int nc;                      // CTAs in that cluster
   size_t coarse_smem;
+  int bf16_hi;                 // levels 1 .. bf16_hi-1 stored in BF16 (0: none)
 };
 
 namespace fm {
@@ -786,16 +827,36 @@ static void launch_vcycle(fm_mgpcg* S, cudaStream_t s, bool dot_last, bool recen
                   (unsigned)sh.s0);
     return dim3((unsigned)((sh.s1 + 1) / 2 + kPairBX - 1) / kPairBX, (unsigned)(sh.s0 + kPairBY - 1) / kPairBY, 1);
   };
+  // level storage: T, or BF16 for levels 1 .. bf16_hi-1 (FP32 solvers with coarse_bf16)
+  using BF = __nv_bfloat16;
+  auto bf = [&](int l) { return std::is_same<T, float>::value && l >= 1 && l < S->bf16_hi; };
+  auto sweep = [&](int l, int phase) {
+    const Shape sh = S->lv[l];
+    if (bf(l)) launch(k_smooth_pair<T, D, BF>, pair_grid(sh), pblk, 0, s, sh, (const BF*)S->r[l], (BF*)S->z[l], phase, S->st);
+    else launch(k_smooth_pair<T, D>, pair_grid(sh), pblk, 0, s, sh, (const T*)r[l], z[l], phase, S->st);
+  };
   for (int l = 0; l < lc; ++l) {
     const Shape sh = S->lv[l];
     const dim3 pg = pair_grid(sh);
     for (int it = 0; it < P.pre_post; ++it) {
-      if (it == 0) launch(k_smooth_first_pair<T, D>, pg, pblk, 0, s, sh, r[l], z[l], S->st, l == 0 && recenter ? 1 : 0);
-      else launch(k_smooth_pair<T, D>, pg, pblk, 0, s, sh, (const T*)r[l], z[l], 0, S->st);
-      launch(k_smooth_pair<T, D>, pg, pblk, 0, s, sh, (const T*)r[l], z[l], 1, S->st);
+      if (it == 0) {
+        if (bf(l)) launch(k_smooth_first_pair<T, D, BF>, pg, pblk, 0, s, sh, (BF*)S->r[l], (BF*)S->z[l], S->st, 0);
+        else launch(k_smooth_first_pair<T, D>, pg, pblk, 0, s, sh, r[l], z[l], S->st, l == 0 && recenter ? 1 : 0);
+      } else {
+        sweep(l, 0);
+      }
+      sweep(l, 1);
     }
     const Shape sc = S->lv[l + 1];
-    launch(k_restrict<T, D>, blocks_for(sc.size(), 256, cap), 256, 0, s, sh, sc, r[l], z[l], r[l + 1], S->st);
+    const unsigned rb = blocks_for(sc.size(), 256, cap);
+    if (bf(l) && bf(l + 1))
+      launch(k_restrict<T, D, BF, BF>, rb, 256, 0, s, sh, sc, (const BF*)S->r[l], (const BF*)S->z[l], (BF*)S->r[l + 1], S->st);
+    else if (bf(l))
+      launch(k_restrict<T, D, BF, T>, rb, 256, 0, s, sh, sc, (const BF*)S->r[l], (const BF*)S->z[l], r[l + 1], S->st);
+    else if (bf(l + 1))
+      launch(k_restrict<T, D, T, BF>, rb, 256, 0, s, sh, sc, (const T*)r[l], (const T*)z[l], (BF*)S->r[l + 1], S->st);
+    else
+      launch(k_restrict<T, D>, rb, 256, 0, s, sh, sc, (const T*)r[l], (const T*)z[l], r[l + 1], S->st);
   }
   const Shape sb = S->lv[L - 1];
   if (S->lc > 0) {
@@ -827,13 +888,19 @@ static void launch_vcycle(fm_mgpcg* S, cudaStream_t s, bool dot_last, bool recen
     const Shape sh = S->lv[l];
     const Shape sc = S->lv[l + 1];
     const unsigned nb = blocks_for(sh.size(), 256, cap);
-    launch(k_prolong<T, D>, nb, 256, 0, s, sh, sc, z[l], z[l + 1], S->st);
-    const dim3 pg = pair_grid(sh);
+    if (bf(l) && bf(l + 1))
+      launch(k_prolong<T, D, BF, BF>, nb, 256, 0, s, sh, sc, (BF*)S->z[l], (const BF*)S->z[l + 1], S->st);
+    else if (bf(l))
+      launch(k_prolong<T, D, BF, T>, nb, 256, 0, s, sh, sc, (BF*)S->z[l], (const T*)z[l + 1], S->st);
+    else if (bf(l + 1))
+      launch(k_prolong<T, D, T, BF>, nb, 256, 0, s, sh, sc, z[l], (const BF*)S->z[l + 1], S->st);
+    else
+      launch(k_prolong<T, D>, nb, 256, 0, s, sh, sc, z[l], (const T*)z[l + 1], S->st);
     for (int it = 0; it < P.pre_post; ++it) {
-      launch(k_smooth_pair<T, D>, pg, pblk, 0, s, sh, (const T*)r[l], z[l], 1, S->st);
+      sweep(l, 1);
       const bool last = dot_last && l == 0 && it == P.pre_post - 1;
       if (last) launch(k_smooth<T, D, true>, kRedBlocks, kRedThreads, 0, s, sh, r[l], z[l], 0, S->part, S->st);
-      else launch(k_smooth_pair<T, D>, pg, pblk, 0, s, sh, (const T*)r[l], z[l], 0, S->st);
+      else sweep(l, 0);
     }
   }
   if (dot_last && L == 1) {
@@ -992,7 +1059,7 @@ int fm_mgpcg_create(const fm_grid* g, int dtype, const fm_mg_params* params, fm_
   if (P.levels < 2 || P.levels > kMaxLevels || P.pre_post < 1 || P.bottom < 0 || P.max_iters < 1 ||
       P.check_every < 0 || (P.bottom_mode != 0 && P.bottom_mode != 1))
     return FM_ERR_ARG;
-  if (P.coarse_bf16) return FM_ERR_ARG;  // not in this build
+  if (P.coarse_bf16 && dtype != FM_F32) return FM_ERR_ARG;
   for (int a = 0; a < g->dim; ++a)
     if (g->n[a] % (1 << (P.levels - 1)) != 0 || (g->n[a] >> (P.levels - 1)) < 1) return FM_ERR_SHAPE;
   fm_mgpcg* S = (fm_mgpcg*)calloc(1, sizeof(fm_mgpcg));
@@ -1009,8 +1076,25 @@ int fm_mgpcg_create(const fm_grid* g, int dtype, const fm_mg_params* params, fm_
     sh.s1 = g->n[1] >> l;
     sh.s2 = g->dim == 3 ? (g->n[2] >> l) : 1;
     S->lv[l] = sh;
-    ok = ok && cudaMalloc(&S->r[l], es * sh.size()) == cudaSuccess;
-    ok = ok && cudaMalloc(&S->z[l], es * sh.size()) == cudaSuccess;
+  }
+  // coarse levels in one cluster launch where they fit
+  plan_coarse(S, es);
+  if (S->lc > 0) {
+    const bool en = dtype == FM_F32 ? (g->dim == 3 ? enable_coarse_kernel<float, 3>(S->coarse_smem)
+                                                   : enable_coarse_kernel<float, 2>(S->coarse_smem))
+                                    : (g->dim == 3 ? enable_coarse_kernel<double, 3>(S->coarse_smem)
+                                                   : enable_coarse_kernel<double, 2>(S->coarse_smem));
+    if (!en) {
+      cudaGetLastError();
+      S->lc = -1;
+    }
+  }
+  // BF16 storage for the per-level coarse levels 1 .. lc-1 (needs the cluster path)
+  S->bf16_hi = (P.coarse_bf16 && S->lc > 1) ? S->lc : 0;
+  for (int l = 0; l < S->L; ++l) {
+    const size_t e = (l >= 1 && l < S->bf16_hi) ? sizeof(__nv_bfloat16) : es;
+    ok = ok && cudaMalloc(&S->r[l], e * S->lv[l].size()) == cudaSuccess;
+    ok = ok && cudaMalloc(&S->z[l], e * S->lv[l].size()) == cudaSuccess;
   }
   const long n0 = S->lv[0].size();
   ok = ok && cudaMalloc(&S->x, es * n0) == cudaSuccess;
@@ -1034,19 +1118,6 @@ int fm_mgpcg_create(const fm_grid* g, int dtype, const fm_mg_params* params, fm_
         e = g->dim == 3 ? cudaFuncSetAttribute(k_bottom<double, 3>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem)
                         : cudaFuncSetAttribute(k_bottom<double, 2>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
       if (e != cudaSuccess) S->bottom_smem = 0;
-    }
-  }
-  if (ok) {
-    plan_coarse(S, es);
-    if (S->lc > 0) {
-      const bool en = dtype == FM_F32 ? (g->dim == 3 ? enable_coarse_kernel<float, 3>(S->coarse_smem)
-                                                     : enable_coarse_kernel<float, 2>(S->coarse_smem))
-                                      : (g->dim == 3 ? enable_coarse_kernel<double, 3>(S->coarse_smem)
-                                                     : enable_coarse_kernel<double, 2>(S->coarse_smem));
-      if (!en) {
-        cudaGetLastError();
-        S->lc = -1;
-      }
     }
   }
   if (!ok) {
@@ -1180,6 +1251,7 @@ int fm_mgpcg_solve_dc(fm_mgpcg* S, int b_dtype, const void* b, double* x, double
     if (outer >= max_outer) { status = FM_ERR_NOT_CONVERGED; break; }
     launch(k_dc_load, kRedBlocks, kRedThreads, 0, s, n, (const double*)work, (float*)S->r[0], (float*)S->x, S->part,
            (const DevState*)S->st);
+    launch(k_dc_set_tol, 1, 1, 0, s, S->st, rel_tol, 0);
     int it = 0;
     double rtr = 0;
     const int st = run_solve<float>(S, s, &it, &rtr);  // reaching max_iters is fine: the outer loop corrects
@@ -1189,6 +1261,7 @@ int fm_mgpcg_solve_dc(fm_mgpcg* S, int b_dtype, const void* b, double* x, double
     ++outer;
     residual(2);
   }
+  launch(k_dc_set_tol, 1, 1, 0, s, S->st, 0.0, 1);
   if (outer_iters) *outer_iters = outer;
   if (inner_iters) *inner_iters = inner;
   if (rel_res) *rel_res = rel;

@@ -29,14 +29,17 @@ class MGPCG:
     def __init__(self, N: Sequence[int], dtype=torch.float32, *, base_level: int = 3, levels: Optional[int] = None,
                  pre_post: int = 2, bottom: int = 50, bottom_mode: int = 0, max_iters: int = 400,
                  abs_tol: float = 1e-12, rel_tol: float = 0.0, eps: float = 1e-12, check_every: int = 4,
-                 raise_on_nonconvergence: bool = False):
+                 raise_on_nonconvergence: bool = False, coarse_bf16: bool = False):
+        """coarse_bf16 (FP32 solvers): store the per-level coarse grids between the
+        finest level and the shared-memory-resident ones in BF16 (arithmetic stays
+        FP32); the preconditioner then no longer equals the FP32 V-cycle bit for bit."""
         self.N = tuple(int(n) for n in N)
         self.grid = GridSpec(self.N)
         self.dtype = dtype
         if levels is None:
             levels = int(math.log2(min(self.N))) - base_level + 1
         self.params = _lib.MGParams(levels, pre_post, bottom, bottom_mode, max_iters, abs_tol, rel_tol, eps,
-                                    check_every, 0)
+                                    check_every, int(coarse_bf16))
         self.raise_on_nonconvergence = raise_on_nonconvergence
         self._h = C.c_void_p()
         _lib.check(_lib.lib().fm_mgpcg_create(C.byref(self.grid.c_grid()), _lib.dtype_code(dtype),

@@ -36,6 +36,9 @@ def test_invalid_arguments_rejected_without_device(fm):
     assert lib.fm_mgpcg_create(C.byref(g), 0, C.byref(p), C.byref(h)) == 2
     p = fm._lib.MGParams(5, 2, 50, 0, 400, 1e-12, 0.0, 1e-12, 4, 0)  # 8 not divisible by 2^4
     assert lib.fm_mgpcg_create(C.byref(g), 0, C.byref(p), C.byref(h)) == 1
+    p = fm._lib.MGParams(2, 2, 50, 0, 400, 1e-12, 0.0, 1e-12, 4, 1)  # BF16 coarse levels need an FP32 solver
+    assert lib.fm_mgpcg_create(C.byref(g), 1, C.byref(p), C.byref(h)) == 2
+    assert lib.fm_mgpcg_solve_dc(None, 0, None, None, None, 1e-10, 5, None, None, None, None) == 2
     assert lib.fm_project(None, None, None, None, None, None, None, None) == 2
     assert lib.fm_mg_vcycle(None, None, None, None) == 2
 

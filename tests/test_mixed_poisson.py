@@ -81,6 +81,32 @@ def test_mixed_solve_matches_oracle_fp64(fm, cuda):
     assert rel <= 1e-11 and err < 1e-9, (rel, err)
 
 
+@pytest.mark.parametrize("shape,levels", [((128, 128, 128), 5), ((1024, 1024), 8)])
+def test_bf16_coarse_levels(fm, cuda, shape, levels):
+    """BF16 storage of the per-level coarse grids (64^3 at 128^3; 512^2, 256^2
+    at 1024^2): the mixed solve still reaches the FP64 tolerance, and one V-cycle
+    stays within BF16 rounding of the FP32 V-cycle."""
+    import importlib
+
+    C = importlib.import_module("differentiable-flowmap_b200.configs")
+    b = torch.tensor(_rhs(C, shape), device=cuda)
+    s32 = fm.MGPCG(shape, torch.float32, levels=levels, abs_tol=0.0, rel_tol=1e-8, max_iters=100)
+    sbf = fm.MGPCG(shape, torch.float32, levels=levels, abs_tol=0.0, rel_tol=1e-8, max_iters=100, coarse_bf16=True)
+    z32 = s32.apply_preconditioner(b)
+    zbf = sbf.apply_preconditioner(b)
+    dz = float((zbf - z32).norm() / z32.norm())
+    assert 0 < dz < 2e-2, dz  # BF16 keeps 8 significant bits on the coarse corrections
+    x, outer, inner, rel = sbf.solve_mixed(b, rel_tol=1e-10, max_outer=12)
+    x32, outer32, inner32, rel32 = s32.solve_mixed(b, rel_tol=1e-10, max_outer=12)
+    assert rel <= 1e-10 and outer <= outer32 + 2, (rel, outer, inner, outer32, inner32)
+    err = float((_gauge_t(x) - _gauge_t(x32)).norm() / _gauge_t(x32).norm())
+    assert err < 1e-8, err
+
+
+def _gauge_t(x):
+    return x - x.mean()
+
+
 def test_mixed_solve_fp64_rhs_and_limits(fm, cuda):
     """FP64 right-hand side; max_outer = 0 reports the initial residual and
     FM_ERR_NOT_CONVERGED; a zero right-hand side returns x = 0 at once."""
