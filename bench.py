@@ -51,9 +51,10 @@ def parse():
     ap.add_argument("--no-roofline", action="store_true",
                     help="skip the dominant-kernel roofline timing (used for profiler runs, which need W >= 1 only; "
                          "a reported bench value needs W >= 3)")
-    ap.add_argument("--workload", default="gradient", choices=["gradient", "poisson"],
+    ap.add_argument("--workload", default="gradient", choices=["gradient", "poisson", "vortex2d"],
                     help="gradient: the headline 3D gradient benchmark; poisson: the mixed-precision Poisson solve "
-                         "(seeded k^-5/3 divergence RHS, all-Neumann, --poisson-res^3)")
+                         "(seeded k^-5/3 divergence RHS, all-Neumann, --poisson-res^3); vortex2d: the 2D vortex "
+                         "optimisation gradient dL/dtheta (256^2, 100 steps, 4 vortices)")
     ap.add_argument("--poisson-res", type=int, default=256)
     ap.add_argument("--poisson-inner-tol", type=float, default=1e-8,
                     help="relative z.r tolerance of the FP32 inner solves of the mixed Poisson solve")
@@ -268,12 +269,73 @@ def run_poisson(a):
     return 0
 
 
+def run_vortex2d(a):
+    """2D vortex optimisation gradient: theta (4 vortices: strength, centre;
+    seed 0) -> u0 -> 100 steps (256^2, dt = 0.5 dx, reinit 10, RK2, solid-style
+    MGPCG) -> L = sum (omega - omega*)^2 (target: seed 1) -> adjoint -> dL/dtheta.
+    One bench step = one gradient; error of dL/dtheta vs an FP64 run."""
+    import numpy as np
+    import torch
+
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    torch.cuda.set_device(local)
+    dev = torch.device("cuda", local)
+    S = importlib.import_module("differentiable-flowmap_b200.simulator")
+    C = importlib.import_module("differentiable-flowmap_b200.configs")
+    vx = importlib.import_module("differentiable-flowmap_b200.vortex")
+
+    def problem(dtype, rel_tol, abs_tol=0.0, max_iters=400):
+        cfg = C.vortex2d_config(res=256, steps=100, reinit_every=10, dtype=dtype, rel_tol=rel_tol, abs_tol=abs_tol,
+                                max_iters=max_iters)
+        return vx.VortexProblem(S.LFM_Diff_Simulator(config=cfg, device=dev))
+
+    def timed(p, omt):
+        for _ in range(a.warmup):
+            p.gradient(theta, omt)
+        torch.cuda.synchronize(dev)
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record()
+        for _ in range(a.steps):
+            loss, dth = p.gradient(theta, omt)
+        e1.record()
+        torch.cuda.synchronize(dev)
+        return e0.elapsed_time(e1) / a.steps, loss, dth
+
+    theta = C.vortex2d_theta(0)
+    p32 = problem(torch.float32, 1e-6)
+    omt = p32.final_vorticity(C.vortex2d_theta(1))
+    ms, loss, dth = timed(p32, omt)
+    p64 = problem(torch.float64, 1e-20)
+    l64, d64 = p64.gradient(theta, omt.double())
+    # the reference solver's own criterion (solid MGPCG: absolute rTr < 1e-14)
+    pabs = problem(torch.float32, 0.0, abs_tol=1e-14, max_iters=100)
+    ms_abs, l_abs, d_abs = timed(pabs, omt)
+    line = {"metric": "2D vortex dL/dtheta evaluations/s, 256^2, 100 steps, 4 vortices", "value": 1e3 / ms,
+            "unit": "grads/s", "n_gpus": 1, "steps": a.steps, "warmup": a.warmup, "ms_per_step": ms,
+            "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic",
+            "config": {"workload": "2D vortex optimisation gradient, 256^2, dt 1/512, reinit 10, RK2, 12 parameters",
+                       "theta_seed": 0, "target_seed": 1},
+            "loss": loss, "dtheta": [float(x) for x in dth],
+            "solver": "relative z.r 1e-6",
+            "dtheta_rel_err_vs_fp64": float(np.linalg.norm(dth - d64) / np.linalg.norm(d64)),
+            "loss_rel_err_vs_fp64": abs(loss - l64) / abs(l64),
+            "reference_abs_criterion": {"solver": "absolute rTr < 1e-14, at most 100 iterations", "ms": ms_abs,
+                                        "grads_per_s": 1e3 / ms_abs,
+                                        "dtheta_rel_err_vs_fp64": float(np.linalg.norm(d_abs - d64) /
+                                                                        np.linalg.norm(d64)),
+                                        "loss_rel_err_vs_fp64": abs(l_abs - l64) / abs(l64)}}
+    print(json.dumps(line), flush=True)
+    return 0
+
+
 def main():
     a = parse()
     if a.impl == "reference":
         return run_reference(a)
     if a.workload == "poisson":
         return run_poisson(a)
+    if a.workload == "vortex2d":
+        return run_vortex2d(a)
 
     import torch
     import torch.distributed as dist

@@ -76,6 +76,27 @@ def shape2d_config(res=256, steps=200, reinit_every=12, rk=2, dt=0.01, dtype=tor
                          store_dtype=store_dtype, solver=solver)
 
 
+def vortex2d_config(res=256, steps=100, reinit_every=10, rk=2, dtype=torch.float32, rel_tol=1e-6, abs_tol=0.0,
+                    max_iters=400, check_every=0):
+    """2D vortex optimisation: res^2, dx = 1/res, dt = 0.5 dx, 100 steps, reinit
+    every 10, RK2, solid-style MGPCG (base level 4: 5 levels at 256^2, 20 bottom
+    sweeps as 10 x (R,B) + 10 x (B,R)), empty mask, no passive scalar."""
+    solver = SolverConfig(base_level=4, levels=max(2, int(math.log2(res)) - 4 + 1), bottom=20, bottom_mode=1,
+                          max_iters=max_iters, abs_tol=abs_tol, rel_tol=rel_tol,
+                          eps=1e-12 if dtype == torch.float32 else 0.0, check_every=check_every)
+    return FlowmapConfig(res=(res, res), dx=1.0 / res, dt=0.5 / res, total_steps=steps, reinit_every=reinit_every,
+                         RK_number=rk, backward_u=True, add_passive_scalar=False, dtype=dtype, solver=solver)
+
+
+def vortex2d_theta(seed=0, nv=4):
+    """theta = [w_0..w_{K-1}, cx_0..cx_{K-1}, cy_0..cy_{K-1}]: strengths U[-1,1],
+    centres U[0.25,0.75]^2."""
+    rng = np.random.default_rng(seed)
+    w = rng.uniform(-1.0, 1.0, nv)
+    c = rng.uniform(0.25, 0.75, (nv, 2))
+    return np.concatenate([w, c[:, 0], c[:, 1]])
+
+
 def shape2d_inputs(res=256, seed_rect=10, seed_disc=11, seed_u=12, u_std=0.01):
     """rho0: union of 3 rectangles (sides U[0.1,0.3]); rho*: union of 3 discs
     (radii U[0.05,0.15]); u0 cell-centred N(0, u_std^2) split to faces."""

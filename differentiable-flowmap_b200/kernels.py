@@ -197,3 +197,48 @@ def store(src, dst, stream=None):
 
 def laplacian(g: GridSpec, p, Ap, stream=None):
     check(_lib.lib().fm_laplacian(C.byref(g.c_grid()), _dt(p), ptr(p), ptr(Ap), stream_ptr(stream)), "fm_laplacian")
+
+
+# ---------------------------------------------------------------------------
+# 2D vortex problem
+# ---------------------------------------------------------------------------
+def _theta_arg(theta):
+    import numpy as _np
+
+    th = _np.ascontiguousarray(_np.asarray(theta, dtype=_np.float64))
+    if th.ndim != 1 or th.size % 3 != 0:
+        raise _lib.FlowmapError(2, "theta must hold 3K values [w.., cx.., cy..]")
+    return th, th.size // 3, th.ctypes.data_as(C.POINTER(C.c_double))
+
+
+def vortex_velocity_2d(g: GridSpec, dx: float, theta, ux, uy, stream=None):
+    """Faces of the point-vortex velocity of theta (split_central_vector of the centre values)."""
+    _chk_mac(g, (ux, uy), "u")
+    th, nv, tp = _theta_arg(theta)
+    check(_lib.lib().fm_vortex_velocity_2d(C.byref(g.c_grid()), _dt(ux), dx, nv, tp, ptr(ux), ptr(uy),
+                                           stream_ptr(stream)), "fm_vortex_velocity_2d")
+
+
+def vortex_velocity_grad_2d(g: GridSpec, dx: float, theta, lam_x, lam_y, stream=None):
+    """d<lam, u(theta)>/d theta as a device FP64 tensor of 3K entries."""
+    th, nv, tp = _theta_arg(theta)
+    work = torch.empty(592 * 3 * nv, dtype=torch.float64, device=lam_x.device)
+    grad = torch.empty(3 * nv, dtype=torch.float64, device=lam_x.device)
+    check(_lib.lib().fm_vortex_velocity_grad_2d(C.byref(g.c_grid()), _dt(lam_x), dx, nv, tp, ptr(lam_x), ptr(lam_y),
+                                                ptr(work), ptr(grad), stream_ptr(stream)),
+          "fm_vortex_velocity_grad_2d")
+    return grad
+
+
+def vorticity_2d(g: GridSpec, dx: float, ux, uy, omega, stream=None):
+    _chk_mac(g, (ux, uy), "u")
+    check(_lib.lib().fm_vorticity_2d(C.byref(g.c_grid()), _dt(ux), dx, ptr(ux), ptr(uy), ptr(omega),
+                                     stream_ptr(stream)), "fm_vorticity_2d")
+
+
+def vorticity_loss_2d(g: GridSpec, dx: float, ux, uy, omega_target, lam_x, lam_y, work, part, loss, stream=None):
+    """loss (device FP64, 1 entry) = sum (omega - omega*)^2; lam = (d omega/d u)^T 2 (omega - omega*)."""
+    _chk_mac(g, (ux, uy), "u")
+    check(_lib.lib().fm_vorticity_loss_2d(C.byref(g.c_grid()), _dt(ux), dx, ptr(ux), ptr(uy), ptr(omega_target),
+                                          ptr(work), ptr(part), ptr(lam_x), ptr(lam_y), ptr(loss), stream_ptr(stream)),
+          "fm_vorticity_loss_2d")

@@ -374,9 +374,14 @@ class LFM_Diff_Simulator(LFM_Simulator):
     def forward_step_midpoint(self, write_flow_map=True, write_passive=True, control_force_para=None):
         return self.step_midpoint(write_flow_map, write_passive, control_force_para)
 
-    def init_gradient(self, theta=None, target_passive=None):
+    def init_gradient(self, theta=None, target_passive=None, target_vorticity=None):
         """Loss and adjoint seed (3D/lfm_midpoint_diff_simulator.py:336-376, case 11):
-        L = sum (s - s*)^2, adj_passive = 2 (s - s*), adj_u = 0; psi, T reset."""
+        L = sum (s - s*)^2, adj_passive = 2 (s - s*), adj_u = 0; psi, T reset.
+        With ``target_vorticity`` (2D): L = sum (omega - omega*)^2 over the cells,
+        adj_u = (d omega / d u)^T 2 (omega - omega*), adj_passive = 0."""
+        if target_vorticity is not None:
+            self._seed_vorticity(target_vorticity)
+            return
         if target_passive is not None:
             self.target_passive = torch.empty(self.grid.shape, dtype=self.cfg.dtype, device=self.device)
             self.target_passive.copy_(_as_tensor(target_passive), non_blocking=True)
@@ -390,6 +395,29 @@ class LFM_Diff_Simulator(LFM_Simulator):
         diff = self.passive - self.target_passive
         self.adj_passive.copy_(2 * diff)
         self.loss = float(torch.sum(diff.double() ** 2))
+        self._finish_seed()
+
+    def _seed_vorticity(self, target_vorticity):
+        if self.dim != 2:
+            raise FlowmapError(1, "a vorticity loss needs a 2D simulator")
+        g, dev = self.grid, self.device
+        if getattr(self, "_vort_work", None) is None:
+            self._vort_target = torch.empty(g.shape, dtype=self.cfg.dtype, device=dev)
+            self._vort_work = torch.empty(g.shape, dtype=self.cfg.dtype, device=dev)
+            self._vort_part = torch.empty(592, dtype=torch.float64, device=dev)
+            self._vort_loss = torch.empty(1, dtype=torch.float64, device=dev)
+        self._vort_target.copy_(_as_tensor(target_vorticity), non_blocking=True)
+        self.final_ind = self.step_num[None] + 1
+        for c in range(self.dim):
+            self.H_prev[c].zero_()
+            self.H_prev_prev[c].zero_()
+        K.vorticity_loss_2d(g, self.dx, self.u[0], self.u[1], self._vort_target, self.adj_u[0], self.adj_u[1],
+                            self._vort_work, self._vort_part, self._vort_loss)
+        self.adj_passive.zero_()
+        self.loss = float(self._vort_loss.item())
+        self._finish_seed()
+
+    def _finish_seed(self):
         self.step_num[None] = self.final_ind
         _copy_mac(self.init_adj_u, self.adj_u)
         self.init_adj_passive.copy_(self.adj_passive)
@@ -489,14 +517,16 @@ class LFM_Diff_Simulator(LFM_Simulator):
             self.reset_to_identity(self.psi, self.psi_f, self.T_f)
 
     # --------------------------------------------------------- driver
-    def gradient(self, u0, passive0, target_passive):
-        """Full forward + adjoint: returns (loss, dL/du0 as a list of face tensors)."""
+    def gradient(self, u0, passive0=None, target_passive=None, target_vorticity=None):
+        """Full forward + adjoint: returns (loss, dL/du0 as a list of face tensors).
+        The loss is the final passive L2 (``target_passive``) or, in 2D, the final
+        vorticity L2 (``target_vorticity``)."""
         self.init(theta=u0, init_passive_np=passive0)
         while True:
             _, final = self.forward_step_midpoint()
             if final:
                 break
-        self.init_gradient(target_passive=target_passive)
+        self.init_gradient(target_passive=target_passive, target_vorticity=target_vorticity)
         while True:
             _, done = self.backtrack_step_midpoint()
             if done:

@@ -269,6 +269,33 @@ int fm_project_noalloc(const fm_grid *g, int dtype, const fm_mg_params *params, 
 /* Apply the Neumann Laplacian: Ap = A p (for tests and defect correction). */
 int fm_laplacian(const fm_grid *g, int dtype, const void *p, void *Ap, void *stream);
 
+/* ------------------------------------------------------------------------
+ * 2D vortex problem (the vortex optimisation's control map and loss).
+ * theta = [w_0..w_{K-1}, cx_0..cx_{K-1}, cy_0..cy_{K-1}], K <= 64, host array.
+ * ------------------------------------------------------------------------ */
+/* Face velocity of K Gaussian-core point vortices: at every cell centre X the
+ * sum of angular_vel_func(|X-c_k|, 0.02, -0.01) w_k (-(X-c_k).y, (X-c_k).x)
+ * (2D/vortex/init_conditions.py:142-145, 386-414), split to the faces with
+ * clamped samples (split_central_vector, 2D/vortex/taichi_utils.py:158-167). */
+int fm_vortex_velocity_2d(const fm_grid *g, int dtype, double dx, int nv, const double *theta, void *ux, void *uy,
+                          void *stream);
+/* grad[3K] (device, FP64) = sum over faces of lambda . d u / d theta, the
+ * analytic form of the reference's finite-difference calculate_dtheta_ind
+ * (2D/vortex/optimize_vortex.py:193-220).  work: device FP64 scratch of
+ * 592 * 3K entries. */
+int fm_vortex_velocity_grad_2d(const fm_grid *g, int dtype, double dx, int nv, const double *theta, const void *lam_x,
+                               const void *lam_y, double *work, double *grad, void *stream);
+/* omega (cell grid) = curl of the face-averaged centre velocity with clamped
+ * samples (get_central_vector, curl: 2D/vortex/taichi_utils.py:153-156, 199-205). */
+int fm_vorticity_2d(const fm_grid *g, int dtype, double dx, const void *ux, const void *uy, void *omega, void *stream);
+/* Final-vorticity loss and adjoint seed: *loss (device FP64) = sum (omega - omega*)^2,
+ * lam = (d omega / d u)^T 2 (omega - omega*) on the faces.  work: cell-grid
+ * scratch of the dtype; part: device FP64 scratch of 592 entries.  The
+ * vorticity loss has no reference counterpart (the reference's vortex loss is
+ * on passive scalars, 2D/vortex/lfm_midpoint_diff_simulator.py:165-174). */
+int fm_vorticity_loss_2d(const fm_grid *g, int dtype, double dx, const void *ux, const void *uy, const void *omega_target,
+                         void *work, double *part, void *lam_x, void *lam_y, double *loss, void *stream);
+
 #ifdef __cplusplus
 }
 #endif

@@ -169,18 +169,25 @@ class OracleSim:
                                             [x.copy() for x in self.F_f])
 
     # -------------------------------------------------------------- adjoint
-    def init_gradient(self, target):
+    def init_gradient(self, target=None, seed=None):
+        """Passive loss seed (case 11), or seed = (loss, [adj_u faces]) for a velocity loss."""
         o, d = self.o, self.dim
         self.final_ind = self.step_num + 1
         self.adj_u = o.zeros_mac()
-        self.init_adj_u = o.zeros_mac()
         self.src = o.zeros_mac()
         self.H_prev, self.H_prev_prev = o.zeros_mac(), o.zeros_mac()
         self.mid_u = o.zeros_mac()
         self.adj_passive_f = o.zeros_mac()
-        diff = self.passive - target
-        self.adj_passive = (2 * diff).astype(o.dtype)
-        self.loss = float(np.sum(diff.astype(np.float64) ** 2))
+        if seed is not None:
+            self.loss = float(seed[0])
+            for c in range(d):
+                self.adj_u[c][...] = seed[1][c]
+            self.adj_passive = o.zeros_cell()
+        else:
+            diff = self.passive - target
+            self.adj_passive = (2 * diff).astype(o.dtype)
+            self.loss = float(np.sum(diff.astype(np.float64) ** 2))
+        self.init_adj_u = [x.copy() for x in self.adj_u]
         self.init_adj_passive = self.adj_passive.copy()
         self.step_num = self.final_ind
         if self.backward_u:
@@ -271,6 +278,22 @@ class OracleSim:
         while not self.step_midpoint():
             pass
         self.init_gradient(target)
+        while not self.backtrack_step_midpoint():
+            pass
+        return self.loss, [x.copy() for x in self.adj_u]
+
+    def gradient_vorticity(self, u0, omega_target):
+        """2D final-vorticity loss L = sum (omega - omega*)^2 (vortex_oracle.py)."""
+        import vortex_oracle as V
+
+        self.init(u0, np.zeros(self.res))
+        while not self.step_midpoint():
+            pass
+        om = V.vorticity(self.u[0], self.u[1], self.dx)
+        diff = om.astype(np.float64) - np.asarray(omega_target, np.float64)
+        g = (2 * diff).astype(self.o.dtype)
+        adj = [x.astype(self.o.dtype) for x in V.vorticity_adjoint(g, self.dx)]
+        self.init_gradient(seed=(float(np.sum(diff * diff)), adj))
         while not self.backtrack_step_midpoint():
             pass
         return self.loss, [x.copy() for x in self.adj_u]
