@@ -51,7 +51,7 @@ def parse():
     ap.add_argument("--no-roofline", action="store_true",
                     help="skip the dominant-kernel roofline timing (used for profiler runs, which need W >= 1 only; "
                          "a reported bench value needs W >= 3)")
-    ap.add_argument("--workload", default="gradient", choices=["gradient", "poisson", "vortex2d"],
+    ap.add_argument("--workload", default="gradient", choices=["gradient", "poisson", "vortex2d", "vortex2d-batch"],
                     help="gradient: the headline 3D gradient benchmark; poisson: the mixed-precision Poisson solve "
                          "(seeded k^-5/3 divergence RHS, all-Neumann, --poisson-res^3); vortex2d: the 2D vortex "
                          "optimisation gradient dL/dtheta (256^2, 100 steps, 4 vortices)")
@@ -328,6 +328,51 @@ def run_vortex2d(a):
     return 0
 
 
+def run_vortex2d_batch(a):
+    """16 vortex-optimisation instances (4 x 128^2, 4 x 192^2, 4 x 256^2,
+    4 x 384^2; 100 steps, reinit 10, dt = 0.5 dx; control seeds 100+i, target
+    seeds 200+i) advanced concurrently, one stream and host thread each; one
+    bench step = one gradient of every instance.  Compared with the same
+    instances run one after another."""
+    import numpy as np
+    import torch
+
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    torch.cuda.set_device(local)
+    dev = torch.device("cuda", local)
+    B = importlib.import_module("differentiable-flowmap_b200.batch")
+    bat = B.BatchedVortex(device=dev)
+
+    def timed(concurrent):
+        for _ in range(a.warmup):
+            bat.gradients(concurrent)
+        torch.cuda.synchronize(dev)
+        t0 = time.perf_counter()
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record()
+        for _ in range(a.steps):
+            res = bat.gradients(concurrent)
+        e1.record()
+        torch.cuda.synchronize(dev)
+        return e0.elapsed_time(e1) / a.steps, (time.perf_counter() - t0) * 1e3 / a.steps, res
+
+    ms_seq, wall_seq, seq = timed(False)
+    ms_conc, wall_conc, conc = timed(True)
+    n = len(bat.instances)
+    errs = [float(np.linalg.norm(dc - ds) / np.linalg.norm(ds)) for (_, dc), (_, ds) in zip(conc, seq)]
+    line = {"metric": "batched 2D vortex gradients/s, 16 instances (4 x 128^2, 192^2, 256^2, 384^2), 100 steps",
+            "value": n * 1e3 / ms_conc, "unit": "grads/s", "n_gpus": 1, "steps": a.steps, "warmup": a.warmup,
+            "ms_per_step": ms_conc, "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
+            "dtype": "f32", "data": "synthetic",
+            "config": {"workload": "16 concurrent vortex instances, one stream + host thread each",
+                       "sizes": [inst.res for inst in bat.instances]},
+            "sequential": {"grads_per_s": n * 1e3 / ms_seq, "ms_per_batch": ms_seq},
+            "concurrent_over_sequential": ms_seq / ms_conc,
+            "per_instance_dtheta_rel_err_vs_unbatched": errs}
+    print(json.dumps(line), flush=True)
+    return 0
+
+
 def main():
     a = parse()
     if a.impl == "reference":
@@ -336,6 +381,8 @@ def main():
         return run_poisson(a)
     if a.workload == "vortex2d":
         return run_vortex2d(a)
+    if a.workload == "vortex2d-batch":
+        return run_vortex2d_batch(a)
 
     import torch
     import torch.distributed as dist
