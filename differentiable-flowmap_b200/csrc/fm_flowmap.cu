@@ -16,10 +16,13 @@ namespace fm {
 
 constexpr int kThreads = 256;
 
-// CTAs per SM the march kernel is compiled for (2 caps it at 128 registers).
-#ifndef FM_MARCH_MIN_BLOCKS
-#define FM_MARCH_MIN_BLOCKS 2
-#endif
+// CTAs per SM the march kernel is compiled for: 3 in FP32 (80 registers; 0.697
+// vs 0.723 ms per 128^3 RK4 launch at 2 CTAs / 128 registers), 2 in FP64 (80
+// registers would spill over 1 KB per thread there).
+template <typename T>
+constexpr int march_min_blocks() {
+  return sizeof(T) == 4 ? 3 : 2;
+}
 
 // Midpoint (RK2) / RK4 backtrace from X through u0 (3D/flowmap.py:210-219, :257-262).
 template <typename T, int D, int RK>
@@ -185,7 +188,7 @@ __device__ __forceinline__ MarchJob<T> pick_job(const MarchJobs<T>& jobs, int y)
 // RK2_grid / RK4_grid (with T) and RK*_grid_only_psi (without); blockIdx.y
 // selects the job (face grids and/or the centre map of one march).
 template <typename T, int D, int RK>
-__global__ void __launch_bounds__(kThreads, FM_MARCH_MIN_BLOCKS) k_march(fm_grid g, T dx, T dt, MarchJobs<T> jobs, Mac<T> u) {
+__global__ void __launch_bounds__(kThreads, march_min_blocks<T>()) k_march(fm_grid g, T dx, T dt, MarchJobs<T> jobs, Mac<T> u) {
   const MarchJob<T> job = pick_job(jobs, blockIdx.y);
   const Shape s = job.face >= 0 ? face_shape(g, job.face) : cell_shape(g);
   const long N = s.size();
