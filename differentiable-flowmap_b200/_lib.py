@@ -99,6 +99,7 @@ SIGNATURES = {
     "fm_advect_scalar_grid_pair": [GP, I, I, D, D] + [P] * 7 + [P],
     "fm_mg_vcycle": [P, P, P, P],
     "fm_mgpcg_solve_dc": [P, I, P, P, P, D, I, P, C.POINTER(I), C.POINTER(I), C.POINTER(D)],
+    "fm_clamp_extrema": [GP, I, I, P, P, P, P],
     "fm_vortex_velocity_2d": [GP, I, D, I, C.POINTER(D), P, P, P],
     "fm_vortex_velocity_grad_2d": [GP, I, D, I, C.POINTER(D), P, P, P, P, P],
     "fm_vorticity_2d": [GP, I, D, P, P, P, P],

@@ -6,6 +6,7 @@
 // exactly the BF16-rounded FP32 value.
 #include <cuda_bf16.h>
 
+#include "fm_common.cuh"
 #include "fm_internal.h"
 
 namespace fm {
@@ -61,4 +62,56 @@ extern "C" int fm_convert(long n, int src_dtype, const void* src, int dst_dtype,
   if (src_dtype == FM_F64) return convert_from<double>(n, src, dst_dtype, dst, s, (unsigned)blocks);
   if (src_dtype == FM_BF16) return convert_from<__nv_bfloat16>(n, src, dst_dtype, dst, s, (unsigned)blocks);
   return FM_ERR_DTYPE;
+}
+
+// ---------------------------------------------------------------------------
+// BFECC clamp: dst = clamp(src, min, max of ref over the 2*dim axis neighbours),
+// neighbours sampled with the index clamp of sample() (clamp_u,
+// 3D/flowmap.py:324-334, 2D/vortex/flowmap.py:333-341).  The centre value of
+// ref is not part of the bounds, as in the reference.
+// ---------------------------------------------------------------------------
+namespace fm {
+
+template <typename T, int D>
+__global__ void k_clamp_extrema(Shape s, const T* __restrict__ src, const T* __restrict__ ref, T* __restrict__ dst) {
+  const long n = s.size();
+  for (long q = (long)blockIdx.x * blockDim.x + threadIdx.x; q < n; q += (long)gridDim.x * blockDim.x) {
+    int i, j, k;
+    unflatten(s, q, i, j, k);
+    const int im = i > 0 ? i - 1 : 0, ip = i < s.s0 - 1 ? i + 1 : s.s0 - 1;
+    const int jm = j > 0 ? j - 1 : 0, jp = j < s.s1 - 1 ? j + 1 : s.s1 - 1;
+    T mx = ref[s.idx(im, j, k)], mn = mx, v;
+    v = ref[s.idx(ip, j, k)]; mx = fmax(mx, v); mn = fmin(mn, v);
+    v = ref[s.idx(i, jm, k)]; mx = fmax(mx, v); mn = fmin(mn, v);
+    v = ref[s.idx(i, jp, k)]; mx = fmax(mx, v); mn = fmin(mn, v);
+    if (D == 3) {
+      const int km = k > 0 ? k - 1 : 0, kp = k < s.s2 - 1 ? k + 1 : s.s2 - 1;
+      v = ref[s.idx(i, j, km)]; mx = fmax(mx, v); mn = fmin(mn, v);
+      v = ref[s.idx(i, j, kp)]; mx = fmax(mx, v); mn = fmin(mn, v);
+    }
+    dst[q] = fmin(fmax(src[q], mn), mx);
+  }
+}
+
+}  // namespace fm
+
+extern "C" int fm_clamp_extrema(const fm_grid* g, int dtype, int face, const void* src, const void* ref, void* dst,
+                                void* stream) {
+  using namespace fm;
+  const int st = validate_grid(g, dtype);
+  if (st) return st;
+  if (face < -1 || face >= g->dim) return FM_ERR_ARG;
+  if (!src || !ref || !dst) return FM_ERR_ARG;
+  const Shape s = face >= 0 ? face_shape(*g, face) : cell_shape(*g);
+  long b = (s.size() + 255) / 256;
+  if (b > 148L * 16) b = 148L * 16;
+  cudaStream_t cs = (cudaStream_t)stream;
+  if (dtype == FM_F32) {
+    if (g->dim == 3) launch(k_clamp_extrema<float, 3>, (unsigned)b, 256, 0, cs, s, (const float*)src, (const float*)ref, (float*)dst);
+    else launch(k_clamp_extrema<float, 2>, (unsigned)b, 256, 0, cs, s, (const float*)src, (const float*)ref, (float*)dst);
+  } else {
+    if (g->dim == 3) launch(k_clamp_extrema<double, 3>, (unsigned)b, 256, 0, cs, s, (const double*)src, (const double*)ref, (double*)dst);
+    else launch(k_clamp_extrema<double, 2>, (unsigned)b, 256, 0, cs, s, (const double*)src, (const double*)ref, (double*)dst);
+  }
+  return check_cuda();
 }

@@ -187,6 +187,17 @@ def convert(src, dst, stream=None):
                                 ptr(dst), stream_ptr(stream)), "fm_convert")
 
 
+def clamp_extrema(g: GridSpec, src, ref, dst, stream=None):
+    """dst = clamp(src, extrema of ref over the axis neighbours) (clamp_u); grid inferred from the shape."""
+    face = g.which_grid(src)
+    if ref.shape != src.shape or dst.shape != src.shape or ref.dtype != src.dtype or dst.dtype != src.dtype:
+        raise _lib.FlowmapError(1, "clamp_extrema: src, ref and dst must share shape and dtype")
+    if dst.data_ptr() == ref.data_ptr():
+        raise _lib.FlowmapError(2, "clamp_extrema: dst may not alias ref")
+    check(_lib.lib().fm_clamp_extrema(C.byref(g.c_grid()), _dt(src), face, ptr(src), ptr(ref), ptr(dst),
+                                      stream_ptr(stream)), "fm_clamp_extrema")
+
+
 def store(src, dst, stream=None):
     """Copy into a trajectory store slot: device memcpy when dtypes match, else fm_convert."""
     if src.dtype == dst.dtype:

@@ -122,8 +122,6 @@ class LFM_Simulator:
             cfg = replace(cfg, dt=dt)
         if reinit_every is not None:
             cfg = replace(cfg, reinit_every=reinit_every)
-        if cfg.BFECC_clamp or cfg.use_short_BFECC:
-            raise FlowmapError(2, "BFECC_clamp / use_short_BFECC are not supported by this build")
         if not torch.cuda.is_available():
             raise FlowmapError(6, "LFM_Simulator needs a CUDA device (no CPU fallback)")
         self.cfg = cfg
@@ -163,6 +161,16 @@ class LFM_Simulator:
         self.final_passive = torch.zeros_like(self.passive)
         self.init_passive = torch.zeros_like(self.passive)
         self.err_passive = torch.zeros_like(self.passive)
+
+        # BFECC clamp (tmp fields) and short BFECC (one-step temporary maps)
+        if cfg.BFECC_clamp:
+            self.tmp_u = _mac(g, dt_, dev)
+            self.tmp_passive = torch.zeros_like(self.passive)
+        if cfg.use_short_BFECC:
+            self.psi_tem = torch.zeros((self.dim,) + g.shape, dtype=dt_, device=dev)
+            self.phi_tem = torch.zeros((self.dim,) + g.shape, dtype=dt_, device=dev)
+            self.psi_f_tem, self.T_f_tem = _vec_face(g, dt_, dev), _vec_face(g, dt_, dev)
+            self.phi_f_tem, self.F_f_tem = _vec_face(g, dt_, dev), _vec_face(g, dt_, dev)
 
         self.step_num = _Scalar(-1)
         self.frame_idx = _Scalar(0)
@@ -209,19 +217,40 @@ class LFM_Simulator:
         K.march_map(self.grid, self.cfg.RK_number, self.dx, dt, psi_c, psi_f, T_f, u)
 
     def BFECC(self, init_u, u, err_u, T_f, psi_f, F_f, phi_f):
-        """BFECC (3D/flowmap.py:405-434, BFECC_clamp=False) in three fused launches:
-        u = T.init(psi); err = 0.5*(F.u(phi) - init); u = u - T.err(psi)."""
+        """BFECC (3D/flowmap.py:405-434) in three fused launches:
+        u = T.init(psi); err = 0.5*(F.u(phi) - init); u = u - T.err(psi).
+        With BFECC_clamp the last value is clamped to the extrema of the first
+        pass's neighbours (clamp_u) before it replaces u."""
         g, dx = self.grid, self.dx
         K.pullback_u(g, dx, init_u, u, T_f, psi_f)
         K.pullback_u(g, dx, u, err_u, F_f, phi_f, alpha=0.5, beta=-1.0, base=init_u)
-        K.pullback_u(g, dx, err_u, u, T_f, psi_f, alpha=-1.0, beta=-1.0, base=u)
+        if not self.cfg.BFECC_clamp:
+            K.pullback_u(g, dx, err_u, u, T_f, psi_f, alpha=-1.0, beta=-1.0, base=u)
+            return
+        K.pullback_u(g, dx, err_u, self.tmp_u, T_f, psi_f, alpha=-1.0, beta=-1.0, base=u)
+        for c in range(self.dim):
+            K.clamp_extrema(g, self.tmp_u[c], u[c], err_u[c])
+            u[c].copy_(err_u[c])
 
     def BFECC_scalar(self, init_s, s, err_s, psi, phi):
-        """BFECC_scalar (3D/flowmap.py:436-452, BFECC_clamp=False)."""
+        """BFECC_scalar (3D/flowmap.py:436-452), clamped like BFECC with BFECC_clamp."""
         g, dx = self.grid, self.dx
         K.pullback_scalar(g, dx, init_s, s, psi)
         K.pullback_scalar(g, dx, s, err_s, phi, alpha=0.5, beta=-1.0, base=init_s)
-        K.pullback_scalar(g, dx, err_s, s, psi, alpha=-1.0, beta=-1.0, base=s)
+        if not self.cfg.BFECC_clamp:
+            K.pullback_scalar(g, dx, err_s, s, psi, alpha=-1.0, beta=-1.0, base=s)
+            return
+        K.pullback_scalar(g, dx, err_s, self.tmp_passive, psi, alpha=-1.0, beta=-1.0, base=s)
+        K.clamp_extrema(g, self.tmp_passive, s, err_s)
+        s.copy_(err_s)
+
+    def _short_maps(self, u, dt, centre: bool):
+        """One-step temporary maps of use_short_BFECC: psi_tem with dt, phi_tem
+        with -dt, from identity (3D/lfm_midpoint_simulator.py:725-739)."""
+        self.reset_to_identity(self.psi_tem, self.psi_f_tem, self.T_f_tem)
+        self.reset_to_identity(self.phi_tem, self.phi_f_tem, self.F_f_tem)
+        self._march(self.psi_tem if centre else None, self.psi_f_tem, self.T_f_tem, u, dt)
+        self._march(self.phi_tem if centre else None, self.phi_f_tem, self.F_f_tem, u, -dt)
 
     def project(self, u):
         self.solver.project(u)
@@ -296,8 +325,8 @@ class LFM_Simulator:
             self._march(self.psi, self.psi_f, self.T_f, um, self.dt)
 
     def step_flow_map(self, j: int, curr_dt: float):
-        """3D/lfm_midpoint_simulator.py:684-807 with add_control_force=False,
-        use_short_BFECC=False, viscosity=0."""
+        """3D/lfm_midpoint_simulator.py:684-807 with add_control_force=False and
+        viscosity=0; use_short_BFECC and BFECC_clamp as configured."""
         cfg = self.cfg
         n = self.step_num[None]
         _copy_mac(self.ad_u, self.u)
@@ -309,11 +338,20 @@ class LFM_Simulator:
             if self._ring is not None:
                 self._ring[j][c].copy_(self.u[c])
         self.march_phi_grid(self.u)
-        if cfg.add_passive_scalar:
-            self._advect_scalar_grid(self.u, self.passive, self.final_passive, curr_dt)
-            self.passive, self.final_passive = self.final_passive, self.passive
-        self._advect_u_grid(self.u, self.ad_u, self.final_u, curr_dt)
-        self.u, self.final_u = self.final_u, self.u
+        if cfg.use_short_BFECC:
+            # BFECC through one-step maps instead of the semi-Lagrangian advection
+            # (3D/lfm_midpoint_simulator.py:725-745); the BFECC result replaces u
+            self._short_maps(self.u, curr_dt, cfg.add_passive_scalar)
+            if cfg.add_passive_scalar:
+                self.BFECC_scalar(self.passive, self.final_passive, self.err_passive, self.psi_tem, self.phi_tem)
+                self.passive, self.final_passive = self.final_passive, self.passive
+            self.BFECC(self.ad_u, self.u, self.err_u, self.T_f_tem, self.psi_f_tem, self.F_f_tem, self.phi_f_tem)
+        else:
+            if cfg.add_passive_scalar:
+                self._advect_scalar_grid(self.u, self.passive, self.final_passive, curr_dt)
+                self.passive, self.final_passive = self.final_passive, self.passive
+            self._advect_u_grid(self.u, self.ad_u, self.final_u, curr_dt)
+            self.u, self.final_u = self.final_u, self.u
         self.project(self.u)
 
         if j == self.reinit_every - 1:
@@ -429,6 +467,30 @@ class LFM_Diff_Simulator(LFM_Simulator):
     def march_psi_grid(self, dt):
         self._march(self.psi, self.psi_f, self.T_f, self.mid_u, dt)
 
+    def _backtrack_short_bfecc(self, curr_dt):
+        """use_short_BFECC branch of the adjoint step (3D/lfm_midpoint_diff_simulator.py:440-485):
+        adj_u (and adj_passive, and u / passive with backward_u) go back by BFECC
+        through one-step maps of the midpoint velocity (psi_tem with -dt, phi_tem
+        with +dt).  The reference adds the adjoint source here with -2 dt (the
+        semi-Lagrangian branch uses -dt); kept as it is."""
+        cfg = self.cfg
+        self._short_maps(self.mid_u, -curr_dt, cfg.add_passive_scalar)
+        maps = (self.T_f_tem, self.psi_f_tem, self.F_f_tem, self.phi_f_tem)
+        self.BFECC(self.adj_u, self.final_u, self.err_u, *maps)
+        for c in range(self.dim):
+            K.add_fields(self.final_u[c], self.src[c], self.adj_u[c], -2 * curr_dt)
+        if cfg.add_passive_scalar:
+            self.BFECC_scalar(self.adj_passive, self.final_passive, self.err_passive, self.psi_tem, self.phi_tem)
+            self.adj_passive, self.final_passive = self.final_passive, self.adj_passive
+            for c in range(self.dim):
+                K.add_fields(self.adj_u[c], self.adj_passive_f[c], self.adj_u[c], -curr_dt)
+        if cfg.backward_u:
+            if cfg.add_passive_scalar:
+                self.BFECC_scalar(self.passive, self.final_passive, self.err_passive, self.psi_tem, self.phi_tem)
+                self.passive, self.final_passive = self.final_passive, self.passive
+            self.BFECC(self.u, self.final_u, self.err_u, *maps)
+            self.u, self.final_u = self.final_u, self.u
+
     def backtrack_step_midpoint(self, write_gradient=False, write_passive=False, control_force_para=None):
         """3D/lfm_midpoint_diff_simulator.py:390-419."""
         if control_force_para is not None:
@@ -453,27 +515,30 @@ class LFM_Diff_Simulator(LFM_Simulator):
             K.nabla_scalar_adjoint(g, dx, self.passive, self.adj_passive, self.adj_passive_f)
 
         rk = cfg.RK_number
-        if cfg.backward_u:
-            # adj_u and u go back along the same midpoint velocity: one backtrace
-            K.advect_u_grid_pair(g, rk, dx, -curr_dt, self.mid_u, self.adj_u, self.final_u, self.u, self.err_u)
-            self.adj_u, self.final_u = self.final_u, self.adj_u
-            self.u, self.err_u = self.err_u, self.u
+        if cfg.use_short_BFECC:
+            self._backtrack_short_bfecc(curr_dt)
         else:
-            self._advect_u_grid(self.mid_u, self.adj_u, self.final_u, -curr_dt)
-            self.adj_u, self.final_u = self.final_u, self.adj_u
-        for c in range(self.dim):
-            K.add_fields(self.adj_u[c], self.src[c], self.adj_u[c], -curr_dt)
-        if cfg.add_passive_scalar:
-            if cfg.backward_u:  # passive and adj_passive along the same backtrace
-                K.advect_scalar_grid_pair(g, rk, dx, -curr_dt, self.mid_u, self.passive, self.final_passive,
-                                          self.adj_passive, self.err_passive)
-                self.passive, self.final_passive = self.final_passive, self.passive
-                self.adj_passive, self.err_passive = self.err_passive, self.adj_passive
+            if cfg.backward_u:
+                # adj_u and u go back along the same midpoint velocity: one backtrace
+                K.advect_u_grid_pair(g, rk, dx, -curr_dt, self.mid_u, self.adj_u, self.final_u, self.u, self.err_u)
+                self.adj_u, self.final_u = self.final_u, self.adj_u
+                self.u, self.err_u = self.err_u, self.u
             else:
-                self._advect_scalar_grid(self.mid_u, self.adj_passive, self.final_passive, -curr_dt)
-                self.adj_passive, self.final_passive = self.final_passive, self.adj_passive
+                self._advect_u_grid(self.mid_u, self.adj_u, self.final_u, -curr_dt)
+                self.adj_u, self.final_u = self.final_u, self.adj_u
             for c in range(self.dim):
-                K.add_fields(self.adj_u[c], self.adj_passive_f[c], self.adj_u[c], -curr_dt)
+                K.add_fields(self.adj_u[c], self.src[c], self.adj_u[c], -curr_dt)
+            if cfg.add_passive_scalar:
+                if cfg.backward_u:  # passive and adj_passive along the same backtrace
+                    K.advect_scalar_grid_pair(g, rk, dx, -curr_dt, self.mid_u, self.passive, self.final_passive,
+                                              self.adj_passive, self.err_passive)
+                    self.passive, self.final_passive = self.final_passive, self.passive
+                    self.adj_passive, self.err_passive = self.err_passive, self.adj_passive
+                else:
+                    self._advect_scalar_grid(self.mid_u, self.adj_passive, self.final_passive, -curr_dt)
+                    self.adj_passive, self.final_passive = self.final_passive, self.adj_passive
+                for c in range(self.dim):
+                    K.add_fields(self.adj_u[c], self.adj_passive_f[c], self.adj_u[c], -curr_dt)
 
         self.march_psi_grid(curr_dt)
         # Adams-Bashforth index: adjoint steps already taken in this interval

@@ -269,6 +269,12 @@ int fm_project_noalloc(const fm_grid *g, int dtype, const fm_mg_params *params, 
 /* Apply the Neumann Laplacian: Ap = A p (for tests and defect correction). */
 int fm_laplacian(const fm_grid *g, int dtype, const void *p, void *Ap, void *stream);
 
+/* BFECC clamp (clamp_u, 3D/flowmap.py:324-334; 2D/vortex/flowmap.py:333-341):
+ * dst = clamp(src, min, max of ref over the 2*dim axis neighbours), neighbours
+ * sampled with sample()'s index clamp, on grid `face` (0..dim-1 a face grid,
+ * -1 the cell grid).  dst may not alias ref. */
+int fm_clamp_extrema(const fm_grid *g, int dtype, int face, const void *src, const void *ref, void *dst, void *stream);
+
 /* ------------------------------------------------------------------------
  * 2D vortex problem (the vortex optimisation's control map and loss).
  * theta = [w_0..w_{K-1}, cx_0..cx_{K-1}, cy_0..cy_{K-1}], K <= 64, host array.

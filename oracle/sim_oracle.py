@@ -24,14 +24,35 @@ import numpy as np
 from oracle import MGParams, Oracle
 
 
+def clamp_u(u, u1):
+    """clamp_u (3D/flowmap.py:324-334, 2D/vortex/flowmap.py:333-341): u clamped to
+    the min/max of u1 over the axis neighbours, sampled with sample()'s index clamp."""
+    lo = hi = None
+    for a in range(u1.ndim):
+        n = u1.shape[a]
+        for idx in (np.maximum(np.arange(n) - 1, 0), np.minimum(np.arange(n) + 1, n - 1)):
+            v = np.take(u1, idx, axis=a)
+            lo = v if lo is None else np.minimum(lo, v)
+            hi = v if hi is None else np.maximum(hi, v)
+    return np.minimum(np.maximum(u, lo), hi).astype(u1.dtype)
+
+
 class OracleSim:
     def __init__(self, res, dx, dt, reinit_every, total_steps, rk=4, backward_u=True, passive=True,
-                 trajectory_loss=False, prec="f64", mg=None):
+                 trajectory_loss=False, prec="f64", mg=None, bfecc_clamp=False, short_bfecc=False):
         self.o = Oracle(tuple(res), prec)
         self.dim = len(res)
         self.res = tuple(res)
         self.dx, self.dt, self.R, self.total_steps = dx, dt, reinit_every, total_steps
         self.rk, self.backward_u, self.passive_on, self.trajectory_loss = rk, backward_u, passive, trajectory_loss
+        self.bfecc_clamp, self.short = bfecc_clamp, short_bfecc
+        if short_bfecc:
+            o = self.o
+            self.psi_tem, self.phi_tem = o.zeros_cell(self.dim), o.zeros_cell(self.dim)
+            self.psi_f_tem = [o.zeros_face(c, self.dim) for c in range(self.dim)]
+            self.T_tem = [o.zeros_face(c, self.dim) for c in range(self.dim)]
+            self.phi_f_tem = [o.zeros_face(c, self.dim) for c in range(self.dim)]
+            self.F_tem = [o.zeros_face(c, self.dim) for c in range(self.dim)]
         self.mg = mg if mg is not None else MGParams(max(2, int(np.log2(min(res))) - 2), 2, 50, 0, 400, 1e-12, 0.0,
                                                     1e-12)
         o = self.o
@@ -76,6 +97,11 @@ class OracleSim:
         o.advect_u(err_u, tmp_u, T_f, psi_f, self.dx)
         for c in range(self.dim):
             err_u[c][...] = u[c] + (-1.0) * tmp_u[c]        # add_fields(u, tmp, err, -1)
+        if self.bfecc_clamp:
+            for c in range(self.dim):
+                tmp_u[c][...] = clamp_u(err_u[c], u[c])     # clamp_u(err, u, tmp)
+                u[c][...] = tmp_u[c]                        # copy_to(tmp, u)
+            return
         for c in range(self.dim):
             u[c][...] = err_u[c]                            # copy_to(err, u)
 
@@ -87,7 +113,24 @@ class OracleSim:
         err_s[...] = 0.5 * err_s
         o.advect_scalar(err_s, tmp_s, psi, self.dx)
         err_s[...] = s + (-1.0) * tmp_s
+        if self.bfecc_clamp:
+            tmp_s[...] = clamp_u(err_s, s)
+            s[...] = tmp_s
+            return
         s[...] = err_s
+
+    def short_maps(self, u, dt, centre):
+        """use_short_BFECC's one-step maps: psi_tem with dt, phi_tem with -dt
+        (3D/lfm_midpoint_simulator.py:725-739, diff :441-450)."""
+        self.reset_to_identity(self.psi_tem, self.psi_f_tem, self.T_tem)
+        self.reset_to_identity(self.phi_tem, self.phi_f_tem, self.F_tem)
+        if centre:
+            self.RK_grid_only_psi(self.psi_tem, u, dt)
+            self.RK_grid_only_psi(self.phi_tem, u, -dt)
+        for c in range(self.dim):
+            self.RK_grid(c, self.psi_f_tem[c], self.T_tem[c], u, dt)
+        for c in range(self.dim):
+            self.RK_grid(c, self.phi_f_tem[c], self.F_tem[c], u, -dt)
 
     # -------------------------------------------------------------- forward
     def init(self, u0, passive0):
@@ -142,12 +185,21 @@ class OracleSim:
         self.velocity_storage[j] = [x.copy() for x in self.u]
         self.march_phi_grid()
         self.store_mid[self.step_num] = [x.copy() for x in self.u]
-        if self.passive_on:
-            o.advect_scalar_grid(self.rk, self.u, self.passive, self.final_passive, self.dx, dt)
-            self.passive[...] = self.final_passive
-        o.advect_u_grid(self.rk, self.u, self.ad_u, self.final_u, self.dx, dt)
-        for c in range(d):
-            self.u[c][...] = self.final_u[c]
+        if self.short:
+            self.short_maps(self.u, dt, self.passive_on)
+            if self.passive_on:
+                self.BFECC_scalar(self.passive, self.final_passive, self.err_passive, self.tmp_passive,
+                                  self.psi_tem, self.phi_tem)
+                self.passive[...] = self.final_passive
+            self.BFECC(self.ad_u, self.u, self.err_u, self.tmp_u, self.T_tem, self.psi_f_tem, self.F_tem,
+                       self.phi_f_tem)
+        else:
+            if self.passive_on:
+                o.advect_scalar_grid(self.rk, self.u, self.passive, self.final_passive, self.dx, dt)
+                self.passive[...] = self.final_passive
+            o.advect_u_grid(self.rk, self.u, self.ad_u, self.final_u, self.dx, dt)
+            for c in range(d):
+                self.u[c][...] = self.final_u[c]
         self.Poisson(self.u)
         n = self.step_num
         if j == self.R - 1:
@@ -218,23 +270,44 @@ class OracleSim:
         o.calculate_nabla_u_w(self.u if self.backward_u else self.mid_u, self.adj_u, self.src, dx)
         if self.passive_on:
             o.calculate_nabla_scalar_adjoint(self.passive, self.adj_passive, self.adj_passive_f, dx)
-        o.advect_u_grid(self.rk, self.mid_u, self.adj_u, self.final_u, dx, -dt)
-        for c in range(d):
-            self.adj_u[c][...] = self.final_u[c]
-        if self.backward_u:
+        if self.short:  # 3D/lfm_midpoint_diff_simulator.py:440-485
+            self.short_maps(self.mid_u, -dt, self.passive_on)
+            maps = (self.T_tem, self.psi_f_tem, self.F_tem, self.phi_f_tem)
+            self.BFECC(self.adj_u, self.final_u, self.err_u, self.tmp_u, *maps)
+            for c in range(d):
+                self.adj_u[c][...] = self.final_u[c] + (-2 * dt) * self.src[c]
             if self.passive_on:
-                o.advect_scalar_grid(self.rk, self.mid_u, self.passive, self.final_passive, dx, -dt)
-                self.passive[...] = self.final_passive
-            o.advect_u_grid(self.rk, self.mid_u, self.u, self.final_u, dx, -dt)
+                self.BFECC_scalar(self.adj_passive, self.final_passive, self.err_passive, self.tmp_passive,
+                                  self.psi_tem, self.phi_tem)
+                self.adj_passive[...] = self.final_passive
+                for c in range(d):
+                    self.adj_u[c][...] = self.adj_u[c] + (-dt) * self.adj_passive_f[c]
+            if self.backward_u:
+                if self.passive_on:
+                    self.BFECC_scalar(self.passive, self.final_passive, self.err_passive, self.tmp_passive,
+                                      self.psi_tem, self.phi_tem)
+                    self.passive[...] = self.final_passive
+                self.BFECC(self.u, self.final_u, self.err_u, self.tmp_u, *maps)
+                for c in range(d):
+                    self.u[c][...] = self.final_u[c]
+        else:
+            o.advect_u_grid(self.rk, self.mid_u, self.adj_u, self.final_u, dx, -dt)
             for c in range(d):
-                self.u[c][...] = self.final_u[c]
-        for c in range(d):
-            self.adj_u[c][...] = self.adj_u[c] + (-dt) * self.src[c]
-        if self.passive_on:
-            o.advect_scalar_grid(self.rk, self.mid_u, self.adj_passive, self.final_passive, dx, -dt)
-            self.adj_passive[...] = self.final_passive
+                self.adj_u[c][...] = self.final_u[c]
+            if self.backward_u:
+                if self.passive_on:
+                    o.advect_scalar_grid(self.rk, self.mid_u, self.passive, self.final_passive, dx, -dt)
+                    self.passive[...] = self.final_passive
+                o.advect_u_grid(self.rk, self.mid_u, self.u, self.final_u, dx, -dt)
+                for c in range(d):
+                    self.u[c][...] = self.final_u[c]
             for c in range(d):
-                self.adj_u[c][...] = self.adj_u[c] + (-dt) * self.adj_passive_f[c]
+                self.adj_u[c][...] = self.adj_u[c] + (-dt) * self.src[c]
+            if self.passive_on:
+                o.advect_scalar_grid(self.rk, self.mid_u, self.adj_passive, self.final_passive, dx, -dt)
+                self.adj_passive[...] = self.final_passive
+                for c in range(d):
+                    self.adj_u[c][...] = self.adj_u[c] + (-dt) * self.adj_passive_f[c]
         self.march_psi_grid(dt)
         interval_last = min((n // self.R) * self.R + self.R - 1, self.total_steps - 1)
         ind = interval_last - n

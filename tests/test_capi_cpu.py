@@ -41,6 +41,9 @@ def test_invalid_arguments_rejected_without_device(fm):
     assert lib.fm_mgpcg_solve_dc(None, 0, None, None, None, 1e-10, 5, None, None, None, None) == 2
     assert lib.fm_project(None, None, None, None, None, None, None, None) == 2
     assert lib.fm_mg_vcycle(None, None, None, None) == 2
+    assert lib.fm_clamp_extrema(C.byref(bad_dim), 0, -1, None, None, None, None) == 1
+    assert lib.fm_clamp_extrema(C.byref(g), 0, 3, None, None, None, None) == 2  # face >= dim
+    assert lib.fm_clamp_extrema(C.byref(g), 0, -1, None, None, None, None) == 2  # NULL fields
 
 
 def test_no_cpu_fallback(fm):
