@@ -37,6 +37,16 @@ __host__ __device__ __forceinline__ int axis_len(const Shape& s, int a) {
   return a == 0 ? s.s0 : (a == 1 ? s.s1 : s.s2);
 }
 
+// Round-to-nearest arithmetic that the compiler may not fuse into FMAs, for
+// code that must round exactly as the reference's separate multiplies and
+// adds do (the MG operators, the Gaussian-force support test).
+__device__ __forceinline__ float rn_add(float a, float b) { return __fadd_rn(a, b); }
+__device__ __forceinline__ double rn_add(double a, double b) { return __dadd_rn(a, b); }
+__device__ __forceinline__ float rn_sub(float a, float b) { return __fsub_rn(a, b); }
+__device__ __forceinline__ double rn_sub(double a, double b) { return __dsub_rn(a, b); }
+__device__ __forceinline__ float rn_mul(float a, float b) { return __fmul_rn(a, b); }
+__device__ __forceinline__ double rn_mul(double a, double b) { return __dmul_rn(a, b); }
+
 // Flat index -> (i, j, k).  Grids stay below 2^32 entries (validate_grid), so
 // 32-bit unsigned division suffices; 64-bit division would cost ~5x more.
 __device__ __forceinline__ void unflatten(const Shape& s, long q, int& i, int& j, int& k) {

@@ -59,16 +59,6 @@ struct DevState {
 // ---------------------------------------------------------------------------
 // helpers
 // ---------------------------------------------------------------------------
-// Round-to-nearest arithmetic that the compiler may not fuse into FMAs: the
-// MG operators then round exactly as the reference's separate multiply and
-// subtract do.
-__device__ __forceinline__ float rn_add(float a, float b) { return __fadd_rn(a, b); }
-__device__ __forceinline__ double rn_add(double a, double b) { return __dadd_rn(a, b); }
-__device__ __forceinline__ float rn_sub(float a, float b) { return __fsub_rn(a, b); }
-__device__ __forceinline__ double rn_sub(double a, double b) { return __dsub_rn(a, b); }
-__device__ __forceinline__ float rn_mul(float a, float b) { return __fmul_rn(a, b); }
-__device__ __forceinline__ double rn_mul(double a, double b) { return __dmul_rn(a, b); }
-
 // x / nd for the RBGS update, nd = number of in-domain neighbours (0..6),
 // rounded exactly as the IEEE division.  FP32: nd = s * d with s a power of
 // two (exact scaling) and d in {1, 3, 5}; q0 = y * RN(1/d), e = y - q0 * d

@@ -253,3 +253,39 @@ def vorticity_loss_2d(g: GridSpec, dx: float, ux, uy, omega_target, lam_x, lam_y
     check(_lib.lib().fm_vorticity_loss_2d(C.byref(g.c_grid()), _dt(ux), dx, ptr(ux), ptr(uy), ptr(omega_target),
                                           ptr(work), ptr(part), ptr(lam_x), ptr(lam_y), ptr(loss), stream_ptr(stream)),
           "fm_vorticity_loss_2d")
+
+
+def _chk_gaussians(g: GridSpec, center, inv_radius, strength, dtype):
+    n = int(inv_radius.shape[0])
+    for name, t, shape in (("center", center, (n, g.dim)), ("inv_radius", inv_radius, (n,)),
+                           ("strength", strength, (n, g.dim))):
+        if tuple(t.shape) != shape:
+            raise _lib.FlowmapError(1, f"{name} has shape {tuple(t.shape)}, expected {shape}")
+        if t.dtype != dtype:
+            raise _lib.FlowmapError(7, f"{name} is {t.dtype}, the fields are {dtype}")
+    return n
+
+
+def gaussian_force(g: GridSpec, dx: float, center, inv_radius, strength, f, stream=None):
+    """apply_gausion_force_kernel: every face of ``f`` = the sum of the Gaussians
+    reaching it (device parameter tensors: center n x dim, inv_radius n, strength n x dim)."""
+    _chk_mac(g, f, "f")
+    n = _chk_gaussians(g, center, inv_radius, strength, f[0].dtype)
+    check(_lib.lib().fm_gaussian_force(C.byref(g.c_grid()), _dt(f[0]), dx, n, ptr(center), ptr(inv_radius),
+                                       ptr(strength), *_mac3(f), stream_ptr(stream)), "fm_gaussian_force")
+
+
+def gaussian_force_grad(g: GridSpec, dx: float, center, inv_radius, strength, adj_u, out=None, stream=None):
+    """calculate_adj_gausion_force_kernel: (adj_center, adj_strength, penalty_center,
+    penalty_strength), device FP64 tensors of shape n x dim (written into ``out`` if given)."""
+    _chk_mac(g, adj_u, "adj_u")
+    n = _chk_gaussians(g, center, inv_radius, strength, adj_u[0].dtype)
+    if out is None:
+        out = tuple(torch.empty((n, g.dim), dtype=torch.float64, device=adj_u[0].device) for _ in range(4))
+    for t in out:
+        if t.dtype != torch.float64 or tuple(t.shape) != (n, g.dim):
+            raise _lib.FlowmapError(1, "gaussian_force_grad outputs are FP64 n x dim")
+    check(_lib.lib().fm_gaussian_force_grad(C.byref(g.c_grid()), _dt(adj_u[0]), dx, n, ptr(center), ptr(inv_radius),
+                                            ptr(strength), *_mac3(adj_u), *[ptr(t) for t in out],
+                                            stream_ptr(stream)), "fm_gaussian_force_grad")
+    return out

@@ -66,6 +66,8 @@ class FlowmapConfig:
     add_passive_scalar: bool = True
     BFECC_clamp: bool = False
     use_short_BFECC: bool = False
+    add_control_force: bool = False  # Gaussian control forces (control_force_para per step)
+    control_num: int = 0             # capacity: most Gaussians one step may pass
     trajectory_loss: bool = False  # reference's no-force branch: loss over reinit frames
     dtype: torch.dtype = torch.float32
     store_dtype: Optional[torch.dtype] = None  # checkpoint storage dtype (None: dtype)
@@ -87,6 +89,55 @@ class _Scalar:
 
     def __setitem__(self, k, v):
         self.v = v
+
+
+class DeviceField:
+    """A device tensor read back like a Taichi field (``.to_numpy()``)."""
+
+    def __init__(self, t: torch.Tensor):
+        self.tensor = t
+
+    def to_numpy(self):
+        return self.tensor.cpu().numpy()
+
+
+class _GaussianParams:
+    """Device copies of one step's Gaussian parameters (center n x dim, inverse
+    radius n, strength n x dim), uploaded from host arrays through two pinned
+    staging buffers so that an upload never waits for the GPU: a buffer is
+    rewritten only after the copy that last read it has completed."""
+
+    def __init__(self, cap: int, dim: int, dtype, device):
+        self.cap, self.dim, self.dtype = cap, dim, dtype
+        self.per = 2 * dim + 1
+        self.dev = torch.empty(max(cap, 1) * self.per, dtype=dtype, device=device)
+        self.host = [torch.empty(max(cap, 1) * self.per, dtype=dtype).pin_memory() for _ in range(2)]
+        self.events = [None, None]
+        self.k = 0
+
+    def load(self, para):
+        n = int(para["n"])
+        if n < 0 or n > self.cap:
+            raise FlowmapError(8, f"{n} Gaussians exceed control_num={self.cap}")
+        c, r, st = para["c"], para["r"], para["s"]
+        dim = self.dim
+        if all(isinstance(x, torch.Tensor) and x.is_cuda for x in (c, r, st)):
+            return (c[:n].to(self.dtype).contiguous(), r[:n].to(self.dtype).contiguous(),
+                    st[:n].to(self.dtype).contiguous())
+        h = self.host[self.k]
+        if self.events[self.k] is not None:
+            self.events[self.k].synchronize()
+        for off, x, cnt in ((0, c, n * dim), (n * dim, r, n), (n * dim + n, st, n * dim)):
+            a = x.detach().cpu() if isinstance(x, torch.Tensor) else torch.from_numpy(np.ascontiguousarray(x))
+            h[off:off + cnt].copy_(a.reshape(-1)[:cnt])
+        m = n * self.per
+        self.dev[:m].copy_(h[:m], non_blocking=True)
+        ev = torch.cuda.Event()
+        ev.record()
+        self.events[self.k] = ev
+        self.k ^= 1
+        return (self.dev[:n * dim].view(n, dim), self.dev[n * dim:n * dim + n],
+                self.dev[n * dim + n:m].view(n, dim))
 
 
 def _mac(grid: GridSpec, dtype, device, fill=0.0):
@@ -171,6 +222,14 @@ class LFM_Simulator:
             self.phi_tem = torch.zeros((self.dim,) + g.shape, dtype=dt_, device=dev)
             self.psi_f_tem, self.T_f_tem = _vec_face(g, dt_, dev), _vec_face(g, dt_, dev)
             self.phi_f_tem, self.F_f_tem = _vec_face(g, dt_, dev), _vec_face(g, dt_, dev)
+
+        # Gaussian control forces: the force field and the parameter staging
+        self.control_force = None
+        if cfg.add_control_force:
+            if cfg.control_num < 0:
+                raise FlowmapError(2, "control_num must be >= 0")
+            self.control_force = _mac(g, dt_, dev)
+            self._gf = _GaussianParams(cfg.control_num, self.dim, dt_, dev)
 
         self.step_num = _Scalar(-1)
         self.frame_idx = _Scalar(0)
@@ -292,10 +351,21 @@ class LFM_Simulator:
     def final_condition(self):
         return self.step_num[None] == self.total_steps - 1
 
+    def apply_gausion_force(self, f, center, inverse_radius, strength, num):
+        """3D/lfm_midpoint_simulator.py:309-314: f = the Gaussians' force field."""
+        c, r, st = self._gf.load({"c": center, "r": inverse_radius, "s": strength, "n": num})
+        K.gaussian_force(self.grid, self.dx, c, r, st, f)
+
+    def _control_params(self, control_force_para):
+        if control_force_para is None:
+            raise FlowmapError(2, "add_control_force needs control_force_para for every step")
+        return self._gf.load(control_force_para)
+
     def step_midpoint(self, write_flow_map=True, write_passive=True, control_force_para=None):
-        """One leapfrog step (3D/lfm_midpoint_simulator.py:648-682)."""
-        if control_force_para is not None:
-            raise FlowmapError(2, "control forces are not supported by this build")
+        """One leapfrog step (3D/lfm_midpoint_simulator.py:648-682).  With
+        add_control_force, ``control_force_para`` = {"c": centers n x dim,
+        "r": inverse radii n, "s": strengths n x dim, "n": n} for this step
+        (numpy arrays or tensors); otherwise it is ignored, as in the reference."""
         self.step_num[None] += 1
         n = self.step_num[None]
         if n >= self.total_steps:
@@ -303,7 +373,7 @@ class LFM_Simulator:
         j = n % self.reinit_every
         if self.store_passive is not None:
             K.store(self.passive, self.store_passive[n])
-        self.step_flow_map(j, self.dt)
+        self.step_flow_map(j, self.dt, control_force_para)
         if self.final_condition() and self.store_passive is not None:
             K.store(self.passive, self.store_passive[n + 1])
         return False, self.final_condition()
@@ -324,13 +394,19 @@ class LFM_Simulator:
                 um = [m[interval_start + s] for m in self.store_mid]
             self._march(self.psi, self.psi_f, self.T_f, um, self.dt)
 
-    def step_flow_map(self, j: int, curr_dt: float):
-        """3D/lfm_midpoint_simulator.py:684-807 with add_control_force=False and
-        viscosity=0; use_short_BFECC and BFECC_clamp as configured."""
+    def step_flow_map(self, j: int, curr_dt: float, control_force_para=None):
+        """3D/lfm_midpoint_simulator.py:684-807 with viscosity=0; use_short_BFECC,
+        BFECC_clamp and add_control_force as configured.  The control force is
+        evaluated once per step: the reference evaluates it twice with the same
+        parameters, which gives the same field."""
         cfg = self.cfg
         n = self.step_num[None]
         _copy_mac(self.ad_u, self.u)
         self._advect_u_grid(self.ad_u, self.ad_u, self.u, 0.5 * curr_dt)
+        if cfg.add_control_force:  # 3D/lfm_midpoint_simulator.py:694-706
+            K.gaussian_force(self.grid, self.dx, *self._control_params(control_force_para), self.control_force)
+            for c in range(self.dim):
+                K.add_fields(self.u[c], self.control_force[c], self.u[c], 0.5 * curr_dt)
         self.project(self.u)
         # write_velocity + RW_Cache("u"): the midpoint velocity of step n
         for c in range(self.dim):
@@ -352,6 +428,10 @@ class LFM_Simulator:
                 self.passive, self.final_passive = self.final_passive, self.passive
             self._advect_u_grid(self.u, self.ad_u, self.final_u, curr_dt)
             self.u, self.final_u = self.final_u, self.u
+        if cfg.add_control_force:  # 3D/lfm_midpoint_simulator.py:755-760
+            for c in range(self.dim):
+                K.add_fields(self.u[c], self.control_force[c], self.u[c], curr_dt)
+            K.accumulate_init(self.grid, self.dx, curr_dt, self.control_force, self.init_u, self.F_f, self.phi_f)
         self.project(self.u)
 
         if j == self.reinit_every - 1:
@@ -392,6 +472,15 @@ class LFM_Diff_Simulator(LFM_Simulator):
         self.init_adj_passive = torch.zeros_like(self.adj_passive)
         self.adj_passive_f = _mac(g, dt_, dev)
         self.mid_u = _mac(g, dt_, dev)
+        if self.cfg.add_control_force:
+            # calculate_adj_gausion_force outputs (3D/lfm_midpoint_diff_simulator.py:47-60)
+            cap = max(self.cfg.control_num, 1)
+            z = [torch.zeros((cap, self.dim), dtype=torch.float64, device=dev) for _ in range(4)]
+            self.adj_gaussion_force_center, self.adj_gaussion_force_strength = DeviceField(z[0]), DeviceField(z[1])
+            self.penalty_gaussion_force_center = DeviceField(z[2])
+            self.penalty_gaussion_force_strength = DeviceField(z[3])
+            self._gf_rows = 0
+        self.control_force_grads = {}
         self.target_passive = None
         self.target_trajectory = None
         self.loss = 0.0
@@ -491,23 +580,43 @@ class LFM_Diff_Simulator(LFM_Simulator):
             self.BFECC(self.u, self.final_u, self.err_u, *maps)
             self.u, self.final_u = self.final_u, self.u
 
+    def calculate_adj_gausion_force(self, adj_u, center, inverse_radius, strength, num):
+        """3D/lfm_midpoint_diff_simulator.py:63-69: the four per-Gaussian sums into
+        adj_gaussion_force_center / _strength and penalty_gaussion_force_center /
+        _strength (rows past ``num`` zero, as after the reference's fill(0))."""
+        self._adj_gaussian(adj_u, self._gf.load({"c": center, "r": inverse_radius, "s": strength, "n": num}))
+
+    def _adj_gaussian(self, adj_u, params):
+        n = params[1].shape[0]
+        outs = [f.tensor for f in (self.adj_gaussion_force_center, self.adj_gaussion_force_strength,
+                                   self.penalty_gaussion_force_center, self.penalty_gaussion_force_strength)]
+        if n < self._gf_rows:
+            for t in outs:
+                t[n:self._gf_rows].zero_()
+        self._gf_rows = n
+        K.gaussian_force_grad(self.grid, self.dx, *params, adj_u, out=[t[:n] for t in outs])
+
     def backtrack_step_midpoint(self, write_gradient=False, write_passive=False, control_force_para=None):
-        """3D/lfm_midpoint_diff_simulator.py:390-419."""
-        if control_force_para is not None:
-            raise FlowmapError(2, "control forces are not supported by this build")
+        """3D/lfm_midpoint_diff_simulator.py:390-419.  With add_control_force,
+        ``control_force_para`` holds the parameters of the step being undone; the
+        parameter gradients are left in adj_gaussion_force_* / penalty_gaussion_force_*."""
         self.step_num[None] -= 1
         n = self.step_num[None]
         j = n % self.reinit_every
         if self.cfg.add_passive_scalar and not self.cfg.backward_u:
             K.store(self.store_passive[n + 1], self.passive)
-        self.backtrack_flow_map(j, self.dt)
+        self.backtrack_flow_map(j, self.dt, control_force_para)
         return False, n == 0
 
-    def backtrack_flow_map(self, j: int, curr_dt: float):
-        """3D/lfm_midpoint_diff_simulator.py:421-594 with add_control_force=False,
-        use_short_BFECC=False."""
+    def backtrack_flow_map(self, j: int, curr_dt: float, control_force_para=None):
+        """3D/lfm_midpoint_diff_simulator.py:421-594 with viscosity=0."""
         cfg, g, dx = self.cfg, self.grid, self.dx
         n = self.step_num[None]
+        if cfg.add_control_force:  # 3D/lfm_midpoint_diff_simulator.py:423-427
+            params = self._control_params(control_force_para)
+            if cfg.backward_u:
+                K.gaussian_force(g, dx, *params, self.control_force)
+            self._adj_gaussian(self.adj_u, params)
         for c in range(self.dim):
             K.store(self.store_mid[c][n], self.mid_u[c])
         K.nabla_u_w(g, dx, self.u if cfg.backward_u else self.mid_u, self.adj_u, self.src)
@@ -551,6 +660,10 @@ class LFM_Diff_Simulator(LFM_Simulator):
             K.accumulate_init(g, dx, -curr_dt, self.adj_passive_f, self.init_adj_u, self.T_f, self.psi_f)
         self.project(self.adj_u)  # Poisson_adj
         if cfg.backward_u:
+            if cfg.add_control_force:  # 3D/lfm_midpoint_diff_simulator.py:525-530
+                for c in range(self.dim):
+                    K.add_fields(self.u[c], self.control_force[c], self.u[c], -curr_dt)
+                K.accumulate_init(g, dx, -curr_dt, self.control_force, self.init_u, self.T_f, self.psi_f)
             self.project(self.u)
 
         if j == 0:
@@ -582,18 +695,33 @@ class LFM_Diff_Simulator(LFM_Simulator):
             self.reset_to_identity(self.psi, self.psi_f, self.T_f)
 
     # --------------------------------------------------------- driver
-    def gradient(self, u0, passive0=None, target_passive=None, target_vorticity=None):
+    def gradient(self, u0, passive0=None, target_passive=None, target_vorticity=None, control_forces=None):
         """Full forward + adjoint: returns (loss, dL/du0 as a list of face tensors).
         The loss is the final passive L2 (``target_passive``) or, in 2D, the final
-        vorticity L2 (``target_vorticity``)."""
+        vorticity L2 (``target_vorticity``).  With add_control_force,
+        ``control_forces[n]`` is step n's control_force_para, and the per-step
+        parameter gradients are kept in ``control_force_grads[n]`` = (adj_center,
+        adj_strength, penalty_center, penalty_strength), device FP64 n x dim."""
+        cf = self.cfg.add_control_force
+        if cf and control_forces is None:
+            raise FlowmapError(2, "add_control_force needs control_forces (one control_force_para per step)")
+        self.control_force_grads = {}
         self.init(theta=u0, init_passive_np=passive0)
         while True:
-            _, final = self.forward_step_midpoint()
+            para = control_forces[self.step_num[None] + 1] if cf else None
+            _, final = self.forward_step_midpoint(control_force_para=para)
             if final:
                 break
         self.init_gradient(target_passive=target_passive, target_vorticity=target_vorticity)
         while True:
-            _, done = self.backtrack_step_midpoint()
+            n = self.step_num[None] - 1
+            _, done = self.backtrack_step_midpoint(control_force_para=control_forces[n] if cf else None)
+            if cf:
+                rows = self._gf_rows
+                self.control_force_grads[n] = tuple(
+                    f.tensor[:rows].clone() for f in (self.adj_gaussion_force_center, self.adj_gaussion_force_strength,
+                                                      self.penalty_gaussion_force_center,
+                                                      self.penalty_gaussion_force_strength))
             if done:
                 break
         # the solver's device-side counters, read once per gradient (one stream sync)

@@ -276,6 +276,27 @@ int fm_laplacian(const fm_grid *g, int dtype, const void *p, void *Ap, void *str
 int fm_clamp_extrema(const fm_grid *g, int dtype, int face, const void *src, const void *ref, void *dst, void *stream);
 
 /* ------------------------------------------------------------------------
+ * Gaussian control forces.  n Gaussians, device arrays of the dtype:
+ * center n x dim (row-major), inv_radius n (r = 1/radius^2), strength n x dim.
+ * ------------------------------------------------------------------------ */
+/* f_c(X) = sum over I with q_I(X) = |X - c_I|^2 r_I < 5 of exp(-q_I(X)) strength_I[c]
+ * on every face of component c, summed in ascending I (apply_gausion_force_kernel,
+ * 3D/lfm_midpoint_simulator.py:309-344; 2D/shape/lfm_midpoint_simulator.py:283-299).
+ * Every face is written (0 where no Gaussian reaches it).  0 <= n <= 2^24. */
+int fm_gaussian_force(const fm_grid *g, int dtype, double dx, int n, const void *center, const void *inv_radius,
+                      const void *strength, void *f_x, void *f_y, void *f_z, void *stream);
+/* Per-Gaussian sums over the faces of its support (calculate_adj_gausion_force_kernel,
+ * 3D/lfm_midpoint_diff_simulator.py:63-110; 2D/shape/lfm_midpoint_diff_simulator.py:75-103):
+ * adj_strength[I][c] = sum e a_c, adj_center[I] = sum_c sum s_c e 2 (X - c_I) r a_c,
+ * penalty_strength[I][c] = sum 2 f e, penalty_center[I] = sum_c sum 2 f s_c e 2 (X - c_I) r,
+ * e = exp(-q), f = e s_c, a = adj_{x,y,z}.  Outputs: device FP64, n x dim each,
+ * overwritten (the reference zero-fills them first); deterministic summation. */
+int fm_gaussian_force_grad(const fm_grid *g, int dtype, double dx, int n, const void *center, const void *inv_radius,
+                           const void *strength, const void *adj_x, const void *adj_y, const void *adj_z,
+                           double *adj_center, double *adj_strength, double *penalty_center, double *penalty_strength,
+                           void *stream);
+
+/* ------------------------------------------------------------------------
  * 2D vortex problem (the vortex optimisation's control map and loss).
  * theta = [w_0..w_{K-1}, cx_0..cx_{K-1}, cy_0..cy_{K-1}], K <= 64, host array.
  * ------------------------------------------------------------------------ */

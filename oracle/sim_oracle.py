@@ -9,8 +9,8 @@ sequences, which the product fuses):
   adjoint  3D/lfm_midpoint_diff_simulator.py:336-594 (init_gradient case 11,
            backtrack_step_midpoint, backtrack_flow_map)
   BFECC    3D/flowmap.py:405-452
-with add_control_force=False, use_short_BFECC=False, BFECC_clamp=False,
-viscosity=0 and empty obstacle masks.  The trajectory the reference writes to
+with viscosity=0 and empty obstacle masks; use_short_BFECC, BFECC_clamp and
+Gaussian control forces (add_control_force) as the constructor selects.  The trajectory the reference writes to
 .npy files is kept in Python lists.  Two documented extensions match the
 product: a run whose last reinit interval is partial stores that interval's
 forward map at the last step, and the Adams-Bashforth index counts adjoint
@@ -21,6 +21,7 @@ from __future__ import annotations
 
 import numpy as np
 
+import force_oracle
 from oracle import MGParams, Oracle
 
 
@@ -39,13 +40,17 @@ def clamp_u(u, u1):
 
 class OracleSim:
     def __init__(self, res, dx, dt, reinit_every, total_steps, rk=4, backward_u=True, passive=True,
-                 trajectory_loss=False, prec="f64", mg=None, bfecc_clamp=False, short_bfecc=False):
+                 trajectory_loss=False, prec="f64", mg=None, bfecc_clamp=False, short_bfecc=False,
+                 control_forces=None):
         self.o = Oracle(tuple(res), prec)
         self.dim = len(res)
         self.res = tuple(res)
         self.dx, self.dt, self.R, self.total_steps = dx, dt, reinit_every, total_steps
         self.rk, self.backward_u, self.passive_on, self.trajectory_loss = rk, backward_u, passive, trajectory_loss
         self.bfecc_clamp, self.short = bfecc_clamp, short_bfecc
+        # per step n: (center n x dim, inv_radius n, strength n x dim) in the run's dtype
+        self.cf = control_forces
+        self.cf_grads = {}
         if short_bfecc:
             o = self.o
             self.psi_tem, self.phi_tem = o.zeros_cell(self.dim), o.zeros_cell(self.dim)
@@ -164,6 +169,11 @@ class OracleSim:
         for step in reversed(range(curr_step)):
             self.march_no_neural(step)
 
+    def control_force(self, n):
+        """apply_gausion_force with step n's parameters (force_oracle.py)."""
+        cen, inv_r, st = self.cf[n]
+        return force_oracle.gaussian_force(self.res, self.dx, cen, inv_r, st)
+
     def step_midpoint(self):
         self.step_num += 1
         n = self.step_num
@@ -181,6 +191,10 @@ class OracleSim:
         for c in range(d):
             self.ad_u[c][...] = self.u[c]
         o.advect_u_grid(self.rk, self.ad_u, self.ad_u, self.u, self.dx, 0.5 * dt)
+        if self.cf is not None:  # 3D/lfm_midpoint_simulator.py:694-706
+            f = self.control_force(self.step_num)
+            for c in range(d):
+                self.u[c][...] = self.u[c] + (0.5 * dt) * f[c]
         self.Poisson(self.u)
         self.velocity_storage[j] = [x.copy() for x in self.u]
         self.march_phi_grid()
@@ -200,6 +214,11 @@ class OracleSim:
             o.advect_u_grid(self.rk, self.u, self.ad_u, self.final_u, self.dx, dt)
             for c in range(d):
                 self.u[c][...] = self.final_u[c]
+        if self.cf is not None:  # 3D/lfm_midpoint_simulator.py:755-760
+            f = self.control_force(self.step_num)
+            for c in range(d):
+                self.u[c][...] = self.u[c] + dt * f[c]
+            o.accumulate_init(f, self.init_u, self.F_f, self.phi_f, self.dx, dt)
         self.Poisson(self.u)
         n = self.step_num
         if j == self.R - 1:
@@ -265,6 +284,10 @@ class OracleSim:
     def backtrack_flow_map(self, j, dt):
         o, d, dx = self.o, self.dim, self.dx
         n = self.step_num
+        if self.cf is not None:  # 3D/lfm_midpoint_diff_simulator.py:423-427
+            f_ctrl = self.control_force(n) if self.backward_u else None
+            cen, inv_r, st = self.cf[n]
+            self.cf_grads[n] = force_oracle.gaussian_force_grad(self.res, dx, cen, inv_r, st, self.adj_u)
         for c in range(d):
             self.mid_u[c][...] = self.store_mid[n][c]
         o.calculate_nabla_u_w(self.u if self.backward_u else self.mid_u, self.adj_u, self.src, dx)
@@ -317,6 +340,10 @@ class OracleSim:
             o.accumulate_init(self.adj_passive_f, self.init_adj_u, self.T_f, self.psi_f, dx, -dt)
         self.Poisson(self.adj_u)
         if self.backward_u:
+            if self.cf is not None:  # 3D/lfm_midpoint_diff_simulator.py:525-530
+                for c in range(d):
+                    self.u[c][...] = self.u[c] + (-dt) * f_ctrl[c]
+                o.accumulate_init(f_ctrl, self.init_u, self.T_f, self.psi_f, dx, -dt)
             self.Poisson(self.u)
         if j == 0:
             phi, phi_f, F_f = self.store_maps[n // self.R]
