@@ -53,7 +53,8 @@ def parse():
                          "a reported bench value needs W >= 3)")
     ap.add_argument("--gaussians", type=int, default=3000, help="Gaussian control forces per step (shape3d-forces)")
     ap.add_argument("--workload", default="gradient",
-                    choices=["gradient", "poisson", "vortex2d", "vortex2d-batch", "shape3d-forces"],
+                    choices=["gradient", "poisson", "vortex2d", "vortex2d-batch", "shape3d-forces",
+                             "force-kernels"],
                     help="gradient: the headline 3D gradient benchmark; poisson: the mixed-precision Poisson solve "
                          "(seeded k^-5/3 divergence RHS, all-Neumann, --poisson-res^3); vortex2d: the 2D vortex "
                          "optimisation gradient dL/dtheta (256^2, 100 steps, 4 vortices); shape3d-forces: the 3D "
@@ -403,16 +404,7 @@ def run_shape3d_forces(a):
                                rel_tol=1e-6 if dtype == torch.float32 else 1e-20)
         return replace(cfg, add_control_force=forces, control_num=ng)
 
-    rng = np.random.default_rng(40)
-    ks = np.array([1, 1, 1, 1, 2, 3, 4, 5, 6, 7, 8, 9], dtype=np.float64)  # 3D/optimize_shape_G_R.py:21-34
-    host = []
-    for n in range(steps):
-        inv_r = 1.0 / (rng.choice(ks, size=ng) * dx) ** 2
-        cen = rng.uniform(0.0, 1.0, size=(ng, 3))
-        v = rng.normal(size=(ng, 3))
-        st = rng.uniform(5e-3, 2e-2, size=(ng, 1)) * 2.0 * v / np.linalg.norm(v, axis=1, keepdims=True)
-        host.append({"c": cen.astype(np.float32), "r": inv_r.astype(np.float32), "s": st.astype(np.float32),
-                     "n": ng})
+    host = _case11_gaussians(res, ng, steps)
     devp = [{k: (torch.tensor(v, device=dev) if k != "n" else v) for k, v in p.items()} for p in host]
     u0, rho0, rho_t = C.shape3d_inputs(res)
     f32 = torch.float32
@@ -486,6 +478,8 @@ def run_shape3d_forces(a):
                "param_grads_rel_l2": (pnum / pden) ** 0.5 if pden > 0 else None}
         del s64
 
+    stored = getattr(sim, "store_force", None) is not None
+    nforce = steps if stored else 2 * steps
     h2d = sum(x.numel() * 4 for x in h_u0) + h_r0.numel() * 4 + h_rt.numel() * 4 + steps * ng * 7 * 4 * 2
     d2h = sum(x.numel() * 4 for x in h_grad) + 8
     line = {"metric": "3D fwd+adjoint grads/s with Gaussian control forces, 128^3, 120 steps, 3000 Gaussians/step",
@@ -500,9 +494,99 @@ def run_shape3d_forces(a):
             "gpu_launches": launches,
             "without_forces": {"grads_per_s": 1e3 / ms_nof, "ms_per_grad": ms_nof},
             "force_kernels": {"k_gauss_force_us": us_force, "k_gauss_grad_us": us_grad,
-                              "launches_per_grad": {"k_gauss_force": 2 * steps, "k_gauss_grad": steps},
-                              "ms_per_grad": (2 * steps * us_force + steps * us_grad) / 1e3},
+                              "launches_per_grad": {"k_gauss_force": nforce, "k_gauss_grad": steps},
+                              "ms_per_grad": (nforce * us_force + steps * us_grad) / 1e3,
+                              "adjoint_force": "read from the forward's store" if stored else "re-evaluated"},
             "error_vs_fp64": err}
+    print(json.dumps(line), flush=True)
+    return 0
+
+
+def _case11_gaussians(res, ng, steps, seed=40):
+    """Seeded synthetic Gaussian parameters per step, drawn as the reference's
+    3D optimiser draws radii and centres (3D/optimize_shape_G_R.py:21-53);
+    strengths |s| in [0.01, 0.04] in a uniform direction."""
+    import numpy as np
+
+    dx = 1.0 / res
+    rng = np.random.default_rng(seed)
+    ks = np.array([1, 1, 1, 1, 2, 3, 4, 5, 6, 7, 8, 9], dtype=np.float64)
+    out = []
+    for _ in range(steps):
+        inv_r = 1.0 / (rng.choice(ks, size=ng) * dx) ** 2
+        cen = rng.uniform(0.0, 1.0, size=(ng, 3))
+        v = rng.normal(size=(ng, 3))
+        st = rng.uniform(5e-3, 2e-2, size=(ng, 1)) * 2.0 * v / np.linalg.norm(v, axis=1, keepdims=True)
+        out.append({"c": cen.astype(np.float32), "r": inv_r.astype(np.float32), "s": st.astype(np.float32),
+                    "n": ng})
+    return out
+
+
+def _pairs_in_support(p, res):
+    """Exact count of (face, Gaussian) pairs with |X - c|^2 r < 5 (float64)."""
+    import numpy as np
+
+    dx = 1.0 / res
+    pairs = 0
+    for k in range(3):
+        ax = [(np.arange(res + (1 if a == k else 0)) + (0.0 if a == k else 0.5)) * dx for a in range(3)]
+        for I in range(p["n"]):
+            rad = np.sqrt(5.0 / p["r"][I])
+            sel = [np.abs(ax[a] - p["c"][I, a]) < rad for a in range(3)]
+            x, y, z = (ax[a][sel[a]] - p["c"][I, a] for a in range(3))
+            d2 = x[:, None, None] ** 2 + y[None, :, None] ** 2 + z[None, None, :] ** 2
+            pairs += int(np.count_nonzero(d2 * p["r"][I] < 5.0))
+    return pairs
+
+
+def run_force_kernels(a):
+    """The two Gaussian-force kernels alone at --res^3 with --gaussians Gaussians
+    (case-11 draws), FP32: fm_gaussian_force (every face) and
+    fm_gaussian_force_grad (per-Gaussian sums against a seeded adjoint field).
+    Unit of work: a (face, Gaussian) pair inside the support, counted exactly."""
+    import torch
+
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    torch.cuda.set_device(local)
+    dev = torch.device("cuda", local)
+    K = importlib.import_module("differentiable-flowmap_b200.kernels")
+    fm = importlib.import_module("differentiable-flowmap_b200")
+    res, ng = a.res, a.gaussians
+    dx = 1.0 / res
+    p = _case11_gaussians(res, ng, 1)[0]
+    c, r, st = (torch.tensor(p[k], device=dev) for k in ("c", "r", "s"))
+    g = K.GridSpec((res, res, res))
+    f = [torch.empty(g.face_shape(k), dtype=torch.float32, device=dev) for k in range(3)]
+    gen = torch.Generator(device=dev).manual_seed(7)
+    adj = [torch.randn(g.face_shape(k), dtype=torch.float32, device=dev, generator=gen) for k in range(3)]
+    pairs = _pairs_in_support(p, res)
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+
+    def timed(fn):
+        for _ in range(a.warmup):
+            fn()
+        torch.cuda.synchronize(dev)
+        e0.record()
+        for _ in range(a.steps):
+            fn()
+        e1.record()
+        torch.cuda.synchronize(dev)
+        return e0.elapsed_time(e1) * 1e3 / a.steps
+
+    fm._lib.launch_count(reset=True)
+    us_f = timed(lambda: K.gaussian_force(g, dx, c, r, st, f))
+    us_g = timed(lambda: K.gaussian_force_grad(g, dx, c, r, st, adj))
+    launches = fm._lib.launch_count(reset=True)
+    line = {"metric": "Gaussian control-force kernel, (face, Gaussian) pairs/s", "value": pairs / (us_f * 1e-6),
+            "unit": "pairs/s", "n_gpus": 1, "steps": a.steps, "warmup": a.warmup, "ms_per_step": us_f / 1e3,
+            "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32",
+            "data": "synthetic",
+            "config": {"workload": f"fm_gaussian_force / fm_gaussian_force_grad at {res}^3, {ng} Gaussians "
+                                   "(case-11 radius and centre draws, seed 40)",
+                       "pairs_in_support": pairs,
+                       "l2": "inputs (25 MB per field) fit in L2; the kernels are compute-bound"},
+            "gpu_launches": launches,
+            "k_gauss_force_us": us_f, "k_gauss_grad_us": us_g, "grad_pairs_per_s": pairs / (us_g * 1e-6)}
     print(json.dumps(line), flush=True)
     return 0
 
@@ -519,6 +603,8 @@ def main():
         return run_vortex2d_batch(a)
     if a.workload == "shape3d-forces":
         return run_shape3d_forces(a)
+    if a.workload == "force-kernels":
+        return run_force_kernels(a)
 
     import torch
     import torch.distributed as dist

@@ -13,21 +13,35 @@
 // the faces of its support of
 //     adj_strength[c] += e a_c            adj_center += s_c e 2 (X - c) r a_c
 //     pen_strength[c] += 2 f e            pen_center += 2 f s_c e 2 (X - c) r
-// with e = exp(-q), f = e s_c and a the adjoint velocity, in the reference's
-// operation order per face, accumulated in FP64.
+// with e = exp(-q), f = e s_c and a the adjoint velocity.
 //
-// B200 mapping.  3000 Gaussians against every face is compute work, so both
-// kernels cull by support first:
+// Inclusion is decided exactly as the reference rounds it: s2 = sum (X - c)^2
+// (left to right, no FMA contraction), d = sqrt(s2), q = (d d) r, q < 5.
+// Off the boundary (s2 r outside 5 (1 -+ 1e-4)) the decision cannot depend on
+// the rounding of d d and is taken without the square root (against
+// 5 (1 -+ 1e-4) / r - s2_other, for the faces of a column).  The weight uses
+// the Gaussian's separability, exp(-r s2) = exp(-r s2_other) exp(-r dz^2),
+// which differs from exp(-q) by a few ulps.
+//
+// B200 mapping.  3000 Gaussians against every face is compute work.  Both
+// kernels give each thread a column of faces along the fastest axis (k in 3D,
+// j in 2D), tabulate per Gaussian the squared offsets and the factors
+// exp(-r dx_a^2) in shared memory (every axis in the force kernel, the column
+// axis in the adjoint), and combine the other axes once per (column,
+// Gaussian); a face then costs two shared loads, a compare and an FMA.
 //  * k_gauss_force: one CTA per tile of cells (16x16 in 2D, 8x8x8 in 3D).  The
-//    CTA walks the Gaussians in chunks of 256, keeps those whose support ball
-//    (radius sqrt(5/r), widened) reaches the tile's box, compacted in
-//    ascending order into shared memory (ballot + popc prefix), and every
-//    thread accumulates its faces over that list.  The cull is a superset of
-//    the exact per-face test, which decides inclusion with the reference's
-//    rounding (no FMA contraction), so culling never changes a sum.
-//  * k_gauss_grad: one CTA per Gaussian over the face-index box of its
-//    support; fixed-order warp-shuffle + shared-memory reduction, so the
-//    result is deterministic (the reference's atomics are not).
+//    CTA walks the Gaussians in chunks of 256 and appends those whose support
+//    ball (radius sqrt(5/r), widened) reaches the tile's box to a list in
+//    shared memory, in ascending order (ballot + popc prefix); once the list
+//    could not take another chunk, or at the end, it tabulates the listed
+//    Gaussians a sub-chunk at a time and every thread accumulates its column
+//    segment over them in list order.  The cull is a superset of the exact test.
+//  * k_gauss_grad: one CTA per Gaussian over the columns of its support box;
+//    each column's faces are summed in registers of the run's type and
+//    flushed to FP64 per column; fixed-order warp-shuffle + shared-memory
+//    reduction, so the result is deterministic (the reference's atomics are
+//    not).  Gaussians with r <= 0 or a support wider than the table take a
+//    per-face path in the reference's operation order.
 #include <math.h>
 
 #include "fm_common.cuh"
@@ -38,31 +52,49 @@ namespace fm {
 constexpr int kGfThreads = 256;
 constexpr int kGfWarps = kGfThreads / 32;
 constexpr int kGfMaxN = 1 << 24;
+constexpr int kGfTab = 256;   // column-table capacity of the adjoint kernel (faces)
 
+// Tiles of the force kernel; the column axis is D-1.  SEG: faces per thread
+// along it (one segment per thread: 3D 9*8 + 8*9 + 8*8 = 208, 2D 17*4 + 16*5 = 148).
 template <int D> struct GfTile;
-template <> struct GfTile<2> { static constexpr int B0 = 16, B1 = 16, B2 = 1, F = 2; };  // 17*16 faces <= 2*256
-template <> struct GfTile<3> { static constexpr int B0 = 8, B1 = 8, B2 = 8, F = 3; };    // 9*8*8 faces <= 3*256
+template <> struct GfTile<2> { static constexpr int B0 = 16, B1 = 16, B2 = 1, BC = 16, SEG = 4; };
+template <> struct GfTile<3> { static constexpr int B0 = 8, B1 = 8, B2 = 8, BC = 8, SEG = 9; };
 
-// Relative widening of the support radius used by the culls; far above the
-// few ulps by which the exact test's rounding can move the boundary.
+// Relative widening of the support radius used by the culls and by the
+// square-root-free decisions; far above the few ulps by which the rounding of
+// the exact test can move the boundary.
 constexpr double kGfMargin = 1e-4;
 
-// The exact inclusion test and weight at one face, with the reference's
-// rounding: d = sqrt(sum (X - c)^2), q = (d d) r, included iff q < 5, e = exp(-q).
-// The pre-test rejects, without the square root, faces whose s2 r exceeds 5 by
-// more than the rounding of the exact path can account for.
+// Position of index i along an axis: face grids at i dx on their own axis,
+// (i + 1/2) dx elsewhere (node_pos, 3D/taichi_utils.py:95-128).
+template <typename T>
+__device__ __forceinline__ T gf_pos(int i, bool face, T dx) {
+  T f = (T)i;
+  if (!face) f = f + (T)0.5;
+  return f * dx;
+}
+
+// Inclusion of a face with squared distance s2 (rounded as the reference
+// rounds it) for inverse radius r.
+template <typename T>
+__device__ __forceinline__ bool gf_inside(T s2, T r) {
+  const T t = rn_mul(s2, r);
+  if (t < (T)(5.0 * (1.0 - kGfMargin))) return true;   // r <= 0 lands here too
+  if (t > (T)(5.0 * (1.0 + kGfMargin))) return false;
+  const T d = sqrt(s2);                                   // near the boundary: the exact test
+  return rn_mul(rn_mul(d, d), r) < (T)5;                  // NaN excluded
+}
+
+// The per-face path: exact test and weight at one face.
 template <typename T, int D>
-__device__ __forceinline__ bool gf_weight(const T* p, const T* c, T r, T* dp, T& e, T& q) {
+__device__ __forceinline__ bool gf_weight(const T* p, const T* c, T r, T* dp, T& e) {
 #pragma unroll
   for (int a = 0; a < D; ++a) dp[a] = rn_sub(p[a], c[a]);
   T s2 = rn_mul(dp[0], dp[0]);
 #pragma unroll
   for (int a = 1; a < D; ++a) s2 = rn_add(s2, rn_mul(dp[a], dp[a]));
-  if (r > (T)0 && rn_mul(s2, r) > (T)(5.0 * (1.0 + kGfMargin))) return false;
-  const T d = sqrt(s2);
-  q = rn_mul(rn_mul(d, d), r);
-  if (!(q < (T)5)) return false;
-  e = exp(-q);
+  if (!gf_inside(s2, r)) return false;
+  e = exp(-rn_mul(s2, r));
   return true;
 }
 
@@ -87,8 +119,16 @@ __global__ void __launch_bounds__(kGfThreads) k_gauss_force(fm_grid g, T dx, int
                                                             T* __restrict__ f0, T* __restrict__ f1,
                                                             T* __restrict__ f2) {
   using Tl = GfTile<D>;
-  constexpr int F = Tl::F;
-  __shared__ T s_c[D][kGfThreads], s_s[D][kGfThreads], s_r[kGfThreads];
+  constexpr int CA = D - 1, SEG = Tl::SEG;
+  constexpr int BM = (Tl::B0 > Tl::BC ? Tl::B0 : Tl::BC) + 1;        // table entries per axis and variant
+  constexpr int SUB = sizeof(T) == 4 ? 64 : 32;                       // Gaussians tabulated at a time
+  constexpr int TS = D * 2 * BM;                                      // table entries per Gaussian
+  constexpr int CAP = sizeof(T) == 4 ? 2 * kGfThreads : kGfThreads;  // culled-list capacity
+  __shared__ T s_c[D][CAP], s_s[D][CAP], s_r[CAP];
+  // per tabulated Gaussian l, axis a, variant v (0 cell, 1 face), index q - lo[a]:
+  // squared offset and exp(-r offset^2)
+  __shared__ T t_sq[SUB][D][2][BM], t_ex[SUB][D][2][BM];
+  __shared__ T t_lo[SUB], t_hi[SUB];  // 5 (1 -+ m) / r, or +inf for r <= 0
   __shared__ int s_cnt[kGfWarps];
 
   const int nt1 = (g.n[1] + Tl::B1 - 1) / Tl::B1, nt2 = (g.n[2] + Tl::B2 - 1) / Tl::B2;
@@ -107,13 +147,44 @@ __global__ void __launch_bounds__(kGfThreads) k_gauss_force(fm_grid g, T dx, int
     bhi[a] = ((double)hc[a] + 1.01) * (double)dx;
   }
 
-  T acc[D][F];
+  // this thread's segment: component cc, tile-local other-axis indices io[],
+  // tile-local column indices [k0, k0 + len)
+  int cc = -1, io[2] = {0, 0}, k0 = 0, len = 0;
+  {
+    int q = threadIdx.x;
 #pragma unroll
-  for (int c = 0; c < D; ++c)
+    for (int comp = 0; comp < D; ++comp) {
+      if (cc < 0) {
+        int e[3];
 #pragma unroll
-    for (int m = 0; m < F; ++m) acc[c][m] = (T)0;
+        for (int a = 0; a < 3; ++a) e[a] = hc[a] + (comp == a && hc[a] == g.n[a]) - lo[a];
+        const int nseg = (e[CA] + SEG - 1) / SEG;
+        const int cnt = (D == 3 ? e[0] * e[1] : e[0]) * nseg;
+        if (q < cnt) {
+          cc = comp;
+          const int sg = q % nseg, o = q / nseg;
+          if (D == 3) {
+            io[0] = o / e[1];
+            io[1] = o % e[1];
+          } else {
+            io[0] = o;
+          }
+          k0 = sg * SEG;
+          len = min(SEG, e[CA] - sg * SEG);
+        } else {
+          q -= cnt;
+        }
+      }
+    }
+  }
+  const int v0 = cc == 0 ? 1 : 0, v1 = cc == 1 ? 1 : 0, vc = cc == CA ? 1 : 0;
+
+  T acc[SEG];
+#pragma unroll
+  for (int m = 0; m < SEG; ++m) acc[m] = (T)0;
 
   const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
+  int listed = 0;  // culled Gaussians waiting in the list (uniform across the CTA)
   for (int base = 0; base < n; base += kGfThreads) {
     const int I = base + threadIdx.x;
     T c[D], s[D], r = (T)0;
@@ -130,15 +201,15 @@ __global__ void __launch_bounds__(kGfThreads) k_gauss_force(fm_grid g, T dx, int
     const unsigned m = __ballot_sync(0xffffffffu, hit);
     if (lane == 0) s_cnt[w] = __popc(m);
     __syncthreads();
-    int off = 0, tot = 0;
+    int off = 0, got = 0;
 #pragma unroll
     for (int k = 0; k < kGfWarps; ++k) {
       const int v = s_cnt[k];
       off += k < w ? v : 0;
-      tot += v;
+      got += v;
     }
-    if (hit) {
-      const int slot = off + __popc(m & ((1u << lane) - 1u));
+    if (hit) {  // appended in ascending order after the Gaussians already listed
+      const int slot = listed + off + __popc(m & ((1u << lane) - 1u));
 #pragma unroll
       for (int a = 0; a < D; ++a) {
         s_c[a][slot] = c[a];
@@ -147,47 +218,68 @@ __global__ void __launch_bounds__(kGfThreads) k_gauss_force(fm_grid g, T dx, int
       s_r[slot] = r;
     }
     __syncthreads();
-    if (tot > 0) {
-#pragma unroll
-      for (int cc = 0; cc < D; ++cc) {
-        const int e0 = hc[0] + (cc == 0 && hc[0] == g.n[0]) - lo[0];
-        const int e1 = hc[1] + (cc == 1 && hc[1] == g.n[1]) - lo[1];
-        const int e2 = hc[2] + (cc == 2 && hc[2] == g.n[2]) - lo[2];
-#pragma unroll
-        for (int fm_ = 0; fm_ < F; ++fm_) {
-          const int q = threadIdx.x + fm_ * kGfThreads;
-          if (q >= e0 * e1 * e2) continue;
-          const int k = q % e2, ij = q / e2, j = ij % e1, i = ij / e1;
-          T p[D];
-          node_pos<T, D>(cc, lo[0] + i, lo[1] + j, lo[2] + k, dx, p);
-          T a = acc[cc][fm_];
-          for (int l = 0; l < tot; ++l) {
-            T cl[D], dp[D], e, qq;
-#pragma unroll
-            for (int b = 0; b < D; ++b) cl[b] = s_c[b][l];
-            if (gf_weight<T, D>(p, cl, s_r[l], dp, e, qq)) a = rn_add(a, rn_mul(e, s_s[cc][l]));
+    listed += got;
+    // evaluate once the list could not take another chunk, or at the end
+    if (listed > CAP - kGfThreads || base + kGfThreads >= n) {
+      const int tot = listed;
+      listed = 0;
+      for (int sub = 0; sub < tot; sub += SUB) {
+        const int cnt = min(SUB, tot - sub);
+        for (int x = threadIdx.x; x < cnt * TS; x += kGfThreads) {
+          const int l = x / TS, rem = x - l * TS, a = rem / (2 * BM), rv = rem - a * 2 * BM, v = rv / BM,
+                    q = rv - v * BM;
+          const T rr = s_r[sub + l];
+          const T d = rn_sub(gf_pos<T>(lo[a] + q, v == 1, dx), s_c[a][sub + l]);
+          const T sq = rn_mul(d, d);
+          t_sq[l][a][v][q] = sq;
+          t_ex[l][a][v][q] = exp(-rn_mul(sq, rr));
+          if (rem == 0) {
+            const bool pos = rr > (T)0;
+            t_lo[l] = pos ? (T)(5.0 * (1.0 - kGfMargin)) / rr : (T)INFINITY;
+            t_hi[l] = pos ? (T)(5.0 * (1.0 + kGfMargin)) / rr : (T)INFINITY;
           }
-          acc[cc][fm_] = a;
         }
+        __syncthreads();
+        if (cc >= 0) {
+          for (int l = 0; l < cnt; ++l) {
+            // the other axes once per (column, Gaussian)
+            T sxy = t_sq[l][0][v0][io[0]], exy = t_ex[l][0][v0][io[0]];
+            if (D == 3) {
+              sxy = rn_add(sxy, t_sq[l][1][v1][io[1]]);
+              exy = exy * t_ex[l][1][v1][io[1]];
+            }
+            // dz^2 < A: inside off the boundary; dz^2 > B: outside; between: the exact test
+            const T B = t_hi[l] - sxy;
+            if (B < (T)0) continue;  // the column misses the support
+            const T A = t_lo[l] - sxy, rr = s_r[sub + l];
+            const T ev = exy * s_s[cc][sub + l];
+#pragma unroll
+            for (int q = 0; q < SEG; ++q) {
+              if (q < len) {
+                const T sq = t_sq[l][CA][vc][k0 + q];
+                bool in = sq < A;
+                if (!in && sq <= B) {
+                  const T d = sqrt(rn_add(sxy, sq));
+                  in = rn_mul(rn_mul(d, d), rr) < (T)5;
+                }
+                if (in) acc[q] += ev * t_ex[l][CA][vc][k0 + q];
+              }
+            }
+          }
+        }
+        __syncthreads();  // the next tables / list entries overwrite what was read
       }
     }
-    __syncthreads();  // the next chunk overwrites the list and the counts
   }
 
-#pragma unroll
-  for (int cc = 0; cc < D; ++cc) {
+  if (cc >= 0) {
     const Shape fs = face_shape(g, cc);
-    const int e0 = hc[0] + (cc == 0 && hc[0] == g.n[0]) - lo[0];
-    const int e1 = hc[1] + (cc == 1 && hc[1] == g.n[1]) - lo[1];
-    const int e2 = hc[2] + (cc == 2 && hc[2] == g.n[2]) - lo[2];
+    T* const o = cc == 0 ? f0 : (cc == 1 ? f1 : f2);
+    const long b = D == 3 ? fs.idx(lo[0] + io[0], lo[1] + io[1], lo[2] + k0) : fs.idx(lo[0] + io[0], lo[1] + k0, 0);
+    const long st = D == 3 ? 1 : fs.s2;  // the column axis is contiguous (3D: k; 2D: j with s2 == 1)
 #pragma unroll
-    for (int fm_ = 0; fm_ < F; ++fm_) {
-      const int q = threadIdx.x + fm_ * kGfThreads;
-      if (q >= e0 * e1 * e2) continue;
-      const int k = q % e2, ij = q / e2, j = ij % e1, i = ij / e1;
-      T* const o = cc == 0 ? f0 : (cc == 1 ? f1 : f2);
-      o[fs.idx(lo[0] + i, lo[1] + j, lo[2] + k)] = acc[cc][fm_];
-    }
+    for (int q = 0; q < SEG; ++q)
+      if (q < len) o[b + q * st] = acc[q];
   }
 }
 
@@ -213,15 +305,19 @@ __device__ __forceinline__ void gf_axis_range(double x, double R, double dx, boo
   i1 = (int)b;
 }
 
+// Per-Gaussian sums v[c] adj_strength, v[D+a] adj_center, v[2D+c]
+// pen_strength, v[3D+a] pen_center (FP64).
 template <typename T, int D>
-__global__ void __launch_bounds__(kGfThreads) k_gauss_grad(fm_grid g, T dx, const T* __restrict__ cen,
-                                                           const T* __restrict__ ir, const T* __restrict__ str,
-                                                           const T* __restrict__ a0, const T* __restrict__ a1,
-                                                           const T* __restrict__ a2, double* __restrict__ adj_c,
-                                                           double* __restrict__ adj_s, double* __restrict__ pen_c,
-                                                           double* __restrict__ pen_s) {
-  constexpr int NV = 4 * D;  // adj_strength, adj_center, pen_strength, pen_center
+__global__ void __launch_bounds__(kGfThreads, 4) k_gauss_grad(fm_grid g, T dx, const T* __restrict__ cen,
+                                                              const T* __restrict__ ir, const T* __restrict__ str,
+                                                              const T* __restrict__ a0, const T* __restrict__ a1,
+                                                              const T* __restrict__ a2, double* __restrict__ adj_c,
+                                                              double* __restrict__ adj_s, double* __restrict__ pen_c,
+                                                              double* __restrict__ pen_s) {
+  constexpr int NV = 4 * D;
+  constexpr int CA = D - 1;
   __shared__ double s_red[kGfWarps][NV];
+  __shared__ T t_dp[kGfTab], t_ex[kGfTab];
   const int I = blockIdx.x;
   T c[D], s[D];
 #pragma unroll
@@ -239,7 +335,6 @@ __global__ void __launch_bounds__(kGfThreads) k_gauss_grad(fm_grid g, T dx, cons
 #pragma unroll
     for (int a = 0; a < D; ++a) none = none || !isfinite((double)c[a]);
   }
-  const T* const adj[3] = {a0, a1, a2};
   double v[NV];
 #pragma unroll
   for (int k = 0; k < NV; ++k) v[k] = 0.0;
@@ -248,32 +343,102 @@ __global__ void __launch_bounds__(kGfThreads) k_gauss_grad(fm_grid g, T dx, cons
 #pragma unroll
     for (int cc = 0; cc < D; ++cc) {
       const Shape fs = face_shape(g, cc);
+      const T* const adj = cc == 0 ? a0 : (cc == 1 ? a1 : a2);
       int i0[3] = {0, 0, 0}, i1[3] = {0, 0, 0};
 #pragma unroll
       for (int a = 0; a < D; ++a) gf_axis_range((double)c[a], R, (double)dx, a == cc, axis_len(fs, a), i0[a], i1[a]);
       const int e0 = i1[0] - i0[0] + 1, e1 = i1[1] - i0[1] + 1, e2 = i1[2] - i0[2] + 1;
       if (e0 <= 0 || e1 <= 0 || e2 <= 0) continue;
-      // a face grid holds fewer than 2^32 entries (validate_grid): 32-bit decode
-      const unsigned cnt = (unsigned)e0 * (unsigned)e1 * (unsigned)e2;
+      const int ecol = CA == 2 ? e2 : e1;
       const T sc = s[cc];
-      for (unsigned q = threadIdx.x; q < cnt; q += kGfThreads) {
-        const unsigned ij = q / (unsigned)e2;
-        const int k = (int)(q - ij * (unsigned)e2);
-        const unsigned ii = ij / (unsigned)e1;
-        const int j = (int)(ij - ii * (unsigned)e1), i = (int)ii;
-        T p[D], dp[D], e, qq;
-        node_pos<T, D>(cc, i0[0] + i, i0[1] + j, i0[2] + k, dx, p);
-        if (!gf_weight<T, D>(p, c, r, dp, e, qq)) continue;
-        const T av = adj[cc][fs.idx(i0[0] + i, i0[1] + j, i0[2] + k)];
-        const T f = rn_mul(e, sc);
-        v[cc] += (double)rn_mul(e, av);                       // adj_strength[c]
-        v[2 * D + cc] += (double)rn_mul(rn_mul((T)2, f), e);  // pen_strength[c]
-        const T ga = rn_mul(rn_mul(sc, e), (T)2);             // s e 2
-        const T gp = rn_mul(rn_mul(rn_mul(rn_mul((T)2, f), sc), e), (T)2);  // 2 f s e 2
+      if (r > (T)0 && ecol <= kGfTab) {
+        // column path: the column axis tabulated, the other axes per column
+        __syncthreads();  // the previous component's columns are done with the table
+        for (int q = threadIdx.x; q < ecol; q += kGfThreads) {
+          const T dz = rn_sub(gf_pos<T>(i0[CA] + q, cc == CA, dx), c[CA]);
+          t_dp[q] = dz;
+          t_ex[q] = exp(-rn_mul(rn_mul(dz, dz), r));
+        }
+        __syncthreads();
+        const double k1 = 2.0 * (double)sc * (double)r, k2 = 4.0 * (double)sc * (double)sc * (double)r,
+                     k3 = 2.0 * (double)sc;
+        const double rcap = 5.0 * (1.0 + kGfMargin) / (double)r, off = cc == CA ? 0.0 : 0.5;
+        const T tlo = (T)(5.0 * (1.0 - kGfMargin)) / r, thi = (T)(5.0 * (1.0 + kGfMargin)) / r;
+        const int ncol = D == 3 ? e0 * e1 : e0;
+        for (int col = threadIdx.x; col < ncol; col += kGfThreads) {
+          int io[2] = {0, 0};
+          if (D == 3) {
+            io[0] = i0[0] + col / e1;
+            io[1] = i0[1] + col % e1;
+          } else {
+            io[0] = i0[0] + col;
+          }
+          T dpo[2] = {(T)0, (T)0}, sxy = (T)0;
 #pragma unroll
-        for (int a = 0; a < D; ++a) {
-          v[D + a] += (double)rn_mul(rn_mul(rn_mul(ga, dp[a]), r), av);  // adj_center
-          v[3 * D + a] += (double)rn_mul(rn_mul(gp, dp[a]), r);          // pen_center
+          for (int a = 0; a < CA; ++a) {
+            dpo[a] = rn_sub(gf_pos<T>(io[a], a == cc, dx), c[a]);
+            sxy = a == 0 ? rn_mul(dpo[a], dpo[a]) : rn_add(sxy, rn_mul(dpo[a], dpo[a]));
+          }
+          // dz^2 < A: inside off the boundary; dz^2 > B: outside; between: the exact test
+          const T A = tlo - sxy, B = thi - sxy;
+          if (B < (T)0) continue;  // the column misses the support
+          // the column's included faces lie within |dz| <= sqrt(5 (1 + m) / r - sxy)
+          const double half = sqrt(fmax(rcap - (double)sxy, 0.0)) + 0.01 * (double)dx;
+          const int qa = max(0, (int)ceil(((double)c[CA] - half) / (double)dx - off) - 1 - i0[CA]);
+          const int qb = min(ecol - 1, (int)floor(((double)c[CA] + half) / (double)dx - off) + 1 - i0[CA]);
+          const T exy = exp(-rn_mul(sxy, r));
+          // the column axis is contiguous in memory (3D: k; 2D: j, where s2 == 1)
+          const T* row = adj + (D == 3 ? fs.idx(io[0], io[1], i0[2]) : fs.idx(io[0], i0[1], 0));
+          T sea = (T)0, seaz = (T)0, se2 = (T)0, se2z = (T)0;
+          // straight-line body (weights selected to 0 outside): the loads pipeline
+#pragma unroll 4
+          for (int q = qa; q <= qb; ++q) {
+            const T dz = t_dp[q], sq = rn_mul(dz, dz);
+            bool in = sq < A;
+            if (!in && sq <= B) {  // rare: a face within the margin of the cutoff
+              const T d = sqrt(rn_add(sxy, sq));
+              in = rn_mul(rn_mul(d, d), r) < (T)5;
+            }
+            const T e = exy * t_ex[q], av = __ldg(row + q);
+            const T ea = in ? e * av : (T)0, e2 = in ? e * e : (T)0;  // selects: a NaN outside stays out
+            sea += ea;
+            seaz += ea * dz;
+            se2 += e2;
+            se2z += e2 * dz;
+          }
+          v[cc] += (double)sea;
+          v[2 * D + cc] += k3 * (double)se2;
+#pragma unroll
+          for (int a = 0; a < CA; ++a) {
+            v[D + a] += k1 * (double)dpo[a] * (double)sea;
+            v[3 * D + a] += k2 * (double)dpo[a] * (double)se2;
+          }
+          v[D + CA] += k1 * (double)seaz;
+          v[3 * D + CA] += k2 * (double)se2z;
+        }
+      } else {
+        // per-face path (r <= 0, or a support wider than the table), in the
+        // reference's operation order per face
+        const unsigned cnt = (unsigned)e0 * (unsigned)e1 * (unsigned)e2;  // < 2^32 (validate_grid)
+        for (unsigned q = threadIdx.x; q < cnt; q += kGfThreads) {
+          const unsigned ij = q / (unsigned)e2;
+          const int k = (int)(q - ij * (unsigned)e2);
+          const unsigned ii = ij / (unsigned)e1;
+          const int j = (int)(ij - ii * (unsigned)e1), i = (int)ii;
+          T p[D], dp[D], e;
+          node_pos<T, D>(cc, i0[0] + i, i0[1] + j, i0[2] + k, dx, p);
+          if (!gf_weight<T, D>(p, c, r, dp, e)) continue;
+          const T av = adj[fs.idx(i0[0] + i, i0[1] + j, i0[2] + k)];
+          const T f = rn_mul(e, sc);
+          v[cc] += (double)rn_mul(e, av);
+          v[2 * D + cc] += (double)rn_mul(rn_mul((T)2, f), e);
+          const T ga = rn_mul(rn_mul(sc, e), (T)2);
+          const T gp = rn_mul(rn_mul(rn_mul(rn_mul((T)2, f), sc), e), (T)2);
+#pragma unroll
+          for (int a = 0; a < D; ++a) {
+            v[D + a] += (double)rn_mul(rn_mul(rn_mul(ga, dp[a]), r), av);
+            v[3 * D + a] += (double)rn_mul(rn_mul(gp, dp[a]), r);
+          }
         }
       }
     }

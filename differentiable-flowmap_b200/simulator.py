@@ -68,6 +68,7 @@ class FlowmapConfig:
     use_short_BFECC: bool = False
     add_control_force: bool = False  # Gaussian control forces (control_force_para per step)
     control_num: int = 0             # capacity: most Gaussians one step may pass
+    store_control_force: bool = True  # adjoint with backward_u reads the forward's force fields from HBM
     trajectory_loss: bool = False  # reference's no-force branch: loss over reinit frames
     dtype: torch.dtype = torch.float32
     store_dtype: Optional[torch.dtype] = None  # checkpoint storage dtype (None: dtype)
@@ -356,6 +357,12 @@ class LFM_Simulator:
         c, r, st = self._gf.load({"c": center, "r": inverse_radius, "s": strength, "n": num})
         K.gaussian_force(self.grid, self.dx, c, r, st, f)
 
+    def _force_field(self, n):
+        """Where step n's control force is written: its slot of the trajectory
+        store when the adjoint will read it back, else the scratch field."""
+        st = getattr(self, "store_force", None)
+        return [x[n] for x in st] if st is not None else self.control_force
+
     def _control_params(self, control_force_para):
         if control_force_para is None:
             raise FlowmapError(2, "add_control_force needs control_force_para for every step")
@@ -404,9 +411,10 @@ class LFM_Simulator:
         _copy_mac(self.ad_u, self.u)
         self._advect_u_grid(self.ad_u, self.ad_u, self.u, 0.5 * curr_dt)
         if cfg.add_control_force:  # 3D/lfm_midpoint_simulator.py:694-706
-            K.gaussian_force(self.grid, self.dx, *self._control_params(control_force_para), self.control_force)
+            force = self._force_field(n)
+            K.gaussian_force(self.grid, self.dx, *self._control_params(control_force_para), force)
             for c in range(self.dim):
-                K.add_fields(self.u[c], self.control_force[c], self.u[c], 0.5 * curr_dt)
+                K.add_fields(self.u[c], force[c], self.u[c], 0.5 * curr_dt)
         self.project(self.u)
         # write_velocity + RW_Cache("u"): the midpoint velocity of step n
         for c in range(self.dim):
@@ -430,8 +438,8 @@ class LFM_Simulator:
             self.u, self.final_u = self.final_u, self.u
         if cfg.add_control_force:  # 3D/lfm_midpoint_simulator.py:755-760
             for c in range(self.dim):
-                K.add_fields(self.u[c], self.control_force[c], self.u[c], curr_dt)
-            K.accumulate_init(self.grid, self.dx, curr_dt, self.control_force, self.init_u, self.F_f, self.phi_f)
+                K.add_fields(self.u[c], force[c], self.u[c], curr_dt)
+            K.accumulate_init(self.grid, self.dx, curr_dt, force, self.init_u, self.F_f, self.phi_f)
         self.project(self.u)
 
         if j == self.reinit_every - 1:
@@ -480,6 +488,10 @@ class LFM_Diff_Simulator(LFM_Simulator):
             self.penalty_gaussion_force_center = DeviceField(z[2])
             self.penalty_gaussion_force_strength = DeviceField(z[3])
             self._gf_rows = 0
+            if self.cfg.backward_u and self.cfg.store_control_force:
+                # the forward's force fields, read back by the adjoint instead of re-evaluated
+                self.store_force = [torch.empty((self.total_steps,) + g.face_shape(c), dtype=dt_, device=dev)
+                                    for c in range(self.dim)]
         self.control_force_grads = {}
         self.target_passive = None
         self.target_trajectory = None
@@ -612,10 +624,15 @@ class LFM_Diff_Simulator(LFM_Simulator):
         """3D/lfm_midpoint_diff_simulator.py:421-594 with viscosity=0."""
         cfg, g, dx = self.cfg, self.grid, self.dx
         n = self.step_num[None]
+        force = None
         if cfg.add_control_force:  # 3D/lfm_midpoint_diff_simulator.py:423-427
             params = self._control_params(control_force_para)
             if cfg.backward_u:
-                K.gaussian_force(g, dx, *params, self.control_force)
+                if getattr(self, "store_force", None) is not None:
+                    force = self._force_field(n)  # bitwise the field the forward step evaluated
+                else:
+                    force = self.control_force
+                    K.gaussian_force(g, dx, *params, force)
             self._adj_gaussian(self.adj_u, params)
         for c in range(self.dim):
             K.store(self.store_mid[c][n], self.mid_u[c])
@@ -662,8 +679,8 @@ class LFM_Diff_Simulator(LFM_Simulator):
         if cfg.backward_u:
             if cfg.add_control_force:  # 3D/lfm_midpoint_diff_simulator.py:525-530
                 for c in range(self.dim):
-                    K.add_fields(self.u[c], self.control_force[c], self.u[c], -curr_dt)
-                K.accumulate_init(g, dx, -curr_dt, self.control_force, self.init_u, self.T_f, self.psi_f)
+                    K.add_fields(self.u[c], force[c], self.u[c], -curr_dt)
+                K.accumulate_init(g, dx, -curr_dt, force, self.init_u, self.T_f, self.psi_f)
             self.project(self.u)
 
         if j == 0:

@@ -196,10 +196,11 @@ def test_gaussian_force_grad_matches_oracle(fm, cuda, dtype, res):
 
 # ------------------------------------------------------------------ GPU: simulator
 SIM_CASES = {
-    # name: (res, steps, R, rk, backward_u, dt, gaussians per step)
-    "2d_rk2": ((32, 32), 8, 3, 2, True, 0.01, 40),
-    "2d_rk4_ckpt": ((32, 32), 7, 4, 4, False, 0.01, 40),
-    "3d_rk4": ((16, 16, 16), 6, 4, 4, True, 0.02, 30),
+    # name: (res, steps, R, rk, backward_u, dt, gaussians per step, adjoint reads the stored forces)
+    "2d_rk2": ((32, 32), 8, 3, 2, True, 0.01, 40, True),
+    "2d_rk2_reevaluated": ((32, 32), 8, 3, 2, True, 0.01, 40, False),
+    "2d_rk4_ckpt": ((32, 32), 7, 4, 4, False, 0.01, 40, True),
+    "3d_rk4": ((16, 16, 16), 6, 4, 4, True, 0.02, 30, True),
 }
 
 
@@ -225,7 +226,7 @@ def _levels(res):
 @pytest.mark.gpu
 @pytest.mark.parametrize("name", list(SIM_CASES))
 def test_simulator_with_control_forces_matches_oracle(fm, cuda, name):
-    res, steps, R, rk, bu, dt, ng = SIM_CASES[name]
+    res, steps, R, rk, bu, dt, ng, store = SIM_CASES[name]
     S = importlib.import_module("differentiable-flowmap_b200.simulator")
     u0, rho0, rho_t, forces = _sim_inputs(res, steps, ng, np.float64)
     mg = MGParams(_levels(res), 2, 50, 0, 40, 0.0, 1e-22, 0.0)
@@ -234,7 +235,8 @@ def test_simulator_with_control_forces_matches_oracle(fm, cuda, name):
 
     solver = S.SolverConfig(levels=_levels(res), bottom=50, max_iters=40, abs_tol=0.0, rel_tol=1e-22, eps=0.0)
     cfg = S.FlowmapConfig(res=res, dx=1.0 / res[0], dt=dt, total_steps=steps, reinit_every=R, RK_number=rk,
-                          backward_u=bu, dtype=torch.float64, solver=solver, add_control_force=True, control_num=64)
+                          backward_u=bu, dtype=torch.float64, solver=solver, add_control_force=True, control_num=64,
+                          store_control_force=store)
     sim = S.LFM_Diff_Simulator(config=cfg)
     paras = [{"c": c, "r": r, "s": s, "n": len(r)} for c, r, s in forces]
     lc, gc = sim.gradient(u0, rho0, rho_t, control_forces=paras)
