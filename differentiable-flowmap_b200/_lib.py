@@ -100,6 +100,7 @@ SIGNATURES = {
     "fm_mg_vcycle": [P, P, P, P],
     "fm_mgpcg_solve_dc": [P, I, P, P, P, D, I, P, C.POINTER(I), C.POINTER(I), C.POINTER(D)],
     "fm_clamp_extrema": [GP, I, I, P, P, P, P],
+    "fm_viscous_force_2d": [GP, I, D, D, P, P, P, P, P, P, P, P, P],
     "fm_gaussian_force": [GP, I, D, I, P, P, P, P, P, P, P],
     "fm_gaussian_force_grad": [GP, I, D, I, P, P, P, P, P, P, P, P, P, P, P],
     "fm_vortex_velocity_2d": [GP, I, D, I, C.POINTER(D), P, P, P],

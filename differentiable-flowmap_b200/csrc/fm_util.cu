@@ -115,3 +115,94 @@ extern "C" int fm_clamp_extrema(const fm_grid* g, int dtype, int face, const voi
   }
   return check_cuda();
 }
+
+// ---------------------------------------------------------------------------
+// 2D viscous force (calculate_viscous_force, 2D/vortex/flowmap.py:4-17): on
+// each face grid, vis = nu * (s(i+1,j) + s(i-1,j) + s(i,j+1) + s(i,j-1)
+// - 4 s(i,j)) / dx / dx with sample()'s index clamp, rounded as the reference
+// writes it (no FMA contraction).  With an adjoint velocity it also adds
+// sum adj . vis / nu over both face grids to *dot (calculate_viscous_force_adj,
+// 2D/vortex/flowmap.py:20-35; the reference skips the sum when nu == 0), by a
+// fixed-grid FP64 reduction into `part` and an ordered final sum.
+// ---------------------------------------------------------------------------
+namespace fm {
+
+constexpr int kVisBlocks = 148 * 4;
+constexpr int kVisThreads = 256;
+
+template <typename T>
+__device__ __forceinline__ T vis_at(const T* __restrict__ u, int n0, int n1, int i, int j, T nu, T dx) {
+  const int im = i > 0 ? i - 1 : 0, ip = i < n0 - 1 ? i + 1 : n0 - 1;
+  const int jm = j > 0 ? j - 1 : 0, jp = j < n1 - 1 ? j + 1 : n1 - 1;
+  const T s = rn_add(rn_add(rn_add(u[(long)ip * n1 + j], u[(long)im * n1 + j]), u[(long)i * n1 + jp]),
+                     u[(long)i * n1 + jm]);
+  const T lap = rn_sub(s, rn_mul((T)4, u[(long)i * n1 + j]));
+  return rn_mul(nu, lap) / dx / dx;
+}
+
+template <typename T>
+__global__ void __launch_bounds__(kVisThreads) k_viscous_force(int n0, int n1, T nu, T dx, const T* __restrict__ ux,
+                                                               const T* __restrict__ uy, T* __restrict__ vx,
+                                                               T* __restrict__ vy, const T* __restrict__ ax,
+                                                               const T* __restrict__ ay, double* __restrict__ part) {
+  const long nx = (long)(n0 + 1) * n1, ny = (long)n0 * (n1 + 1);
+  double acc = 0.0;
+  for (long q = (long)blockIdx.x * blockDim.x + threadIdx.x; q < nx + ny; q += (long)gridDim.x * blockDim.x) {
+    if (q < nx) {
+      const int i = (int)(q / n1), j = (int)(q - (long)i * n1);
+      const T v = vis_at(ux, n0 + 1, n1, i, j, nu, dx);
+      vx[q] = v;
+      if (ax) acc += (double)(ax[q] * v / nu);
+    } else {
+      const long r = q - nx;
+      const int i = (int)(r / (n1 + 1)), j = (int)(r - (long)i * (n1 + 1));
+      const T v = vis_at(uy, n0, n1 + 1, i, j, nu, dx);
+      vy[r] = v;
+      if (ax) acc += (double)(ay[r] * v / nu);
+    }
+  }
+  if (!part) return;
+  __shared__ double red[kVisThreads];
+  red[threadIdx.x] = acc;
+  __syncthreads();
+  for (int s = kVisThreads / 2; s > 0; s >>= 1) {
+    if (threadIdx.x < s) red[threadIdx.x] += red[threadIdx.x + s];
+    __syncthreads();
+  }
+  if (threadIdx.x == 0) part[blockIdx.x] = red[0];
+}
+
+__global__ void k_viscous_dot_fin(int nblocks, const double* __restrict__ part, double* __restrict__ dot) {
+  if (threadIdx.x == 0) {
+    double s = 0;
+    for (int b = 0; b < nblocks; ++b) s += part[b];
+    *dot += s;
+  }
+}
+
+}  // namespace fm
+
+extern "C" int fm_viscous_force_2d(const fm_grid* g, int dtype, double nu, double dx, const void* ux, const void* uy,
+                                   void* vis_x, void* vis_y, const void* adj_x, const void* adj_y, double* part,
+                                   double* dot, void* stream) {
+  using namespace fm;
+  const int st = validate_grid(g, dtype);
+  if (st) return st;
+  if (g->dim != 2) return FM_ERR_SHAPE;
+  if (!ux || !uy || !vis_x || !vis_y || !(dx > 0)) return FM_ERR_ARG;
+  const bool with_dot = adj_x || adj_y;
+  if (with_dot && (!adj_x || !adj_y || !part || !dot)) return FM_ERR_ARG;
+  const bool sum = with_dot && nu != 0.0;  // the reference adds nothing when nu == 0
+  cudaStream_t s = (cudaStream_t)stream;
+  const int n0 = g->n[0], n1 = g->n[1];
+  if (dtype == FM_F32)
+    launch(k_viscous_force<float>, kVisBlocks, kVisThreads, 0, s, n0, n1, (float)nu, (float)dx, (const float*)ux,
+           (const float*)uy, (float*)vis_x, (float*)vis_y, sum ? (const float*)adj_x : nullptr,
+           sum ? (const float*)adj_y : nullptr, sum ? part : nullptr);
+  else
+    launch(k_viscous_force<double>, kVisBlocks, kVisThreads, 0, s, n0, n1, nu, dx, (const double*)ux,
+           (const double*)uy, (double*)vis_x, (double*)vis_y, sum ? (const double*)adj_x : nullptr,
+           sum ? (const double*)adj_y : nullptr, sum ? part : nullptr);
+  if (sum) launch(k_viscous_dot_fin, 1, 32, 0, s, kVisBlocks, (const double*)part, dot);
+  return check_cuda();
+}

@@ -289,3 +289,17 @@ def gaussian_force_grad(g: GridSpec, dx: float, center, inv_radius, strength, ad
                                             ptr(strength), *_mac3(adj_u), *[ptr(t) for t in out],
                                             stream_ptr(stream)), "fm_gaussian_force_grad")
     return out
+
+
+def viscous_force_2d(g: GridSpec, nu: float, dx: float, u, vis, adj=None, part=None, dot=None, stream=None):
+    """calculate_viscous_force into ``vis``; with ``adj`` also dot += sum adj . vis / nu
+    (calculate_viscous_force_adj; ``part``: FP64 scratch of 592, ``dot``: FP64 device scalar)."""
+    _chk_mac(g, u, "u")
+    _chk_mac(g, vis, "vis")
+    a = [None, None]
+    if adj is not None:
+        _chk_mac(g, adj, "adj")
+        a = [ptr(adj[0]), ptr(adj[1])]
+    check(_lib.lib().fm_viscous_force_2d(C.byref(g.c_grid()), _dt(u[0]), nu, dx, ptr(u[0]), ptr(u[1]), ptr(vis[0]),
+                                         ptr(vis[1]), a[0], a[1], ptr(part), ptr(dot), stream_ptr(stream)),
+          "fm_viscous_force_2d")

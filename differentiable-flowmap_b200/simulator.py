@@ -69,6 +69,7 @@ class FlowmapConfig:
     add_control_force: bool = False  # Gaussian control forces (control_force_para per step)
     control_num: int = 0             # capacity: most Gaussians one step may pass
     store_control_force: bool = True  # adjoint with backward_u reads the forward's force fields from HBM
+    viscosity: float = 0.0           # 2D viscous term (2D/vortex/hyperparameters.py:26)
     trajectory_loss: bool = False  # reference's no-force branch: loss over reinit frames
     dtype: torch.dtype = torch.float32
     store_dtype: Optional[torch.dtype] = None  # checkpoint storage dtype (None: dtype)
@@ -231,6 +232,14 @@ class LFM_Simulator:
                 raise FlowmapError(2, "control_num must be >= 0")
             self.control_force = _mac(g, dt_, dev)
             self._gf = _GaussianParams(cfg.control_num, self.dim, dt_, dev)
+
+        # 2D viscous term: the field nu * Laplacian(u) of the step's midpoint velocity
+        self.vis = None
+        if cfg.viscosity != 0.0:
+            if self.dim != 2:
+                raise FlowmapError(2, "the viscous term exists in the 2D reference only")
+            self.vis = _mac(g, dt_, dev)
+            self._vis_part = torch.empty(592, dtype=torch.float64, device=dev)
 
         self.step_num = _Scalar(-1)
         self.frame_idx = _Scalar(0)
@@ -402,8 +411,9 @@ class LFM_Simulator:
             self._march(self.psi, self.psi_f, self.T_f, um, self.dt)
 
     def step_flow_map(self, j: int, curr_dt: float, control_force_para=None):
-        """3D/lfm_midpoint_simulator.py:684-807 with viscosity=0; use_short_BFECC,
-        BFECC_clamp and add_control_force as configured.  The control force is
+        """3D/lfm_midpoint_simulator.py:684-807; use_short_BFECC, BFECC_clamp,
+        add_control_force and the 2D viscous term (2D/vortex/lfm_midpoint_simulator.py:
+        552, 607-609) as configured.  The control force is
         evaluated once per step: the reference evaluates it twice with the same
         parameters, which gives the same field."""
         cfg = self.cfg
@@ -416,6 +426,8 @@ class LFM_Simulator:
             for c in range(self.dim):
                 K.add_fields(self.u[c], force[c], self.u[c], 0.5 * curr_dt)
         self.project(self.u)
+        if self.vis is not None:  # 2D/vortex/lfm_midpoint_simulator.py:552
+            K.viscous_force_2d(self.grid, cfg.viscosity, self.dx, self.u, self.vis)
         # write_velocity + RW_Cache("u"): the midpoint velocity of step n
         for c in range(self.dim):
             K.store(self.u[c], self.store_mid[c][n])
@@ -440,6 +452,10 @@ class LFM_Simulator:
             for c in range(self.dim):
                 K.add_fields(self.u[c], force[c], self.u[c], curr_dt)
             K.accumulate_init(self.grid, self.dx, curr_dt, force, self.init_u, self.F_f, self.phi_f)
+        if self.vis is not None:  # 2D/vortex/lfm_midpoint_simulator.py:607-609
+            for c in range(self.dim):
+                K.add_fields(self.u[c], self.vis[c], self.u[c], curr_dt)
+            K.accumulate_init(self.grid, self.dx, curr_dt, self.vis, self.init_u, self.F_f, self.phi_f)
         self.project(self.u)
 
         if j == self.reinit_every - 1:
@@ -493,6 +509,8 @@ class LFM_Diff_Simulator(LFM_Simulator):
                 self.store_force = [torch.empty((self.total_steps,) + g.face_shape(c), dtype=dt_, device=dev)
                                     for c in range(self.dim)]
         self.control_force_grads = {}
+        # d loss / d viscosity as the reference accumulates it (adj_viscous), reset by init_gradient
+        self.adj_viscous = DeviceField(torch.zeros(1, dtype=torch.float64, device=dev))
         self.target_passive = None
         self.target_trajectory = None
         self.loss = 0.0
@@ -558,6 +576,7 @@ class LFM_Diff_Simulator(LFM_Simulator):
 
     def _finish_seed(self):
         self.step_num[None] = self.final_ind
+        self.adj_viscous.tensor.zero_()
         _copy_mac(self.init_adj_u, self.adj_u)
         self.init_adj_passive.copy_(self.adj_passive)
         if self.cfg.backward_u:
@@ -621,7 +640,8 @@ class LFM_Diff_Simulator(LFM_Simulator):
         return False, n == 0
 
     def backtrack_flow_map(self, j: int, curr_dt: float, control_force_para=None):
-        """3D/lfm_midpoint_diff_simulator.py:421-594 with viscosity=0."""
+        """3D/lfm_midpoint_diff_simulator.py:421-594, with the 2D viscous term of
+        2D/vortex/lfm_midpoint_diff_simulator.py:260-401 when viscosity != 0."""
         cfg, g, dx = self.cfg, self.grid, self.dx
         n = self.step_num[None]
         force = None
@@ -636,6 +656,9 @@ class LFM_Diff_Simulator(LFM_Simulator):
             self._adj_gaussian(self.adj_u, params)
         for c in range(self.dim):
             K.store(self.store_mid[c][n], self.mid_u[c])
+        if self.vis is not None:  # 2D/vortex/lfm_midpoint_diff_simulator.py:270-271
+            K.viscous_force_2d(g, cfg.viscosity, dx, self.mid_u, self.vis, adj=self.adj_u, part=self._vis_part,
+                               dot=self.adj_viscous.tensor)
         K.nabla_u_w(g, dx, self.u if cfg.backward_u else self.mid_u, self.adj_u, self.src)
         if cfg.add_passive_scalar:
             K.nabla_scalar_adjoint(g, dx, self.passive, self.adj_passive, self.adj_passive_f)
@@ -675,12 +698,20 @@ class LFM_Diff_Simulator(LFM_Simulator):
                           self.H_prev_prev, interval_last - n)
         if cfg.add_passive_scalar:
             K.accumulate_init(g, dx, -curr_dt, self.adj_passive_f, self.init_adj_u, self.T_f, self.psi_f)
+        if self.vis is not None:  # 2D/vortex/lfm_midpoint_diff_simulator.py:387-389
+            for c in range(self.dim):
+                K.add_fields(self.adj_u[c], self.vis[c], self.adj_u[c], -curr_dt)
+            K.accumulate_init(g, dx, -curr_dt, self.vis, self.init_adj_u, self.T_f, self.psi_f)
         self.project(self.adj_u)  # Poisson_adj
         if cfg.backward_u:
             if cfg.add_control_force:  # 3D/lfm_midpoint_diff_simulator.py:525-530
                 for c in range(self.dim):
                     K.add_fields(self.u[c], force[c], self.u[c], -curr_dt)
                 K.accumulate_init(g, dx, -curr_dt, force, self.init_u, self.T_f, self.psi_f)
+            if self.vis is not None:  # 2D/vortex/lfm_midpoint_diff_simulator.py:399-401
+                for c in range(self.dim):
+                    K.add_fields(self.u[c], self.vis[c], self.u[c], -curr_dt)
+                K.accumulate_init(g, dx, -curr_dt, self.vis, self.init_u, self.T_f, self.psi_f)
             self.project(self.u)
 
         if j == 0:

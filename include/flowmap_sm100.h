@@ -275,6 +275,15 @@ int fm_laplacian(const fm_grid *g, int dtype, const void *p, void *Ap, void *str
  * -1 the cell grid).  dst may not alias ref. */
 int fm_clamp_extrema(const fm_grid *g, int dtype, int face, const void *src, const void *ref, void *dst, void *stream);
 
+/* 2D viscous force (calculate_viscous_force, 2D/vortex/flowmap.py:4-17):
+ * vis = nu (s(i+1,j) + s(i-1,j) + s(i,j+1) + s(i,j-1) - 4 s(i,j)) / dx / dx on
+ * each face grid, samples index-clamped.  With adj_x/adj_y (both or neither)
+ * it also adds sum adj . vis / nu over both grids to *dot (device FP64;
+ * calculate_viscous_force_adj, 2D/vortex/flowmap.py:20-35), nothing when
+ * nu == 0; part: device FP64 scratch of 592 entries. */
+int fm_viscous_force_2d(const fm_grid *g, int dtype, double nu, double dx, const void *ux, const void *uy, void *vis_x,
+                        void *vis_y, const void *adj_x, const void *adj_y, double *part, double *dot, void *stream);
+
 /* ------------------------------------------------------------------------
  * Gaussian control forces.  n Gaussians, device arrays of the dtype:
  * center n x dim (row-major), inv_radius n (r = 1/radius^2), strength n x dim.

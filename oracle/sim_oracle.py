@@ -9,8 +9,10 @@ sequences, which the product fuses):
   adjoint  3D/lfm_midpoint_diff_simulator.py:336-594 (init_gradient case 11,
            backtrack_step_midpoint, backtrack_flow_map)
   BFECC    3D/flowmap.py:405-452
-with viscosity=0 and empty obstacle masks; use_short_BFECC, BFECC_clamp and
-Gaussian control forces (add_control_force) as the constructor selects.  The trajectory the reference writes to
+with empty obstacle masks; use_short_BFECC, BFECC_clamp, Gaussian control
+forces (add_control_force) and the 2D viscous term (2D/vortex/
+lfm_midpoint_simulator.py:552, 607-609; diff :270-271, 387-401) as the
+constructor selects.  The trajectory the reference writes to
 .npy files is kept in Python lists.  Two documented extensions match the
 product: a run whose last reinit interval is partial stores that interval's
 forward map at the last step, and the Adams-Bashforth index counts adjoint
@@ -23,6 +25,21 @@ import numpy as np
 
 import force_oracle
 from oracle import MGParams, Oracle
+
+
+def viscous_force(u, nu, dx):
+    """calculate_viscous_force (2D/vortex/flowmap.py:4-17) on each face grid:
+    nu * (s(i+1,j) + s(i-1,j) + s(i,j+1) + s(i,j-1) - 4 s(i,j)) / dx / dx with
+    sample()'s index clamp, evaluated left to right in the field's dtype."""
+    out = []
+    for x in u:
+        t = x.dtype.type
+        n0, n1 = x.shape
+        ip, im = np.minimum(np.arange(n0) + 1, n0 - 1), np.maximum(np.arange(n0) - 1, 0)
+        jp, jm = np.minimum(np.arange(n1) + 1, n1 - 1), np.maximum(np.arange(n1) - 1, 0)
+        s = ((x[ip, :] + x[im, :]) + x[:, jp]) + x[:, jm]
+        out.append(((t(nu) * (s - t(4) * x)) / t(dx) / t(dx)).astype(x.dtype))
+    return out
 
 
 def clamp_u(u, u1):
@@ -41,7 +58,7 @@ def clamp_u(u, u1):
 class OracleSim:
     def __init__(self, res, dx, dt, reinit_every, total_steps, rk=4, backward_u=True, passive=True,
                  trajectory_loss=False, prec="f64", mg=None, bfecc_clamp=False, short_bfecc=False,
-                 control_forces=None):
+                 control_forces=None, viscosity=0.0):
         self.o = Oracle(tuple(res), prec)
         self.dim = len(res)
         self.res = tuple(res)
@@ -51,6 +68,8 @@ class OracleSim:
         # per step n: (center n x dim, inv_radius n, strength n x dim) in the run's dtype
         self.cf = control_forces
         self.cf_grads = {}
+        self.nu = viscosity  # 2D only, as in the reference
+        self.adj_viscous = 0.0
         if short_bfecc:
             o = self.o
             self.psi_tem, self.phi_tem = o.zeros_cell(self.dim), o.zeros_cell(self.dim)
@@ -196,6 +215,8 @@ class OracleSim:
             for c in range(d):
                 self.u[c][...] = self.u[c] + (0.5 * dt) * f[c]
         self.Poisson(self.u)
+        if self.nu:  # 2D/vortex/lfm_midpoint_simulator.py:552
+            self.vis = viscous_force(self.u, self.nu, self.dx)
         self.velocity_storage[j] = [x.copy() for x in self.u]
         self.march_phi_grid()
         self.store_mid[self.step_num] = [x.copy() for x in self.u]
@@ -219,6 +240,10 @@ class OracleSim:
             for c in range(d):
                 self.u[c][...] = self.u[c] + dt * f[c]
             o.accumulate_init(f, self.init_u, self.F_f, self.phi_f, self.dx, dt)
+        if self.nu:  # 2D/vortex/lfm_midpoint_simulator.py:607-609
+            for c in range(d):
+                self.u[c][...] = self.u[c] + dt * self.vis[c]
+            o.accumulate_init(self.vis, self.init_u, self.F_f, self.phi_f, self.dx, dt)
         self.Poisson(self.u)
         n = self.step_num
         if j == self.R - 1:
@@ -244,6 +269,7 @@ class OracleSim:
         """Passive loss seed (case 11), or seed = (loss, [adj_u faces]) for a velocity loss."""
         o, d = self.o, self.dim
         self.final_ind = self.step_num + 1
+        self.adj_viscous = 0.0
         self.adj_u = o.zeros_mac()
         self.src = o.zeros_mac()
         self.H_prev, self.H_prev_prev = o.zeros_mac(), o.zeros_mac()
@@ -290,6 +316,10 @@ class OracleSim:
             self.cf_grads[n] = force_oracle.gaussian_force_grad(self.res, dx, cen, inv_r, st, self.adj_u)
         for c in range(d):
             self.mid_u[c][...] = self.store_mid[n][c]
+        if self.nu:  # 2D/vortex/lfm_midpoint_diff_simulator.py:270-271
+            self.vis = viscous_force(self.mid_u, self.nu, dx)
+            self.adj_viscous += sum(float(np.sum((self.adj_u[c] * self.vis[c] / self.nu).astype(np.float64)))
+                                    for c in range(d))
         o.calculate_nabla_u_w(self.u if self.backward_u else self.mid_u, self.adj_u, self.src, dx)
         if self.passive_on:
             o.calculate_nabla_scalar_adjoint(self.passive, self.adj_passive, self.adj_passive_f, dx)
@@ -338,12 +368,20 @@ class OracleSim:
                               dx, -2 * dt)
         if self.passive_on:
             o.accumulate_init(self.adj_passive_f, self.init_adj_u, self.T_f, self.psi_f, dx, -dt)
+        if self.nu:  # 2D/vortex/lfm_midpoint_diff_simulator.py:387-389
+            for c in range(d):
+                self.adj_u[c][...] = self.adj_u[c] + (-dt) * self.vis[c]
+            o.accumulate_init(self.vis, self.init_adj_u, self.T_f, self.psi_f, dx, -dt)
         self.Poisson(self.adj_u)
         if self.backward_u:
             if self.cf is not None:  # 3D/lfm_midpoint_diff_simulator.py:525-530
                 for c in range(d):
                     self.u[c][...] = self.u[c] + (-dt) * f_ctrl[c]
                 o.accumulate_init(f_ctrl, self.init_u, self.T_f, self.psi_f, dx, -dt)
+            if self.nu:  # 2D/vortex/lfm_midpoint_diff_simulator.py:399-401
+                for c in range(d):
+                    self.u[c][...] = self.u[c] + (-dt) * self.vis[c]
+                o.accumulate_init(self.vis, self.init_u, self.T_f, self.psi_f, dx, -dt)
             self.Poisson(self.u)
         if j == 0:
             phi, phi_f, F_f = self.store_maps[n // self.R]
