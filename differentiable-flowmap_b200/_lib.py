@@ -100,6 +100,14 @@ SIGNATURES = {
     "fm_mg_vcycle": [P, P, P, P],
     "fm_mgpcg_solve_dc": [P, I, P, P, P, D, I, P, C.POINTER(I), C.POINTER(I), C.POINTER(D)],
     "fm_clamp_extrema": [GP, I, I, P, P, P, P],
+    "fm_solid_create": [GP, I, C.POINTER(MGParams), P, C.POINTER(P)],
+    "fm_solid_destroy": [P],
+    "fm_solid_set_mask": [P, P, P],
+    "fm_solid_vcycle": [P, P, P, P],
+    "fm_solid_solve": [P, P, P, P, C.POINTER(I), C.POINTER(D)],
+    "fm_solid_project": [P, P, P, P, P, P, C.POINTER(I), C.POINTER(D)],
+    "fm_mask_velocity": [GP, I, P, P, P, P, P, P],
+    "fm_mask_passive": [GP, I, P, P, I, P],
     "fm_viscous_force_2d": [GP, I, D, D, P, P, P, P, P, P, P, P, P],
     "fm_gaussian_force": [GP, I, D, I, P, P, P, P, P, P, P],
     "fm_gaussian_force_grad": [GP, I, D, I, P, P, P, P, P, P, P, P, P, P, P],

@@ -303,3 +303,25 @@ def viscous_force_2d(g: GridSpec, nu: float, dx: float, u, vis, adj=None, part=N
     check(_lib.lib().fm_viscous_force_2d(C.byref(g.c_grid()), _dt(u[0]), nu, dx, ptr(u[0]), ptr(u[1]), ptr(vis[0]),
                                          ptr(vis[1]), a[0], a[1], ptr(part), ptr(dot), stream_ptr(stream)),
           "fm_viscous_force_2d")
+
+
+def _mask_arg(g: GridSpec, mask):
+    if tuple(mask.shape) != tuple(g.shape) or mask.dtype != torch.float32:
+        raise _lib.FlowmapError(1, "mask: float32 cell-grid tensor expected")
+    return ptr(mask)
+
+
+def mask_velocity(g: GridSpec, mask, u, bvel=None, stream=None):
+    """mask_velocity_by_boundary (bvel: (dim, *grid) tensor of u's dtype) or, with
+    bvel None, mask_adj_velocity_by_boundary (zero on the faces of solid cells)."""
+    _chk_mac(g, u, "u")
+    if bvel is not None:
+        _chk_vec(g, bvel, -1, "bvel")
+    check(_lib.lib().fm_mask_velocity(C.byref(g.c_grid()), _dt(u[0]), _mask_arg(g, mask), ptr(bvel), *_mac3(u),
+                                      stream_ptr(stream)), "fm_mask_velocity")
+
+
+def mask_passive(g: GridSpec, mask, s, adjoint: bool = False, stream=None):
+    """mask_passive_by_boundary, or mask_adj_passive_by_boundary with adjoint=True."""
+    check(_lib.lib().fm_mask_passive(C.byref(g.c_grid()), _dt(s), _mask_arg(g, mask), ptr(s), int(adjoint),
+                                     stream_ptr(stream)), "fm_mask_passive")

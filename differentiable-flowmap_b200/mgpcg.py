@@ -3,8 +3,9 @@
 ``MGPCG_3`` / ``MGPCG_2`` mirror 3D/mgpcg.py:359-439 and 2D/shape/mgpcg.py:292-368
 (plain all-Neumann solver, base_level 3, bottom smoothing 50, absolute
 tolerance rTr < 1e-12, max 400 iterations).  ``MGPCG_2_solid`` mirrors
-2D/vortex/mgpcg_solid.py:370-458 with an empty obstacle mask (base_level 4,
-20 bottom sweeps as 10 x (R,B) + 10 x (B,R), tol = max(1e-14, 1e-16 zTr0)).
+2D/vortex/mgpcg_solid.py:370-458 (base_level 4, 20 bottom sweeps as
+10 x (R,B) + 10 x (B,R), tol = max(1e-14, 1e-16 zTr0)); with a non-empty
+obstacle mask it is a ``SolidMGPCG`` (libflowmap's fm_solid_*).
 ``Poisson(u_x, u_y[, u_z])`` projects in place; ``Poisson_adj`` is the same
 operation (3D/fast_mgpcg.py:283-323 differs from Poisson only in name).
 
@@ -157,6 +158,125 @@ class MGPCG:
         self.Poisson(*u, verbose=verbose)
 
 
+class SolidMGPCG:
+    """MGPCG with a boundary mask (2D/vortex/mgpcg_solid.py:14-458, dimension-
+    generic): cells with mask > 0 are solid; same interface as MGPCG.  The PCG
+    loop polls its device-side convergence flag every ``check_every`` (>= 1)
+    iterations."""
+
+    def __init__(self, N: Sequence[int], mask: torch.Tensor, dtype=torch.float32, *, base_level: int = 4,
+                 levels: Optional[int] = None, pre_post: int = 2, bottom: int = 20, bottom_mode: int = 1,
+                 max_iters: int = 400, abs_tol: float = 1e-14, rel_tol: float = 1e-16, eps: float = 1e-12,
+                 check_every: int = 4, raise_on_nonconvergence: bool = False):
+        self.N = tuple(int(n) for n in N)
+        self.grid = GridSpec(self.N)
+        self.dtype = dtype
+        if levels is None:
+            levels = int(math.log2(min(self.N))) - base_level + 1
+        self.params = _lib.MGParams(levels, pre_post, bottom, bottom_mode, max_iters, abs_tol, rel_tol, eps,
+                                    max(int(check_every), 1), 0)
+        self.raise_on_nonconvergence = raise_on_nonconvergence
+        self.mask = self._as_mask(mask)
+        self._h = C.c_void_p()
+        _lib.check(_lib.lib().fm_solid_create(C.byref(self.grid.c_grid()), _lib.dtype_code(dtype),
+                                              C.byref(self.params), _lib.ptr(self.mask), C.byref(self._h)),
+                   "fm_solid_create")
+        self.last_iters, self.last_rtr, self.last_converged = 0, 0.0, True
+        self.history = []
+        self._stats = {"solves": 0, "iterations": 0, "not_converged": 0, "nonfinite": 0, "last_iters": 0,
+                       "max_iters_seen": 0, "last_rtr": 0.0}
+
+    def _as_mask(self, mask):
+        m = torch.as_tensor(mask)
+        if tuple(m.shape) != self.N:
+            raise _lib.FlowmapError(1, f"mask shape {tuple(m.shape)} != grid {self.N}")
+        return m.to(device="cuda", dtype=torch.float32).contiguous()
+
+    @property
+    def n_mg_levels(self) -> int:
+        return self.params.levels
+
+    device_mode = False
+
+    def set_mask(self, mask, stream=None):
+        self.mask = self._as_mask(mask)
+        _lib.check(_lib.lib().fm_solid_set_mask(self._h, _lib.ptr(self.mask), _lib.stream_ptr(stream)),
+                   "fm_solid_set_mask")
+
+    def close(self):
+        if self._h:
+            _lib.lib().fm_solid_destroy(self._h)
+            self._h = C.c_void_p()
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def _status(self, st, where, it, rtr):
+        self.last_iters, self.last_rtr, self.last_converged = it.value, rtr.value, st == 0
+        self.history.append((it.value, rtr.value))
+        S = self._stats
+        S["solves"] += 1
+        S["iterations"] += it.value
+        S["last_iters"], S["last_rtr"] = it.value, rtr.value
+        S["max_iters_seen"] = max(S["max_iters_seen"], it.value)
+        if st == 3:
+            S["not_converged"] += 1
+            if self.raise_on_nonconvergence:
+                _lib.check(st, where)
+            return
+        if st == 4:
+            S["nonfinite"] += 1
+            return
+        _lib.check(st, where)
+
+    def project(self, u: Sequence[torch.Tensor], p_out: Optional[torch.Tensor] = None, stream=None):
+        if len(u) != self.grid.dim:
+            raise _lib.FlowmapError(2, "project: wrong number of components")
+        for c, x in enumerate(u):
+            if tuple(x.shape) != self.grid.face_shape(c) or x.dtype != self.dtype:
+                raise _lib.FlowmapError(1, f"project: component {c} shape/dtype mismatch")
+        ps = [_lib.ptr(x) for x in u] + [None] * (3 - len(u))
+        it, rtr = C.c_int(0), C.c_double(0)
+        st = _lib.lib().fm_solid_project(self._h, ps[0], ps[1], ps[2], _lib.ptr(p_out), _lib.stream_ptr(stream),
+                                         C.byref(it), C.byref(rtr))
+        self._status(st, "fm_solid_project", it, rtr)
+
+    def solve(self, b: torch.Tensor, x: torch.Tensor, stream=None):
+        it, rtr = C.c_int(0), C.c_double(0)
+        st = _lib.lib().fm_solid_solve(self._h, _lib.ptr(b), _lib.ptr(x), _lib.stream_ptr(stream), C.byref(it),
+                                       C.byref(rtr))
+        self._status(st, "fm_solid_solve", it, rtr)
+        return it.value, rtr.value
+
+    def apply_preconditioner(self, r: torch.Tensor, z: Optional[torch.Tensor] = None, stream=None) -> torch.Tensor:
+        if tuple(r.shape) != self.N or r.dtype != self.dtype:
+            raise _lib.FlowmapError(1, "apply_preconditioner: r shape/dtype mismatch")
+        if z is None:
+            z = torch.empty_like(r)
+        _lib.check(_lib.lib().fm_solid_vcycle(self._h, _lib.ptr(r), _lib.ptr(z), _lib.stream_ptr(stream)),
+                   "fm_solid_vcycle")
+        return z
+
+    def stats(self, reset: bool = False, stream=None) -> dict:
+        out = dict(self._stats)
+        if reset:
+            for k in self._stats:
+                self._stats[k] = 0.0 if k == "last_rtr" else 0
+        return out
+
+    def Poisson(self, *u, verbose: bool = False):
+        self.project(u)
+        if verbose:
+            print(f"[MGPCG] iters={self.last_iters} |r|={math.sqrt(max(self.last_rtr, 0.0)):.3e} "
+                  f"converged={self.last_converged}")
+
+    def Poisson_adj(self, *u, verbose: bool = False):
+        self.Poisson(*u, verbose=verbose)
+
+
 class MGPCG_3(MGPCG):
     """3D/mgpcg.py:359 MGPCG_3(boundary_types, N, base_level=3)."""
 
@@ -176,12 +296,18 @@ class MGPCG_2(MGPCG):
 
 
 class MGPCG_2_solid(MGPCG):
-    """2D/vortex/mgpcg_solid.py:370 with an empty obstacle mask."""
+    """2D/vortex/mgpcg_solid.py:370.  With a non-empty boundary_mask the
+    constructor returns a SolidMGPCG; with an empty one the all-Neumann solver
+    (the same operator) with the solid variant's settings."""
+
+    def __new__(cls, boundary_types=None, boundary_mask=None, boundary_vel=None, N=(256, 256), base_level=4,
+                real=None, dtype=torch.float32, **kw):
+        if boundary_mask is not None and bool((torch.as_tensor(boundary_mask) > 0).any()):
+            return SolidMGPCG(N, boundary_mask, dtype, base_level=4, **kw)
+        return super().__new__(cls)
 
     def __init__(self, boundary_types=None, boundary_mask=None, boundary_vel=None, N=(256, 256), base_level=4,
                  real=None, dtype=torch.float32, **kw):
-        if boundary_mask is not None and bool((boundary_mask > 0).any()):
-            raise _lib.FlowmapError(2, "MGPCG_2_solid: obstacle masks are not supported by this build")
         kw.setdefault("bottom", 20)
         kw.setdefault("bottom_mode", 1)
         kw.setdefault("abs_tol", 1e-14)

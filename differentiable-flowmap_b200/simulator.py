@@ -33,7 +33,7 @@ import torch
 from . import kernels as K
 from ._lib import FlowmapError
 from .kernels import GridSpec
-from .mgpcg import MGPCG
+from .mgpcg import MGPCG, SolidMGPCG
 
 
 @dataclass
@@ -70,6 +70,8 @@ class FlowmapConfig:
     control_num: int = 0             # capacity: most Gaussians one step may pass
     store_control_force: bool = True  # adjoint with backward_u reads the forward's force fields from HBM
     viscosity: float = 0.0           # 2D viscous term (2D/vortex/hyperparameters.py:26)
+    boundary_mask: Optional[object] = None  # obstacle mask on the cell grid (solid > 0), numpy or tensor
+    boundary_vel: Optional[object] = None   # (dim, *grid) velocity of the solid cells (None: 0)
     trajectory_loss: bool = False  # reference's no-force branch: loss over reinit frames
     dtype: torch.dtype = torch.float32
     store_dtype: Optional[torch.dtype] = None  # checkpoint storage dtype (None: dtype)
@@ -192,9 +194,22 @@ class LFM_Simulator:
         self.store_dtype = cfg.store_dtype or cfg.dtype
 
         sc = cfg.solver
-        self.solver = MGPCG(g.shape, dt_, base_level=sc.base_level, levels=sc.levels, pre_post=sc.pre_post,
-                            bottom=sc.bottom, bottom_mode=sc.bottom_mode, max_iters=sc.max_iters,
-                            abs_tol=sc.abs_tol, rel_tol=sc.rel_tol, eps=sc.eps, check_every=sc.check_every)
+        # obstacles: a non-empty mask selects the solid-aware solver and the mask kernels
+        self.boundary_mask = self.boundary_vel = None
+        if cfg.boundary_mask is not None and bool((torch.as_tensor(cfg.boundary_mask) > 0).any()):
+            self.boundary_mask = torch.as_tensor(cfg.boundary_mask).to(dev, torch.float32).contiguous()
+            if tuple(self.boundary_mask.shape) != tuple(g.shape):
+                raise FlowmapError(1, f"boundary_mask shape {tuple(self.boundary_mask.shape)} != grid {g.shape}")
+            if cfg.boundary_vel is not None:
+                self.boundary_vel = torch.as_tensor(cfg.boundary_vel).to(dev, dt_).contiguous()
+            self.solver = SolidMGPCG(g.shape, self.boundary_mask, dt_, base_level=sc.base_level, levels=sc.levels,
+                                     pre_post=sc.pre_post, bottom=sc.bottom, bottom_mode=sc.bottom_mode,
+                                     max_iters=sc.max_iters, abs_tol=sc.abs_tol, rel_tol=sc.rel_tol, eps=sc.eps,
+                                     check_every=sc.check_every or 4)
+        else:
+            self.solver = MGPCG(g.shape, dt_, base_level=sc.base_level, levels=sc.levels, pre_post=sc.pre_post,
+                                bottom=sc.bottom, bottom_mode=sc.bottom_mode, max_iters=sc.max_iters,
+                                abs_tol=sc.abs_tol, rel_tol=sc.rel_tol, eps=sc.eps, check_every=sc.check_every)
 
         # flow maps: backward (psi, T) and forward (phi, F); centre maps for scalars
         self.psi = torch.zeros((self.dim,) + g.shape, dtype=dt_, device=dev)
@@ -324,6 +339,20 @@ class LFM_Simulator:
     def project(self, u):
         self.solver.project(u)
 
+    def _mask(self, adjoint: bool = False):
+        """mask_velocity_by_boundary / mask_passive_by_boundary and, in the adjoint,
+        their adjoint forms (3D/init_conditions.py:536-578), after a projection."""
+        if self.boundary_mask is None:
+            return
+        g, m = self.grid, self.boundary_mask
+        K.mask_velocity(g, m, self.u, self.boundary_vel)
+        if adjoint:
+            K.mask_velocity(g, m, self.adj_u)
+        if self.cfg.add_passive_scalar:
+            K.mask_passive(g, m, self.passive)
+            if adjoint:
+                K.mask_passive(g, m, self.adj_passive, adjoint=True)
+
     # ------------------------------------------------------------ API
     @property
     def u_x(self):
@@ -353,6 +382,7 @@ class LFM_Simulator:
         if self.cfg.add_passive_scalar and init_passive_np is not None:
             self.passive.copy_(_as_tensor(init_passive_np), non_blocking=True)
             self.init_passive.copy_(self.passive)
+        self._mask()  # 3D/lfm_midpoint_simulator.py:606-608
         self.step_num[None] = -1
         self.frame_idx[None] = 0
         self.reset_to_identity(self.phi, self.phi_f, self.F_f)
@@ -426,6 +456,7 @@ class LFM_Simulator:
             for c in range(self.dim):
                 K.add_fields(self.u[c], force[c], self.u[c], 0.5 * curr_dt)
         self.project(self.u)
+        self._mask()  # 3D/lfm_midpoint_simulator.py:712-714
         if self.vis is not None:  # 2D/vortex/lfm_midpoint_simulator.py:552
             K.viscous_force_2d(self.grid, cfg.viscosity, self.dx, self.u, self.vis)
         # write_velocity + RW_Cache("u"): the midpoint velocity of step n
@@ -457,11 +488,13 @@ class LFM_Simulator:
                 K.add_fields(self.u[c], self.vis[c], self.u[c], curr_dt)
             K.accumulate_init(self.grid, self.dx, curr_dt, self.vis, self.init_u, self.F_f, self.phi_f)
         self.project(self.u)
+        self._mask()  # 3D/lfm_midpoint_simulator.py:769-771
 
         if j == self.reinit_every - 1:
             self.backtrack_psi_grid(self.reinit_every - 1, n - j)
             self.BFECC(self.init_u, self.u, self.err_u, self.T_f, self.psi_f, self.F_f, self.phi_f)
             self.project(self.u)
+            self._mask()  # 3D/lfm_midpoint_simulator.py:787-789
             if cfg.add_passive_scalar:
                 self.BFECC_scalar(self.init_passive, self.passive, self.err_passive, self.psi, self.phi)
                 self.init_passive.copy_(self.passive)
@@ -575,6 +608,7 @@ class LFM_Diff_Simulator(LFM_Simulator):
         self._finish_seed()
 
     def _finish_seed(self):
+        self._mask(adjoint=True)  # 3D/lfm_midpoint_diff_simulator.py:357-361
         self.step_num[None] = self.final_ind
         self.adj_viscous.tensor.zero_()
         _copy_mac(self.init_adj_u, self.adj_u)
@@ -713,6 +747,7 @@ class LFM_Diff_Simulator(LFM_Simulator):
                     K.add_fields(self.u[c], self.vis[c], self.u[c], -curr_dt)
                 K.accumulate_init(g, dx, -curr_dt, self.vis, self.init_u, self.T_f, self.psi_f)
             self.project(self.u)
+        self._mask(adjoint=True)  # 3D/lfm_midpoint_diff_simulator.py:534-538
 
         if j == 0:
             k = n // self.reinit_every
@@ -727,6 +762,7 @@ class LFM_Diff_Simulator(LFM_Simulator):
                 self.BFECC(self.init_u, self.u, self.err_u, self.F_f, self.phi_f, self.T_f, self.psi_f)
                 self.project(self.u)
                 _copy_mac(self.init_u, self.u)
+            self._mask(adjoint=True)  # 3D/lfm_midpoint_diff_simulator.py:572-576
             if cfg.add_passive_scalar:
                 if cfg.trajectory_loss or not cfg.backward_u:
                     K.store(self.store_passive[n], self.passive)

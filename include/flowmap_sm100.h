@@ -285,6 +285,46 @@ int fm_viscous_force_2d(const fm_grid *g, int dtype, double nu, double dx, const
                         void *vis_y, const void *adj_x, const void *adj_y, double *part, double *dot, void *stream);
 
 /* ------------------------------------------------------------------------
+ * Obstacles: MGPCG with a boundary mask and the mask kernels.
+ * mask: device float32 array on the cell grid; the solver treats cells with
+ * mask > 0 as solid (mgpcg_solid.py), the mask kernels cells with mask >= 1
+ * (init_conditions.py), as the reference does.
+ * ------------------------------------------------------------------------ */
+typedef struct fm_solid fm_solid;
+
+/* Allocates a solid-aware MG hierarchy (2D/vortex/mgpcg_solid.py:24-79,
+ * MGPCG_2_solid :370-382; dimension-generic) and, when mask is not NULL,
+ * downsamples it (downsample_bm, :114-127: a coarse cell is solid only when
+ * all its children are).  params as for fm_mgpcg_create (check_every >= 1 is
+ * the polling interval, 0 means 4; coarse_bf16 must be 0).  The only
+ * allocating call. */
+int fm_solid_create(const fm_grid *g, int dtype, const fm_mg_params *params, const float *mask, fm_solid **out);
+int fm_solid_destroy(fm_solid *solver);
+/* Re-derives the level masks from a (new) mask; the reference downsamples
+ * before every solve (:270-272). */
+int fm_solid_set_mask(fm_solid *solver, const float *mask, void *stream);
+/* apply_preconditioner (:249-268) on the fluid cells: z = V-cycle(r). */
+int fm_solid_vcycle(fm_solid *solver, const void *r, void *z, void *stream);
+/* solve (:270-367) of A x = b with recentring; *iters, *rtr as fm_mgpcg_solve. */
+int fm_solid_solve(fm_solid *solver, const void *b, void *x, void *stream, int *iters, double *rtr);
+/* MGPCG_2_solid.Poisson (:447-458): apply_bc (walls and the faces of solid
+ * cells zeroed), divergence (0 in solid cells), solve with k = -1,
+ * u -= grad p, apply_bc; p_out (cell grid) may be NULL. */
+int fm_solid_project(fm_solid *solver, void *ux, void *uy, void *uz, void *p_out, void *stream, int *iters,
+                     double *rtr);
+/* mask_velocity_by_boundary (2D/vortex/init_conditions.py:549-556,
+ * 3D/init_conditions.py:536-544): the faces of solid cells take the boundary
+ * velocity bvel (dim planes on the cell grid, the dtype), or 0 when bvel is
+ * NULL (mask_adj_velocity_by_boundary).  Where two solid cells share a face
+ * the cell on its high side wins (the reference's parallel writes race). */
+int fm_mask_velocity(const fm_grid *g, int dtype, const float *mask, const void *bvel, void *ux, void *uy, void *uz,
+                     void *stream);
+/* mask_passive_by_boundary (:558-571 / :547-561): a solid cell takes the mean
+ * of its fluid 3^dim neighbours, or 0; adjoint != 0: the solid cells are
+ * zeroed (mask_adj_passive_by_boundary). */
+int fm_mask_passive(const fm_grid *g, int dtype, const float *mask, void *s, int adjoint, void *stream);
+
+/* ------------------------------------------------------------------------
  * Gaussian control forces.  n Gaussians, device arrays of the dtype:
  * center n x dim (row-major), inv_radius n (r = 1/radius^2), strength n x dim.
  * ------------------------------------------------------------------------ */

@@ -9,10 +9,12 @@ sequences, which the product fuses):
   adjoint  3D/lfm_midpoint_diff_simulator.py:336-594 (init_gradient case 11,
            backtrack_step_midpoint, backtrack_flow_map)
   BFECC    3D/flowmap.py:405-452
-with empty obstacle masks; use_short_BFECC, BFECC_clamp, Gaussian control
-forces (add_control_force) and the 2D viscous term (2D/vortex/
-lfm_midpoint_simulator.py:552, 607-609; diff :270-271, 387-401) as the
-constructor selects.  The trajectory the reference writes to
+with use_short_BFECC, BFECC_clamp, Gaussian control
+forces (add_control_force), the 2D viscous term (2D/vortex/
+lfm_midpoint_simulator.py:552, 607-609; diff :270-271, 387-401) and an
+obstacle mask (solid-aware MGPCG and the mask kernels after every projection,
+3D/lfm_midpoint_simulator.py:606-608, 712-714, 769-771, 787-789; diff
+:357-361, 534-538, 572-576) as the constructor selects.  The trajectory the reference writes to
 .npy files is kept in Python lists.  Two documented extensions match the
 product: a run whose last reinit interval is partial stores that interval's
 forward map at the last step, and the Adams-Bashforth index counts adjoint
@@ -24,6 +26,7 @@ from __future__ import annotations
 import numpy as np
 
 import force_oracle
+import solid_oracle
 from oracle import MGParams, Oracle
 
 
@@ -58,7 +61,7 @@ def clamp_u(u, u1):
 class OracleSim:
     def __init__(self, res, dx, dt, reinit_every, total_steps, rk=4, backward_u=True, passive=True,
                  trajectory_loss=False, prec="f64", mg=None, bfecc_clamp=False, short_bfecc=False,
-                 control_forces=None, viscosity=0.0):
+                 control_forces=None, viscosity=0.0, mask=None, bvel=None):
         self.o = Oracle(tuple(res), prec)
         self.dim = len(res)
         self.res = tuple(res)
@@ -70,6 +73,9 @@ class OracleSim:
         self.cf_grads = {}
         self.nu = viscosity  # 2D only, as in the reference
         self.adj_viscous = 0.0
+        # obstacle mask (solid > 0): the solid-aware solver and the mask kernels (solid_oracle.py)
+        self.mask = None if mask is None or not np.any(np.asarray(mask) > 0) else np.asarray(mask, np.float32)
+        self.bvel = bvel
         if short_bfecc:
             o = self.o
             self.psi_tem, self.phi_tem = o.zeros_cell(self.dim), o.zeros_cell(self.dim)
@@ -98,8 +104,25 @@ class OracleSim:
 
     # -------------------------------------------------------------- helpers
     def Poisson(self, u):
+        if self.mask is not None:
+            m = self.mg
+            _, it, rtr = solid_oracle.project(u, self.mask, m.levels, max_iters=m.max_iters, abs_tol=m.abs_tol,
+                                              rel_tol=m.rel_tol, eps=m.eps, pre_post=m.pre_post, bottom=m.bottom)
+            self.iters.append(it)
+            return
         it, rtr, conv = self.o.Poisson(self.mg, u)
         self.iters.append(it)
+
+    def _mask(self, adjoint=False):
+        if self.mask is None:
+            return
+        solid_oracle.mask_velocity(self.u, self.mask, self.bvel)
+        if adjoint:
+            solid_oracle.mask_velocity(self.adj_u, self.mask)
+        if self.passive_on:
+            solid_oracle.mask_passive(self.passive, self.mask)
+            if adjoint:
+                solid_oracle.mask_adj_passive(self.adj_passive, self.mask)
 
     def reset_to_identity(self, psi, psi_f, T_f):
         self.o.reset_to_identity(psi, psi_f, T_f, self.dx)
@@ -164,6 +187,7 @@ class OracleSim:
         if self.passive_on:
             self.passive[...] = passive0
             self.init_passive[...] = self.passive
+        self._mask()
         self.step_num = -1
         self.reset_to_identity(self.phi, self.phi_f, self.F_f)
         for c in range(self.dim):
@@ -215,6 +239,7 @@ class OracleSim:
             for c in range(d):
                 self.u[c][...] = self.u[c] + (0.5 * dt) * f[c]
         self.Poisson(self.u)
+        self._mask()
         if self.nu:  # 2D/vortex/lfm_midpoint_simulator.py:552
             self.vis = viscous_force(self.u, self.nu, self.dx)
         self.velocity_storage[j] = [x.copy() for x in self.u]
@@ -245,11 +270,13 @@ class OracleSim:
                 self.u[c][...] = self.u[c] + dt * self.vis[c]
             o.accumulate_init(self.vis, self.init_u, self.F_f, self.phi_f, self.dx, dt)
         self.Poisson(self.u)
+        self._mask()
         n = self.step_num
         if j == self.R - 1:
             self.backtrack_psi_grid(self.R - 1)
             self.BFECC(self.init_u, self.u, self.err_u, self.tmp_u, self.T_f, self.psi_f, self.F_f, self.phi_f)
             self.Poisson(self.u)
+            self._mask()
             if self.passive_on:
                 self.BFECC_scalar(self.init_passive, self.passive, self.err_passive, self.tmp_passive, self.psi,
                                   self.phi)
@@ -284,6 +311,7 @@ class OracleSim:
             diff = self.passive - target
             self.adj_passive = (2 * diff).astype(o.dtype)
             self.loss = float(np.sum(diff.astype(np.float64) ** 2))
+        self._mask(adjoint=True)
         self.init_adj_u = [x.copy() for x in self.adj_u]
         self.init_adj_passive = self.adj_passive.copy()
         self.step_num = self.final_ind
@@ -383,6 +411,7 @@ class OracleSim:
                     self.u[c][...] = self.u[c] + (-dt) * self.vis[c]
                 o.accumulate_init(self.vis, self.init_u, self.T_f, self.psi_f, dx, -dt)
             self.Poisson(self.u)
+        self._mask(adjoint=True)
         if j == 0:
             phi, phi_f, F_f = self.store_maps[n // self.R]
             self.phi[...] = phi
@@ -399,6 +428,7 @@ class OracleSim:
                 self.Poisson(self.u)
                 for c in range(d):
                     self.init_u[c][...] = self.u[c]
+            self._mask(adjoint=True)
             if self.passive_on:
                 if self.trajectory_loss or not self.backward_u:
                     self.passive[...] = self.store_passive[n]
