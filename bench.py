@@ -53,8 +53,8 @@ def parse():
                          "a reported bench value needs W >= 3)")
     ap.add_argument("--gaussians", type=int, default=3000, help="Gaussian control forces per step (shape3d-forces)")
     ap.add_argument("--workload", default="gradient",
-                    choices=["gradient", "poisson", "vortex2d", "vortex2d-batch", "shape3d-forces",
-                             "force-kernels"],
+                    choices=["gradient", "poisson", "vortex2d", "vortex2d-obstacle", "vortex2d-batch",
+                             "shape3d-forces", "force-kernels"],
                     help="gradient: the headline 3D gradient benchmark; poisson: the mixed-precision Poisson solve "
                          "(seeded k^-5/3 divergence RHS, all-Neumann, --poisson-res^3); vortex2d: the 2D vortex "
                          "optimisation gradient dL/dtheta (256^2, 100 steps, 4 vortices); shape3d-forces: the 3D "
@@ -288,9 +288,12 @@ def run_vortex2d(a):
     C = importlib.import_module("differentiable-flowmap_b200.configs")
     vx = importlib.import_module("differentiable-flowmap_b200.vortex")
 
+    obstacle = a.workload == "vortex2d-obstacle"
+    mask = C.leaf_mask(256) if obstacle else None
+
     def problem(dtype, rel_tol, abs_tol=0.0, max_iters=400):
         cfg = C.vortex2d_config(res=256, steps=100, reinit_every=10, dtype=dtype, rel_tol=rel_tol, abs_tol=abs_tol,
-                                max_iters=max_iters)
+                                max_iters=max_iters, check_every=4 if obstacle else 0, boundary_mask=mask)
         return vx.VortexProblem(S.LFM_Diff_Simulator(config=cfg, device=dev))
 
     def timed(p, omt):
@@ -309,16 +312,20 @@ def run_vortex2d(a):
     p32 = problem(torch.float32, 1e-6)
     omt = p32.final_vorticity(C.vortex2d_theta(1))
     ms, loss, dth = timed(p32, omt)
-    p64 = problem(torch.float64, 1e-20)
+    # FP64 reference: solved to its floor (masked solves stall near rTr ~ 1e-15, so a cap of 100 iterations)
+    p64 = problem(torch.float64, 1e-20, max_iters=100 if obstacle else 400)
     l64, d64 = p64.gradient(theta, omt.double())
     # the reference solver's own criterion (solid MGPCG: absolute rTr < 1e-14)
     pabs = problem(torch.float32, 0.0, abs_tol=1e-14, max_iters=100)
     ms_abs, l_abs, d_abs = timed(pabs, omt)
-    line = {"metric": "2D vortex dL/dtheta evaluations/s, 256^2, 100 steps, 4 vortices", "value": 1e3 / ms,
+    name = "2D vortex dL/dtheta evaluations/s, 256^2, 100 steps, 4 vortices" + (", leaf obstacle" if obstacle else "")
+    line = {"metric": name, "value": 1e3 / ms,
             "unit": "grads/s", "n_gpus": 1, "steps": a.steps, "warmup": a.warmup, "ms_per_step": ms,
             "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic",
-            "config": {"workload": "2D vortex optimisation gradient, 256^2, dt 1/512, reinit 10, RK2, 12 parameters",
-                       "theta_seed": 0, "target_seed": 1},
+            "config": {"workload": "2D vortex optimisation gradient, 256^2, dt 1/512, reinit 10, RK2, 12 parameters"
+                                   + (", synthetic leaf obstacle (solid-aware MGPCG, mask kernels)" if obstacle else ""),
+                       "theta_seed": 0, "target_seed": 1,
+                       "obstacle_cells": int(mask.sum()) if obstacle else 0},
             "loss": loss, "dtheta": [float(x) for x in dth],
             "solver": "relative z.r 1e-6",
             "dtheta_rel_err_vs_fp64": float(np.linalg.norm(dth - d64) / np.linalg.norm(d64)),
@@ -597,7 +604,7 @@ def main():
         return run_reference(a)
     if a.workload == "poisson":
         return run_poisson(a)
-    if a.workload == "vortex2d":
+    if a.workload in ("vortex2d", "vortex2d-obstacle"):
         return run_vortex2d(a)
     if a.workload == "vortex2d-batch":
         return run_vortex2d_batch(a)

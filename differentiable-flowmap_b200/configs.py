@@ -77,15 +77,33 @@ def shape2d_config(res=256, steps=200, reinit_every=12, rk=2, dt=0.01, dtype=tor
 
 
 def vortex2d_config(res=256, steps=100, reinit_every=10, rk=2, dtype=torch.float32, rel_tol=1e-6, abs_tol=0.0,
-                    max_iters=400, check_every=0):
+                    max_iters=400, check_every=0, boundary_mask=None):
     """2D vortex optimisation: res^2, dx = 1/res, dt = 0.5 dx, 100 steps, reinit
     every 10, RK2, solid-style MGPCG (base level 4: 5 levels at 256^2, 20 bottom
-    sweeps as 10 x (R,B) + 10 x (B,R)), empty mask, no passive scalar."""
+    sweeps as 10 x (R,B) + 10 x (B,R)), no passive scalar; an optional obstacle
+    mask (solid > 0) selects the solid-aware solver and the mask kernels."""
     solver = SolverConfig(base_level=4, levels=max(2, int(math.log2(res)) - 4 + 1), bottom=20, bottom_mode=1,
                           max_iters=max_iters, abs_tol=abs_tol, rel_tol=rel_tol,
                           eps=1e-12 if dtype == torch.float32 else 0.0, check_every=check_every)
     return FlowmapConfig(res=(res, res), dx=1.0 / res, dt=0.5 / res, total_steps=steps, reinit_every=reinit_every,
-                         RK_number=rk, backward_u=True, add_passive_scalar=False, dtype=dtype, solver=solver)
+                         RK_number=rk, backward_u=True, add_passive_scalar=False, dtype=dtype, solver=solver,
+                         boundary_mask=boundary_mask)
+
+
+def leaf_mask(res=256, center=(0.5, 0.35), length=0.22, width=0.07, angle=0.6):
+    """A synthetic leaf-shaped obstacle (solid = 1) standing in for the
+    reference vortex experiment's leaf mask (2D/vortex/lfm_midpoint_simulator.py:
+    406, a data file): the intersection of two discs (a lens) rotated by
+    ``angle``, plus a one-cell-wide stem."""
+    x = (np.arange(res) + 0.5) / res
+    X, Y = np.meshgrid(x, x, indexing="ij")
+    c, s_ = math.cos(angle), math.sin(angle)
+    u = (X - center[0]) * c + (Y - center[1]) * s_
+    v = -(X - center[0]) * s_ + (Y - center[1]) * c
+    R = (length ** 2 + width ** 2) / (2 * width)
+    lens = ((u ** 2 + (v - (R - width)) ** 2) < R ** 2) & ((u ** 2 + (v + (R - width)) ** 2) < R ** 2)
+    stem = (np.abs(v) < 0.5 / res) & (u < -length) & (u > -length - 0.08)
+    return (lens | stem).astype(np.float32)
 
 
 def vortex2d_theta(seed=0, nv=4):

@@ -59,28 +59,6 @@ struct DevState {
 // ---------------------------------------------------------------------------
 // helpers
 // ---------------------------------------------------------------------------
-// x / nd for the RBGS update, nd = number of in-domain neighbours (0..6),
-// rounded exactly as the IEEE division.  FP32: nd = s * d with s a power of
-// two (exact scaling) and d in {1, 3, 5}; q0 = y * RN(1/d), e = y - q0 * d
-// (exact by FMA), q = q0 + e * RN(1/d).  Checked against the IEEE quotient for
-// all 2^32 float inputs and every nd: equal bit for bit whenever
-// 2^-100 <= |x| <= 2^100; outside that range (zeros, tiny, huge, non-finite)
-// and for nd = 0 the IEEE division is used.  It replaces a division whose
-// latency doubled the time of a coarse-level half-sweep.
-__device__ __forceinline__ float div_nd(float x, int nd) {
-  const float ax = fabsf(x);
-  if (ax >= 0x1p-100f && ax <= 0x1p100f && nd > 0) {
-    const float s = (nd == 2 || nd == 6) ? 0.5f : (nd == 4 ? 0.25f : 1.0f);
-    const float d = (nd == 3 || nd == 6) ? 3.0f : (nd == 5 ? 5.0f : 1.0f);
-    const float rd = (nd == 3 || nd == 6) ? (1.0f / 3.0f) : (nd == 5 ? (1.0f / 5.0f) : 1.0f);
-    const float y = __fmul_rn(x, s);
-    const float q0 = __fmul_rn(y, rd);
-    const float e = __fmaf_rn(-q0, d, y);
-    return __fmaf_rn(e, rd, q0);
-  }
-  return x / (float)nd;
-}
-__device__ __forceinline__ double div_nd(double x, int nd) { return x / (double)nd; }
 
 template <int D>
 __device__ __forceinline__ int parity(int i, int j, int k) {

@@ -18,12 +18,13 @@
 //
 // B200 mapping.  The hierarchy is small next to the flow-map state (256^2:
 // 0.5 MB per level), so the levels are plain global arrays and every step is a
-// grid-stride kernel; the coarsest level runs all its bottom sweeps in one
-// CTA with block barriers.  The PCG loop keeps its scalars (alpha, beta, the
-// inner products, a done flag) on the device: every kernel of an iteration
-// returns at once after convergence, so the host only polls the flag every
-// check_every iterations and the result equals stopping at the exact
-// iteration.
+// grid-stride kernel; the coarsest levels that fit 96 KB of shared memory
+// (down-sweeps, bottom, up-sweeps) run in one CTA out of shared memory.  The PCG loop keeps its
+// scalars (alpha, beta, the inner products, a done flag) on the device: every
+// kernel of an iteration returns at once after convergence, so the host only
+// polls the flag every check_every iterations (a chunk of iterations captured
+// once as a CUDA graph and replayed), and the result equals stopping at the
+// exact iteration.
 //
 // Mask kernels (2D/vortex/init_conditions.py:549-583, 3D/init_conditions.py:
 // 536-578): mask >= 1 is solid there.  mask_velocity writes the boundary
@@ -44,7 +45,7 @@ namespace solid {
 constexpr int kThreads = 256;
 constexpr int kRedBlocks = 148 * 4;
 constexpr int kBottomThreads = 1024;
-constexpr long kBottomMaxCells = 16384;  // coarsest levels up to this size run in one CTA
+constexpr size_t kCoarseSmem = 96 * 1024;  // shared memory for the single-CTA coarse levels
 
 struct State {
   double old_zr, tol, rtr, pAp, new_zr, sum_r;
@@ -68,22 +69,23 @@ __device__ __forceinline__ long stride_of(const Shape& s, int a) {
 // (count, sum) over in-domain fluid neighbours: per axis the right, then the
 // left neighbour (neighbor_sum2 / num_fluid_neighbors2, :141-172)
 template <typename T, int D>
-__device__ __forceinline__ void fluid_nbrs(const T* __restrict__ x, const uint8_t* __restrict__ fl, const Shape& s,
-                                           const int* I, long q, T& n, T& sum) {
-  n = (T)0;
+__device__ __forceinline__ int fluid_nbrs(const T* __restrict__ x, const uint8_t* __restrict__ fl, const Shape& s,
+                                          const int* I, long q, T& sum) {
+  int n = 0;
   sum = (T)0;
 #pragma unroll
   for (int a = 0; a < D; ++a) {
     const long st = stride_of(s, a);
     if (I[a] < axis_len(s, a) - 1 && fl[q + st]) {
       sum = rn_add(sum, x[q + st]);
-      n = n + (T)1;
+      ++n;
     }
     if (I[a] > 0 && fl[q - st]) {
       sum = rn_add(sum, x[q - st]);
-      n = n + (T)1;
+      ++n;
     }
   }
+  return n;
 }
 
 __global__ void k_mask0(long n, const float* __restrict__ mask, uint8_t* __restrict__ fl) {
@@ -104,40 +106,150 @@ __global__ void k_downsample(Shape sf, const uint8_t* __restrict__ ff, Shape sc,
   }
 }
 
+// z = (r + sum) / n with div_nd (rounded as the IEEE quotient)
+template <typename T, int D>
+__device__ __forceinline__ void smooth_at(const Shape& s, T* z, const T* r, const uint8_t* fl, const int* I, long q) {
+  if (!fl[q]) return;
+  T sum;
+  const int n = fluid_nbrs<T, D>(z, fl, s, I, q, sum);
+  z[q] = div_nd(rn_add(r[q], sum), n);
+}
+
 template <typename T, int D>
 __device__ __forceinline__ void smooth_cell(const Shape& s, T* z, const T* r, const uint8_t* fl, long q, int phase) {
   int I[3];
   idx3(s, q, I);
-  if (!fl[q] || ((I[0] + I[1] + I[2]) & 1) != phase) return;
-  T n, sum;
-  fluid_nbrs<T, D>(z, fl, s, I, q, n, sum);
-  z[q] = rn_add(r[q], sum) / n;
+  if (((I[0] + I[1] + I[2]) & 1) != phase) return;
+  smooth_at<T, D>(s, z, r, fl, I, q);
 }
 
+// grid-wide half-sweep: one thread per cell of the colour (row = blockIdx.y
+// (and .z in 3D), the fastest axis holding every other cell)
 template <typename T, int D>
 __global__ void k_smooth(Shape s, T* __restrict__ z, const T* __restrict__ r, const uint8_t* __restrict__ fl,
                          int phase, const State* __restrict__ st) {
   if (st && st->done) return;
-  for (long q = (long)blockIdx.x * blockDim.x + threadIdx.x; q < s.size(); q += (long)gridDim.x * blockDim.x)
-    smooth_cell<T, D>(s, z, r, fl, q, phase);
+  const int t = blockIdx.x * blockDim.x + threadIdx.x;
+  int I[3];
+  if (D == 3) {
+    I[0] = blockIdx.z;
+    I[1] = blockIdx.y;
+    I[2] = 2 * t + ((I[0] + I[1] + phase) & 1);
+    if (I[2] >= s.s2) return;
+  } else {
+    I[0] = blockIdx.y;
+    I[1] = 2 * t + ((I[0] + phase) & 1);
+    I[2] = 0;
+    if (I[1] >= s.s1) return;
+  }
+  smooth_at<T, D>(s, z, r, fl, I, s.idx(I[0], I[1], I[2]));
 }
 
-// all bottom sweeps of a small coarsest level in one CTA
+// launch shape of k_smooth for a level
+inline void smooth_grid(const Shape& s, int dim, dim3& grid, dim3& block) {
+  const int row = dim == 3 ? s.s2 : s.s1, half = (row + 1) / 2;
+  block = dim3(half >= 128 ? 128 : 32 * ((half + 31) / 32));
+  grid = dim3((half + block.x - 1) / block.x, dim == 3 ? s.s1 : s.s0, dim == 3 ? s.s0 : 1);
+}
+
 template <typename T, int D>
-__global__ void __launch_bounds__(kBottomThreads) k_bottom(Shape s, T* __restrict__ z, const T* __restrict__ r,
-                                                           const uint8_t* __restrict__ fl, int bottom, int mode,
-                                                           const State* __restrict__ st) {
-  if (st && st->done) return;
-  const int pairs = mode == 1 ? bottom / 2 : bottom;
-  for (int pass = 0; pass < (mode == 1 ? 2 : 1); ++pass) {
-    for (int it = 0; it < pairs; ++it) {
-      for (int h = 0; h < 2; ++h) {
-        const int phase = pass == 0 ? h : 1 - h;
-        for (long q = threadIdx.x; q < s.size(); q += blockDim.x) smooth_cell<T, D>(s, z, r, fl, q, phase);
-        __syncthreads();
+__device__ __forceinline__ void restrict_cell(const Shape& sf, const T* z, const T* r, const uint8_t* fl,
+                                              const Shape& sc, T* rc, T* zc, long qc) {
+  const T scale = (T)(1.0 / (D - 1.0));
+  int C[3];
+  idx3(sc, qc, C);
+  T acc = (T)0;
+  for (int d0 = 0; d0 < 2; ++d0)
+    for (int d1 = 0; d1 < 2; ++d1)
+      for (int d2 = 0; d2 < (D == 3 ? 2 : 1); ++d2) {
+        int I[3] = {2 * C[0] + d0, 2 * C[1] + d1, D == 3 ? 2 * C[2] + d2 : 0};
+        const long q = sf.idx(I[0], I[1], I[2]);
+        if (!fl[q]) continue;
+        T sum;
+        const T n = (T)fluid_nbrs<T, D>(z, fl, sf, I, q, sum);
+        const T res = rn_sub(r[q], rn_sub(rn_mul(n, z[q]), sum));
+        acc = rn_add(acc, rn_mul(res, scale));
       }
+  rc[qc] = acc;
+  zc[qc] = (T)0;
+}
+
+// The levels lc..L-1 of a V-cycle in one CTA, staged in shared memory: the
+// residual of level lc and every level's fluid flags are loaded, the
+// down-sweeps (with restriction), the bottom sweeps and the up-sweeps (with
+// prolongation) run on shared arrays with block barriers between dependent
+// steps, and z of level lc is written back for the prolongation into lc - 1.
+// z[lc] starts at zero.  The same operations in the same order as the
+// grid-wide kernels, so the V-cycle is unchanged bit for bit.
+struct CoarseLevels {
+  int lc, L, pre_post, bottom, mode;
+  Shape sh[16];
+  const void* r_lc;
+  void* z_lc;
+  const uint8_t* fl[16];
+};
+
+template <typename T>
+constexpr size_t coarse_cell_bytes() { return 2 * sizeof(T) + 1; }
+
+template <typename T, int D>
+__device__ __forceinline__ void sweep_block(const Shape& s, T* z, const T* r, const uint8_t* fl, int phase) {
+  for (long q = threadIdx.x; q < s.size(); q += blockDim.x) smooth_cell<T, D>(s, z, r, fl, q, phase);
+  __syncthreads();
+}
+
+template <typename T, int D>
+__global__ void __launch_bounds__(kBottomThreads) k_coarse(CoarseLevels c, const State* __restrict__ st) {
+  if (st && st->done) return;
+  extern __shared__ __align__(16) unsigned char smem[];
+  T* zs[16];
+  T* rs[16];
+  uint8_t* fs[16];
+  {
+    T* p = (T*)smem;
+    for (int l = c.lc; l < c.L; ++l) {
+      zs[l] = p;
+      p += c.sh[l].size();
+      rs[l] = p;
+      p += c.sh[l].size();
+    }
+    uint8_t* f = (uint8_t*)p;
+    for (int l = c.lc; l < c.L; ++l) {
+      fs[l] = f;
+      f += c.sh[l].size();
     }
   }
+  for (int l = c.lc; l < c.L; ++l)
+    for (long q = threadIdx.x; q < c.sh[l].size(); q += blockDim.x) fs[l][q] = c.fl[l][q];
+  for (long q = threadIdx.x; q < c.sh[c.lc].size(); q += blockDim.x) {
+    rs[c.lc][q] = ((const T*)c.r_lc)[q];
+    zs[c.lc][q] = (T)0;
+  }
+  __syncthreads();
+  for (int l = c.lc; l < c.L - 1; ++l) {
+    for (int i = 0; i < c.pre_post; ++i)
+      for (int ph = 0; ph < 2; ++ph) sweep_block<T, D>(c.sh[l], zs[l], rs[l], fs[l], ph);
+    for (long q = threadIdx.x; q < c.sh[l + 1].size(); q += blockDim.x)
+      restrict_cell<T, D>(c.sh[l], zs[l], rs[l], fs[l], c.sh[l + 1], rs[l + 1], zs[l + 1], q);
+    __syncthreads();
+  }
+  const int b = c.L - 1;
+  const int pairs = c.mode == 1 ? c.bottom / 2 : c.bottom;
+  for (int pass = 0; pass < (c.mode == 1 ? 2 : 1); ++pass)
+    for (int it = 0; it < pairs; ++it)
+      for (int h = 0; h < 2; ++h) sweep_block<T, D>(c.sh[b], zs[b], rs[b], fs[b], pass == 0 ? h : 1 - h);
+  for (int l = c.L - 2; l >= c.lc; --l) {
+    const Shape s = c.sh[l], sc = c.sh[l + 1];
+    for (long q = threadIdx.x; q < s.size(); q += blockDim.x) {
+      int I[3];
+      idx3(s, q, I);
+      zs[l][q] = rn_add(zs[l][q], zs[l + 1][sc.idx(I[0] / 2, I[1] / 2, D == 3 ? I[2] / 2 : 0)]);
+    }
+    __syncthreads();
+    for (int i = 0; i < c.pre_post; ++i)
+      for (int ph = 1; ph >= 0; --ph) sweep_block<T, D>(s, zs[l], rs[l], fs[l], ph);
+  }
+  for (long q = threadIdx.x; q < c.sh[c.lc].size(); q += blockDim.x) ((T*)c.z_lc)[q] = zs[c.lc][q];
 }
 
 // r_c = sum over fluid children (lexicographic) of (r - (n z - sum)) / (dim - 1); z_c = 0
@@ -145,25 +257,8 @@ template <typename T, int D>
 __global__ void k_restrict(Shape sf, const T* __restrict__ z, const T* __restrict__ r, const uint8_t* __restrict__ fl,
                            Shape sc, T* __restrict__ rc, T* __restrict__ zc, const State* __restrict__ st) {
   if (st && st->done) return;
-  const T scale = (T)(1.0 / (D - 1.0));
-  for (long qc = (long)blockIdx.x * blockDim.x + threadIdx.x; qc < sc.size(); qc += (long)gridDim.x * blockDim.x) {
-    int C[3];
-    idx3(sc, qc, C);
-    T acc = (T)0;
-    for (int d0 = 0; d0 < 2; ++d0)
-      for (int d1 = 0; d1 < 2; ++d1)
-        for (int d2 = 0; d2 < (D == 3 ? 2 : 1); ++d2) {
-          int I[3] = {2 * C[0] + d0, 2 * C[1] + d1, D == 3 ? 2 * C[2] + d2 : 0};
-          const long q = sf.idx(I[0], I[1], I[2]);
-          if (!fl[q]) continue;
-          T n, sum;
-          fluid_nbrs<T, D>(z, fl, sf, I, q, n, sum);
-          const T res = rn_sub(r[q], rn_sub(rn_mul(n, z[q]), sum));
-          acc = rn_add(acc, rn_mul(res, scale));
-        }
-    rc[qc] = acc;
-    zc[qc] = (T)0;
-  }
+  for (long qc = (long)blockIdx.x * blockDim.x + threadIdx.x; qc < sc.size(); qc += (long)gridDim.x * blockDim.x)
+    restrict_cell<T, D>(sf, z, r, fl, sc, rc, zc, qc);
 }
 
 template <typename T, int D>
@@ -209,17 +304,25 @@ __global__ void __launch_bounds__(kThreads) k_dot(long n, const T* __restrict__ 
   block_sum_to<T>(acc, part);
 }
 
-__device__ __forceinline__ double sum_parts(const double* part) {
-  double s = 0;
-  for (int b = 0; b < kRedBlocks; ++b) s += part[b];
-  return s;
-}
+constexpr int kFinThreads = 256;
 
 // which: 0 initial zTr (tolerance), 1 alpha, 2 rTr (convergence), 3 mean of r,
-// 4 beta (and the iteration count)
-__global__ void k_fin(int which, const double* __restrict__ part, State* __restrict__ st, long ncells) {
-  if (threadIdx.x != 0 || st->done) return;
-  const double s = sum_parts(part);
+// 4 beta (and the iteration count).  The partials are summed in a fixed order
+// (strided per thread, then a tree), so the result is deterministic.
+__global__ void __launch_bounds__(kFinThreads) k_fin(int which, const double* __restrict__ part,
+                                                     State* __restrict__ st, long ncells) {
+  if (st->done) return;
+  __shared__ double red[kFinThreads];
+  double a = 0.0;
+  for (int b = threadIdx.x; b < kRedBlocks; b += kFinThreads) a += part[b];
+  red[threadIdx.x] = a;
+  __syncthreads();
+  for (int h = kFinThreads / 2; h > 0; h >>= 1) {
+    if (threadIdx.x < h) red[threadIdx.x] += red[threadIdx.x + h];
+    __syncthreads();
+  }
+  if (threadIdx.x != 0) return;
+  const double s = red[0];
   if (which == 0) {
     st->old_zr = s;
     st->tol = fmax(st->abs_tol, s * st->rel_tol);
@@ -263,8 +366,8 @@ __global__ void k_Ap(Shape s, const T* __restrict__ p, const uint8_t* __restrict
     }
     int I[3];
     idx3(s, q, I);
-    T n, sum;
-    fluid_nbrs<T, D>(p, fl, s, I, q, n, sum);
+    T sum;
+    const T n = (T)fluid_nbrs<T, D>(p, fl, s, I, q, sum);
     Ap[q] = rn_sub(rn_mul(n, p[q]), sum);
   }
 }
@@ -424,6 +527,10 @@ struct fm_solid {
   double* part;
   fm::solid::State* st;
   fm::solid::State* st_host;  // pinned
+  // check_every PCG iterations captured once as a graph (replayed per poll)
+  cudaStream_t cap;
+  cudaGraphExec_t chunk;
+  size_t chunk_nodes;
 };
 
 namespace fm {
@@ -436,37 +543,101 @@ inline unsigned blocks_for(long n) {
 }
 
 template <typename T, int D>
+inline void launch_smooth(const Shape& sh, cudaStream_t s, T* z, const T* r, const uint8_t* fl, int phase,
+                          const State* st) {
+  dim3 grid, block;
+  smooth_grid(sh, D, grid, block);
+  launch(k_smooth<T, D>, grid, block, 0, s, sh, z, r, fl, phase, st);
+}
+
+// first level from which the remaining levels fit the coarse kernel's shared
+// memory (L when not even the coarsest one does)
+template <typename T>
+int coarse_start(const fm_solid* S, size_t* bytes) {
+  size_t acc = 0;
+  int lc = S->levels;
+  for (int l = S->levels - 1; l >= 0; --l) {
+    const size_t need = acc + (size_t)S->sh[l].size() * coarse_cell_bytes<T>();
+    if (need > kCoarseSmem) break;
+    acc = need;
+    lc = l;
+  }
+  *bytes = acc;
+  return lc;
+}
+
+template <typename T, int D>
 void vcycle(fm_solid* S, cudaStream_t s, const State* st) {
-  const int L = S->levels;
+  size_t smem = 0;
+  const int L = S->levels, lc = coarse_start<T>(S, &smem);
   launch(k_fill<T>, blocks_for(S->sh[0].size()), kThreads, 0, s, S->sh[0].size(), (T*)S->z[0], st);
-  for (int l = 0; l < L - 1; ++l) {
+  const int down = lc < L ? lc : L - 1;  // levels smoothed and restricted by grid-wide launches
+  for (int l = 0; l < down; ++l) {
     for (int i = 0; i < S->P.pre_post; ++i)
       for (int ph = 0; ph < 2; ++ph)
-        launch(k_smooth<T, D>, blocks_for(S->sh[l].size()), kThreads, 0, s, S->sh[l], (T*)S->z[l], (const T*)S->r[l],
+        launch_smooth<T, D>(S->sh[l], s, (T*)S->z[l], (const T*)S->r[l],
                (const uint8_t*)S->fl[l], ph, st);
     launch(k_restrict<T, D>, blocks_for(S->sh[l + 1].size()), kThreads, 0, s, S->sh[l], (const T*)S->z[l],
            (const T*)S->r[l], (const uint8_t*)S->fl[l], S->sh[l + 1], (T*)S->r[l + 1], (T*)S->z[l + 1], st);
   }
-  const int b = L - 1;
-  if (S->sh[b].size() <= kBottomMaxCells) {
-    launch(k_bottom<T, D>, 1, kBottomThreads, 0, s, S->sh[b], (T*)S->z[b], (const T*)S->r[b], (const uint8_t*)S->fl[b],
-           S->P.bottom, S->P.bottom_mode, st);
+  if (lc < L) {
+    CoarseLevels c;
+    c.lc = lc;
+    c.L = L;
+    c.pre_post = S->P.pre_post;
+    c.bottom = S->P.bottom;
+    c.mode = S->P.bottom_mode;
+    c.r_lc = S->r[lc];
+    c.z_lc = S->z[lc];
+    for (int l = 0; l < L; ++l) {
+      c.sh[l] = S->sh[l];
+      c.fl[l] = S->fl[l];
+    }
+    launch(k_coarse<T, D>, 1, kBottomThreads, smem, s, c, st);
   } else {
+    // even the coarsest level is large: its bottom sweeps as grid-wide launches
+    const int b = L - 1;
     const int pairs = S->P.bottom_mode == 1 ? S->P.bottom / 2 : S->P.bottom;
     for (int pass = 0; pass < (S->P.bottom_mode == 1 ? 2 : 1); ++pass)
       for (int it = 0; it < pairs; ++it)
         for (int h = 0; h < 2; ++h)
-          launch(k_smooth<T, D>, blocks_for(S->sh[b].size()), kThreads, 0, s, S->sh[b], (T*)S->z[b], (const T*)S->r[b],
+          launch_smooth<T, D>(S->sh[b], s, (T*)S->z[b], (const T*)S->r[b],
                  (const uint8_t*)S->fl[b], pass == 0 ? h : 1 - h, st);
   }
-  for (int l = L - 2; l >= 0; --l) {
+  for (int l = down - 1; l >= 0; --l) {
     launch(k_prolong<T, D>, blocks_for(S->sh[l].size()), kThreads, 0, s, S->sh[l], (T*)S->z[l], S->sh[l + 1],
            (const T*)S->z[l + 1], st);
     for (int i = 0; i < S->P.pre_post; ++i)
       for (int ph = 1; ph >= 0; --ph)
-        launch(k_smooth<T, D>, blocks_for(S->sh[l].size()), kThreads, 0, s, S->sh[l], (T*)S->z[l], (const T*)S->r[l],
+        launch_smooth<T, D>(S->sh[l], s, (T*)S->z[l], (const T*)S->r[l],
                (const uint8_t*)S->fl[l], ph, st);
   }
+}
+
+// one PCG iteration (solve(), :318-363), every kernel frozen once st->done is set
+template <typename T, int D>
+void iteration(fm_solid* S, cudaStream_t s) {
+  const long n = S->sh[0].size();
+  const unsigned nb = blocks_for(n);
+  State* st = S->st;
+  T* r = (T*)S->r[0];
+  T* p = (T*)S->p;
+  T* Ap = (T*)S->Ap;
+  const uint8_t* fl = S->fl[0];
+  launch(k_Ap<T, D>, nb, kThreads, 0, s, S->sh[0], (const T*)p, fl, Ap, (const State*)st);
+  launch(k_dot<T>, kRedBlocks, kThreads, 0, s, n, (const T*)p, (const T*)Ap, fl, S->part, (const State*)st);
+  launch(k_fin, 1, kFinThreads, 0, s, 1, (const double*)S->part, st, n);
+  launch(k_update_xr<T>, nb, kThreads, 0, s, n, (T*)S->x, r, (const T*)p, (const T*)Ap, fl, (const State*)st);
+  launch(k_dot<T>, kRedBlocks, kThreads, 0, s, n, (const T*)r, (const T*)r, fl, S->part, (const State*)st);
+  launch(k_fin, 1, kFinThreads, 0, s, 2, (const double*)S->part, st, n);
+  launch(k_dot<T>, kRedBlocks, kThreads, 0, s, n, (const T*)r, (const T*)nullptr, (const uint8_t*)nullptr, S->part,
+         (const State*)st);
+  launch(k_fin, 1, kFinThreads, 0, s, 3, (const double*)S->part, st, n);
+  launch(k_recenter<T>, nb, kThreads, 0, s, n, r, (const State*)st);
+  vcycle<T, D>(S, s, st);
+  launch(k_dot<T>, kRedBlocks, kThreads, 0, s, n, (const T*)S->z[0], (const T*)r, fl, S->part, (const State*)st);
+  launch(k_fin, 1, kFinThreads, 0, s, 4, (const double*)S->part, st, n);
+  launch(k_update_p<T>, nb, kThreads, 0, s, n, p, (const T*)S->z[0], fl, (const State*)st);
 }
 
 template <typename T, int D>
@@ -483,7 +654,6 @@ int solve(fm_solid* S, const void* b, double k, void* x, cudaStream_t s, int* it
   T* r = (T*)S->r[0];
   T* z = (T*)S->z[0];
   T* p = (T*)S->p;
-  T* Ap = (T*)S->Ap;
   T* xs = (T*)S->x;
   const uint8_t* fl = S->fl[0];
   const unsigned nb = blocks_for(n);
@@ -491,33 +661,34 @@ int solve(fm_solid* S, const void* b, double k, void* x, cudaStream_t s, int* it
   // recenter, precondition, p = z, zTr
   launch(k_dot<T>, kRedBlocks, kThreads, 0, s, n, (const T*)r, (const T*)nullptr, (const uint8_t*)nullptr, S->part,
          (const State*)st);
-  launch(k_fin, 1, 32, 0, s, 3, (const double*)S->part, st, n);
+  launch(k_fin, 1, kFinThreads, 0, s, 3, (const double*)S->part, st, n);
   launch(k_recenter<T>, nb, kThreads, 0, s, n, r, (const State*)st);
   vcycle<T, D>(S, s, st);
   launch(k_update_p<T>, nb, kThreads, 0, s, n, p, (const T*)z, fl, (const State*)st);
   launch(k_dot<T>, kRedBlocks, kThreads, 0, s, n, (const T*)z, (const T*)r, fl, S->part, (const State*)st);
-  launch(k_fin, 1, 32, 0, s, 0, (const double*)S->part, st, n);
+  launch(k_fin, 1, kFinThreads, 0, s, 0, (const double*)S->part, st, n);
   const int every = S->P.check_every > 0 ? S->P.check_every : 4;
-  for (int it = 0; it < S->P.max_iters; ++it) {
-    launch(k_Ap<T, D>, nb, kThreads, 0, s, S->sh[0], (const T*)p, fl, Ap, (const State*)st);
-    launch(k_dot<T>, kRedBlocks, kThreads, 0, s, n, (const T*)p, (const T*)Ap, fl, S->part, (const State*)st);
-    launch(k_fin, 1, 32, 0, s, 1, (const double*)S->part, st, n);
-    launch(k_update_xr<T>, nb, kThreads, 0, s, n, xs, r, (const T*)p, (const T*)Ap, fl, (const State*)st);
-    launch(k_dot<T>, kRedBlocks, kThreads, 0, s, n, (const T*)r, (const T*)r, fl, S->part, (const State*)st);
-    launch(k_fin, 1, 32, 0, s, 2, (const double*)S->part, st, n);
-    launch(k_dot<T>, kRedBlocks, kThreads, 0, s, n, (const T*)r, (const T*)nullptr, (const uint8_t*)nullptr, S->part,
-           (const State*)st);
-    launch(k_fin, 1, 32, 0, s, 3, (const double*)S->part, st, n);
-    launch(k_recenter<T>, nb, kThreads, 0, s, n, r, (const State*)st);
-    vcycle<T, D>(S, s, st);
-    launch(k_dot<T>, kRedBlocks, kThreads, 0, s, n, (const T*)z, (const T*)r, fl, S->part, (const State*)st);
-    launch(k_fin, 1, 32, 0, s, 4, (const double*)S->part, st, n);
-    launch(k_update_p<T>, nb, kThreads, 0, s, n, p, (const T*)z, fl, (const State*)st);
-    if ((it + 1) % every == 0 || it + 1 == S->P.max_iters) {
-      if (cudaMemcpyAsync(S->st_host, st, sizeof(State), cudaMemcpyDeviceToHost, s) != cudaSuccess) return FM_ERR_CUDA;
-      if (cudaStreamSynchronize(s) != cudaSuccess) return FM_ERR_CUDA;
-      if (S->st_host->done) break;
+  if (!S->chunk) {
+    // capture check_every iterations once; the captured kernels are counted per replay
+    const long long before = g_launch_count.load();
+    cudaGraph_t graph;
+    if (cudaStreamBeginCapture(S->cap, cudaStreamCaptureModeThreadLocal) != cudaSuccess) return FM_ERR_CUDA;
+    for (int i = 0; i < every; ++i) iteration<T, D>(S, S->cap);
+    if (cudaStreamEndCapture(S->cap, &graph) != cudaSuccess) return FM_ERR_CUDA;
+    g_launch_count.store(before);
+    if (cudaGraphGetNodes(graph, nullptr, &S->chunk_nodes) != cudaSuccess ||
+        cudaGraphInstantiate(&S->chunk, graph, 0) != cudaSuccess) {
+      cudaGraphDestroy(graph);
+      return FM_ERR_CUDA;
     }
+    cudaGraphDestroy(graph);
+  }
+  for (int it = 0; it < S->P.max_iters; it += every) {
+    if (cudaGraphLaunch(S->chunk, s) != cudaSuccess) return FM_ERR_CUDA;
+    count_launch((long long)S->chunk_nodes);
+    if (cudaMemcpyAsync(S->st_host, st, sizeof(State), cudaMemcpyDeviceToHost, s) != cudaSuccess) return FM_ERR_CUDA;
+    if (cudaStreamSynchronize(s) != cudaSuccess) return FM_ERR_CUDA;
+    if (S->st_host->done) break;
   }
   if (cudaMemcpyAsync(S->st_host, st, sizeof(State), cudaMemcpyDeviceToHost, s) != cudaSuccess) return FM_ERR_CUDA;
   if (cudaStreamSynchronize(s) != cudaSuccess) return FM_ERR_CUDA;
@@ -567,6 +738,8 @@ int fm_solid_destroy(fm_solid* S) {
   cudaFree(S->part);
   cudaFree(S->st);
   if (S->st_host) cudaFreeHost(S->st_host);
+  if (S->chunk) cudaGraphExecDestroy(S->chunk);
+  if (S->cap) cudaStreamDestroy(S->cap);
   free(S);
   return FM_OK;
 }
@@ -620,11 +793,19 @@ int fm_solid_create(const fm_grid* g, int dtype, const fm_mg_params* params, con
        cudaMalloc(&S->Ap, n * es) == cudaSuccess && cudaMalloc(&S->div, n * es) == cudaSuccess &&
        cudaMalloc((void**)&S->part, solid::kRedBlocks * sizeof(double)) == cudaSuccess &&
        cudaMalloc((void**)&S->st, sizeof(solid::State)) == cudaSuccess &&
-       cudaMallocHost((void**)&S->st_host, sizeof(solid::State)) == cudaSuccess;
+       cudaMallocHost((void**)&S->st_host, sizeof(solid::State)) == cudaSuccess &&
+       cudaStreamCreateWithFlags(&S->cap, cudaStreamNonBlocking) == cudaSuccess;
   if (!ok) {
     fm_solid_destroy(S);
     return FM_ERR_CUDA;
   }
+  // the coarse-levels kernel may use more than the default 48 KB of shared memory
+  if (dtype == FM_F32)
+    cudaFuncSetAttribute(g->dim == 2 ? solid::k_coarse<float, 2> : solid::k_coarse<float, 3>,
+                         cudaFuncAttributeMaxDynamicSharedMemorySize, (int)solid::kCoarseSmem);
+  else
+    cudaFuncSetAttribute(g->dim == 2 ? solid::k_coarse<double, 2> : solid::k_coarse<double, 3>,
+                         cudaFuncAttributeMaxDynamicSharedMemorySize, (int)solid::kCoarseSmem);
   if (mask) {
     const int ms = fm_solid_set_mask(S, mask, nullptr);
     if (ms == FM_OK) cudaDeviceSynchronize();
