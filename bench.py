@@ -51,6 +51,8 @@ def parse():
     ap.add_argument("--no-roofline", action="store_true",
                     help="skip the dominant-kernel roofline timing (used for profiler runs, which need W >= 1 only; "
                          "a reported bench value needs W >= 3)")
+    ap.add_argument("--mixed-coarse", default="bf16", choices=["bf16", "fp32"],
+                    help="storage of the MG coarse levels in the mixed form")
     ap.add_argument("--gaussians", type=int, default=3000, help="Gaussian control forces per step (shape3d-forces)")
     ap.add_argument("--workload", default="gradient",
                     choices=["gradient", "poisson", "vortex2d", "vortex2d-obstacle", "vortex2d-batch",
@@ -75,7 +77,8 @@ def form_config(C, a, form, dtype):
     mixed = form == "mixed"
     store = torch.bfloat16 if (mixed and dtype == torch.float32) else None
     return C.shape3d_config(res=a.res, steps=a.sim_steps, reinit_every=a.reinit, rk=4, dtype=dtype,
-                            store_dtype=store, backward_u=not mixed, check_every=a.solver_check_every)
+                            store_dtype=store, backward_u=not mixed, check_every=a.solver_check_every,
+                            coarse_bf16=mixed and dtype == torch.float32 and a.mixed_coarse == "bf16")
 
 
 def workload_name(a):
@@ -746,6 +749,7 @@ def main():
                            "res": a.res, "sim_steps": a.sim_steps,
                            "reinit_every": a.reinit, "rk": 4, "backward_u": backward_u,
                            "store_dtype": "bf16" if store is not None else "f32",
+                           "mg_coarse_storage": "bf16" if cfg.solver.coarse_bf16 else "f32",
                            "solver": {"levels": sim.solver.n_mg_levels, "rel_tol": cfg.solver.rel_tol,
                                       "mean_pcg_iters": pcg_iters / solves if solves else None,
                                       "solves_per_grad": solves // max(a.steps, 1),

@@ -37,13 +37,13 @@ def smooth_ball(res, center, radius, dx):
 
 
 def shape3d_config(res=128, steps=150, reinit_every=8, rk=4, dtype=torch.float32, store_dtype=None,
-                   backward_u=True, rel_tol=1e-6, abs_tol=0.0, max_iters=400, check_every=0):
+                   backward_u=True, rel_tol=1e-6, abs_tol=0.0, max_iters=400, check_every=0, coarse_bf16=False):
     """3D smoke shape transition, 128^3: 150 steps, reinit every 8, RK4,
     dt = 0.0085 (3D/hyperparameters.py:268-295 with the stated overrides)."""
     n = int(math.log2(res))
     solver = SolverConfig(base_level=3, levels=n - 3 + 1, bottom=50, bottom_mode=0, max_iters=max_iters,
                           abs_tol=abs_tol, rel_tol=rel_tol, eps=1e-12 if dtype == torch.float32 else 0.0,
-                          check_every=check_every)
+                          check_every=check_every, coarse_bf16=coarse_bf16)
     return FlowmapConfig(res=(res, res, res), dx=1.0 / res, dt=0.0085, total_steps=steps,
                          reinit_every=reinit_every, RK_number=rk, backward_u=backward_u, add_passive_scalar=True,
                          dtype=dtype, store_dtype=store_dtype, solver=solver)

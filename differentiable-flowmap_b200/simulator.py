@@ -50,6 +50,7 @@ class SolverConfig:
     rel_tol: float = 0.0
     eps: float = 1e-12
     check_every: int = 4
+    coarse_bf16: bool = False  # FP32 solvers: per-level coarse grids stored in BF16 (arithmetic FP32)
 
 
 @dataclass
@@ -209,7 +210,8 @@ class LFM_Simulator:
         else:
             self.solver = MGPCG(g.shape, dt_, base_level=sc.base_level, levels=sc.levels, pre_post=sc.pre_post,
                                 bottom=sc.bottom, bottom_mode=sc.bottom_mode, max_iters=sc.max_iters,
-                                abs_tol=sc.abs_tol, rel_tol=sc.rel_tol, eps=sc.eps, check_every=sc.check_every)
+                                abs_tol=sc.abs_tol, rel_tol=sc.rel_tol, eps=sc.eps, check_every=sc.check_every,
+                                coarse_bf16=sc.coarse_bf16 and dt_ == torch.float32)
 
         # flow maps: backward (psi, T) and forward (phi, F); centre maps for scalars
         self.psi = torch.zeros((self.dim,) + g.shape, dtype=dt_, device=dev)
