@@ -347,168 +347,73 @@ def run_vortex2d_batch(a):
     4 x 384^2; 100 steps, reinit 10, dt = 0.5 dx; control seeds 100+i, target
     seeds 200+i) advanced concurrently, one stream and host thread each; one
     bench step = one gradient of every instance.  Compared with the same
-    instances run one after another."""
+    instances run one after another.  Under torchrun the instances are split
+    across the ranks by cost (greedy bin-packing on cells x steps, no collective
+    in the timed loop); the time is the max over ranks."""
     import numpy as np
     import torch
+    import torch.distributed as dist
 
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
     local = int(os.environ.get("LOCAL_RANK", "0"))
     torch.cuda.set_device(local)
     dev = torch.device("cuda", local)
+    if world > 1:
+        from datetime import timedelta
+        dist.init_process_group("nccl", timeout=timedelta(seconds=600), device_id=dev)
     B = importlib.import_module("differentiable-flowmap_b200.batch")
-    bat = B.BatchedVortex(device=dev)
+    sizes, steps = B.DEFAULT_SIZES, 100
+    mine = B.rank_share(sizes, steps, rank, world)
+    bat = B.BatchedVortex(sizes=sizes, steps=steps, device=dev, indices=mine)
+
+    def barrier():
+        if world > 1:
+            dist.barrier()
+
+    def max_over_ranks(x):
+        t = torch.tensor([x], dtype=torch.float64, device=dev)
+        if world > 1:
+            dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        return float(t.item())
 
     def timed(concurrent):
         for _ in range(a.warmup):
             bat.gradients(concurrent)
         torch.cuda.synchronize(dev)
-        t0 = time.perf_counter()
+        barrier()
         e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
         e0.record()
         for _ in range(a.steps):
             res = bat.gradients(concurrent)
         e1.record()
         torch.cuda.synchronize(dev)
-        return e0.elapsed_time(e1) / a.steps, (time.perf_counter() - t0) * 1e3 / a.steps, res
+        barrier()
+        return max_over_ranks(e0.elapsed_time(e1) / a.steps), res
 
-    ms_seq, wall_seq, seq = timed(False)
-    ms_conc, wall_conc, conc = timed(True)
-    n = len(bat.instances)
-    errs = [float(np.linalg.norm(dc - ds) / np.linalg.norm(ds)) for (_, dc), (_, ds) in zip(conc, seq)]
-    line = {"metric": "batched 2D vortex gradients/s, 16 instances (4 x 128^2, 192^2, 256^2, 384^2), 100 steps",
-            "value": n * 1e3 / ms_conc, "unit": "grads/s", "n_gpus": 1, "steps": a.steps, "warmup": a.warmup,
-            "ms_per_step": ms_conc, "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
-            "dtype": "f32", "data": "synthetic",
-            "config": {"workload": "16 concurrent vortex instances, one stream + host thread each",
-                       "sizes": [inst.res for inst in bat.instances]},
-            "sequential": {"grads_per_s": n * 1e3 / ms_seq, "ms_per_batch": ms_seq},
-            "concurrent_over_sequential": ms_seq / ms_conc,
-            "per_instance_dtheta_rel_err_vs_unbatched": errs}
-    print(json.dumps(line), flush=True)
-    return 0
-
-
-def run_shape3d_forces(a):
-    """3D shape transition with Gaussian control forces, the reference's case-11
-    hyperparameters (3D/hyperparameters.py:268-293): 128^3, 120 steps, reinit 12,
-    RK4, dt 0.0085, backward_u, 3000 Gaussians per step (seeded synthetic
-    parameters, force_oracle-style draws made here with numpy).  One bench step =
-    one gradient (forward with forces + adjoint with the per-step parameter sums).
-    value: parameters resident on the device; e2e: numpy parameters staged per
-    step as the reference's from_numpy, plus u0 / rho in and dL/du0 out."""
-    import numpy as np
-    import torch
-
-    local = int(os.environ.get("LOCAL_RANK", "0"))
-    torch.cuda.set_device(local)
-    dev = torch.device("cuda", local)
-    S = importlib.import_module("differentiable-flowmap_b200.simulator")
-    C = importlib.import_module("differentiable-flowmap_b200.configs")
-    K = importlib.import_module("differentiable-flowmap_b200.kernels")
-    from dataclasses import replace
-
-    res, steps, reinit, ng = a.res, 120, 12, a.gaussians
-    dx = 1.0 / res
-
-    def config(dtype, forces=True):
-        cfg = C.shape3d_config(res=res, steps=steps, reinit_every=reinit, rk=4, dtype=dtype,
-                               rel_tol=1e-6 if dtype == torch.float32 else 1e-20)
-        return replace(cfg, add_control_force=forces, control_num=ng)
-
-    host = _case11_gaussians(res, ng, steps)
-    devp = [{k: (torch.tensor(v, device=dev) if k != "n" else v) for k, v in p.items()} for p in host]
-    u0, rho0, rho_t = C.shape3d_inputs(res)
-    f32 = torch.float32
-    d_u0 = [torch.tensor(x, dtype=f32, device=dev) for x in u0]
-    d_r0, d_rt = torch.tensor(rho0, dtype=f32, device=dev), torch.tensor(rho_t, dtype=f32, device=dev)
-    h_u0 = [torch.tensor(x, dtype=f32).pin_memory() for x in u0]
-    h_r0, h_rt = torch.tensor(rho0, dtype=f32).pin_memory(), torch.tensor(rho_t, dtype=f32).pin_memory()
-    h_grad = [torch.empty(x.shape, dtype=f32).pin_memory() for x in u0]
-
-    sim = S.LFM_Diff_Simulator(config=config(f32), device=dev)
-    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
-
-    def timed(fn):
-        for _ in range(a.warmup):
-            fn()
-        torch.cuda.synchronize(dev)
-        e0.record()
-        for _ in range(a.steps):
-            out = fn()
-        e1.record()
-        torch.cuda.synchronize(dev)
-        return e0.elapsed_time(e1) / a.steps, out
-
-    fm = importlib.import_module("differentiable-flowmap_b200")
-    fm._lib.launch_count(reset=True)
-    ms, (loss, grad) = timed(lambda: sim.gradient(d_u0, d_r0, d_rt, control_forces=devp))
-    launches = fm._lib.launch_count(reset=True) // max(a.steps + a.warmup, 1) * a.steps
-
-    def e2e_step():
-        l, g = sim.gradient(h_u0, h_r0, h_rt, control_forces=host)
-        for hg, x in zip(h_grad, g):
-            hg.copy_(x, non_blocking=True)
-        return float(l), g
-
-    ms_e2e, _ = timed(e2e_step)
-    nof = S.LFM_Diff_Simulator(config=config(f32, forces=False), device=dev)
-    ms_nof, _ = timed(lambda: nof.gradient(d_u0, d_r0, d_rt))
-    del nof
-
-    # the two force kernels on step 0's parameters and the live adjoint velocity
-    g = sim.grid
-    p0 = devp[0]
-    reps = 20
-    e0.record()
-    for _ in range(reps):
-        K.gaussian_force(g, dx, p0["c"], p0["r"], p0["s"], sim.control_force)
-    e1.record()
-    torch.cuda.synchronize(dev)
-    us_force = e0.elapsed_time(e1) * 1e3 / reps
-    e0.record()
-    for _ in range(reps):
-        K.gaussian_force_grad(g, dx, p0["c"], p0["r"], p0["s"], sim.adj_u)
-    e1.record()
-    torch.cuda.synchronize(dev)
-    us_grad = e0.elapsed_time(e1) * 1e3 / reps
-
-    err = None
-    if not a.no_error:
-        s64 = S.LFM_Diff_Simulator(config=config(torch.float64), device=dev)
-        dp64 = [{k: (v.double() if k != "n" else v) for k, v in p.items()} for p in devp]
-        l64, g64 = s64.gradient([x.double() for x in d_u0], d_r0.double(), d_rt.double(), control_forces=dp64)
-        num = sum(float(((x.double() - y) ** 2).sum()) for x, y in zip(grad, g64))
-        den = sum(float((y ** 2).sum()) for y in g64)
-        pnum = pden = 0.0
-        for n in range(steps):
-            for k in (0, 1):
-                x, y = sim.control_force_grads[n][k], s64.control_force_grads[n][k]
-                pnum += float(((x - y) ** 2).sum())
-                pden += float((y ** 2).sum())
-        err = {"grad_u0_rel_l2": (num / den) ** 0.5, "loss_rel": abs(float(loss) - l64) / abs(l64),
-               "param_grads_rel_l2": (pnum / pden) ** 0.5 if pden > 0 else None}
-        del s64
-
-    stored = getattr(sim, "store_force", None) is not None
-    nforce = steps if stored else 2 * steps
-    h2d = sum(x.numel() * 4 for x in h_u0) + h_r0.numel() * 4 + h_rt.numel() * 4 + steps * ng * 7 * 4 * 2
-    d2h = sum(x.numel() * 4 for x in h_grad) + 8
-    line = {"metric": "3D fwd+adjoint grads/s with Gaussian control forces, 128^3, 120 steps, 3000 Gaussians/step",
-            "value": 1e3 / ms, "unit": "grads/s", "n_gpus": 1, "steps": a.steps, "warmup": a.warmup,
-            "ms_per_step": ms, "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32",
-            "data": "synthetic",
-            "config": {"workload": f"3D shape transition with control forces {res}^3, {steps} steps, reinit {reinit}, "
-                                   f"RK4, {ng} Gaussians per step (case-11 hyperparameters)",
-                       "form": "plain (backward_u)", "parameters": "seeded synthetic, strengths |s| in [0.01, 0.04]",
-                       "l2": "working set and trajectory stores exceed the 126 MB L2; no flush needed"},
-            "e2e": {"value": 1e3 / ms_e2e, "unit": "grads/s", "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": d2h},
-            "gpu_launches": launches,
-            "without_forces": {"grads_per_s": 1e3 / ms_nof, "ms_per_grad": ms_nof},
-            "force_kernels": {"k_gauss_force_us": us_force, "k_gauss_grad_us": us_grad,
-                              "launches_per_grad": {"k_gauss_force": nforce, "k_gauss_grad": steps},
-                              "ms_per_grad": (nforce * us_force + steps * us_grad) / 1e3,
-                              "adjoint_force": "read from the forward's store" if stored else "re-evaluated"},
-            "error_vs_fp64": err}
-    print(json.dumps(line), flush=True)
+    ms_seq, seq = timed(False)
+    ms_conc, conc = timed(True)
+    errs = {i: float(np.linalg.norm(dc - ds) / np.linalg.norm(ds)) for i, (_, dc), (_, ds) in zip(mine, conc, seq)}
+    errs = B.gather_results(errs)
+    n = len(sizes)
+    if rank == 0:
+        line = {"metric": "batched 2D vortex gradients/s, 16 instances (4 x 128^2, 192^2, 256^2, 384^2), 100 steps",
+                "value": n * 1e3 / ms_conc, "unit": "grads/s", "n_gpus": world, "steps": a.steps,
+                "warmup": a.warmup, "ms_per_step": ms_conc, "higher_is_better": True,
+                "scaling": "strong" if world > 1 else "weak", "vs_baseline": None, "dtype": "f32",
+                "data": "synthetic",
+                "config": {"workload": "16 concurrent vortex instances, one stream + host thread each",
+                           "sizes": list(sizes),
+                           "parallelism": (f"instances split over {world} ranks by cost, no collective in the "
+                                           "timed loop; time = max over ranks") if world > 1 else "single GPU",
+                           "rank_shares": [B.rank_share(sizes, steps, r, world) for r in range(world)]},
+                "sequential": {"grads_per_s": n * 1e3 / ms_seq, "ms_per_batch": ms_seq},
+                "concurrent_over_sequential": ms_seq / ms_conc,
+                "per_instance_dtheta_rel_err_vs_unbatched": [errs[i] for i in range(n)]}
+        print(json.dumps(line), flush=True)
+    if world > 1:
+        dist.barrier()
+        dist.destroy_process_group()
     return 0
 
 

@@ -36,16 +36,68 @@ class VortexInstance:
     dtheta: Optional[np.ndarray] = None
 
 
-class BatchedVortex:
-    """16-instance batch of BASELINE config 4: 4 x 128^2, 4 x 192^2, 4 x 256^2, 4 x 384^2."""
+DEFAULT_SIZES = (128,) * 4 + (192,) * 4 + (256,) * 4 + (384,) * 4
 
-    def __init__(self, sizes: Sequence[int] = (128,) * 4 + (192,) * 4 + (256,) * 4 + (384,) * 4, steps: int = 100,
+
+def instance_cost(res: int, steps: int) -> int:
+    """Work of one 2D instance's gradient: cells x steps (every kernel is per cell)."""
+    return res * res * steps
+
+
+def partition(costs: Sequence[float], world: int) -> List[List[int]]:
+    """Instances across ``world`` ranks by greedy bin-packing: the costliest
+    first (ties by index), each to the least-loaded rank (ties to the lowest).
+    Deterministic; every instance lands on exactly one rank; each rank's list
+    is in ascending instance order."""
+    if world < 1:
+        raise ValueError("world must be >= 1")
+    load = [0.0] * world
+    out: List[List[int]] = [[] for _ in range(world)]
+    for i in sorted(range(len(costs)), key=lambda k: (-costs[k], k)):
+        r = min(range(world), key=lambda k: (load[k], k))
+        out[r].append(i)
+        load[r] += costs[i]
+    return [sorted(x) for x in out]
+
+
+def rank_share(sizes: Sequence[int], steps: int, rank: int, world: int) -> List[int]:
+    """The global instance indices rank ``rank`` of ``world`` advances."""
+    return partition([instance_cost(n, steps) for n in sizes], world)[rank]
+
+
+def gather_results(local: dict, group=None) -> dict:
+    """Merge every rank's {instance index: result} (torch.distributed
+    all_gather_object; called after the timed region)."""
+    import torch.distributed as dist
+
+    if not (dist.is_available() and dist.is_initialized()):
+        return dict(local)
+    parts = [None] * dist.get_world_size(group)
+    dist.all_gather_object(parts, local, group=group)
+    out = {}
+    for p in parts:
+        overlap = set(out) & set(p)
+        if overlap:
+            raise RuntimeError(f"instances {sorted(overlap)} reported by two ranks")
+        out.update(p)
+    return out
+
+
+class BatchedVortex:
+    """16-instance batch of BASELINE config 4: 4 x 128^2, 4 x 192^2, 4 x 256^2, 4 x 384^2.
+    ``indices`` selects the global instances this process advances (a rank's
+    share); seeds follow the global index, so results do not depend on the
+    partition."""
+
+    def __init__(self, sizes: Sequence[int] = DEFAULT_SIZES, steps: int = 100,
                  reinit_every: int = 10, dtype=torch.float32, rel_tol: float = 1e-6, control_seed0: int = 100,
-                 target_seed0: int = 200, device=None):
+                 target_seed0: int = 200, device=None, indices: Optional[Sequence[int]] = None):
         _lib.lib()  # load the library once, before any worker thread
         self.device = torch.device(device) if device is not None else torch.device("cuda", torch.cuda.current_device())
         self.instances: List[VortexInstance] = []
-        for i, n in enumerate(sizes):
+        self.indices = list(range(len(sizes))) if indices is None else list(indices)
+        for i in self.indices:
+            n = sizes[i]
             cfg = vortex2d_config(res=n, steps=steps, reinit_every=reinit_every, dtype=dtype, rel_tol=rel_tol)
             stream = torch.cuda.Stream(device=self.device)
             with torch.cuda.stream(stream):
