@@ -393,6 +393,15 @@ def run_vortex2d_batch(a):
 
     ms_seq, seq = timed(False)
     ms_conc, conc = timed(True)
+    # the same batch with every block size at the default 256, for comparison
+    T = importlib.import_module("differentiable-flowmap_b200.tune")
+    tuned = {n: {k: v["threads"] for k, v in t.items()} for n, t in bat.tuning.items()}
+    for n in bat.tuning:
+        T.reset((n, n))
+    ms_default, _ = timed(True)
+    for n, t in tuned.items():
+        for k, th in t.items():
+            T.set_threads(k, (n, n), th)
     errs = {i: float(np.linalg.norm(dc - ds) / np.linalg.norm(ds)) for i, (_, dc), (_, ds) in zip(mine, conc, seq)}
     errs = B.gather_results(errs)
     n = len(sizes)
@@ -408,6 +417,8 @@ def run_vortex2d_batch(a):
                                            "timed loop; time = max over ranks") if world > 1 else "single GPU",
                            "rank_shares": [B.rank_share(sizes, steps, r, world) for r in range(world)]},
                 "sequential": {"grads_per_s": n * 1e3 / ms_seq, "ms_per_batch": ms_seq},
+                "autotuned_block_sizes": {str(k): v for k, v in tuned.items()},
+                "untuned_256_threads": {"grads_per_s": n * 1e3 / ms_default, "ms_per_batch": ms_default},
                 "concurrent_over_sequential": ms_seq / ms_conc,
                 "per_instance_dtheta_rel_err_vs_unbatched": [errs[i] for i in range(n)]}
         print(json.dumps(line), flush=True)

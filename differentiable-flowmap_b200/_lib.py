@@ -100,6 +100,8 @@ SIGNATURES = {
     "fm_mg_vcycle": [P, P, P, P],
     "fm_mgpcg_solve_dc": [P, I, P, P, P, D, I, P, C.POINTER(I), C.POINTER(I), C.POINTER(D)],
     "fm_clamp_extrema": [GP, I, I, P, P, P, P],
+    "fm_tune_set": [I, GP, I],
+    "fm_tune_get": [I, GP],
     "fm_solid_create": [GP, I, C.POINTER(MGParams), P, C.POINTER(P)],
     "fm_solid_destroy": [P],
     "fm_solid_set_mask": [P, P, P],

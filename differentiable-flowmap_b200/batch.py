@@ -84,18 +84,28 @@ def gather_results(local: dict, group=None) -> dict:
 
 
 class BatchedVortex:
-    """16-instance batch of BASELINE config 4: 4 x 128^2, 4 x 192^2, 4 x 256^2, 4 x 384^2.
-    ``indices`` selects the global instances this process advances (a rank's
-    share); seeds follow the global index, so results do not depend on the
-    partition."""
+    """16-instance batch: 4 x 128^2, 4 x 192^2, 4 x 256^2, 4 x 384^2 vortex
+    optimisations.  ``indices`` selects the global instances this process
+    advances (a rank's share); seeds follow the global index, so results do not
+    depend on the partition.  ``autotune`` picks the gather kernels' block
+    sizes per instance shape first (tune.py)."""
 
     def __init__(self, sizes: Sequence[int] = DEFAULT_SIZES, steps: int = 100,
                  reinit_every: int = 10, dtype=torch.float32, rel_tol: float = 1e-6, control_seed0: int = 100,
-                 target_seed0: int = 200, device=None, indices: Optional[Sequence[int]] = None):
+                 target_seed0: int = 200, device=None, indices: Optional[Sequence[int]] = None,
+                 autotune: bool = True):
         _lib.lib()  # load the library once, before any worker thread
         self.device = torch.device(device) if device is not None else torch.device("cuda", torch.cuda.current_device())
         self.instances: List[VortexInstance] = []
         self.indices = list(range(len(sizes))) if indices is None else list(indices)
+        # block sizes of the gather kernels per instance shape (tune.py); results do not change
+        self.tuning = {}
+        if autotune:
+            from . import tune
+
+            with torch.cuda.device(self.device):
+                for n in sorted({sizes[i] for i in self.indices}):
+                    self.tuning[n] = tune.autotune((n, n), dtype, rk=2, device=self.device)
         for i in self.indices:
             n = sizes[i]
             cfg = vortex2d_config(res=n, steps=steps, reinit_every=reinit_every, dtype=dtype, rel_tol=rel_tol)

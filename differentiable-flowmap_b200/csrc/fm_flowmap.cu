@@ -12,6 +12,9 @@
 #include "fm_internal.h"
 #include "fm_q2.cuh"
 
+#include <mutex>
+#include <unordered_map>
+
 namespace fm {
 
 constexpr int kThreads = 256;
@@ -307,8 +310,31 @@ static inline long max_face(const fm_grid& g) {
   for (int c = 0; c < g.dim; ++c) m = face_shape(g, c).size() > m ? face_shape(g, c).size() : m;
   return m;
 }
-static inline dim3 grid_for(long n, int ycount) {
-  return dim3((unsigned)((n + kThreads - 1) / kThreads), (unsigned)ycount, 1);
+static inline dim3 grid_for(long n, int ycount, int threads = kThreads) {
+  return dim3((unsigned)((n + threads - 1) / threads), (unsigned)ycount, 1);
+}
+
+// Block sizes picked by the autotuner (fm_tune_set), per kernel class and grid
+// shape; 256 when none was set.  Every kernel here computes each node
+// independently, so the block size changes only the speed, never a result.
+struct TuneKey {
+  int kind, dim, n0, n1, n2;
+  bool operator==(const TuneKey& o) const {
+    return kind == o.kind && dim == o.dim && n0 == o.n0 && n1 == o.n1 && n2 == o.n2;
+  }
+};
+struct TuneHash {
+  size_t operator()(const TuneKey& k) const {
+    return ((((size_t)k.kind * 31 + k.dim) * 1000003 + k.n0) * 1000003 + k.n1) * 1000003 + k.n2;
+  }
+};
+static std::mutex g_tune_mu;
+static std::unordered_map<TuneKey, int, TuneHash> g_tune;
+
+static inline int tuned_threads(int kind, const fm_grid& g) {
+  std::lock_guard<std::mutex> lk(g_tune_mu);
+  auto it = g_tune.find(TuneKey{kind, g.dim, g.n[0], g.n[1], g.n[2]});
+  return it == g_tune.end() ? kThreads : it->second;
 }
 
 template <typename T>
@@ -336,21 +362,22 @@ static inline bool mac_ok(const fm_grid& g, const void* x, const void* y, const 
 template <typename T>
 static int advect_u_grid_t(const fm_grid& g, int rk, double dx, double dt, Mac<T> u0, Mac<T> u1, MacW<T> u2,
                            Mac<T> u1b, MacW<T> u2b, cudaStream_t st) {
-  dim3 grid = grid_for(max_face(g), g.dim);
-  FM_DISPATCH_D(g, if (rk == 2) k_advect_u_grid<T, D, 2><<<grid, kThreads, 0, st>>>(g, (T)dx, (T)dt, u0, u1, u2,
-                                                                                     u1b, u2b);
-                else k_advect_u_grid<T, D, 4><<<grid, kThreads, 0, st>>>(g, (T)dx, (T)dt, u0, u1, u2, u1b, u2b));
+  const int th = tuned_threads(FM_TUNE_ADVECT_U, g);
+  dim3 grid = grid_for(max_face(g), g.dim, th);
+  FM_DISPATCH_D(g, if (rk == 2) k_advect_u_grid<T, D, 2><<<grid, th, 0, st>>>(g, (T)dx, (T)dt, u0, u1, u2, u1b,
+                                                                               u2b);
+                else k_advect_u_grid<T, D, 4><<<grid, th, 0, st>>>(g, (T)dx, (T)dt, u0, u1, u2, u1b, u2b));
   return check_launch();
 }
 
 template <typename T>
 static int advect_scalar_grid_t(const fm_grid& g, int rk, double dx, double dt, Mac<T> u0, const T* s1, T* s2,
                                 const T* s1b, T* s2b, cudaStream_t st) {
-  dim3 grid = grid_for(cell_shape(g).size(), 1);
-  FM_DISPATCH_D(g, if (rk == 2) k_advect_scalar_grid<T, D, 2><<<grid, kThreads, 0, st>>>(g, (T)dx, (T)dt, u0, s1,
-                                                                                         s2, s1b, s2b);
-                else k_advect_scalar_grid<T, D, 4><<<grid, kThreads, 0, st>>>(g, (T)dx, (T)dt, u0, s1, s2, s1b,
-                                                                              s2b));
+  const int th = tuned_threads(FM_TUNE_ADVECT_SCALAR, g);
+  dim3 grid = grid_for(cell_shape(g).size(), 1, th);
+  FM_DISPATCH_D(g, if (rk == 2) k_advect_scalar_grid<T, D, 2><<<grid, th, 0, st>>>(g, (T)dx, (T)dt, u0, s1, s2,
+                                                                                   s1b, s2b);
+                else k_advect_scalar_grid<T, D, 4><<<grid, th, 0, st>>>(g, (T)dx, (T)dt, u0, s1, s2, s1b, s2b));
   return check_launch();
 }
 
@@ -363,9 +390,10 @@ static int march_t(const fm_grid& g, int rk, double dx, double dt, const MarchJo
     long m = jobs.j[i].face >= 0 ? face_shape(g, jobs.j[i].face).size() : cell_shape(g).size();
     n = m > n ? m : n;
   }
-  dim3 grid = grid_for(n, njobs);
-  FM_DISPATCH_D(g, if (rk == 2) k_march<T, D, 2><<<grid, kThreads, 0, st>>>(g, (T)dx, (T)dt, jobs, u);
-                else k_march<T, D, 4><<<grid, kThreads, 0, st>>>(g, (T)dx, (T)dt, jobs, u));
+  const int th = tuned_threads(FM_TUNE_MARCH, g);
+  dim3 grid = grid_for(n, njobs, th);
+  FM_DISPATCH_D(g, if (rk == 2) k_march<T, D, 2><<<grid, th, 0, st>>>(g, (T)dx, (T)dt, jobs, u);
+                else k_march<T, D, 4><<<grid, th, 0, st>>>(g, (T)dx, (T)dt, jobs, u));
   return check_launch();
 }
 
@@ -478,15 +506,16 @@ int fm_pullback_u(const fm_grid* g, int dtype, double dx, const void* u0x, const
   if (!mac_ok(*g, u0x, u0y, u0z) || !mac_ok(*g, outx, outy, outz) || !mac_ok(*g, Tx, Ty, Tz) ||
       !mac_ok(*g, psix, psiy, psiz) || (beta != 0.0 && !mac_ok(*g, basex, basey, basez)))
     return FM_ERR_ARG;
-  dim3 grid = grid_for(max_face(*g), g->dim);
+  const int th = tuned_threads(FM_TUNE_PULLBACK_U, *g);
+  dim3 grid = grid_for(max_face(*g), g->dim, th);
   cudaStream_t s = FM_STREAM(stream);
   if (dtype == FM_F32) {
-    FM_DISPATCH_D(*g, k_pullback_u<float, D><<<grid, kThreads, 0, s>>>(
+    FM_DISPATCH_D(*g, k_pullback_u<float, D><<<grid, th, 0, s>>>(
                           *g, (float)dx, mac<float>(u0x, u0y, u0z), macw<float>(outx, outy, outz),
                           mac<float>(Tx, Ty, Tz), mac<float>(psix, psiy, psiz), (float)alpha, (float)beta,
                           mac<float>(basex, basey, basez)));
   } else {
-    FM_DISPATCH_D(*g, k_pullback_u<double, D><<<grid, kThreads, 0, s>>>(
+    FM_DISPATCH_D(*g, k_pullback_u<double, D><<<grid, th, 0, s>>>(
                           *g, dx, mac<double>(u0x, u0y, u0z), macw<double>(outx, outy, outz),
                           mac<double>(Tx, Ty, Tz), mac<double>(psix, psiy, psiz), alpha, beta,
                           mac<double>(basex, basey, basez)));
@@ -499,14 +528,15 @@ int fm_pullback_scalar(const fm_grid* g, int dtype, double dx, const void* s0, v
   int st = validate_grid(g, dtype);
   if (st) return st;
   if (!s0 || !out || !psi || (beta != 0.0 && !base)) return FM_ERR_ARG;
-  dim3 grid = grid_for(cell_shape(*g).size(), 1);
+  const int th = tuned_threads(FM_TUNE_PULLBACK_SCALAR, *g);
+  dim3 grid = grid_for(cell_shape(*g).size(), 1, th);
   cudaStream_t s = FM_STREAM(stream);
   if (dtype == FM_F32) {
-    FM_DISPATCH_D(*g, k_pullback_scalar<float, D><<<grid, kThreads, 0, s>>>(
+    FM_DISPATCH_D(*g, k_pullback_scalar<float, D><<<grid, th, 0, s>>>(
                           *g, (float)dx, (const float*)s0, (float*)out, (const float*)psi, (float)alpha,
                           (float)beta, (const float*)base));
   } else {
-    FM_DISPATCH_D(*g, k_pullback_scalar<double, D><<<grid, kThreads, 0, s>>>(
+    FM_DISPATCH_D(*g, k_pullback_scalar<double, D><<<grid, th, 0, s>>>(
                           *g, dx, (const double*)s0, (double*)out, (const double*)psi, alpha, beta,
                           (const double*)base));
   }
@@ -523,7 +553,8 @@ int fm_accumulate_init(const fm_grid* g, int dtype, double dx, double dt, int ab
       !mac_ok(*g, phix, phiy, phiz) || ind < 0)
     return FM_ERR_ARG;
   if (ab3 && (!mac_ok(*g, Hpx, Hpy, Hpz) || !mac_ok(*g, Hppx, Hppy, Hppz))) return FM_ERR_ARG;
-  dim3 grid = grid_for(max_face(*g), g->dim);
+  const int th = tuned_threads(FM_TUNE_ACCUMULATE, *g);
+  dim3 grid = grid_for(max_face(*g), g->dim, th);
   cudaStream_t s = FM_STREAM(stream);
   if (dtype == FM_F32) {
     auto f = mac<float>(fx, fy, fz);
@@ -532,9 +563,9 @@ int fm_accumulate_init(const fm_grid* g, int dtype, double dx, double dt, int ab
     auto ph = mac<float>(phix, phiy, phiz);
     auto hp = macw<float>(Hpx, Hpy, Hpz);
     auto hpp = macw<float>(Hppx, Hppy, Hppz);
-    FM_DISPATCH_D(*g, if (ab3) k_accumulate<float, D, true><<<grid, kThreads, 0, s>>>(*g, (float)dx, (float)dt, ind,
+    FM_DISPATCH_D(*g, if (ab3) k_accumulate<float, D, true><<<grid, th, 0, s>>>(*g, (float)dx, (float)dt, ind,
                                                                                        f, in, F, ph, hp, hpp);
-                  else k_accumulate<float, D, false><<<grid, kThreads, 0, s>>>(*g, (float)dx, (float)dt, ind, f,
+                  else k_accumulate<float, D, false><<<grid, th, 0, s>>>(*g, (float)dx, (float)dt, ind, f,
                                                                                in, F, ph, hp, hpp));
   } else {
     auto f = mac<double>(fx, fy, fz);
@@ -543,9 +574,9 @@ int fm_accumulate_init(const fm_grid* g, int dtype, double dx, double dt, int ab
     auto ph = mac<double>(phix, phiy, phiz);
     auto hp = macw<double>(Hpx, Hpy, Hpz);
     auto hpp = macw<double>(Hppx, Hppy, Hppz);
-    FM_DISPATCH_D(*g, if (ab3) k_accumulate<double, D, true><<<grid, kThreads, 0, s>>>(*g, dx, dt, ind, f, in, F,
+    FM_DISPATCH_D(*g, if (ab3) k_accumulate<double, D, true><<<grid, th, 0, s>>>(*g, dx, dt, ind, f, in, F,
                                                                                         ph, hp, hpp);
-                  else k_accumulate<double, D, false><<<grid, kThreads, 0, s>>>(*g, dx, dt, ind, f, in, F, ph, hp,
+                  else k_accumulate<double, D, false><<<grid, th, 0, s>>>(*g, dx, dt, ind, f, in, F, ph, hp,
                                                                                 hpp));
   }
   return check_launch();
@@ -592,3 +623,22 @@ int fm_add_fields(int dtype, long n, const void* f1, const void* f2, void* dest,
 }
 
 }  // extern "C"
+
+// Autotuner table (see tuned_threads): threads per block for one kernel class
+// on one grid shape; 32..256 in multiples of 32, or 0 to restore the default.
+int fm_tune_set(int kind, const fm_grid* g, int threads) {
+  using namespace fm;
+  if (!g || kind < 0 || kind >= FM_TUNE_KINDS) return FM_ERR_ARG;
+  if (threads != 0 && (threads < 32 || threads > kThreads || threads % 32 != 0)) return FM_ERR_ARG;
+  std::lock_guard<std::mutex> lk(g_tune_mu);
+  const TuneKey k{kind, g->dim, g->n[0], g->n[1], g->n[2]};
+  if (threads == 0) g_tune.erase(k);
+  else g_tune[k] = threads;
+  return FM_OK;
+}
+
+int fm_tune_get(int kind, const fm_grid* g) {
+  using namespace fm;
+  if (!g || kind < 0 || kind >= FM_TUNE_KINDS) return -FM_ERR_ARG;
+  return tuned_threads(kind, *g);
+}

@@ -285,6 +285,27 @@ int fm_viscous_force_2d(const fm_grid *g, int dtype, double nu, double dx, const
                         void *vis_y, const void *adj_x, const void *adj_y, double *part, double *dot, void *stream);
 
 /* ------------------------------------------------------------------------
+ * Launch tuning (no reference counterpart: the reference's kernels are
+ * scheduled by Taichi).  The gather kernels compute every node independently,
+ * so their block size changes only the speed; the autotuner (tune.py) times
+ * the candidates on one grid shape and stores the fastest here.
+ * ------------------------------------------------------------------------ */
+enum {
+    FM_TUNE_ADVECT_U = 0,        /* fm_advect_u_grid(_pair) */
+    FM_TUNE_ADVECT_SCALAR = 1,   /* fm_advect_scalar_grid(_pair) */
+    FM_TUNE_MARCH = 2,           /* fm_march_map, fm_rk_grid */
+    FM_TUNE_PULLBACK_U = 3,      /* fm_pullback_u */
+    FM_TUNE_PULLBACK_SCALAR = 4, /* fm_pullback_scalar */
+    FM_TUNE_ACCUMULATE = 5,      /* fm_accumulate_init */
+    FM_TUNE_KINDS = 6
+};
+/* Threads per block for kernel class `kind` on grid g: 32..256 in multiples of
+ * 32, or 0 for the default (256).  Thread-safe; applies to later launches. */
+int fm_tune_set(int kind, const fm_grid *g, int threads);
+/* The block size launches of `kind` on g use (256 unless set); -FM_ERR_ARG on a bad kind. */
+int fm_tune_get(int kind, const fm_grid *g);
+
+/* ------------------------------------------------------------------------
  * Obstacles: MGPCG with a boundary mask and the mask kernels.
  * mask: device float32 array on the cell grid; the solver treats cells with
  * mask > 0 as solid (mgpcg_solid.py), the mask kernels cells with mask >= 1

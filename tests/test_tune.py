@@ -1,0 +1,48 @@
+"""Launch autotuner: the block-size table (fm_tune_set / fm_tune_get) and the
+guarantee that tuning changes no result (the gather kernels compute every node
+independently): a vortex gradient is bit for bit the same with every kernel
+class forced to 64-thread blocks and at the default 256."""
+import ctypes as C
+import importlib
+
+import numpy as np
+import pytest
+import torch
+
+
+def test_tune_table_arguments(fm):
+    lib = fm._lib.lib()
+    g = fm._lib.Grid(2, (C.c_int * 3)(96, 64, 1))
+    assert lib.fm_tune_get(0, C.byref(g)) == 256
+    assert lib.fm_tune_set(0, C.byref(g), 48) == 2      # not a multiple of 32
+    assert lib.fm_tune_set(0, C.byref(g), 512) == 2     # above the kernels' launch bound
+    assert lib.fm_tune_set(9, C.byref(g), 64) == 2      # no such kernel class
+    assert lib.fm_tune_set(2, C.byref(g), 128) == 0
+    assert lib.fm_tune_get(2, C.byref(g)) == 128
+    other = fm._lib.Grid(2, (C.c_int * 3)(64, 96, 1))
+    assert lib.fm_tune_get(2, C.byref(other)) == 256    # per shape
+    assert lib.fm_tune_set(2, C.byref(g), 0) == 0
+    assert lib.fm_tune_get(2, C.byref(g)) == 256
+
+
+@pytest.mark.gpu
+def test_block_sizes_change_no_result(fm, cuda):
+    S = importlib.import_module("differentiable-flowmap_b200.simulator")
+    Cf = importlib.import_module("differentiable-flowmap_b200.configs")
+    vx = importlib.import_module("differentiable-flowmap_b200.vortex")
+    T = importlib.import_module("differentiable-flowmap_b200.tune")
+    res = 64
+    cfg = Cf.vortex2d_config(res=res, steps=12, reinit_every=5)
+    p = vx.VortexProblem(S.LFM_Diff_Simulator(config=cfg))
+    th, omt = Cf.vortex2d_theta(3), p.final_vorticity(Cf.vortex2d_theta(4))
+    T.reset((res, res))
+    l0, d0 = p.gradient(th, omt)
+    for k in T.KINDS:
+        T.set_threads(k, (res, res), 64)
+    l1, d1 = p.gradient(th, omt)
+    report = T.autotune((res, res), reps=3)
+    l2, d2 = p.gradient(th, omt)
+    T.reset((res, res))
+    assert l0 == l1 == l2
+    assert np.array_equal(d0, d1) and np.array_equal(d0, d2)
+    assert set(report) == set(T.KINDS) and all(r["threads"] in T.CANDIDATES for r in report.values())
