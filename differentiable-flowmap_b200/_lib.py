@@ -16,6 +16,7 @@ HEADER_PATH = os.path.join(_HERE, "..", "include", "flowmap_sm100.h")
 
 FM_F32, FM_F64 = 0, 1
 FM_OK = 0
+FM_ERR_CUDA = 6
 STATUS = {
     0: "FM_OK",
     1: "FM_ERR_SHAPE",
@@ -120,6 +121,7 @@ SIGNATURES = {
 }
 RESTYPES = {"fm_launch_count": C.c_longlong}
 SIGNATURES["fm_launch_count"] = [I]
+SIGNATURES["fm_last_cuda_error"] = [C.c_char_p, I]
 
 _lib = None
 
@@ -148,10 +150,21 @@ def launch_count(reset: bool = False) -> int:
     return int(lib().fm_launch_count(1 if reset else 0))
 
 
+def last_cuda_error():
+    """(code, name) of the CUDA error behind the library's last FM_ERR_CUDA."""
+    buf = C.create_string_buffer(64)
+    code = lib().fm_last_cuda_error(buf, 64)
+    return code, buf.value.decode()
+
+
 def check(status: int, where: str):
     if status != FM_OK:
         if status == 3:
             raise NotConvergedError(status, where)
+        if status == FM_ERR_CUDA:
+            code, name = last_cuda_error()
+            if code:
+                where = f"{where} ({name} = {code})"
         raise FlowmapError(status, where)
 
 

@@ -116,13 +116,38 @@ class BatchedVortex:
             self.instances.append(VortexInstance(n, vortex2d_theta(control_seed0 + i), omt, prob, stream))
         torch.cuda.synchronize(self.device)
 
+    def capture(self):
+        """Record every instance's gradient as one CUDA graph (untimed setup;
+        runs one eager gradient per instance first)."""
+        for inst in self.instances:
+            with torch.cuda.device(self.device), torch.cuda.stream(inst.stream):
+                inst.problem.capture(inst.theta, inst.omega_target)
+        torch.cuda.synchronize(self.device)
+        self.captured = True
+
     def _run(self, inst: VortexInstance):
         with torch.cuda.device(self.device), torch.cuda.stream(inst.stream):
             inst.loss, inst.dtheta = inst.problem.gradient(inst.theta, inst.omega_target)
 
-    def gradients(self, concurrent: bool = True):
-        """One gradient per instance; concurrent=False runs them one after another."""
-        if not concurrent:
+    def gradients(self, concurrent: bool = True, graphs: bool = False):
+        """One gradient per instance; concurrent=False runs them one after another.
+        graphs=True replays the captured graphs (capture() first): one graph
+        launch per instance on its stream, all issued from this thread, then the
+        losses and dL/dtheta are read back instance by instance."""
+        if graphs:
+            if not getattr(self, "captured", False):
+                raise RuntimeError("gradients(graphs=True): call capture() first")
+            with torch.cuda.device(self.device):
+                for inst in self.instances:
+                    with torch.cuda.stream(inst.stream):
+                        inst.problem.launch_gradient(inst.theta)
+                        if not concurrent:
+                            inst.loss, inst.dtheta = inst.problem.finish_gradient(inst.theta)
+                if concurrent:
+                    for inst in self.instances:
+                        with torch.cuda.stream(inst.stream):
+                            inst.loss, inst.dtheta = inst.problem.finish_gradient(inst.theta)
+        elif not concurrent:
             for inst in self.instances:
                 self._run(inst)
         else:

@@ -3,6 +3,8 @@
 #include <cuda_runtime.h>
 
 #include <atomic>
+#include <mutex>
+#include <unordered_map>
 #include <utility>
 
 #include "../../include/flowmap_sm100.h"
@@ -30,15 +32,40 @@ inline int validate_grid(const fm_grid* g, int dtype) {
 extern std::atomic<long long> g_launch_count;
 inline void count_launch(long long n = 1) { g_launch_count.fetch_add(n, std::memory_order_relaxed); }
 
+// The CUDA error behind the most recent FM_ERR_CUDA (fm_last_cuda_error()).
+extern std::atomic<int> g_last_cuda_error;
+inline int cuda_fail(cudaError_t e) {
+  g_last_cuda_error.store((int)e, std::memory_order_relaxed);
+  return FM_ERR_CUDA;
+}
+
 inline int check_cuda() {
   cudaError_t e = cudaGetLastError();
-  return e == cudaSuccess ? FM_OK : FM_ERR_CUDA;
+  return e == cudaSuccess ? FM_OK : cuda_fail(e);
 }
 
 // After an entry point's single kernel launch.
 inline int check_launch() {
   count_launch();
   return check_cuda();
+}
+
+// Raise-only setting of a kernel's dynamic shared-memory limit.  The attribute
+// is per kernel and process-wide, while solvers of different sizes need
+// different amounts: setting it to each new solver's need would lower it under
+// what an earlier, larger solver launches (its later launches, and any launch
+// recorded into a graph after that, would fail).  Thread-safe.
+template <typename... KArgs>
+inline bool raise_smem_limit(void (*k)(KArgs...), size_t smem) {
+  static std::mutex mu;
+  static std::unordered_map<const void*, size_t> limit;
+  std::lock_guard<std::mutex> lock(mu);
+  size_t& cur = limit[(const void*)k];
+  if (smem <= cur) return true;
+  if (cudaFuncSetAttribute((const void*)k, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem) != cudaSuccess)
+    return false;
+  cur = smem;
+  return true;
 }
 
 // Launch helper that counts the launch.

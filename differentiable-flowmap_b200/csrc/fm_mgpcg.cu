@@ -31,6 +31,7 @@
 namespace fm {
 
 std::atomic<long long> g_launch_count{0};
+std::atomic<int> g_last_cuda_error{0};
 
 constexpr int kRedBlocks = 148 * 4;  // fixed reduction grid: 4 CTAs per SM
 constexpr int kRedThreads = 256;
@@ -729,8 +730,7 @@ static void plan_coarse(fm_mgpcg* S, size_t es) {
 
 template <typename T, int D>
 static bool enable_coarse_kernel(size_t smem) {
-  return cudaFuncSetAttribute(k_mg_coarse<T, D>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem) ==
-         cudaSuccess;
+  return raise_smem_limit(k_mg_coarse<T, D>, smem);
 }
 
 static inline unsigned blocks_for(long n, int threads, long cap) {
@@ -958,9 +958,64 @@ static int build_prologue_graph(fm_mgpcg* S) {
   return FM_OK;
 }
 
+// True while `s` records into a CUDA graph (a caller capturing a whole
+// gradient); the solver then adds its work to that graph instead of launching
+// its own executable graphs.
+static bool stream_capturing(cudaStream_t s) {
+  cudaStreamCaptureStatus cs = cudaStreamCaptureStatusNone;
+  if (cudaStreamIsCapturing(s, &cs) != cudaSuccess) return false;
+  return cs == cudaStreamCaptureStatusActive;
+}
+
+// A device-mode solve recorded into the graph being captured on `s`: the
+// prologue's kernels go onto `s`, and the PCG loop becomes a conditional WHILE
+// node appended to the captured graph (after the prologue), its body one PCG
+// iteration and k_loop_cond recorded from S->cap.  Every solve recorded this
+// way owns its own node and condition handle.
+template <typename T>
+static int capture_solve(fm_mgpcg* S, cudaStream_t s) {
+  const int D = S->g.dim;
+  if (D == 3) launch_prologue<T, 3>(S, s); else launch_prologue<T, 2>(S, s);
+  cudaError_t e = cudaGetLastError();
+  if (e != cudaSuccess) return cuda_fail(e);
+  cudaStreamCaptureStatus cs;
+  cudaGraph_t graph = nullptr;
+  const cudaGraphNode_t* deps = nullptr;
+  size_t ndeps = 0;
+  if ((e = cudaStreamGetCaptureInfo(s, &cs, nullptr, &graph, &deps, &ndeps)) != cudaSuccess) return cuda_fail(e);
+  if (cs != cudaStreamCaptureStatusActive) return cuda_fail(cudaErrorStreamCaptureInvalidated);
+  cudaGraphConditionalHandle h;
+  if ((e = cudaGraphConditionalHandleCreate(&h, graph, 1, cudaGraphCondAssignDefault)) != cudaSuccess)
+    return cuda_fail(e);
+  cudaGraphNodeParams cp = {cudaGraphNodeTypeConditional};
+  cp.conditional.handle = h;
+  cp.conditional.type = cudaGraphCondTypeWhile;
+  cp.conditional.size = 1;
+  cudaGraphNode_t node;
+  if ((e = cudaGraphAddNode(&node, graph, deps, ndeps, &cp)) != cudaSuccess) return cuda_fail(e);
+  if ((e = cudaStreamUpdateCaptureDependencies(s, &node, 1, cudaStreamSetCaptureDependencies)) != cudaSuccess)
+    return cuda_fail(e);
+  cudaGraph_t body = cp.conditional.phGraph_out[0];
+  if ((e = cudaStreamBeginCaptureToGraph(S->cap, body, nullptr, nullptr, 0, cudaStreamCaptureModeThreadLocal)) !=
+      cudaSuccess)
+    return cuda_fail(e);
+  const long long before = g_launch_count.load();
+  if (D == 3) launch_iteration<T, 3>(S, S->cap); else launch_iteration<T, 2>(S, S->cap);
+  launch(k_loop_cond, 1, 1, 0, S->cap, h, S->st);
+  g_launch_count.fetch_sub(g_launch_count.load() - before);  // the loop body runs a data-dependent number of times
+  cudaGraph_t captured = nullptr;
+  if ((e = cudaStreamEndCapture(S->cap, &captured)) != cudaSuccess) return cuda_fail(e);
+  return FM_OK;
+}
+
 template <typename T>
 static int run_solve(fm_mgpcg* S, cudaStream_t s, int* iters, double* rtr) {
   const int D = S->g.dim;
+  if (stream_capturing(s)) {
+    // recorded, not run: no host read of the outcome, no host-checked loop
+    if (iters || rtr || S->P.check_every != 0) return FM_ERR_ARG;
+    return capture_solve<T>(S, s);
+  }
   if (!S->prologue) {
     const int e = build_prologue_graph<T>(S);
     if (e) return e;
@@ -1078,14 +1133,15 @@ int fm_mgpcg_create(const fm_grid* g, int dtype, const fm_mg_params* params, fm_
   if (ok && smem <= 200 * 1024 && nb <= kBottomMaxCells) {
     S->bottom_smem = smem;
     if (smem > 48 * 1024) {
-      cudaError_t e;
+      bool e;
       if (dtype == FM_F32)
-        e = g->dim == 3 ? cudaFuncSetAttribute(k_bottom<float, 3>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem)
-                        : cudaFuncSetAttribute(k_bottom<float, 2>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+        e = g->dim == 3 ? raise_smem_limit(k_bottom<float, 3>, smem) : raise_smem_limit(k_bottom<float, 2>, smem);
       else
-        e = g->dim == 3 ? cudaFuncSetAttribute(k_bottom<double, 3>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem)
-                        : cudaFuncSetAttribute(k_bottom<double, 2>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
-      if (e != cudaSuccess) S->bottom_smem = 0;
+        e = g->dim == 3 ? raise_smem_limit(k_bottom<double, 3>, smem) : raise_smem_limit(k_bottom<double, 2>, smem);
+      if (!e) {
+        cudaGetLastError();
+        S->bottom_smem = 0;
+      }
     }
   }
   if (!ok) {
@@ -1288,6 +1344,17 @@ int fm_abi_version(void) { return 1; }
 long long fm_launch_count(int reset) {
   if (reset) return g_launch_count.exchange(0);
   return g_launch_count.load();
+}
+
+int fm_last_cuda_error(char* buf, int len) {
+  const int e = g_last_cuda_error.load();
+  if (buf && len > 0) {
+    const char* name = e ? cudaGetErrorName((cudaError_t)e) : "cudaSuccess";
+    int i = 0;
+    for (; name && name[i] && i < len - 1; ++i) buf[i] = name[i];
+    buf[i] = 0;
+  }
+  return e;
 }
 
 const char* fm_status_string(int status) {

@@ -642,6 +642,10 @@ void iteration(fm_solid* S, cudaStream_t s) {
 
 template <typename T, int D>
 int solve(fm_solid* S, const void* b, double k, void* x, cudaStream_t s, int* iters, double* rtr) {
+  // the masked solve polls its convergence word from the host: it cannot be
+  // recorded into a caller's CUDA graph
+  cudaStreamCaptureStatus cs = cudaStreamCaptureStatusNone;
+  if (cudaStreamIsCapturing(s, &cs) != cudaSuccess || cs != cudaStreamCaptureStatusNone) return FM_ERR_ARG;
   const long n = S->sh[0].size();
   State h{};
   h.max_iters = S->P.max_iters;

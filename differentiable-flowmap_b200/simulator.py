@@ -30,6 +30,7 @@ from typing import Dict, List, Optional, Sequence
 import numpy as np
 import torch
 
+from . import _lib
 from . import kernels as K
 from ._lib import FlowmapError
 from .kernels import GridSpec
@@ -549,6 +550,8 @@ class LFM_Diff_Simulator(LFM_Simulator):
         self.target_passive = None
         self.target_trajectory = None
         self.loss = 0.0
+        self._loss_dev = None
+        self._capturing = False
         self.final_ind = None
 
     @property
@@ -586,7 +589,8 @@ class LFM_Diff_Simulator(LFM_Simulator):
             self.H_prev_prev[c].zero_()
         diff = self.passive - self.target_passive
         self.adj_passive.copy_(2 * diff)
-        self.loss = float(torch.sum(diff.double() ** 2))
+        self._loss_dev = torch.sum(diff.double() ** 2)
+        self.loss = None if self._capturing else float(self._loss_dev)
         self._finish_seed()
 
     def _seed_vorticity(self, target_vorticity):
@@ -606,7 +610,8 @@ class LFM_Diff_Simulator(LFM_Simulator):
         K.vorticity_loss_2d(g, self.dx, self.u[0], self.u[1], self._vort_target, self.adj_u[0], self.adj_u[1],
                             self._vort_work, self._vort_part, self._vort_loss)
         self.adj_passive.zero_()
-        self.loss = float(self._vort_loss.item())
+        self._loss_dev = self._vort_loss
+        self.loss = None if self._capturing else float(self._vort_loss.item())
         self._finish_seed()
 
     def _finish_seed(self):
@@ -810,8 +815,80 @@ class LFM_Diff_Simulator(LFM_Simulator):
                                                       self.penalty_gaussion_force_strength))
             if done:
                 break
+        if self._capturing:
+            return None, self.adj_u
         # the solver's device-side counters, read once per gradient (one stream sync)
         self.solver_stats = self.solver.stats(reset=True)
         if self.solver_stats and self.solver_stats["nonfinite"]:
             raise FlowmapError(4, f"{self.solver_stats['nonfinite']} projection(s) hit a non-finite residual")
         return self.loss, [x.clone() for x in self.adj_u]
+
+    def capture_gradient(self, u0, passive0=None, target_passive=None, target_vorticity=None, stream=None):
+        """Record ``gradient(u0, ...)`` as one CUDA graph and return its GradientGraph.
+
+        The inputs must be device tensors that stay alive: the graph copies from
+        them on every replay, so refill them in place between replays.  One eager
+        gradient runs first (it creates every lazily allocated buffer outside the
+        capture and leaves the same results).  Not available with control forces, a
+        trajectory loss, an obstacle mask (the masked solver polls its convergence
+        from the host) or a host-checked solver (check_every > 0)."""
+        cfg = self.cfg
+        if cfg.add_control_force or cfg.trajectory_loss or self.boundary_mask is not None:
+            raise FlowmapError(2, "capture_gradient: control forces, trajectory loss and obstacles are not capturable")
+        if not getattr(self.solver, "device_mode", False):
+            raise FlowmapError(2, "capture_gradient needs the device-side solver (check_every = 0)")
+        for x in list(u0) + [passive0, target_passive, target_vorticity]:
+            if x is not None and not (isinstance(x, torch.Tensor) and x.is_cuda):
+                raise FlowmapError(2, "capture_gradient: inputs must be device tensors")
+        self.gradient(u0, passive0, target_passive, target_vorticity)
+        s = stream if stream is not None else torch.cuda.Stream(device=self.device)
+        torch.cuda.synchronize(self.device)
+        before = _lib.launch_count()
+        graph = torch.cuda.CUDAGraph()
+        self._capturing = True
+        try:
+            with torch.cuda.graph(graph, stream=s, capture_error_mode="thread_local"):
+                self.gradient(u0, passive0, target_passive, target_vorticity)
+        finally:
+            self._capturing = False
+        kernels = _lib.launch_count() - before
+        roles = {k: getattr(self, k) for k in _ROLES if hasattr(self, k)}
+        return GradientGraph(self, graph, roles, self._loss_dev, kernels)
+
+
+# fields whose tensors the steps exchange by reference (ping-pong buffers)
+_ROLES = ("u", "final_u", "err_u", "adj_u", "passive", "final_passive", "adj_passive", "err_passive")
+
+
+class GradientGraph:
+    """One whole forward + adjoint gradient recorded as a CUDA graph
+    (``LFM_Diff_Simulator.capture_gradient``).  ``replay()`` re-runs it on the
+    current contents of the input tensors given at capture time, on the current
+    stream, with one graph launch; the simulator's fields (adj_u, u, ...) then
+    hold that run's results, as after ``gradient()``.  The projections inside
+    are device-side PCG loops (conditional WHILE nodes), so the replay needs no
+    host decision.  Results are bit-identical to the eager gradient: the graph
+    holds the same kernels in the same order."""
+
+    def __init__(self, sim, graph, roles, loss_dev, kernels):
+        self.sim = sim
+        self.graph = graph
+        self.roles = roles
+        self.loss_dev = loss_dev
+        self.kernels = kernels  # kernel nodes recorded outside the PCG loop bodies
+
+    def replay(self):
+        self.graph.replay()
+        for k, v in self.roles.items():
+            setattr(self.sim, k, v)
+
+    def loss(self) -> float:
+        """The last replay's loss (synchronises with the current stream)."""
+        return float(self.loss_dev.item())
+
+    def stats(self) -> dict:
+        """Solver counters accumulated since the last read (synchronises)."""
+        st = self.sim.solver.stats(reset=True)
+        if st and st["nonfinite"]:
+            raise FlowmapError(4, f"{st['nonfinite']} projection(s) hit a non-finite residual")
+        return st

@@ -67,3 +67,30 @@ class VortexProblem:
         loss, _ = self.sim.gradient(self.velocity(theta), target_vorticity=omega_target)
         self.loss = loss
         return loss, self.calculate_dtheta(theta)
+
+    # ---- the same gradient replayed from one CUDA graph
+    def capture(self, theta, omega_target: torch.Tensor):
+        """Record the gradient as one CUDA graph (LFM_Diff_Simulator.capture_gradient)
+        with u0(theta) and omega_target as its inputs; graph_gradient then
+        evaluates any theta with the same number of vortices in one graph launch."""
+        self._u0 = self.velocity(theta)
+        self._omega_target = omega_target
+        self.graph = self.sim.capture_gradient(self._u0, target_vorticity=omega_target)
+        return self.graph
+
+    def launch_gradient(self, theta):
+        """The asynchronous part of graph_gradient: u0(theta) into the graph's
+        input and one graph launch, on the current stream."""
+        if getattr(self, "graph", None) is None:
+            raise RuntimeError("launch_gradient: call capture() first")
+        K.vortex_velocity_2d(self.grid, self.dx, theta, self._u0[0], self._u0[1])
+        self.graph.replay()
+
+    def finish_gradient(self, theta):
+        """(L, dL/dtheta) of the last launch_gradient (synchronises the stream)."""
+        self.loss = self.graph.loss()
+        return self.loss, self.calculate_dtheta(theta)
+
+    def graph_gradient(self, theta):
+        self.launch_gradient(theta)
+        return self.finish_gradient(theta)

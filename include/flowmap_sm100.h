@@ -52,6 +52,11 @@ const char *fm_status_string(int status);
  * zeroes it. */
 long long fm_launch_count(int reset);
 
+/* The CUDA runtime error code (cudaError_t) behind the most recent
+ * FM_ERR_CUDA returned by any entry point (0 if none), with its name written
+ * to buf (at most len bytes, NUL-terminated) when buf is not NULL. */
+int fm_last_cuda_error(char *buf, int len);
+
 /* advect_u_grid: semi-Lagrangian advection, RK2 (midpoint) or RK4 backtrace
  * of the face nodes through u0, then u2_c = (u1 sampled at the foot)_c.
  * Replaces RK2_advect_u_grid / RK4_advect_u_grid (3D/flowmap.py:202-282,
