@@ -741,7 +741,8 @@ def dominant_kernel_roofline(fm, sim, dev, stream):
     # stages x (3 components x 195 for value + gradient + (grad u).t, plus 6 stencil
     # setups x 12) + 60 for the stage sums; per centre node 4 x (3 x 78 + 6 x 10) + 30
     flops = nface * (4 * (3 * 195 + 6 * 12) + 60) + ncell * (4 * (3 * 78 + 6 * 10) + 30)
-    fp32_peak = fp32_peak_tflops(dev)
+    fp32 = fp32_peak_tflops(dev, fm)
+    fp32_peak = fp32["peak"]
     fp32_achieved = flops / (ms / 1e3) / 1e12
     return {"kernel": "k_march<float,3,4> (fm_march_map)", "bound": "hbm", "achieved": achieved, "peak": hbm,
             "unit": "GB/s", "frac": achieved / hbm, "traffic": MARCH_DRAM_BYTES_PER_LAUNCH, "ms_per_launch": ms,
@@ -750,7 +751,9 @@ def dominant_kernel_roofline(fm, sim, dev, stream):
                               "profiles/k_march_rk4_3d128.txt",
             "fp32": {"achieved": fp32_achieved, "peak": fp32_peak, "unit": "TFLOP/s", "frac": fp32_achieved / fp32_peak,
                      "flops_per_launch": flops,
-                     "peak_source": "measured here: cuBLAS FP32 GEMM 8192^3, TF32 off, best of 5"},
+                     "peak_source": ("measured here: the best of an FMA-chain probe (fm_fp32_fma_probe, scalar "
+                                     "and paired-lane FMAs) and cuBLAS FP32 GEMM 8192^3 with TF32 off"),
+                     "measured": fp32},
             "note": "gather kernel: FP32-issue bound (ncu: 501 M warp instructions per launch, issue active 60 %, "
                     "L1 hit 96 %); its HBM fraction is low by construction, the fp32 entry is its bound"}
 
@@ -760,30 +763,50 @@ def dominant_kernel_roofline(fm, sim, dev, stream):
 MARCH_DRAM_BYTES_PER_LAUNCH = 365_579_264
 
 
-def fp32_peak_tflops(dev):
-    """FP32 CUDA-core throughput measured on this GPU: cuBLAS SGEMM with TF32 disabled."""
+def fp32_peak_tflops(dev, fm):
+    """FP32 CUDA-core throughput measured on this GPU, TFLOP/s: an FMA-chain
+    probe (scalar fmaf and paired-lane FMAs, 8 CTAs of 256 threads per SM) and
+    cuBLAS SGEMM with TF32 disabled; "peak" is the best of the three."""
+    import ctypes as _C
+
     import torch
 
+    def best_of(fn, reps=5):
+        fn()
+        torch.cuda.synchronize(dev)
+        best = None
+        for _ in range(reps):
+            e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            e0.record()
+            fn()
+            e1.record()
+            torch.cuda.synchronize(dev)
+            t = e0.elapsed_time(e1) / 1e3
+            best = t if best is None else min(best, t)
+        return best
+
+    out = {}
+    blocks = torch.cuda.get_device_properties(dev).multi_processor_count * 8
+    iters = 65536
+    buf = torch.empty(blocks * 256, dtype=torch.float32, device=dev)
+    lib = fm._lib.lib()
+    stream = _C.c_void_p(torch.cuda.current_stream(dev).cuda_stream)
+    for name, paired in (("fma_scalar", 0), ("fma_paired", 1)):
+        def run(p=paired):
+            fm._lib.check(lib.fm_fp32_fma_probe(p, blocks, iters, _C.c_void_p(buf.data_ptr()), stream),
+                          "fm_fp32_fma_probe")
+        out[name] = blocks * 256.0 * iters * 32 / best_of(run) / 1e12
     prev = torch.backends.cuda.matmul.allow_tf32
     torch.backends.cuda.matmul.allow_tf32 = False
     try:
         n = 8192
         x = torch.randn(n, n, device=dev)
         y = torch.randn(n, n, device=dev)
-        torch.mm(x, y)
-        torch.cuda.synchronize(dev)
-        best = None
-        for _ in range(5):
-            e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
-            e0.record()
-            torch.mm(x, y)
-            e1.record()
-            torch.cuda.synchronize(dev)
-            t = e0.elapsed_time(e1) / 1e3
-            best = t if best is None else min(best, t)
-        return 2.0 * n ** 3 / best / 1e12
+        out["sgemm"] = 2.0 * n ** 3 / best_of(lambda: torch.mm(x, y)) / 1e12
     finally:
         torch.backends.cuda.matmul.allow_tf32 = prev
+    out["peak"] = max(out["fma_scalar"], out["fma_paired"], out["sgemm"])
+    return out
 
 
 if __name__ == "__main__":

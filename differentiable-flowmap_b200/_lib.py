@@ -122,6 +122,7 @@ SIGNATURES = {
 RESTYPES = {"fm_launch_count": C.c_longlong}
 SIGNATURES["fm_launch_count"] = [I]
 SIGNATURES["fm_last_cuda_error"] = [C.c_char_p, I]
+SIGNATURES["fm_fp32_fma_probe"] = [I, I, I, P, P]
 
 _lib = None
 

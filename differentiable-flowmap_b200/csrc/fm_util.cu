@@ -206,3 +206,54 @@ extern "C" int fm_viscous_force_2d(const fm_grid* g, int dtype, double nu, doubl
   if (sum) launch(k_viscous_dot_fin, 1, 32, 0, s, kVisBlocks, (const double*)part, dot);
   return check_cuda();
 }
+
+// ---------------------------------------------------------------------------
+// FP32 FMA throughput probe (the denominator of the gather kernels' roofline).
+// Every thread runs 16 independent FMA chains of `iters` steps -- 16 scalar
+// fmaf chains, or 8 chains of paired __ffma2_rn (two FMAs per instruction) --
+// and writes their sum, so no chain is optimised away.  x <- x * a + b with
+// |a| < 1 keeps every value finite.  FLOPs = blocks * 256 * iters * 32.
+// ---------------------------------------------------------------------------
+namespace fm {
+
+constexpr int kProbeThreads = 256;
+
+template <bool PAIRED>
+__global__ void __launch_bounds__(kProbeThreads) k_fma_probe(int iters, float a, float b, float* __restrict__ out) {
+  const int gid = blockIdx.x * kProbeThreads + threadIdx.x;
+  float acc = 0.f;
+  if constexpr (PAIRED) {
+    float2 x[8];
+#pragma unroll
+    for (int i = 0; i < 8; ++i) x[i] = make_float2(1e-3f * threadIdx.x + i, 2e-3f * threadIdx.x - i);
+    const float2 A = make_float2(a, a), B = make_float2(b, b);
+    for (int it = 0; it < iters; ++it) {
+#pragma unroll
+      for (int i = 0; i < 8; ++i) x[i] = __ffma2_rn(x[i], A, B);
+    }
+#pragma unroll
+    for (int i = 0; i < 8; ++i) acc += x[i].x + x[i].y;
+  } else {
+    float x[16];
+#pragma unroll
+    for (int i = 0; i < 16; ++i) x[i] = 1e-3f * threadIdx.x + i;
+    for (int it = 0; it < iters; ++it) {
+#pragma unroll
+      for (int i = 0; i < 16; ++i) x[i] = fmaf(x[i], a, b);
+    }
+#pragma unroll
+    for (int i = 0; i < 16; ++i) acc += x[i];
+  }
+  out[gid] = acc;
+}
+
+}  // namespace fm
+
+extern "C" int fm_fp32_fma_probe(int paired, int blocks, int iters, float* out, void* stream) {
+  using namespace fm;
+  if (blocks < 1 || iters < 1 || !out) return FM_ERR_ARG;
+  cudaStream_t s = (cudaStream_t)stream;
+  if (paired) launch(k_fma_probe<true>, blocks, kProbeThreads, 0, s, iters, 0.9999999f, 1e-7f, out);
+  else launch(k_fma_probe<false>, blocks, kProbeThreads, 0, s, iters, 0.9999999f, 1e-7f, out);
+  return check_cuda();
+}

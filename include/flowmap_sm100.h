@@ -57,6 +57,13 @@ long long fm_launch_count(int reset);
  * to buf (at most len bytes, NUL-terminated) when buf is not NULL. */
 int fm_last_cuda_error(char *buf, int len);
 
+/* FP32 FMA throughput probe (no reference counterpart; measures the FP32 peak
+ * the gather kernels are reported against): `blocks` CTAs of 256 threads each
+ * run 16 independent FMA chains of `iters` steps -- scalar fmaf, or paired
+ * two-lane FMAs when paired != 0 -- and write one float per thread to `out`
+ * (blocks * 256 floats).  FLOPs per launch = blocks * 256 * iters * 32. */
+int fm_fp32_fma_probe(int paired, int blocks, int iters, float *out, void *stream);
+
 /* advect_u_grid: semi-Lagrangian advection, RK2 (midpoint) or RK4 backtrace
  * of the face nodes through u0, then u2_c = (u1 sampled at the foot)_c.
  * Replaces RK2_advect_u_grid / RK4_advect_u_grid (3D/flowmap.py:202-282,

@@ -44,6 +44,9 @@ def test_invalid_arguments_rejected_without_device(fm):
     assert lib.fm_clamp_extrema(C.byref(bad_dim), 0, -1, None, None, None, None) == 1
     assert lib.fm_clamp_extrema(C.byref(g), 0, 3, None, None, None, None) == 2  # face >= dim
     assert lib.fm_clamp_extrema(C.byref(g), 0, -1, None, None, None, None) == 2  # NULL fields
+    assert lib.fm_fp32_fma_probe(0, 0, 16, None, None) == 2
+    assert lib.fm_fp32_fma_probe(1, 4, 0, None, None) == 2
+    assert lib.fm_tune_set(0, C.byref(g), 33) == 2
 
 
 def test_no_cpu_fallback(fm):
@@ -59,3 +62,8 @@ def test_launch_counter_exported(fm):
     n0 = fm._lib.launch_count(reset=True)
     assert fm._lib.launch_count() == 0
     assert isinstance(n0, int)
+
+
+def test_last_cuda_error_reported(fm):
+    code, name = fm._lib.last_cuda_error()
+    assert isinstance(code, int) and name.startswith("cuda")
