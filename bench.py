@@ -38,7 +38,8 @@ def parse():
     ap.add_argument("--steps", type=int, default=3)
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
-    ap.add_argument("--form", default="both", choices=["plain", "mixed", "both"])
+    ap.add_argument("--form", default="all", choices=["plain", "mixed", "checkpointed", "both", "all"],
+                    help="both: plain + mixed; all: plain + checkpointed + mixed (the headline form last)")
     ap.add_argument("--no-error", action="store_true", help="skip the FP64 reference runs")
     ap.add_argument("--solver-check-every", type=int, default=0,
                     help="0: device-side PCG loop (CUDA-graph WHILE node); k: host polls every k iterations "
@@ -69,16 +70,22 @@ def parse():
 
 def form_config(C, a, form, dtype):
     """plain: the reference's FP32 drop-in (backward_u=True: the adjoint re-advects
-    u backwards and re-projects it); mixed: the checkpointed form (backward_u=False:
-    the adjoint reads the stored trajectory; midpoint velocities in BF16, passive
-    in FP32), FP64 reductions."""
+    u backwards and re-projects it); mixed: backward_u=False, the adjoint reads the
+    stored trajectory (midpoint velocities in BF16, passive in FP32), BF16 MG coarse
+    levels, FP64 reductions; checkpointed: the mixed form keeping only the state at
+    each reinit interval's start, the adjoint replaying every interval."""
     import torch
 
-    mixed = form == "mixed"
+    from dataclasses import replace
+
+    ckpt = form == "checkpointed"
+    mixed = form == "mixed" or ckpt
     store = torch.bfloat16 if (mixed and dtype == torch.float32) else None
-    return C.shape3d_config(res=a.res, steps=a.sim_steps, reinit_every=a.reinit, rk=4, dtype=dtype,
-                            store_dtype=store, backward_u=not mixed, check_every=a.solver_check_every,
-                            coarse_bf16=mixed and dtype == torch.float32 and a.mixed_coarse == "bf16")
+    cfg = C.shape3d_config(res=a.res, steps=a.sim_steps, reinit_every=a.reinit, rk=4, dtype=dtype,
+                           store_dtype=store, backward_u=not mixed, check_every=a.solver_check_every,
+                           coarse_bf16=mixed and dtype == torch.float32 and a.mixed_coarse == "bf16")
+    # checkpointed: the mixed form with interval checkpointing (the adjoint replays each interval)
+    return replace(cfg, recompute=True) if ckpt else cfg
 
 
 def workload_name(a):
@@ -559,12 +566,13 @@ def main():
     S = importlib.import_module("differentiable-flowmap_b200.simulator")
     lib = fm._lib
 
-    forms = ["plain", "mixed"] if a.form == "both" else [a.form]
+    forms = {"both": ["plain", "mixed"], "all": ["plain", "checkpointed", "mixed"]}.get(a.form, [a.form])
     head = forms[-1]
     sims, cfgs = {}, {}
     for f in forms:
         cfgs[f] = form_config(C, a, f, torch.float32)
         sims[f] = S.LFM_Diff_Simulator(config=cfgs[f], device=dev)
+    sims_bytes = {f: x.trajectory_bytes() for f, x in sims.items()}
     sim, cfg = sims[head], cfgs[head]
     store = cfg.store_dtype
     backward_u = cfg.backward_u
@@ -687,7 +695,9 @@ def main():
                 "e2e": e2e, "gpu_launches": launches, "clocks": clk, "roofline": roof,
                 "forms": {f: {"value": r["value"], "ms_per_step": r["ms_per_step"], "gpu_launches": r["launches"],
                               "backward_u": cfgs[f].backward_u,
-                              "velocity_store": "bf16" if cfgs[f].store_dtype == torch.bfloat16 else "f32",
+                              "velocity_store": ("f32 ring of one interval, replayed" if cfgs[f].recompute else
+                                                 "bf16" if cfgs[f].store_dtype == torch.bfloat16 else "f32"),
+                              "trajectory_gb": sims_bytes[f] / 1e9,
                               "grad_error_vs_fp64": errors.get(f)} for f, r in results.items()}}
         if "plain" in results and "mixed" in results:
             line["mixed_over_plain"] = results["mixed"]["value"] / results["plain"]["value"]

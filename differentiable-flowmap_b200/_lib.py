@@ -123,6 +123,7 @@ RESTYPES = {"fm_launch_count": C.c_longlong}
 SIGNATURES["fm_launch_count"] = [I]
 SIGNATURES["fm_last_cuda_error"] = [C.c_char_p, I]
 SIGNATURES["fm_fp32_fma_probe"] = [I, I, I, P, P]
+SIGNATURES["fm_set_pdl"] = [I]
 
 _lib = None
 
@@ -149,6 +150,11 @@ def lib() -> C.CDLL:
 def launch_count(reset: bool = False) -> int:
     """Kernels launched by libflowmap_sm100.so so far (graph launches included)."""
     return int(lib().fm_launch_count(1 if reset else 0))
+
+
+def set_pdl(enable: bool) -> bool:
+    """Programmatic dependent launch for the solver kernels; returns the previous setting."""
+    return bool(lib().fm_set_pdl(1 if enable else 0))
 
 
 def last_cuda_error():

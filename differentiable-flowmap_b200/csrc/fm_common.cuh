@@ -15,6 +15,19 @@
 
 namespace fm {
 
+// Programmatic dependent launch (sm_90+).  A kernel launched with the
+// programmatic-serialization attribute may become resident while its
+// predecessor in the stream still runs; griddepcontrol.wait blocks until that
+// predecessor has completed and its writes are visible, and
+// launch_dependents lets the next kernel's CTAs be scheduled.  Both are no-ops
+// for an ordinary launch.  Called first thing in a kernel, before any global
+// memory access, this hides only launch latency: no access ever overlaps the
+// predecessor.
+__device__ __forceinline__ void pdl_begin() {
+  asm volatile("griddepcontrol.wait;" ::: "memory");
+  asm volatile("griddepcontrol.launch_dependents;" ::: "memory");
+}
+
 struct Shape {
   int s0, s1, s2;
   __host__ __device__ __forceinline__ long size() const { return (long)s0 * s1 * s2; }

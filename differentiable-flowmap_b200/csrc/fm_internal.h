@@ -68,10 +68,37 @@ inline bool raise_smem_limit(void (*k)(KArgs...), size_t smem) {
   return true;
 }
 
+// Launches through launch_pdl use programmatic dependent launch unless it is
+// switched off (fm_set_pdl); their kernels start with pdl_begin().
+extern std::atomic<int> g_pdl;
+
 // Launch helper that counts the launch.
 template <typename... KArgs, typename... Args>
 inline void launch(void (*k)(KArgs...), dim3 grid, dim3 block, size_t smem, cudaStream_t s, Args&&... args) {
   k<<<grid, block, smem, s>>>(std::forward<Args>(args)...);
+  count_launch();
+}
+
+// As launch(), with the programmatic-serialization attribute: the kernel's CTAs
+// may be scheduled before its stream predecessor finishes and wait for it in
+// pdl_begin().  Only for kernels whose first statement is pdl_begin().
+template <typename... KArgs, typename... Args>
+inline void launch_pdl(void (*k)(KArgs...), dim3 grid, dim3 block, size_t smem, cudaStream_t s, Args&&... args) {
+  if (!g_pdl.load(std::memory_order_relaxed)) {
+    launch(k, grid, block, smem, s, std::forward<Args>(args)...);
+    return;
+  }
+  cudaLaunchConfig_t cfg = {};
+  cfg.gridDim = grid;
+  cfg.blockDim = block;
+  cfg.dynamicSmemBytes = smem;
+  cfg.stream = s;
+  cudaLaunchAttribute attr[1];
+  attr[0].id = cudaLaunchAttributeProgrammaticStreamSerialization;
+  attr[0].val.programmaticStreamSerializationAllowed = 1;
+  cfg.attrs = attr;
+  cfg.numAttrs = 1;
+  cudaLaunchKernelEx(&cfg, k, std::forward<Args>(args)...);
   count_launch();
 }
 

@@ -249,6 +249,7 @@ __device__ __forceinline__ void prolong_ring(T* zf, const Shape& sf, int i0, int
 
 template <typename T, int D>
 __global__ void __launch_bounds__(kCoarseThreads, 1) k_mg_coarse(CoarseArgs a, const DevState* st) {
+  pdl_begin();
   namespace cg = cooperative_groups;
   if (st->done) return;  // same value in every CTA of the cluster
   cg::cluster_group cluster = cg::this_cluster();

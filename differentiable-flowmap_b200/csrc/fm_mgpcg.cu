@@ -32,6 +32,7 @@ namespace fm {
 
 std::atomic<long long> g_launch_count{0};
 std::atomic<int> g_last_cuda_error{0};
+std::atomic<int> g_pdl{1};
 
 constexpr int kRedBlocks = 148 * 4;  // fixed reduction grid: 4 CTAs per SM
 constexpr int kRedThreads = 256;
@@ -164,6 +165,7 @@ __device__ __forceinline__ void sum_partials(const double* __restrict__ part, do
 template <typename T, int D>
 __global__ void __launch_bounds__(kRedThreads) k_div_bc(fm_grid g, MacW<T> u, T* __restrict__ r, T* __restrict__ x,
                                                         double* __restrict__ part) {
+  pdl_begin();
   const Shape cs = cell_shape(g);
   double sum = 0;
   FM_GRID_STRIDE(q, cs.size()) {
@@ -194,6 +196,7 @@ __global__ void __launch_bounds__(kRedThreads) k_div_bc(fm_grid g, MacW<T> u, T*
 template <typename T>
 __global__ void __launch_bounds__(kRedThreads) k_load_rhs(long n, const T* __restrict__ b, T* __restrict__ r,
                                                           T* __restrict__ x, double* __restrict__ part) {
+  pdl_begin();
   double sum = 0;
   FM_GRID_STRIDE(q, n) {
     const T v = b[q];
@@ -209,6 +212,7 @@ __global__ void __launch_bounds__(kRedThreads) k_load_rhs(long n, const T* __res
 // ---------------------------------------------------------------------------
 template <typename TB>
 __global__ void __launch_bounds__(kRedThreads) k_dc_sum(long n, const TB* __restrict__ b, double* __restrict__ part) {
+  pdl_begin();
   double sum = 0;
   FM_GRID_STRIDE(q, n) sum += (double)b[q];
   block_reduce2(sum, 0.0, part + 2 * blockIdx.x);
@@ -216,6 +220,7 @@ __global__ void __launch_bounds__(kRedThreads) k_dc_sum(long n, const TB* __rest
 
 // which = 0: dc_mean = sum / n;  1: dc_b2 = dc_r2 = sum of squares;  2: dc_r2 = sum of squares
 __global__ void k_dc_fin(DevState* st, const double* part, double n, int which) {
+  pdl_begin();
   double a, b;
   sum_partials(part, a, b);
   if (threadIdx.x == 0) {
@@ -232,6 +237,7 @@ template <typename TB, int D>
 __global__ void __launch_bounds__(kRedThreads) k_dc_residual(Shape s, const TB* __restrict__ b,
                                                              const double* __restrict__ x, double* __restrict__ work,
                                                              double* __restrict__ part, const DevState* st) {
+  pdl_begin();
   const double mean = st->dc_mean;
   double acc = 0;
   FM_GRID_STRIDE(q, s.size()) {
@@ -252,6 +258,7 @@ __global__ void __launch_bounds__(kRedThreads) k_dc_residual(Shape s, const TB* 
 __global__ void __launch_bounds__(kRedThreads) k_dc_load(long n, const double* __restrict__ work,
                                                          float* __restrict__ r, float* __restrict__ x,
                                                          double* __restrict__ part, const DevState* st) {
+  pdl_begin();
   const double inv = 1.0 / sqrt(st->dc_r2);
   double sum = 0;
   FM_GRID_STRIDE(q, n) {
@@ -266,12 +273,14 @@ __global__ void __launch_bounds__(kRedThreads) k_dc_load(long n, const double* _
 // rTr floor of the next inner solve (unit-norm right-hand side): a correction
 // only has to bring |r| down to rel_tol |b|, with a factor 2 margin; 0 clears it.
 __global__ void k_dc_set_tol(DevState* st, double rel_tol, int clear) {
+  pdl_begin();
   const double t = clear ? 0.0 : 0.5 * rel_tol * sqrt(st->dc_b2 / st->dc_r2);
   st->dc_tol = t * t;
 }
 
 // x += |r| * e
 __global__ void k_dc_update(long n, double* __restrict__ x, const float* __restrict__ e, const DevState* st) {
+  pdl_begin();
   const double s = sqrt(st->dc_r2);
   FM_GRID_STRIDE(q, n) x[q] += s * (double)e[q];
 }
@@ -279,6 +288,7 @@ __global__ void k_dc_update(long n, double* __restrict__ x, const float* __restr
 // subtract_grad_p + apply_bc (3D/mgpcg.py:401-427)
 template <typename T, int D>
 __global__ void k_subgrad_bc(fm_grid g, const T* __restrict__ p, MacW<T> u) {
+  pdl_begin();
   const int c = blockIdx.y;
   const Shape fs = face_shape(g, c);
   const Shape cs = cell_shape(g);
@@ -296,6 +306,7 @@ __global__ void k_subgrad_bc(fm_grid g, const T* __restrict__ p, MacW<T> u) {
 // scalar finalizers (one CTA)
 // ---------------------------------------------------------------------------
 __global__ void k_fin_mean(DevState* st, const double* part, double n) {
+  pdl_begin();
   double a, b;
   sum_partials(part, a, b);
   if (threadIdx.x == 0) {
@@ -306,6 +317,7 @@ __global__ void k_fin_mean(DevState* st, const double* part, double n) {
 }
 
 __global__ void k_fin_alpha(DevState* st, const double* part, double eps) {
+  pdl_begin();
   if (st->done) return;
   double a, b;
   sum_partials(part, a, b);
@@ -327,6 +339,7 @@ __device__ __forceinline__ void finish_solve(DevState* st) {
 }
 
 __global__ void k_fin_conv(DevState* st, const double* part, double n) {
+  pdl_begin();
   if (st->done) return;
   double a, b;
   sum_partials(part, a, b);
@@ -340,12 +353,14 @@ __global__ void k_fin_conv(DevState* st, const double* part, double n) {
 
 // Last node of the while-loop body: keep iterating until the solve is done.
 __global__ void k_loop_cond(cudaGraphConditionalHandle h, DevState* st) {
+  pdl_begin();
   st->bodies += 1;
   cudaGraphSetConditional(h, st->done ? 0u : 1u);
 }
 
 __global__ void k_fin_beta(DevState* st, const double* part, double eps, double abs_tol, double rel_tol,
                            int max_iters, int first) {
+  pdl_begin();
   if (st->done) return;
   double a, b;
   sum_partials(part, a, b);
@@ -373,6 +388,7 @@ __global__ void k_fin_beta(DevState* st, const double* part, double eps, double 
 template <typename T, int D>
 __global__ void __launch_bounds__(kRedThreads) k_Ap_dot(Shape s, const T* __restrict__ p, T* __restrict__ Ap,
                                                         double* __restrict__ part, const DevState* st) {
+  pdl_begin();
   if (st->done) return;
   double acc = 0;
   FM_GRID_STRIDE(q, s.size()) {
@@ -392,6 +408,7 @@ template <typename T>
 __global__ void __launch_bounds__(kRedThreads) k_update_xr(long n, T* __restrict__ x, T* __restrict__ r,
                                                            const T* __restrict__ p, const T* __restrict__ Ap,
                                                            double* __restrict__ part, const DevState* st) {
+  pdl_begin();
   if (st->done) return;
   const T alpha = (T)st->alpha;
   double rr = 0, rs = 0;
@@ -407,6 +424,7 @@ __global__ void __launch_bounds__(kRedThreads) k_update_xr(long n, T* __restrict
 
 template <typename T>
 __global__ void k_update_p(long n, T* __restrict__ p, const T* __restrict__ z, const DevState* st, int first) {
+  pdl_begin();
   if (st->done) return;
   const T beta = (T)st->beta;
   FM_GRID_STRIDE(q, n) p[q] = first ? z[q] : rn_add(z[q], rn_mul(beta, p[q]));
@@ -418,6 +436,7 @@ __global__ void k_update_p(long n, T* __restrict__ p, const T* __restrict__ z, c
 // First red sweep from z == 0 (fuses z.fill(0)); optionally recentres r.
 template <typename T, int D>
 __global__ void k_smooth_first(Shape s, T* __restrict__ r, T* __restrict__ z, const DevState* st, int recenter) {
+  pdl_begin();
   if (st->done) return;
   const T mean = recenter ? (T)st->mean : (T)0;
   FM_GRID_STRIDE(q, s.size()) {
@@ -475,6 +494,7 @@ __device__ __forceinline__ T nb_sum32(const S* __restrict__ x, const Shape& s, u
 template <typename T, int D, typename S = T>
 __global__ void __launch_bounds__(kPairBX* kPairBY) k_smooth_pair(Shape s, const S* __restrict__ r, S* z, int phase,
                                                                  const DevState* st) {
+  pdl_begin();
   if (st->done) return;
   int i, j, k;
   if (!pair_coords<D>(s, i, j, k)) return;
@@ -492,6 +512,7 @@ __global__ void __launch_bounds__(kPairBX* kPairBY) k_smooth_pair(Shape s, const
 template <typename T, int D, typename S = T>
 __global__ void __launch_bounds__(kPairBX* kPairBY) k_smooth_first_pair(Shape s, S* __restrict__ r, S* __restrict__ z,
                                                                        const DevState* st, int recenter) {
+  pdl_begin();
   if (st->done) return;
   int i, j, k;
   if (!pair_coords<D>(s, i, j, k)) return;
@@ -518,6 +539,7 @@ __global__ void __launch_bounds__(kPairBX* kPairBY) k_smooth_first_pair(Shape s,
 template <typename T, int D, bool DOT>
 __global__ void __launch_bounds__(kRedThreads) k_smooth(Shape s, const T* __restrict__ r, T* z, int phase,
                                                         double* __restrict__ part, const DevState* st) {
+  pdl_begin();
   if (st->done) return;
   double acc = 0;
   FM_GRID_STRIDE(q, s.size()) {
@@ -542,6 +564,7 @@ __global__ void __launch_bounds__(kRedThreads) k_smooth(Shape s, const T* __rest
 template <typename T, int D, typename SF = T, typename SC = T>
 __global__ void k_restrict(Shape sf, Shape sc, const SF* __restrict__ rf, const SF* __restrict__ zf,
                            SC* __restrict__ rc, const DevState* st) {
+  pdl_begin();
   if (st->done) return;
   const T scale = (T)1.0 / (T)(D - 1.0);
   FM_GRID_STRIDE(q, sc.size()) {
@@ -568,6 +591,7 @@ __global__ void k_restrict(Shape sf, Shape sc, const SF* __restrict__ rf, const 
 // prolongate(l) (3D/mgpcg.py:165-168)
 template <typename T, int D, typename SF = T, typename SC = T>
 __global__ void k_prolong(Shape sf, Shape sc, SF* __restrict__ zf, const SC* __restrict__ zc, const DevState* st) {
+  pdl_begin();
   if (st->done) return;
   FM_GRID_STRIDE(q, sf.size()) {
     int i, j, k;
@@ -581,6 +605,7 @@ __global__ void k_prolong(Shape sf, Shape sc, SF* __restrict__ zf, const SC* __r
 template <typename T, int D>
 __global__ void k_bottom(Shape s, const T* __restrict__ r, T* __restrict__ z, int bottom, int mode,
                          const DevState* st) {
+  pdl_begin();
   if (st->done) return;
   extern __shared__ unsigned char smem_raw[];
   T* zs = reinterpret_cast<T*>(smem_raw);
@@ -640,6 +665,7 @@ __global__ void k_bottom(Shape s, const T* __restrict__ r, T* __restrict__ z, in
 
 template <typename T, int D>
 __global__ void k_laplacian(Shape s, const T* __restrict__ p, T* __restrict__ Ap) {
+  pdl_begin();
   FM_GRID_STRIDE(q, s.size()) {
     int i, j, k;
     unflatten(s, q, i, j, k);
@@ -765,13 +791,15 @@ static void launch_coarse(fm_mgpcg* S, cudaStream_t s) {
   cfg.blockDim = dim3(kCoarseThreads, 1, 1);
   cfg.dynamicSmemBytes = S->coarse_smem;
   cfg.stream = s;
-  cudaLaunchAttribute attr[1];
+  cudaLaunchAttribute attr[2];
   attr[0].id = cudaLaunchAttributeClusterDimension;
   attr[0].val.clusterDim.x = (unsigned)S->nc;
   attr[0].val.clusterDim.y = 1;
   attr[0].val.clusterDim.z = 1;
+  attr[1].id = cudaLaunchAttributeProgrammaticStreamSerialization;
+  attr[1].val.programmaticStreamSerializationAllowed = 1;
   cfg.attrs = attr;
-  cfg.numAttrs = 1;
+  cfg.numAttrs = g_pdl.load(std::memory_order_relaxed) ? 2 : 1;
   const DevState* st = S->st;
   cudaLaunchKernelEx(&cfg, k_mg_coarse<T, D>, a, st);
   count_launch(1);
@@ -800,16 +828,16 @@ static void launch_vcycle(fm_mgpcg* S, cudaStream_t s, bool dot_last, bool recen
   auto bf = [&](int l) { return std::is_same<T, float>::value && l >= 1 && l < S->bf16_hi; };
   auto sweep = [&](int l, int phase) {
     const Shape sh = S->lv[l];
-    if (bf(l)) launch(k_smooth_pair<T, D, BF>, pair_grid(sh), pblk, 0, s, sh, (const BF*)S->r[l], (BF*)S->z[l], phase, S->st);
-    else launch(k_smooth_pair<T, D>, pair_grid(sh), pblk, 0, s, sh, (const T*)r[l], z[l], phase, S->st);
+    if (bf(l)) launch_pdl(k_smooth_pair<T, D, BF>, pair_grid(sh), pblk, 0, s, sh, (const BF*)S->r[l], (BF*)S->z[l], phase, S->st);
+    else launch_pdl(k_smooth_pair<T, D>, pair_grid(sh), pblk, 0, s, sh, (const T*)r[l], z[l], phase, S->st);
   };
   for (int l = 0; l < lc; ++l) {
     const Shape sh = S->lv[l];
     const dim3 pg = pair_grid(sh);
     for (int it = 0; it < P.pre_post; ++it) {
       if (it == 0) {
-        if (bf(l)) launch(k_smooth_first_pair<T, D, BF>, pg, pblk, 0, s, sh, (BF*)S->r[l], (BF*)S->z[l], S->st, 0);
-        else launch(k_smooth_first_pair<T, D>, pg, pblk, 0, s, sh, r[l], z[l], S->st, l == 0 && recenter ? 1 : 0);
+        if (bf(l)) launch_pdl(k_smooth_first_pair<T, D, BF>, pg, pblk, 0, s, sh, (BF*)S->r[l], (BF*)S->z[l], S->st, 0);
+        else launch_pdl(k_smooth_first_pair<T, D>, pg, pblk, 0, s, sh, r[l], z[l], S->st, l == 0 && recenter ? 1 : 0);
       } else {
         sweep(l, 0);
       }
@@ -818,32 +846,32 @@ static void launch_vcycle(fm_mgpcg* S, cudaStream_t s, bool dot_last, bool recen
     const Shape sc = S->lv[l + 1];
     const unsigned rb = blocks_for(sc.size(), 256, cap);
     if (bf(l) && bf(l + 1))
-      launch(k_restrict<T, D, BF, BF>, rb, 256, 0, s, sh, sc, (const BF*)S->r[l], (const BF*)S->z[l], (BF*)S->r[l + 1], S->st);
+      launch_pdl(k_restrict<T, D, BF, BF>, rb, 256, 0, s, sh, sc, (const BF*)S->r[l], (const BF*)S->z[l], (BF*)S->r[l + 1], S->st);
     else if (bf(l))
-      launch(k_restrict<T, D, BF, T>, rb, 256, 0, s, sh, sc, (const BF*)S->r[l], (const BF*)S->z[l], r[l + 1], S->st);
+      launch_pdl(k_restrict<T, D, BF, T>, rb, 256, 0, s, sh, sc, (const BF*)S->r[l], (const BF*)S->z[l], r[l + 1], S->st);
     else if (bf(l + 1))
-      launch(k_restrict<T, D, T, BF>, rb, 256, 0, s, sh, sc, (const T*)r[l], (const T*)z[l], (BF*)S->r[l + 1], S->st);
+      launch_pdl(k_restrict<T, D, T, BF>, rb, 256, 0, s, sh, sc, (const T*)r[l], (const T*)z[l], (BF*)S->r[l + 1], S->st);
     else
-      launch(k_restrict<T, D>, rb, 256, 0, s, sh, sc, (const T*)r[l], (const T*)z[l], r[l + 1], S->st);
+      launch_pdl(k_restrict<T, D>, rb, 256, 0, s, sh, sc, (const T*)r[l], (const T*)z[l], r[l + 1], S->st);
   }
   const Shape sb = S->lv[L - 1];
   if (S->lc > 0) {
     launch_coarse<T, D>(S, s);
   } else if (S->bottom_smem) {
-    launch(k_bottom<T, D>, 1, kBottomThreads, S->bottom_smem, s, sb, r[L - 1], z[L - 1], P.bottom, P.bottom_mode,
+    launch_pdl(k_bottom<T, D>, 1, kBottomThreads, S->bottom_smem, s, sb, r[L - 1], z[L - 1], P.bottom, P.bottom_mode,
            S->st);
   } else {
     // large coarsest level: per-sweep launches (z zero-filled by the first sweep)
     const unsigned nb = blocks_for(sb.size(), 256, cap);
     int first = 1;
     auto pair = [&](int a, int b) {
-      if (first && a == 0) launch(k_smooth_first<T, D>, nb, 256, 0, s, sb, r[L - 1], z[L - 1], S->st, L == 1 ? 1 : 0);
+      if (first && a == 0) launch_pdl(k_smooth_first<T, D>, nb, 256, 0, s, sb, r[L - 1], z[L - 1], S->st, L == 1 ? 1 : 0);
       else {
         if (first) cudaMemsetAsync(z[L - 1], 0, sizeof(T) * sb.size(), s);
-        launch(k_smooth<T, D, false>, nb, 256, 0, s, sb, r[L - 1], z[L - 1], a, nullptr, S->st);
+        launch_pdl(k_smooth<T, D, false>, nb, 256, 0, s, sb, r[L - 1], z[L - 1], a, nullptr, S->st);
       }
       first = 0;
-      launch(k_smooth<T, D, false>, nb, 256, 0, s, sb, r[L - 1], z[L - 1], b, nullptr, S->st);
+      launch_pdl(k_smooth<T, D, false>, nb, 256, 0, s, sb, r[L - 1], z[L - 1], b, nullptr, S->st);
     };
     if (P.bottom_mode == 0) for (int i = 0; i < P.bottom; ++i) pair(0, 1);
     else {
@@ -857,23 +885,23 @@ static void launch_vcycle(fm_mgpcg* S, cudaStream_t s, bool dot_last, bool recen
     const Shape sc = S->lv[l + 1];
     const unsigned nb = blocks_for(sh.size(), 256, cap);
     if (bf(l) && bf(l + 1))
-      launch(k_prolong<T, D, BF, BF>, nb, 256, 0, s, sh, sc, (BF*)S->z[l], (const BF*)S->z[l + 1], S->st);
+      launch_pdl(k_prolong<T, D, BF, BF>, nb, 256, 0, s, sh, sc, (BF*)S->z[l], (const BF*)S->z[l + 1], S->st);
     else if (bf(l))
-      launch(k_prolong<T, D, BF, T>, nb, 256, 0, s, sh, sc, (BF*)S->z[l], (const T*)z[l + 1], S->st);
+      launch_pdl(k_prolong<T, D, BF, T>, nb, 256, 0, s, sh, sc, (BF*)S->z[l], (const T*)z[l + 1], S->st);
     else if (bf(l + 1))
-      launch(k_prolong<T, D, T, BF>, nb, 256, 0, s, sh, sc, z[l], (const BF*)S->z[l + 1], S->st);
+      launch_pdl(k_prolong<T, D, T, BF>, nb, 256, 0, s, sh, sc, z[l], (const BF*)S->z[l + 1], S->st);
     else
-      launch(k_prolong<T, D>, nb, 256, 0, s, sh, sc, z[l], (const T*)z[l + 1], S->st);
+      launch_pdl(k_prolong<T, D>, nb, 256, 0, s, sh, sc, z[l], (const T*)z[l + 1], S->st);
     for (int it = 0; it < P.pre_post; ++it) {
       sweep(l, 1);
       const bool last = dot_last && l == 0 && it == P.pre_post - 1;
-      if (last) launch(k_smooth<T, D, true>, kRedBlocks, kRedThreads, 0, s, sh, r[l], z[l], 0, S->part, S->st);
+      if (last) launch_pdl(k_smooth<T, D, true>, kRedBlocks, kRedThreads, 0, s, sh, r[l], z[l], 0, S->part, S->st);
       else sweep(l, 0);
     }
   }
   if (dot_last && L == 1) {
     // single-level: z.r over the bottom result
-    launch(k_smooth<T, D, true>, kRedBlocks, kRedThreads, 0, s, sb, r[0], z[0], 2 /* no update */, S->part, S->st);
+    launch_pdl(k_smooth<T, D, true>, kRedBlocks, kRedThreads, 0, s, sb, r[0], z[0], 2 /* no update */, S->part, S->st);
   }
 }
 
@@ -887,23 +915,23 @@ static void launch_iteration(fm_mgpcg* S, cudaStream_t s) {
   T* Ap = (T*)S->Ap;
   T* r0 = (T*)S->r[0];
   T* z0 = (T*)S->z[0];
-  launch(k_Ap_dot<T, D>, kRedBlocks, kRedThreads, 0, s, s0, p, Ap, S->part, S->st);
-  launch(k_fin_alpha, 1, 256, 0, s, S->st, S->part, S->P.eps);
-  launch(k_update_xr<T>, kRedBlocks, kRedThreads, 0, s, n, x, r0, p, Ap, S->part, S->st);
-  launch(k_fin_conv, 1, 256, 0, s, S->st, S->part, (double)n);
+  launch_pdl(k_Ap_dot<T, D>, kRedBlocks, kRedThreads, 0, s, s0, p, Ap, S->part, S->st);
+  launch_pdl(k_fin_alpha, 1, 256, 0, s, S->st, S->part, S->P.eps);
+  launch_pdl(k_update_xr<T>, kRedBlocks, kRedThreads, 0, s, n, x, r0, p, Ap, S->part, S->st);
+  launch_pdl(k_fin_conv, 1, 256, 0, s, S->st, S->part, (double)n);
   launch_vcycle<T, D>(S, s, true);
-  launch(k_fin_beta, 1, 256, 0, s, S->st, S->part, S->P.eps, S->P.abs_tol, S->P.rel_tol, S->P.max_iters, 0);
-  launch(k_update_p<T>, blocks_for(n, 256, 148L * 16), 256, 0, s, n, p, z0, S->st, 0);
+  launch_pdl(k_fin_beta, 1, 256, 0, s, S->st, S->part, S->P.eps, S->P.abs_tol, S->P.rel_tol, S->P.max_iters, 0);
+  launch_pdl(k_update_p<T>, blocks_for(n, 256, 148L * 16), 256, 0, s, n, p, z0, S->st, 0);
 }
 
 // Prologue after r0 = b and partial sums of b: recentre, V-cycle, p = z, zTr.
 template <typename T, int D>
 static void launch_prologue(fm_mgpcg* S, cudaStream_t s) {
   const long n = S->lv[0].size();
-  launch(k_fin_mean, 1, 256, 0, s, S->st, S->part, (double)n);
+  launch_pdl(k_fin_mean, 1, 256, 0, s, S->st, S->part, (double)n);
   launch_vcycle<T, D>(S, s, true);
-  launch(k_fin_beta, 1, 256, 0, s, S->st, S->part, S->P.eps, S->P.abs_tol, S->P.rel_tol, S->P.max_iters, 1);
-  launch(k_update_p<T>, blocks_for(n, 256, 148L * 16), 256, 0, s, n, (T*)S->p, (T*)S->z[0], S->st, 1);
+  launch_pdl(k_fin_beta, 1, 256, 0, s, S->st, S->part, S->P.eps, S->P.abs_tol, S->P.rel_tol, S->P.max_iters, 1);
+  launch_pdl(k_update_p<T>, blocks_for(n, 256, 148L * 16), 256, 0, s, n, (T*)S->p, (T*)S->z[0], S->st, 1);
 }
 
 // Device mode: one graph holding a conditional WHILE node whose body is one PCG
@@ -929,7 +957,7 @@ static int build_loop_graph(fm_mgpcg* S) {
       break;
     const long long before = g_launch_count.load();
     if (D == 3) launch_iteration<T, 3>(S, S->cap); else launch_iteration<T, 2>(S, S->cap);
-    launch(k_loop_cond, 1, 1, 0, S->cap, h, S->st);
+    launch_pdl(k_loop_cond, 1, 1, 0, S->cap, h, S->st);
     S->loop_kernels = g_launch_count.load() - before;
     g_launch_count.fetch_sub(S->loop_kernels);
     cudaGraph_t captured = nullptr;
@@ -1001,7 +1029,7 @@ static int capture_solve(fm_mgpcg* S, cudaStream_t s) {
     return cuda_fail(e);
   const long long before = g_launch_count.load();
   if (D == 3) launch_iteration<T, 3>(S, S->cap); else launch_iteration<T, 2>(S, S->cap);
-  launch(k_loop_cond, 1, 1, 0, S->cap, h, S->st);
+  launch_pdl(k_loop_cond, 1, 1, 0, S->cap, h, S->st);
   g_launch_count.fetch_sub(g_launch_count.load() - before);  // the loop body runs a data-dependent number of times
   cudaGraph_t captured = nullptr;
   if ((e = cudaStreamEndCapture(S->cap, &captured)) != cudaSuccess) return cuda_fail(e);
@@ -1183,20 +1211,20 @@ int fm_project(fm_mgpcg* S, void* ux, void* uy, void* uz, void* p_out, void* str
   dim3 fgrid((unsigned)((maxf + 255) / 256), (unsigned)g.dim, 1);
   if (S->dtype == FM_F32) {
     MacW<float> u{{(float*)ux, (float*)uy, (float*)uz}};
-    if (g.dim == 3) launch(k_div_bc<float, 3>, kRedBlocks, kRedThreads, 0, s, g, u, (float*)S->r[0], (float*)S->x, S->part);
-    else launch(k_div_bc<float, 2>, kRedBlocks, kRedThreads, 0, s, g, u, (float*)S->r[0], (float*)S->x, S->part);
+    if (g.dim == 3) launch_pdl(k_div_bc<float, 3>, kRedBlocks, kRedThreads, 0, s, g, u, (float*)S->r[0], (float*)S->x, S->part);
+    else launch_pdl(k_div_bc<float, 2>, kRedBlocks, kRedThreads, 0, s, g, u, (float*)S->r[0], (float*)S->x, S->part);
     status = run_solve<float>(S, s, iters, rtr);
     if (status == FM_ERR_CUDA) return status;
-    if (g.dim == 3) launch(k_subgrad_bc<float, 3>, fgrid, 256, 0, s, g, (const float*)S->x, u);
-    else launch(k_subgrad_bc<float, 2>, fgrid, 256, 0, s, g, (const float*)S->x, u);
+    if (g.dim == 3) launch_pdl(k_subgrad_bc<float, 3>, fgrid, 256, 0, s, g, (const float*)S->x, u);
+    else launch_pdl(k_subgrad_bc<float, 2>, fgrid, 256, 0, s, g, (const float*)S->x, u);
   } else {
     MacW<double> u{{(double*)ux, (double*)uy, (double*)uz}};
-    if (g.dim == 3) launch(k_div_bc<double, 3>, kRedBlocks, kRedThreads, 0, s, g, u, (double*)S->r[0], (double*)S->x, S->part);
-    else launch(k_div_bc<double, 2>, kRedBlocks, kRedThreads, 0, s, g, u, (double*)S->r[0], (double*)S->x, S->part);
+    if (g.dim == 3) launch_pdl(k_div_bc<double, 3>, kRedBlocks, kRedThreads, 0, s, g, u, (double*)S->r[0], (double*)S->x, S->part);
+    else launch_pdl(k_div_bc<double, 2>, kRedBlocks, kRedThreads, 0, s, g, u, (double*)S->r[0], (double*)S->x, S->part);
     status = run_solve<double>(S, s, iters, rtr);
     if (status == FM_ERR_CUDA) return status;
-    if (g.dim == 3) launch(k_subgrad_bc<double, 3>, fgrid, 256, 0, s, g, (const double*)S->x, u);
-    else launch(k_subgrad_bc<double, 2>, fgrid, 256, 0, s, g, (const double*)S->x, u);
+    if (g.dim == 3) launch_pdl(k_subgrad_bc<double, 3>, fgrid, 256, 0, s, g, (const double*)S->x, u);
+    else launch_pdl(k_subgrad_bc<double, 2>, fgrid, 256, 0, s, g, (const double*)S->x, u);
   }
   if (p_out) cudaMemcpyAsync(p_out, S->x, (S->dtype == FM_F32 ? 4 : 8) * n, cudaMemcpyDeviceToDevice, s);
   if (check_cuda()) return FM_ERR_CUDA;
@@ -1209,10 +1237,10 @@ int fm_mgpcg_solve(fm_mgpcg* S, const void* b, void* x, void* stream, int* iters
   const long n = S->lv[0].size();
   int status;
   if (S->dtype == FM_F32) {
-    launch(k_load_rhs<float>, kRedBlocks, kRedThreads, 0, s, n, (const float*)b, (float*)S->r[0], (float*)S->x, S->part);
+    launch_pdl(k_load_rhs<float>, kRedBlocks, kRedThreads, 0, s, n, (const float*)b, (float*)S->r[0], (float*)S->x, S->part);
     status = run_solve<float>(S, s, iters, rtr);
   } else {
-    launch(k_load_rhs<double>, kRedBlocks, kRedThreads, 0, s, n, (const double*)b, (double*)S->r[0], (double*)S->x, S->part);
+    launch_pdl(k_load_rhs<double>, kRedBlocks, kRedThreads, 0, s, n, (const double*)b, (double*)S->r[0], (double*)S->x, S->part);
     status = run_solve<double>(S, s, iters, rtr);
   }
   if (status == FM_ERR_CUDA) return status;
@@ -1248,19 +1276,19 @@ int fm_mgpcg_solve_dc(fm_mgpcg* S, int b_dtype, const void* b, double* x, double
   const long n = s0.size();
   const int D = S->g.dim;
   const unsigned nb = blocks_for(n, 256, 148L * 16);
-  if (b_dtype == FM_F32) launch(k_dc_sum<float>, kRedBlocks, kRedThreads, 0, s, n, (const float*)b, S->part);
-  else launch(k_dc_sum<double>, kRedBlocks, kRedThreads, 0, s, n, (const double*)b, S->part);
-  launch(k_dc_fin, 1, 256, 0, s, S->st, S->part, (double)n, 0);
+  if (b_dtype == FM_F32) launch_pdl(k_dc_sum<float>, kRedBlocks, kRedThreads, 0, s, n, (const float*)b, S->part);
+  else launch_pdl(k_dc_sum<double>, kRedBlocks, kRedThreads, 0, s, n, (const double*)b, S->part);
+  launch_pdl(k_dc_fin, 1, 256, 0, s, S->st, S->part, (double)n, 0);
   if (cudaMemsetAsync(x, 0, sizeof(double) * n, s) != cudaSuccess) return FM_ERR_CUDA;
   auto residual = [&](int which) {
     if (b_dtype == FM_F32) {
-      if (D == 3) launch(k_dc_residual<float, 3>, kRedBlocks, kRedThreads, 0, s, s0, (const float*)b, x, work, S->part, S->st);
-      else launch(k_dc_residual<float, 2>, kRedBlocks, kRedThreads, 0, s, s0, (const float*)b, x, work, S->part, S->st);
+      if (D == 3) launch_pdl(k_dc_residual<float, 3>, kRedBlocks, kRedThreads, 0, s, s0, (const float*)b, x, work, S->part, S->st);
+      else launch_pdl(k_dc_residual<float, 2>, kRedBlocks, kRedThreads, 0, s, s0, (const float*)b, x, work, S->part, S->st);
     } else {
-      if (D == 3) launch(k_dc_residual<double, 3>, kRedBlocks, kRedThreads, 0, s, s0, (const double*)b, x, work, S->part, S->st);
-      else launch(k_dc_residual<double, 2>, kRedBlocks, kRedThreads, 0, s, s0, (const double*)b, x, work, S->part, S->st);
+      if (D == 3) launch_pdl(k_dc_residual<double, 3>, kRedBlocks, kRedThreads, 0, s, s0, (const double*)b, x, work, S->part, S->st);
+      else launch_pdl(k_dc_residual<double, 2>, kRedBlocks, kRedThreads, 0, s, s0, (const double*)b, x, work, S->part, S->st);
     }
-    launch(k_dc_fin, 1, 256, 0, s, S->st, S->part, (double)n, which);
+    launch_pdl(k_dc_fin, 1, 256, 0, s, S->st, S->part, (double)n, which);
   };
   residual(1);
   int outer = 0, inner = 0, status = FM_OK;
@@ -1273,19 +1301,19 @@ int fm_mgpcg_solve_dc(fm_mgpcg* S, int b_dtype, const void* b, double* x, double
     if (!isfinite(rel)) { status = FM_ERR_NONFINITE; break; }
     if (rel <= rel_tol || r2 == 0.0) break;
     if (outer >= max_outer) { status = FM_ERR_NOT_CONVERGED; break; }
-    launch(k_dc_load, kRedBlocks, kRedThreads, 0, s, n, (const double*)work, (float*)S->r[0], (float*)S->x, S->part,
+    launch_pdl(k_dc_load, kRedBlocks, kRedThreads, 0, s, n, (const double*)work, (float*)S->r[0], (float*)S->x, S->part,
            (const DevState*)S->st);
-    launch(k_dc_set_tol, 1, 1, 0, s, S->st, rel_tol, 0);
+    launch_pdl(k_dc_set_tol, 1, 1, 0, s, S->st, rel_tol, 0);
     int it = 0;
     double rtr = 0;
     const int st = run_solve<float>(S, s, &it, &rtr);  // reaching max_iters is fine: the outer loop corrects
     inner += it;
     if (st == FM_ERR_CUDA || st == FM_ERR_NONFINITE) { status = st; break; }
-    launch(k_dc_update, nb, 256, 0, s, n, x, (const float*)S->x, (const DevState*)S->st);
+    launch_pdl(k_dc_update, nb, 256, 0, s, n, x, (const float*)S->x, (const DevState*)S->st);
     ++outer;
     residual(2);
   }
-  launch(k_dc_set_tol, 1, 1, 0, s, S->st, 0.0, 1);
+  launch_pdl(k_dc_set_tol, 1, 1, 0, s, S->st, 0.0, 1);
   if (outer_iters) *outer_iters = outer;
   if (inner_iters) *inner_iters = inner;
   if (rel_res) *rel_res = rel;
@@ -1330,11 +1358,11 @@ int fm_laplacian(const fm_grid* g, int dtype, const void* p, void* Ap, void* str
   cudaStream_t cs = (cudaStream_t)stream;
   unsigned nb = blocks_for(s.size(), 256, 148L * 16);
   if (dtype == FM_F32) {
-    if (g->dim == 3) launch(k_laplacian<float, 3>, nb, 256, 0, cs, s, (const float*)p, (float*)Ap);
-    else launch(k_laplacian<float, 2>, nb, 256, 0, cs, s, (const float*)p, (float*)Ap);
+    if (g->dim == 3) launch_pdl(k_laplacian<float, 3>, nb, 256, 0, cs, s, (const float*)p, (float*)Ap);
+    else launch_pdl(k_laplacian<float, 2>, nb, 256, 0, cs, s, (const float*)p, (float*)Ap);
   } else {
-    if (g->dim == 3) launch(k_laplacian<double, 3>, nb, 256, 0, cs, s, (const double*)p, (double*)Ap);
-    else launch(k_laplacian<double, 2>, nb, 256, 0, cs, s, (const double*)p, (double*)Ap);
+    if (g->dim == 3) launch_pdl(k_laplacian<double, 3>, nb, 256, 0, cs, s, (const double*)p, (double*)Ap);
+    else launch_pdl(k_laplacian<double, 2>, nb, 256, 0, cs, s, (const double*)p, (double*)Ap);
   }
   return check_cuda();
 }
@@ -1344,6 +1372,10 @@ int fm_abi_version(void) { return 1; }
 long long fm_launch_count(int reset) {
   if (reset) return g_launch_count.exchange(0);
   return g_launch_count.load();
+}
+
+int fm_set_pdl(int enable) {
+  return g_pdl.exchange(enable ? 1 : 0);
 }
 
 int fm_last_cuda_error(char* buf, int len) {
@@ -1496,20 +1528,20 @@ extern "C" int fm_project_noalloc(const fm_grid* g, int dtype, const fm_mg_param
   int status;
   if (dtype == FM_F32) {
     MacW<float> u{{(float*)ux, (float*)uy, (float*)uz}};
-    if (gg.dim == 3) launch(k_div_bc<float, 3>, kRedBlocks, kRedThreads, 0, s, gg, u, (float*)S.r[0], (float*)S.x, S.part);
-    else launch(k_div_bc<float, 2>, kRedBlocks, kRedThreads, 0, s, gg, u, (float*)S.r[0], (float*)S.x, S.part);
+    if (gg.dim == 3) launch_pdl(k_div_bc<float, 3>, kRedBlocks, kRedThreads, 0, s, gg, u, (float*)S.r[0], (float*)S.x, S.part);
+    else launch_pdl(k_div_bc<float, 2>, kRedBlocks, kRedThreads, 0, s, gg, u, (float*)S.r[0], (float*)S.x, S.part);
     status = run_solve_direct<float>(&S, s, iters, rtr);
     if (status == FM_ERR_CUDA) return status;
-    if (gg.dim == 3) launch(k_subgrad_bc<float, 3>, fgrid, 256, 0, s, gg, (const float*)S.x, u);
-    else launch(k_subgrad_bc<float, 2>, fgrid, 256, 0, s, gg, (const float*)S.x, u);
+    if (gg.dim == 3) launch_pdl(k_subgrad_bc<float, 3>, fgrid, 256, 0, s, gg, (const float*)S.x, u);
+    else launch_pdl(k_subgrad_bc<float, 2>, fgrid, 256, 0, s, gg, (const float*)S.x, u);
   } else {
     MacW<double> u{{(double*)ux, (double*)uy, (double*)uz}};
-    if (gg.dim == 3) launch(k_div_bc<double, 3>, kRedBlocks, kRedThreads, 0, s, gg, u, (double*)S.r[0], (double*)S.x, S.part);
-    else launch(k_div_bc<double, 2>, kRedBlocks, kRedThreads, 0, s, gg, u, (double*)S.r[0], (double*)S.x, S.part);
+    if (gg.dim == 3) launch_pdl(k_div_bc<double, 3>, kRedBlocks, kRedThreads, 0, s, gg, u, (double*)S.r[0], (double*)S.x, S.part);
+    else launch_pdl(k_div_bc<double, 2>, kRedBlocks, kRedThreads, 0, s, gg, u, (double*)S.r[0], (double*)S.x, S.part);
     status = run_solve_direct<double>(&S, s, iters, rtr);
     if (status == FM_ERR_CUDA) return status;
-    if (gg.dim == 3) launch(k_subgrad_bc<double, 3>, fgrid, 256, 0, s, gg, (const double*)S.x, u);
-    else launch(k_subgrad_bc<double, 2>, fgrid, 256, 0, s, gg, (const double*)S.x, u);
+    if (gg.dim == 3) launch_pdl(k_subgrad_bc<double, 3>, fgrid, 256, 0, s, gg, (const double*)S.x, u);
+    else launch_pdl(k_subgrad_bc<double, 2>, fgrid, 256, 0, s, gg, (const double*)S.x, u);
   }
   if (check_cuda()) return FM_ERR_CUDA;
   return status;

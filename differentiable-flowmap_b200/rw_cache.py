@@ -205,6 +205,8 @@ def export_forward(sim, log_dir: str, n_steps: int = N_STEPS) -> Dict[str, str]:
     reinit interval "phi", the face maps ("phi_xyz" / "phi_xy") and "F", and
     final/{u_x,u_y[,u_z]}_{N}, final_ind_0 = [N], final/s_{N}.  Returns the
     directories used."""
+    if sim.store_mid is None:
+        raise ValueError("export_forward needs the full trajectory store (recompute=False)")
     dim = sim.dim
     d = _dirs(log_dir, dim)
     cache = RW_Cache(n_steps)
@@ -240,6 +242,8 @@ def import_forward(sim, log_dir: str) -> int:
     so its runs end on a whole interval; export_forward also writes the map of
     a final partial interval, which this reader accepts.  The passive scalar
     per step is read when ``sim`` keeps a passive store."""
+    if sim.store_mid is None:
+        raise ValueError("import_forward needs the full trajectory store (recompute=False)")
     dim, res = sim.dim, sim.grid.shape
     d = _dirs(log_dir, dim)
     cache = RW_Cache()

@@ -77,7 +77,21 @@ class FlowmapConfig:
     trajectory_loss: bool = False  # reference's no-force branch: loss over reinit frames
     dtype: torch.dtype = torch.float32
     store_dtype: Optional[torch.dtype] = None  # checkpoint storage dtype (None: dtype)
+    # Interval checkpointing: the forward keeps only (u, passive) at the start of
+    # each reinit interval, and the adjoint recomputes each interval's forward
+    # steps before undoing them (about 7x less trajectory memory at 128^3, one
+    # more forward pass of time).  Needs backward_u=False.
+    recompute: bool = False
     solver: SolverConfig = field(default_factory=SolverConfig)
+
+    def validate(self):
+        """Reject option combinations the simulator does not implement."""
+        if self.recompute:
+            bad = [name for name, on in (("backward_u", self.backward_u), ("add_control_force", self.add_control_force),
+                                         ("viscosity", self.viscosity != 0.0), ("use_short_BFECC", self.use_short_BFECC),
+                                         ("trajectory_loss", self.trajectory_loss)) if on]
+            if bad:
+                raise FlowmapError(2, f"recompute (interval checkpointing) does not support {', '.join(bad)}")
 
     @property
     def dim(self) -> int:
@@ -179,6 +193,7 @@ class LFM_Simulator:
             cfg = replace(cfg, dt=dt)
         if reinit_every is not None:
             cfg = replace(cfg, reinit_every=reinit_every)
+        cfg.validate()
         if not torch.cuda.is_available():
             raise FlowmapError(6, "LFM_Simulator needs a CUDA device (no CPU fallback)")
         self.cfg = cfg
@@ -262,15 +277,32 @@ class LFM_Simulator:
         self.step_num = _Scalar(-1)
         self.frame_idx = _Scalar(0)
         self.total_steps = cfg.total_steps
+        self._recomputing = False
         self._alloc_stores()
         self.reset_to_identity(self.phi, self.phi_f, self.F_f)
 
     # ------------------------------------------------------------ stores
     def _alloc_stores(self):
-        """Device-resident trajectory for the adjoint (replaces RW_Cache disk I/O)."""
+        """Device-resident trajectory for the adjoint (replaces RW_Cache disk I/O).
+        Full form: every step's midpoint velocity, the passive scalar of every
+        step and the forward maps at every interval end.  Interval checkpointing
+        (recompute): (u, passive) at the start of every interval plus the final
+        state, and one interval's midpoint velocities and passives, regenerated
+        by the adjoint."""
         g, steps, dev = self.grid, self.total_steps, self.device
-        n_int = (steps + self.reinit_every - 1) // self.reinit_every
+        R = self.reinit_every
+        n_int = (steps + R - 1) // R
         sd, wd = self.store_dtype, self.cfg.dtype
+        self.store_mid = self.store_phi = self.store_phi_f = self.store_F_f = self.store_passive = None
+        self.ckpt_u = self.ckpt_passive = self._ring_passive = None
+        if self.cfg.recompute:
+            self.ckpt_u = [torch.zeros((n_int + 1,) + g.face_shape(c), dtype=wd, device=dev) for c in range(self.dim)]
+            if self.cfg.add_passive_scalar:
+                self.ckpt_passive = torch.zeros((n_int + 1,) + g.shape, dtype=wd, device=dev)
+                self._ring_passive = torch.zeros((R + 1,) + g.shape, dtype=wd, device=dev)
+            self._ring = [[torch.zeros(g.face_shape(c), dtype=wd, device=dev) for c in range(self.dim)]
+                          for _ in range(R)]
+            return
         self.store_mid = [torch.zeros((steps,) + g.face_shape(c), dtype=sd, device=dev) for c in range(self.dim)]
         # flow maps (positions and Jacobians) stay in the working dtype: a BF16
         # position would be ~0.5 cells off at 128^3
@@ -288,7 +320,25 @@ class LFM_Simulator:
             self._ring = None
         else:
             self._ring = [[torch.zeros(g.face_shape(c), dtype=self.cfg.dtype, device=dev) for c in range(self.dim)]
-                          for _ in range(self.reinit_every)]
+                          for _ in range(R)]
+
+    def trajectory_bytes(self) -> int:
+        """Device bytes held for the adjoint (stores, checkpoints, rings)."""
+        ts = []
+        for x in (self.store_mid, self.store_phi_f, self.store_F_f, self.ckpt_u, self._ring):
+            if x is not None:
+                ts += [t for row in x for t in (row if isinstance(row, list) else [row])]
+        ts += [x for x in (self.store_phi, self.store_passive, self.ckpt_passive, self._ring_passive)
+               if x is not None]
+        return sum(t.numel() * t.element_size() for t in ts)
+
+    def _checkpoint(self, k: int):
+        """Interval checkpointing: the state at the start of interval k (slot
+        n_int: the state after the last step)."""
+        for c in range(self.dim):
+            self.ckpt_u[c][k].copy_(self.u[c])
+        if self.ckpt_passive is not None:
+            self.ckpt_passive[k].copy_(self.passive)
 
     # ------------------------------------------------------------ kernels
     def reset_to_identity(self, psi, psi_f, T_f):
@@ -422,9 +472,13 @@ class LFM_Simulator:
         j = n % self.reinit_every
         if self.store_passive is not None:
             K.store(self.passive, self.store_passive[n])
+        if self.ckpt_u is not None and j == 0:
+            self._checkpoint(n // self.reinit_every)
         self.step_flow_map(j, self.dt, control_force_para)
         if self.final_condition() and self.store_passive is not None:
             K.store(self.passive, self.store_passive[n + 1])
+        if self.final_condition() and self.ckpt_u is not None:
+            self._checkpoint((self.total_steps + self.reinit_every - 1) // self.reinit_every)
         return False, self.final_condition()
 
     def march_phi_grid(self, u):
@@ -464,7 +518,8 @@ class LFM_Simulator:
             K.viscous_force_2d(self.grid, cfg.viscosity, self.dx, self.u, self.vis)
         # write_velocity + RW_Cache("u"): the midpoint velocity of step n
         for c in range(self.dim):
-            K.store(self.u[c], self.store_mid[c][n])
+            if self.store_mid is not None:
+                K.store(self.u[c], self.store_mid[c][n])
             if self._ring is not None:
                 self._ring[j][c].copy_(self.u[c])
         self.march_phi_grid(self.u)
@@ -493,6 +548,11 @@ class LFM_Simulator:
         self.project(self.u)
         self._mask()  # 3D/lfm_midpoint_simulator.py:769-771
 
+        if self._recomputing:
+            # an interval replayed for the adjoint: it needs the midpoint
+            # velocities, passives and end-of-interval maps, not the reinit
+            # (the next interval's start state is its checkpoint)
+            return
         if j == self.reinit_every - 1:
             self.backtrack_psi_grid(self.reinit_every - 1, n - j)
             self.BFECC(self.init_u, self.u, self.err_u, self.T_f, self.psi_f, self.F_f, self.phi_f)
@@ -501,20 +561,54 @@ class LFM_Simulator:
             if cfg.add_passive_scalar:
                 self.BFECC_scalar(self.init_passive, self.passive, self.err_passive, self.psi, self.phi)
                 self.init_passive.copy_(self.passive)
-            k = n // self.reinit_every
-            self.store_phi[k].copy_(self.phi)
-            for c in range(self.dim):
-                self.store_phi_f[c][k].copy_(self.phi_f[c])
-                self.store_F_f[c][k].copy_(self.F_f[c])
+            self._store_maps(n // self.reinit_every)
             self.reset_to_identity(self.phi, self.phi_f, self.F_f)
             _copy_mac(self.init_u, self.u)
         elif n == self.total_steps - 1:
             # a final partial interval: keep its forward map for the adjoint
-            k = n // self.reinit_every
-            self.store_phi[k].copy_(self.phi)
-            for c in range(self.dim):
-                self.store_phi_f[c][k].copy_(self.phi_f[c])
-                self.store_F_f[c][k].copy_(self.F_f[c])
+            self._store_maps(n // self.reinit_every)
+
+    def _store_maps(self, k: int):
+        """The forward maps at the end of interval k (the adjoint's BFECC at j == 0);
+        with interval checkpointing the adjoint regenerates them instead."""
+        if self.store_phi is None:
+            return
+        self.store_phi[k].copy_(self.phi)
+        for c in range(self.dim):
+            self.store_phi_f[c][k].copy_(self.phi_f[c])
+            self.store_F_f[c][k].copy_(self.F_f[c])
+
+    def _recompute_interval(self, k: int):
+        """Interval checkpointing: replay the forward steps of interval k from its
+        checkpoint, keeping their midpoint velocities (ring) and passives
+        (passive ring, the interval end from checkpoint k+1), and leaving the
+        interval-end forward maps in phi, phi_f, F_f.  The replay runs the same
+        kernels on the same inputs as the forward, so every value equals the
+        forward's.  Only the forward's buffers are touched (with backward_u=False
+        the adjoint keeps none of its state in them)."""
+        R = self.reinit_every
+        n0 = k * R
+        last = min(n0 + R - 1, self.total_steps - 1)
+        saved = self.step_num[None]
+        for c in range(self.dim):
+            self.u[c].copy_(self.ckpt_u[c][k])
+        if self.ckpt_passive is not None:
+            self.passive.copy_(self.ckpt_passive[k])
+            self.init_passive.copy_(self.passive)
+        _copy_mac(self.init_u, self.u)
+        self.reset_to_identity(self.phi, self.phi_f, self.F_f)
+        self._recomputing = True
+        try:
+            for n in range(n0, last + 1):
+                self.step_num[None] = n
+                if self._ring_passive is not None:
+                    self._ring_passive[n - n0].copy_(self.passive)
+                self.step_flow_map(n - n0, self.dt)
+        finally:
+            self._recomputing = False
+            self.step_num[None] = saved
+        if self._ring_passive is not None:
+            self._ring_passive[last + 1 - n0].copy_(self.ckpt_passive[k + 1])
 
 
 class LFM_Diff_Simulator(LFM_Simulator):
@@ -675,8 +769,14 @@ class LFM_Diff_Simulator(LFM_Simulator):
         self.step_num[None] -= 1
         n = self.step_num[None]
         j = n % self.reinit_every
+        n0 = n - j
+        if self.ckpt_u is not None and n == min(n0 + self.reinit_every, self.total_steps) - 1:
+            self._recompute_interval(n // self.reinit_every)  # first adjoint step of this interval
         if self.cfg.add_passive_scalar and not self.cfg.backward_u:
-            K.store(self.store_passive[n + 1], self.passive)
+            if self._ring_passive is not None:
+                self.passive.copy_(self._ring_passive[n + 1 - n0])
+            else:
+                K.store(self.store_passive[n + 1], self.passive)
         self.backtrack_flow_map(j, self.dt, control_force_para)
         return False, n == 0
 
@@ -696,7 +796,10 @@ class LFM_Diff_Simulator(LFM_Simulator):
                     K.gaussian_force(g, dx, *params, force)
             self._adj_gaussian(self.adj_u, params)
         for c in range(self.dim):
-            K.store(self.store_mid[c][n], self.mid_u[c])
+            if self.store_mid is not None:
+                K.store(self.store_mid[c][n], self.mid_u[c])
+            else:
+                self.mid_u[c].copy_(self._ring[j][c])
         if self.vis is not None:  # 2D/vortex/lfm_midpoint_diff_simulator.py:270-271
             K.viscous_force_2d(g, cfg.viscosity, dx, self.mid_u, self.vis, adj=self.adj_u, part=self._vis_part,
                                dot=self.adj_viscous.tensor)
@@ -758,10 +861,11 @@ class LFM_Diff_Simulator(LFM_Simulator):
 
         if j == 0:
             k = n // self.reinit_every
-            self.phi.copy_(self.store_phi[k])
-            for c in range(self.dim):
-                self.phi_f[c].copy_(self.store_phi_f[c][k])
-                self.F_f[c].copy_(self.store_F_f[c][k])
+            if self.store_phi is not None:  # with interval checkpointing phi, F hold the replayed interval's maps
+                self.phi.copy_(self.store_phi[k])
+                for c in range(self.dim):
+                    self.phi_f[c].copy_(self.store_phi_f[c][k])
+                    self.F_f[c].copy_(self.store_F_f[c][k])
             self.BFECC(self.init_adj_u, self.adj_u, self.err_u, self.F_f, self.phi_f, self.T_f, self.psi_f)
             self.project(self.adj_u)
             _copy_mac(self.init_adj_u, self.adj_u)
@@ -771,7 +875,9 @@ class LFM_Diff_Simulator(LFM_Simulator):
                 _copy_mac(self.init_u, self.u)
             self._mask(adjoint=True)  # 3D/lfm_midpoint_diff_simulator.py:572-576
             if cfg.add_passive_scalar:
-                if cfg.trajectory_loss or not cfg.backward_u:
+                if self._ring_passive is not None:
+                    self.passive.copy_(self._ring_passive[0])
+                elif cfg.trajectory_loss or not cfg.backward_u:
                     K.store(self.store_passive[n], self.passive)
                 else:
                     self.BFECC_scalar(self.init_passive, self.passive, self.err_passive, self.phi, self.psi)

@@ -57,6 +57,14 @@ long long fm_launch_count(int reset);
  * to buf (at most len bytes, NUL-terminated) when buf is not NULL. */
 int fm_last_cuda_error(char *buf, int len);
 
+/* Programmatic dependent launch for the pressure solver's kernels (on by
+ * default): each kernel's CTAs may be scheduled while its stream predecessor
+ * finishes, and wait for it before their first memory access, hiding launch
+ * latency in the solver's chain of small kernels.  Results do not depend on
+ * it.  enable = 0 switches it off for later launches; returns the previous
+ * setting. */
+int fm_set_pdl(int enable);
+
 /* FP32 FMA throughput probe (no reference counterpart; measures the FP32 peak
  * the gather kernels are reported against): `blocks` CTAs of 256 threads each
  * run 16 independent FMA chains of `iters` steps -- scalar fmaf, or paired

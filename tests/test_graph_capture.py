@@ -103,3 +103,25 @@ def test_solvers_of_different_sizes_coexist(fm, cuda):
             s.project(u)
             st = s.stats(reset=True)
             assert st["solves"] == 1 and st["nonfinite"] == 0 and st["not_converged"] == 0
+
+
+def test_programmatic_dependent_launch_changes_no_result(fm, cuda):
+    """The solver kernels' programmatic dependent launch (on by default) only
+    overlaps launch latency: a gradient is bit-identical with it switched off,
+    eager and replayed from a graph."""
+    S, Cf, vx = _mods()
+    cfg = Cf.vortex2d_config(res=64, steps=10, reinit_every=5)
+    p = vx.VortexProblem(S.LFM_Diff_Simulator(config=cfg))
+    omt = p.final_vorticity(Cf.vortex2d_theta(9))
+    th = Cf.vortex2d_theta(3)
+    prev = fm._lib.set_pdl(True)
+    try:
+        l_on, d_on = p.gradient(th, omt)
+        p.capture(th, omt)
+        l_g, d_g = p.graph_gradient(th)
+        fm._lib.set_pdl(False)
+        l_off, d_off = p.gradient(th, omt)
+    finally:
+        fm._lib.set_pdl(prev)
+    assert l_on == l_off == l_g
+    assert np.array_equal(d_on, d_off) and np.array_equal(d_on, d_g)
