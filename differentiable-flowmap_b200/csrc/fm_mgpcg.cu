@@ -162,32 +162,64 @@ __device__ __forceinline__ void sum_partials(const double* __restrict__ part, do
 // ---------------------------------------------------------------------------
 // apply_bc + divergence + init(r = -div) + x = 0, with partial sums of r for
 // the recentring (3D/mgpcg.py:368-399, :76-84, :179-185).
+// Each thread takes kDivUnroll cells of its grid-stride sequence at a time and
+// issues all their face loads before any store, so 6 x kDivUnroll loads are in
+// flight (a plain grid-stride loop waits one memory latency per cell).  The
+// hoisting is safe: the only faces written are domain-wall faces, and every
+// cell that reads one replaces the loaded value by 0.  The per-thread sum runs
+// over the same cells in the same order as the plain loop.
+constexpr int kDivUnroll = 2;
+
 template <typename T, int D>
-__global__ void __launch_bounds__(kRedThreads) k_div_bc(fm_grid g, MacW<T> u, T* __restrict__ r, T* __restrict__ x,
-                                                        double* __restrict__ part) {
+__global__ void __launch_bounds__(kRedThreads, 4) k_div_bc(fm_grid g, MacW<T> u, T* __restrict__ r,
+                                                           T* __restrict__ x, double* __restrict__ part) {
   pdl_begin();
   const Shape cs = cell_shape(g);
-  double sum = 0;
-  FM_GRID_STRIDE(q, cs.size()) {
-    int I[3];
-    unflatten(cs, q, I[0], I[1], I[2]);
-    T acc = 0;
+  const unsigned n = (unsigned)cs.size();  // every field has fewer than 2^32 entries
+  const unsigned stride = gridDim.x * blockDim.x;
+  unsigned fstep[3];  // face offset of the high face of a cell, per component
 #pragma unroll
-    for (int c = 0; c < D; ++c) {
-      const Shape fs = face_shape(g, c);
-      const long ql = fs.idx(I[0], I[1], I[2]);
-      const long step = c == 0 ? (long)fs.s1 * fs.s2 : (c == 1 ? fs.s2 : 1);
-      const long qr = ql + step;
-      T vl = u.c[c][ql], vr = u.c[c][qr];
-      if (I[c] == 0) { vl = 0; u.c[c][ql] = 0; }
-      if (I[c] == axis_len(cs, c) - 1) { vr = 0; u.c[c][qr] = 0; }
-      if (c == 0) acc = vr - vl;
-      else { acc = acc + vr; acc = acc - vl; }
+  for (int c = 0; c < D; ++c) {
+    const Shape fs = face_shape(g, c);
+    fstep[c] = c == 0 ? (unsigned)fs.s1 * fs.s2 : (c == 1 ? (unsigned)fs.s2 : 1u);
+  }
+  double sum = 0;
+  for (unsigned base = blockIdx.x * blockDim.x + threadIdx.x; base < n; base += kDivUnroll * stride) {
+    T vl[kDivUnroll][3], vr[kDivUnroll][3];
+    unsigned qf[kDivUnroll][3];
+    int I[kDivUnroll][3];
+#pragma unroll
+    for (int m = 0; m < kDivUnroll; ++m) {
+      const unsigned q = base + m * stride;
+      if (q >= n) break;
+      unflatten(cs, q, I[m][0], I[m][1], I[m][2]);
+#pragma unroll
+      for (int c = 0; c < D; ++c) {
+        const Shape fs = face_shape(g, c);
+        const unsigned ql = ((unsigned)I[m][0] * fs.s1 + I[m][1]) * fs.s2 + I[m][2];
+        qf[m][c] = ql;
+        vl[m][c] = u.c[c][ql];
+        vr[m][c] = u.c[c][ql + fstep[c]];
+      }
     }
-    const T b = acc * (T)-1;
-    r[q] = b;
-    x[q] = 0;
-    sum += (double)b;
+#pragma unroll
+    for (int m = 0; m < kDivUnroll; ++m) {
+      const unsigned q = base + m * stride;
+      if (q >= n) break;
+      T acc = 0;
+#pragma unroll
+      for (int c = 0; c < D; ++c) {
+        T a = vl[m][c], b = vr[m][c];
+        if (I[m][c] == 0) { a = 0; u.c[c][qf[m][c]] = 0; }
+        if (I[m][c] == axis_len(cs, c) - 1) { b = 0; u.c[c][qf[m][c] + fstep[c]] = 0; }
+        if (c == 0) acc = b - a;
+        else { acc = acc + b; acc = acc - a; }
+      }
+      const T bq = acc * (T)-1;
+      r[q] = bq;
+      x[q] = 0;
+      sum += (double)bq;
+    }
   }
   block_reduce2(sum, 0.0, part + 2 * blockIdx.x);
 }
@@ -385,21 +417,65 @@ __global__ void k_fin_beta(DevState* st, const double* part, double eps, double 
 // ---------------------------------------------------------------------------
 // PCG vector kernels
 // ---------------------------------------------------------------------------
+// Neighbour values of cell (i, j, k) at 32-bit index q in the reference's
+// summation order (+i, -i, +j, -j, +k, -k), 0 where the neighbour is outside.
+// Summing all six (or four) from +0.0 gives the skipping sum bit for bit: a
+// round-to-nearest sum that starts at +0.0 is never -0.0, so adding +0.0
+// changes nothing.
+template <typename T, int D>
+__device__ __forceinline__ void nb_load(const T* x, const Shape& s, unsigned q, int i, int j, int k, T* v) {
+  const unsigned si = (unsigned)s.s1 * s.s2, sj = s.s2;
+  v[0] = i < s.s0 - 1 ? x[q + si] : (T)0;
+  v[1] = i > 0 ? x[q - si] : (T)0;
+  v[2] = j < s.s1 - 1 ? x[q + sj] : (T)0;
+  v[3] = j > 0 ? x[q - sj] : (T)0;
+  if (D == 3) {
+    v[4] = k < s.s2 - 1 ? x[q + 1] : (T)0;
+    v[5] = k > 0 ? x[q - 1] : (T)0;
+  }
+}
+template <typename T, int D>
+__device__ __forceinline__ T nb_add(const T* v) {
+  T acc = 0;
+#pragma unroll
+  for (int m = 0; m < 2 * D; ++m) acc += v[m];
+  return acc;
+}
+
+// The grid-stride vector kernels below take kVecUnroll cells of a thread's
+// sequence at a time and issue all their loads before any store (memory-level
+// parallelism); the per-thread partial sums keep the cell order of a plain
+// grid-stride loop.
+constexpr int kVecUnroll = 2;
+
 template <typename T, int D>
 __global__ void __launch_bounds__(kRedThreads) k_Ap_dot(Shape s, const T* __restrict__ p, T* __restrict__ Ap,
                                                         double* __restrict__ part, const DevState* st) {
   pdl_begin();
   if (st->done) return;
+  const unsigned n = (unsigned)s.size(), stride = gridDim.x * blockDim.x;
   double acc = 0;
-  FM_GRID_STRIDE(q, s.size()) {
-    int i, j, k;
-    unflatten(s, q, i, j, k);
-    T diag;
-    const T nb = nb_sum<T, D>(p, s, i, j, k, diag);
-    const T pv = p[q];
-    const T a = rn_sub(rn_mul(diag, pv), nb);
-    Ap[q] = a;
-    acc += (double)pv * (double)a;
+  for (unsigned base = blockIdx.x * blockDim.x + threadIdx.x; base < n; base += kVecUnroll * stride) {
+    T v[kVecUnroll][6], pv[kVecUnroll];
+    int nd[kVecUnroll];
+#pragma unroll
+    for (int m = 0; m < kVecUnroll; ++m) {
+      const unsigned q = base + m * stride;
+      if (q >= n) break;
+      int i, j, k;
+      unflatten(s, q, i, j, k);
+      nb_load<T, D>(p, s, q, i, j, k, v[m]);
+      pv[m] = p[q];
+      nd[m] = diag_of<D>(s, i, j, k);
+    }
+#pragma unroll
+    for (int m = 0; m < kVecUnroll; ++m) {
+      const unsigned q = base + m * stride;
+      if (q >= n) break;
+      const T a = rn_sub(rn_mul((T)nd[m], pv[m]), nb_add<T, D>(v[m]));
+      Ap[q] = a;
+      acc += (double)pv[m] * (double)a;
+    }
   }
   block_reduce2(acc, 0.0, part + 2 * blockIdx.x);
 }
@@ -536,25 +612,47 @@ __global__ void __launch_bounds__(kPairBX* kPairBY) k_smooth_first_pair(Shape s,
 }
 
 // smooth(l, phase) (3D/mgpcg.py:170-177); with part != nullptr also z.r over all cells.
+// A half-sweep reads only cells of the other colour and writes only cells of
+// colour `phase`, so the hoisted loads never see a value written in this launch.
 template <typename T, int D, bool DOT>
 __global__ void __launch_bounds__(kRedThreads) k_smooth(Shape s, const T* __restrict__ r, T* z, int phase,
                                                         double* __restrict__ part, const DevState* st) {
   pdl_begin();
   if (st->done) return;
+  const unsigned n = (unsigned)s.size(), stride = gridDim.x * blockDim.x;
   double acc = 0;
-  FM_GRID_STRIDE(q, s.size()) {
-    int i, j, k;
-    unflatten(s, q, i, j, k);
-    T zv;
-    if (parity<D>(i, j, k) == phase) {
-      T diag;
-      const T nb = nb_sum<T, D>(z, s, i, j, k, diag);
-      zv = div_nd(r[q] + nb, diag_of<D>(s, i, j, k));
-      z[q] = zv;
-    } else {
-      zv = z[q];
+  for (unsigned base = blockIdx.x * blockDim.x + threadIdx.x; base < n; base += kVecUnroll * stride) {
+    T v[kVecUnroll][6], rv[kVecUnroll], zo[kVecUnroll];
+    int nd[kVecUnroll];
+    bool upd[kVecUnroll];
+#pragma unroll
+    for (int m = 0; m < kVecUnroll; ++m) {
+      const unsigned q = base + m * stride;
+      if (q >= n) break;
+      int i, j, k;
+      unflatten(s, q, i, j, k);
+      upd[m] = parity<D>(i, j, k) == phase;
+      rv[m] = r[q];
+      if (upd[m]) {
+        nb_load<T, D>(z, s, q, i, j, k, v[m]);
+        nd[m] = diag_of<D>(s, i, j, k);
+      } else {
+        zo[m] = z[q];
+      }
     }
-    if (DOT) acc += (double)zv * (double)r[q];
+#pragma unroll
+    for (int m = 0; m < kVecUnroll; ++m) {
+      const unsigned q = base + m * stride;
+      if (q >= n) break;
+      T zv;
+      if (upd[m]) {
+        zv = div_nd(rv[m] + nb_add<T, D>(v[m]), nd[m]);
+        z[q] = zv;
+      } else {
+        zv = zo[m];
+      }
+      if (DOT) acc += (double)zv * (double)rv[m];
+    }
   }
   if (DOT) block_reduce2(acc, 0.0, part + 2 * blockIdx.x);
 }
