@@ -321,7 +321,26 @@ def run_vortex2d(a):
     theta = C.vortex2d_theta(0)
     p32 = problem(torch.float32, 1e-6)
     omt = p32.final_vorticity(C.vortex2d_theta(1))
-    ms, loss, dth = timed(p32, omt)
+    ms_eager, loss_e, dth_e = timed(p32, omt)
+    # the headline: the same gradient recorded once as a CUDA graph and replayed (no obstacle: the masked
+    # solver polls its convergence from the host and is not capturable)
+    graphed = not obstacle
+    if graphed:
+        p32.capture(theta, omt)
+        for _ in range(a.warmup):
+            p32.graph_gradient(theta)
+        torch.cuda.synchronize(dev)
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record()
+        for _ in range(a.steps):
+            loss, dth = p32.graph_gradient(theta)
+        e1.record()
+        torch.cuda.synchronize(dev)
+        ms = e0.elapsed_time(e1) / a.steps
+        if loss != loss_e or not np.array_equal(dth, dth_e):
+            raise RuntimeError("graph replay differs from the eager gradient")
+    else:
+        ms, loss, dth = ms_eager, loss_e, dth_e
     # FP64 reference: solved to its floor (masked solves stall near rTr ~ 1e-15, so a cap of 100 iterations)
     p64 = problem(torch.float64, 1e-20, max_iters=100 if obstacle else 400)
     l64, d64 = p64.gradient(theta, omt.double())
@@ -335,7 +354,9 @@ def run_vortex2d(a):
             "config": {"workload": "2D vortex optimisation gradient, 256^2, dt 1/512, reinit 10, RK2, 12 parameters"
                                    + (", synthetic leaf obstacle (solid-aware MGPCG, mask kernels)" if obstacle else ""),
                        "theta_seed": 0, "target_seed": 1,
-                       "obstacle_cells": int(mask.sum()) if obstacle else 0},
+                       "obstacle_cells": int(mask.sum()) if obstacle else 0,
+                       "launch": "one CUDA graph per gradient (capture_gradient)" if graphed else "eager"},
+            "eager": {"grads_per_s": 1e3 / ms_eager, "ms": ms_eager},
             "loss": loss, "dtheta": [float(x) for x in dth],
             "solver": "relative z.r 1e-6",
             "dtheta_rel_err_vs_fp64": float(np.linalg.norm(dth - d64) / np.linalg.norm(d64)),
