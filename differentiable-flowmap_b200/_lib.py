@@ -109,6 +109,7 @@ SIGNATURES = {
     "fm_solid_vcycle": [P, P, P, P],
     "fm_solid_solve": [P, P, P, P, C.POINTER(I), C.POINTER(D)],
     "fm_solid_project": [P, P, P, P, P, P, C.POINTER(I), C.POINTER(D)],
+    "fm_solid_stats": [P, P, I, C.POINTER(MGStats)],
     "fm_mask_velocity": [GP, I, P, P, P, P, P, P],
     "fm_mask_passive": [GP, I, P, P, I, P],
     "fm_viscous_force_2d": [GP, I, D, D, P, P, P, P, P, P, P, P, P],

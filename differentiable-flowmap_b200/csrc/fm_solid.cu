@@ -52,7 +52,45 @@ struct State {
   double alpha, beta, mean;
   int done, iters, converged, max_iters;
   double abs_tol, rel_tol, eps;
+  int loops;  // device-side loop bodies run in this solve (a hard bound on the WHILE node)
 };
+
+// Outcome of every solve, accumulated on the device (fm_solid_stats).
+struct Stats {
+  long long solves, iterations, not_converged, nonfinite, bodies;
+  int last_iters, max_iters_seen;
+  double last_rtr;
+};
+
+// The solve's scalars from the parameters (replaces a host copy, so that a
+// recorded graph does not depend on host memory).
+__global__ void k_state_init(State* st, int max_iters, double abs_tol, double rel_tol, double eps) {
+  State h{};
+  h.max_iters = max_iters;
+  h.abs_tol = abs_tol;
+  h.rel_tol = rel_tol;
+  h.eps = eps;
+  *st = h;
+}
+
+// Device mode: the WHILE node runs the next PCG iteration while the solve is
+// not done; the body count is bounded by max_iters + 1 whatever the flags say.
+__global__ void k_loop_cond(cudaGraphConditionalHandle h, State* st, Stats* stats) {
+  st->loops += 1;
+  stats->bodies += 1;
+  cudaGraphSetConditional(h, (!st->done && st->loops <= st->max_iters) ? 1u : 0u);
+}
+
+__global__ void k_stats(const State* st, Stats* out) {
+  const bool nf = !isfinite(st->rtr);
+  out->solves += 1;
+  out->iterations += st->iters;
+  out->nonfinite += nf ? 1 : 0;
+  out->not_converged += (!nf && !st->converged) ? 1 : 0;
+  out->last_iters = st->iters;
+  if (st->iters > out->max_iters_seen) out->max_iters_seen = st->iters;
+  out->last_rtr = st->rtr;
+}
 
 __device__ __forceinline__ void idx3(const Shape& s, long q, int* I) {
   int i, j, k;
@@ -527,10 +565,15 @@ struct fm_solid {
   double* part;
   fm::solid::State* st;
   fm::solid::State* st_host;  // pinned
+  fm::solid::Stats* stats;
+  fm::solid::Stats* stats_host;  // pinned
   // check_every PCG iterations captured once as a graph (replayed per poll)
   cudaStream_t cap;
   cudaGraphExec_t chunk;
   size_t chunk_nodes;
+  // device mode (check_every == 0): a graph with a conditional WHILE node
+  cudaGraphExec_t loop;
+  long long loop_kernels;  // kernels per loop body
 };
 
 namespace fm {
@@ -640,20 +683,83 @@ void iteration(fm_solid* S, cudaStream_t s) {
   launch(k_update_p<T>, nb, kThreads, 0, s, n, p, (const T*)S->z[0], fl, (const State*)st);
 }
 
+// The PCG loop as a conditional WHILE node appended to `graph` after `deps`
+// (the body, one iteration and k_loop_cond, recorded from S->cap); *node_out
+// receives the node.
+template <typename T, int D>
+int add_loop_node(fm_solid* S, cudaGraph_t graph, const cudaGraphNode_t* deps, size_t ndeps, cudaGraphNode_t* node_out) {
+  cudaGraphConditionalHandle h;
+  cudaError_t e;
+  if ((e = cudaGraphConditionalHandleCreate(&h, graph, 1, cudaGraphCondAssignDefault)) != cudaSuccess)
+    return cuda_fail(e);
+  cudaGraphNodeParams cp = {cudaGraphNodeTypeConditional};
+  cp.conditional.handle = h;
+  cp.conditional.type = cudaGraphCondTypeWhile;
+  cp.conditional.size = 1;
+  if ((e = cudaGraphAddNode(node_out, graph, deps, ndeps, &cp)) != cudaSuccess) return cuda_fail(e);
+  cudaGraph_t body = cp.conditional.phGraph_out[0];
+  if ((e = cudaStreamBeginCaptureToGraph(S->cap, body, nullptr, nullptr, 0, cudaStreamCaptureModeThreadLocal)) !=
+      cudaSuccess)
+    return cuda_fail(e);
+  const long long before = g_launch_count.load();
+  iteration<T, D>(S, S->cap);
+  launch(k_loop_cond, 1, 1, 0, S->cap, h, S->st, S->stats);
+  S->loop_kernels = g_launch_count.load() - before;
+  g_launch_count.fetch_sub(S->loop_kernels);  // counted per body run (fm_solid_stats)
+  cudaGraph_t captured = nullptr;
+  if ((e = cudaStreamEndCapture(S->cap, &captured)) != cudaSuccess) return cuda_fail(e);
+  return FM_OK;
+}
+
+// Device mode: the PCG loop without host polling.  Outside a capture it is one
+// launch of a graph built once; inside a caller's capture the WHILE node is
+// appended to the graph being recorded.
+template <typename T, int D>
+int device_loop(fm_solid* S, cudaStream_t s, bool capturing) {
+  if (capturing) {
+    cudaStreamCaptureStatus cs;
+    cudaGraph_t graph = nullptr;
+    const cudaGraphNode_t* deps = nullptr;
+    size_t ndeps = 0;
+    cudaError_t e;
+    if ((e = cudaStreamGetCaptureInfo(s, &cs, nullptr, &graph, &deps, &ndeps)) != cudaSuccess) return cuda_fail(e);
+    cudaGraphNode_t node;
+    const int st = add_loop_node<T, D>(S, graph, deps, ndeps, &node);
+    if (st) return st;
+    if ((e = cudaStreamUpdateCaptureDependencies(s, &node, 1, cudaStreamSetCaptureDependencies)) != cudaSuccess)
+      return cuda_fail(e);
+    return FM_OK;
+  }
+  if (!S->loop) {
+    cudaGraph_t graph = nullptr;
+    cudaError_t e;
+    if ((e = cudaGraphCreate(&graph, 0)) != cudaSuccess) return cuda_fail(e);
+    cudaGraphNode_t node;
+    int st = add_loop_node<T, D>(S, graph, nullptr, 0, &node);
+    if (!st && (e = cudaGraphInstantiate(&S->loop, graph, 0)) != cudaSuccess) {
+      S->loop = nullptr;
+      st = cuda_fail(e);
+    }
+    cudaGraphDestroy(graph);
+    if (st) return st;
+  }
+  cudaError_t e;
+  if ((e = cudaGraphLaunch(S->loop, s)) != cudaSuccess) return cuda_fail(e);
+  return FM_OK;
+}
+
 template <typename T, int D>
 int solve(fm_solid* S, const void* b, double k, void* x, cudaStream_t s, int* iters, double* rtr) {
-  // the masked solve polls its convergence word from the host: it cannot be
-  // recorded into a caller's CUDA graph
+  // check_every == 0: device-side loop (capturable into a caller's graph when
+  // no outcome is read back); otherwise the host polls every check_every
+  // iterations, which cannot be recorded
   cudaStreamCaptureStatus cs = cudaStreamCaptureStatusNone;
-  if (cudaStreamIsCapturing(s, &cs) != cudaSuccess || cs != cudaStreamCaptureStatusNone) return FM_ERR_ARG;
+  if (cudaStreamIsCapturing(s, &cs) != cudaSuccess) return FM_ERR_CUDA;
+  const bool capturing = cs != cudaStreamCaptureStatusNone;
+  const bool device = S->P.check_every == 0;
+  if (capturing && (!device || iters || rtr)) return FM_ERR_ARG;
   const long n = S->sh[0].size();
-  State h{};
-  h.max_iters = S->P.max_iters;
-  h.abs_tol = S->P.abs_tol;
-  h.rel_tol = S->P.rel_tol;
-  h.eps = S->P.eps;
-  *S->st_host = h;
-  if (cudaMemcpyAsync(S->st, S->st_host, sizeof(State), cudaMemcpyHostToDevice, s) != cudaSuccess) return FM_ERR_CUDA;
+  launch(k_state_init, 1, 1, 0, s, S->st, S->P.max_iters, S->P.abs_tol, S->P.rel_tol, S->P.eps);
   State* st = S->st;
   T* r = (T*)S->r[0];
   T* z = (T*)S->z[0];
@@ -671,7 +777,22 @@ int solve(fm_solid* S, const void* b, double k, void* x, cudaStream_t s, int* it
   launch(k_update_p<T>, nb, kThreads, 0, s, n, p, (const T*)z, fl, (const State*)st);
   launch(k_dot<T>, kRedBlocks, kThreads, 0, s, n, (const T*)z, (const T*)r, fl, S->part, (const State*)st);
   launch(k_fin, 1, kFinThreads, 0, s, 0, (const double*)S->part, st, n);
-  const int every = S->P.check_every > 0 ? S->P.check_every : 4;
+  if (device) {
+    const int dl = device_loop<T, D>(S, s, capturing);
+    if (dl) return dl;
+    launch(k_stats, 1, 1, 0, s, (const State*)st, S->stats);
+    if (x != nullptr && x != S->x) cudaMemcpyAsync(x, S->x, n * sizeof(T), cudaMemcpyDeviceToDevice, s);
+    if (!iters && !rtr) return check_cuda();  // asynchronous: the outcome goes to fm_solid_stats
+    if (cudaMemcpyAsync(S->st_host, st, sizeof(State), cudaMemcpyDeviceToHost, s) != cudaSuccess) return FM_ERR_CUDA;
+    if (cudaStreamSynchronize(s) != cudaSuccess) return FM_ERR_CUDA;
+    if (iters) *iters = S->st_host->iters;
+    if (rtr) *rtr = S->st_host->rtr;
+    const int cst = check_cuda();
+    if (cst) return cst;
+    if (!isfinite(S->st_host->rtr)) return FM_ERR_NONFINITE;
+    return S->st_host->converged ? FM_OK : FM_ERR_NOT_CONVERGED;
+  }
+  const int every = S->P.check_every;
   if (!S->chunk) {
     // capture check_every iterations once; the captured kernels are counted per replay
     const long long before = g_launch_count.load();
@@ -694,6 +815,7 @@ int solve(fm_solid* S, const void* b, double k, void* x, cudaStream_t s, int* it
     if (cudaStreamSynchronize(s) != cudaSuccess) return FM_ERR_CUDA;
     if (S->st_host->done) break;
   }
+  launch(k_stats, 1, 1, 0, s, (const State*)st, S->stats);
   if (cudaMemcpyAsync(S->st_host, st, sizeof(State), cudaMemcpyDeviceToHost, s) != cudaSuccess) return FM_ERR_CUDA;
   if (cudaStreamSynchronize(s) != cudaSuccess) return FM_ERR_CUDA;
   if (x != nullptr && x != S->x) cudaMemcpyAsync(x, S->x, n * sizeof(T), cudaMemcpyDeviceToDevice, s);
@@ -713,7 +835,7 @@ int project(fm_solid* S, void* const* u, void* p_out, cudaStream_t s, int* iters
   launch(k_div<T, D>, blocks_for(S->sh[0].size()), kThreads, 0, s, g, (const T*)u[0], (const T*)u[1],
          (const T*)(D == 3 ? u[2] : nullptr), (const uint8_t*)S->fl[0], (T*)S->div);
   const int st = solve<T, D>(S, S->div, -1.0, nullptr, s, iters, rtr);
-  if (st != FM_OK && st != FM_ERR_NOT_CONVERGED) return st;
+  if (st != FM_OK && st != FM_ERR_NOT_CONVERGED && st != FM_ERR_NONFINITE) return st;
   for (int c = 0; c < D; ++c) {
     launch(k_grad<T, D>, blocks_for(face_shape(g, c).size()), kThreads, 0, s, g, c, (T*)u[c], (const T*)S->x);
     launch(k_bc<T, D>, blocks_for(face_shape(g, c).size()), kThreads, 0, s, g, c, (T*)u[c], (const uint8_t*)S->fl[0]);
@@ -741,8 +863,11 @@ int fm_solid_destroy(fm_solid* S) {
   cudaFree(S->div);
   cudaFree(S->part);
   cudaFree(S->st);
+  cudaFree(S->stats);
   if (S->st_host) cudaFreeHost(S->st_host);
+  if (S->stats_host) cudaFreeHost(S->stats_host);
   if (S->chunk) cudaGraphExecDestroy(S->chunk);
+  if (S->loop) cudaGraphExecDestroy(S->loop);
   if (S->cap) cudaStreamDestroy(S->cap);
   free(S);
   return FM_OK;
@@ -771,7 +896,7 @@ int fm_solid_create(const fm_grid* g, int dtype, const fm_mg_params* params, con
   const int st = validate_grid(g, dtype);
   if (st) return st;
   const fm_mg_params& P = *params;
-  if (P.levels < 1 || P.levels > 16 || P.pre_post < 0 || P.bottom < 0 || P.max_iters < 1 ||
+  if (P.levels < 1 || P.levels > 16 || P.pre_post < 0 || P.bottom < 0 || P.max_iters < 1 || P.check_every < 0 ||
       (P.bottom_mode != 0 && P.bottom_mode != 1) || P.coarse_bf16)
     return FM_ERR_ARG;
   for (int a = 0; a < g->dim; ++a)
@@ -798,7 +923,10 @@ int fm_solid_create(const fm_grid* g, int dtype, const fm_mg_params* params, con
        cudaMalloc((void**)&S->part, solid::kRedBlocks * sizeof(double)) == cudaSuccess &&
        cudaMalloc((void**)&S->st, sizeof(solid::State)) == cudaSuccess &&
        cudaMallocHost((void**)&S->st_host, sizeof(solid::State)) == cudaSuccess &&
+       cudaMalloc((void**)&S->stats, sizeof(solid::Stats)) == cudaSuccess &&
+       cudaMallocHost((void**)&S->stats_host, sizeof(solid::Stats)) == cudaSuccess &&
        cudaStreamCreateWithFlags(&S->cap, cudaStreamNonBlocking) == cudaSuccess;
+  if (ok) ok = cudaMemset(S->stats, 0, sizeof(solid::Stats)) == cudaSuccess;
   if (!ok) {
     fm_solid_destroy(S);
     return FM_ERR_CUDA;
@@ -822,6 +950,33 @@ int fm_solid_create(const fm_grid* g, int dtype, const fm_mg_params* params, con
   }
   *out = S;
   return check_cuda();
+}
+
+int fm_solid_stats(fm_solid* S, void* stream, int reset, fm_mg_stats* out) {
+  using namespace fm::solid;
+  if (!S || !out) return FM_ERR_ARG;
+  cudaStream_t s = (cudaStream_t)stream;
+  if (cudaMemcpyAsync(S->stats_host, S->stats, sizeof(Stats), cudaMemcpyDeviceToHost, s) != cudaSuccess)
+    return FM_ERR_CUDA;
+  if (cudaStreamSynchronize(s) != cudaSuccess) return FM_ERR_CUDA;
+  const Stats h = *S->stats_host;
+  out->solves = h.solves;
+  out->iterations = h.iterations;
+  out->not_converged = h.not_converged;
+  out->nonfinite = h.nonfinite;
+  out->last_iters = h.last_iters;
+  out->max_iters_seen = h.max_iters_seen;
+  out->last_rtr = h.last_rtr;
+  fm::count_launch(h.bodies * S->loop_kernels);  // kernels run inside device-mode loops since the last read
+  Stats z = h;
+  z.bodies = 0;
+  if (reset) z.solves = z.iterations = z.not_converged = z.nonfinite = 0, z.last_iters = z.max_iters_seen = 0,
+             z.last_rtr = 0.0;
+  *S->stats_host = z;
+  if (cudaMemcpyAsync(S->stats, S->stats_host, sizeof(Stats), cudaMemcpyHostToDevice, s) != cudaSuccess)
+    return FM_ERR_CUDA;
+  if (cudaStreamSynchronize(s) != cudaSuccess) return FM_ERR_CUDA;
+  return fm::check_cuda();
 }
 
 int fm_solid_vcycle(fm_solid* S, const void* r, void* z, void* stream) {

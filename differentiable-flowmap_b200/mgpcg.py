@@ -173,8 +173,10 @@ class SolidMGPCG:
         self.dtype = dtype
         if levels is None:
             levels = int(math.log2(min(self.N))) - base_level + 1
+        if int(check_every) < 0:
+            raise _lib.FlowmapError(2, "check_every must be >= 0")
         self.params = _lib.MGParams(levels, pre_post, bottom, bottom_mode, max_iters, abs_tol, rel_tol, eps,
-                                    max(int(check_every), 1), 0)
+                                    int(check_every), 0)
         self.raise_on_nonconvergence = raise_on_nonconvergence
         self.mask = self._as_mask(mask)
         self._h = C.c_void_p()
@@ -196,7 +198,11 @@ class SolidMGPCG:
     def n_mg_levels(self) -> int:
         return self.params.levels
 
-    device_mode = False
+    @property
+    def device_mode(self) -> bool:
+        """check_every == 0: the PCG loop runs on the device; project() returns
+        at once and the outcome is read by stats()."""
+        return self.params.check_every == 0
 
     def set_mask(self, mask, stream=None):
         self.mask = self._as_mask(mask)
@@ -239,6 +245,11 @@ class SolidMGPCG:
             if tuple(x.shape) != self.grid.face_shape(c) or x.dtype != self.dtype:
                 raise _lib.FlowmapError(1, f"project: component {c} shape/dtype mismatch")
         ps = [_lib.ptr(x) for x in u] + [None] * (3 - len(u))
+        if self.device_mode:
+            st = _lib.lib().fm_solid_project(self._h, ps[0], ps[1], ps[2], _lib.ptr(p_out), _lib.stream_ptr(stream),
+                                             None, None)
+            _lib.check(st, "fm_solid_project")
+            return
         it, rtr = C.c_int(0), C.c_double(0)
         st = _lib.lib().fm_solid_project(self._h, ps[0], ps[1], ps[2], _lib.ptr(p_out), _lib.stream_ptr(stream),
                                          C.byref(it), C.byref(rtr))
@@ -261,11 +272,16 @@ class SolidMGPCG:
         return z
 
     def stats(self, reset: bool = False, stream=None) -> dict:
-        out = dict(self._stats)
+        """Cumulative solver outcome, counted on the device (synchronises the stream)."""
+        s = _lib.MGStats()
+        _lib.check(_lib.lib().fm_solid_stats(self._h, _lib.stream_ptr(stream), int(reset), C.byref(s)),
+                   "fm_solid_stats")
         if reset:
             for k in self._stats:
                 self._stats[k] = 0.0 if k == "last_rtr" else 0
-        return out
+        return {"solves": s.solves, "iterations": s.iterations, "not_converged": s.not_converged,
+                "nonfinite": s.nonfinite, "last_iters": s.last_iters, "max_iters_seen": s.max_iters_seen,
+                "last_rtr": s.last_rtr}
 
     def Poisson(self, *u, verbose: bool = False):
         self.project(u)

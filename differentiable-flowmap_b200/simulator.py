@@ -222,7 +222,7 @@ class LFM_Simulator:
             self.solver = SolidMGPCG(g.shape, self.boundary_mask, dt_, base_level=sc.base_level, levels=sc.levels,
                                      pre_post=sc.pre_post, bottom=sc.bottom, bottom_mode=sc.bottom_mode,
                                      max_iters=sc.max_iters, abs_tol=sc.abs_tol, rel_tol=sc.rel_tol, eps=sc.eps,
-                                     check_every=sc.check_every or 4)
+                                     check_every=sc.check_every)
         else:
             self.solver = MGPCG(g.shape, dt_, base_level=sc.base_level, levels=sc.levels, pre_post=sc.pre_post,
                                 bottom=sc.bottom, bottom_mode=sc.bottom_mode, max_iters=sc.max_iters,
@@ -935,12 +935,12 @@ class LFM_Diff_Simulator(LFM_Simulator):
         The inputs must be device tensors that stay alive: the graph copies from
         them on every replay, so refill them in place between replays.  One eager
         gradient runs first (it creates every lazily allocated buffer outside the
-        capture and leaves the same results).  Not available with control forces, a
-        trajectory loss, an obstacle mask (the masked solver polls its convergence
-        from the host) or a host-checked solver (check_every > 0)."""
+        capture and leaves the same results).  Not available with control forces (their
+        parameters are staged from the host every step), a trajectory loss (read on
+        the host) or a host-checked solver (check_every > 0)."""
         cfg = self.cfg
-        if cfg.add_control_force or cfg.trajectory_loss or self.boundary_mask is not None:
-            raise FlowmapError(2, "capture_gradient: control forces, trajectory loss and obstacles are not capturable")
+        if cfg.add_control_force or cfg.trajectory_loss:
+            raise FlowmapError(2, "capture_gradient: control forces and a trajectory loss are not capturable")
         if not getattr(self.solver, "device_mode", False):
             raise FlowmapError(2, "capture_gradient needs the device-side solver (check_every = 0)")
         for x in list(u0) + [passive0, target_passive, target_vorticity]:

@@ -336,11 +336,17 @@ typedef struct fm_solid fm_solid;
 /* Allocates a solid-aware MG hierarchy (2D/vortex/mgpcg_solid.py:24-79,
  * MGPCG_2_solid :370-382; dimension-generic) and, when mask is not NULL,
  * downsamples it (downsample_bm, :114-127: a coarse cell is solid only when
- * all its children are).  params as for fm_mgpcg_create (check_every >= 1 is
- * the polling interval, 0 means 4; coarse_bf16 must be 0).  The only
- * allocating call. */
+ * all its children are).  params as for fm_mgpcg_create: check_every >= 1 is
+ * the host polling interval; 0 runs the PCG loop on the device (a graph
+ * conditional WHILE node: no host synchronisation, and a solve on a capturing
+ * stream is recorded into the caller's graph); coarse_bf16 must be 0.  The
+ * only allocating call. */
 int fm_solid_create(const fm_grid *g, int dtype, const fm_mg_params *params, const float *mask, fm_solid **out);
 int fm_solid_destroy(fm_solid *solver);
+/* Cumulative outcome of the solver's solves (as fm_mgpcg_stats; synchronises
+ * `stream`).  With check_every == 0 and iters/rtr NULL, fm_solid_solve and
+ * fm_solid_project return before the solve ends and report only here. */
+int fm_solid_stats(fm_solid *solver, void *stream, int reset, fm_mg_stats *out);
 /* Re-derives the level masks from a (new) mask; the reference downsamples
  * before every solve (:270-272). */
 int fm_solid_set_mask(fm_solid *solver, const float *mask, void *stream);

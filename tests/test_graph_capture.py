@@ -78,11 +78,40 @@ def test_batched_graphs_equal_eager(fm, cuda):
 def test_capture_refuses_host_polled_configs(fm, cuda):
     S, Cf, _ = _mods()
     mask = Cf.leaf_mask(32)
-    cfg = Cf.vortex2d_config(res=32, steps=4, reinit_every=2, boundary_mask=mask)
+    cfg = Cf.vortex2d_config(res=32, steps=4, reinit_every=2, boundary_mask=mask, check_every=4)
     sim = S.LFM_Diff_Simulator(config=cfg)
     u0 = [torch.zeros(sim.grid.face_shape(c), device="cuda") for c in range(2)]
     with pytest.raises(S.FlowmapError):
         sim.capture_gradient(u0, target_vorticity=torch.zeros(sim.grid.shape, device="cuda"))
+
+
+def test_obstacle_gradient_device_loop_and_graph(fm, cuda):
+    """The masked solver's device-side PCG loop (check_every = 0) equals host
+    polling bit for bit, and a masked gradient replays from one graph."""
+    S, Cf, vx = _mods()
+    mask = Cf.leaf_mask(64)
+    th, tgt = Cf.vortex2d_theta(3), Cf.vortex2d_theta(9)
+
+    def problem(check_every):
+        cfg = Cf.vortex2d_config(res=64, steps=10, reinit_every=5, boundary_mask=mask, check_every=check_every)
+        return vx.VortexProblem(S.LFM_Diff_Simulator(config=cfg))
+
+    host, dev = problem(4), problem(0)
+    assert not host.sim.solver.device_mode and dev.sim.solver.device_mode
+    omt = host.final_vorticity(tgt)
+    host.sim.solver.stats(reset=True)  # count the gradient's solves only
+    lh, dh = host.gradient(th, omt)
+    sh = host.sim.solver_stats
+    ld, dd = dev.gradient(th, omt)
+    sd = dev.sim.solver_stats
+    assert lh == ld and np.array_equal(dh, dd)
+    for k in ("solves", "iterations", "not_converged", "nonfinite", "max_iters_seen"):
+        assert sh[k] == sd[k], k
+    dev.capture(th, omt)
+    lg, dg = dev.graph_gradient(th)
+    assert lg == lh and np.array_equal(dg, dh)
+    st = dev.graph.stats()
+    assert st["solves"] == sd["solves"] and st["iterations"] == sd["iterations"]
 
 
 def test_solvers_of_different_sizes_coexist(fm, cuda):
