@@ -430,7 +430,15 @@ def run_vortex2d_batch(a):
     for n, t in tuned.items():
         for k, th in t.items():
             T.set_threads(k, (n, n), th)
-    # every instance's gradient recorded as one CUDA graph, replayed on its stream
+    # every instance's gradient recorded as one CUDA graph, replayed on its stream; first with every block
+    # size at the default 256, then (the headline) with the tuned sizes
+    for n in bat.tuning:
+        T.reset((n, n))
+    bat.capture()
+    ms_graph_default, _ = timed(True, graphs=True)
+    for n, t in tuned.items():
+        for k, th in t.items():
+            T.set_threads(k, (n, n), th)
     bat.capture()
     ms_graph, graph = timed(True, graphs=True)
     errs = {i: float(np.linalg.norm(dc - ds) / np.linalg.norm(ds)) for i, (_, dc), (_, ds) in zip(mine, graph, seq)}
@@ -457,6 +465,8 @@ def run_vortex2d_batch(a):
                 "autotuned_block_sizes": {str(k): v for k, v in tuned.items()},
                 "untuned_256_threads": {"grads_per_s": n * 1e3 / ms_default, "ms_per_batch": ms_default,
                                         "note": "eager concurrent"},
+                "graphs_untuned_256_threads": {"grads_per_s": n * 1e3 / ms_graph_default,
+                                               "ms_per_batch": ms_graph_default},
                 "graph_over_sequential": ms_seq / ms_graph,
                 "per_instance_dtheta_rel_err_vs_unbatched": [errs[i] for i in range(n)]}
         print(json.dumps(line), flush=True)

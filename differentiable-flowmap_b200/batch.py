@@ -103,9 +103,12 @@ class BatchedVortex:
         if autotune:
             from . import tune
 
+            # each shape timed as it runs here: as many concurrent copies as the
+            # batch has instances
             with torch.cuda.device(self.device):
                 for n in sorted({sizes[i] for i in self.indices}):
-                    self.tuning[n] = tune.autotune((n, n), dtype, rk=2, device=self.device)
+                    self.tuning[n] = tune.autotune((n, n), dtype, rk=2, device=self.device,
+                                                   concurrency=len(self.indices))
         for i in self.indices:
             n = sizes[i]
             cfg = vortex2d_config(res=n, steps=steps, reinit_every=reinit_every, dtype=dtype, rel_tol=rel_tol)

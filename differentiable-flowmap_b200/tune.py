@@ -6,8 +6,11 @@ change only how the grid fills the 148 SMs -- which matters for the small 2D
 grids of the batched vortex instances (a 128^2 face grid is 64 blocks of 256).
 ``autotune(shape)`` times each candidate block size on seeded fields of that
 grid shape with CUDA events, keeps the fastest per kernel class in the
-library's table (fm_tune_set) and returns the timings.  Results are cached per
-(shape, dtype, RK order) for the process.
+library's table (fm_tune_set) and returns the timings.  With concurrency = k
+the candidate runs as k copies on k streams at once (each on its own fields),
+which is how the kernel meets the GPU inside a batch of concurrent instances:
+a block size that is fastest alone can lose under contention.  Results are
+cached per (shape, dtype, RK order, concurrency) for the process.
 """
 from __future__ import annotations
 
@@ -76,27 +79,40 @@ def _workloads(shape, dtype, rk, device):
 
 
 def autotune(shape: Sequence[int], dtype=torch.float32, rk: int = 2, candidates: Sequence[int] = CANDIDATES,
-             reps: int = 20, device=None) -> Dict[str, dict]:
+             reps: int = 20, device=None, concurrency: int = 1) -> Dict[str, dict]:
     """Pick and store the fastest block size per kernel class for ``shape``;
-    returns {kind: {"threads": best, "us": {candidate: microseconds}}}."""
-    key = (tuple(shape), dtype, rk, tuple(candidates))
+    returns {kind: {"threads": best, "us": {candidate: microseconds per launch
+    round (all ``concurrency`` copies)}}}."""
+    key = (tuple(shape), dtype, rk, tuple(candidates), int(concurrency))
     if key in _cache:
         return _cache[key]
     dev = torch.device(device) if device is not None else torch.device("cuda", torch.cuda.current_device())
-    work = _workloads(shape, dtype, rk, dev)
+    k = max(int(concurrency), 1)
+    works = [_workloads(shape, dtype, rk, dev) for _ in range(k)]
+    streams = [torch.cuda.Stream(device=dev) for _ in range(k)]
+    main = torch.cuda.current_stream(dev)
     e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+
+    def round_(kind, n):
+        # n launches of `kind` on each stream, the streams running side by side
+        for st, w in zip(streams, works):
+            st.wait_stream(main)
+            with torch.cuda.stream(st):
+                for _ in range(n):
+                    w[kind]()
+        for st in streams:
+            main.wait_stream(st)
+
     result = {}
-    for kind, fn in work.items():
+    for kind in works[0]:
         times = {}
         for th in candidates:
             set_threads(kind, shape, th)
-            for _ in range(3):
-                fn()
+            round_(kind, 3)
             torch.cuda.synchronize(dev)
-            e0.record()
-            for _ in range(reps):
-                fn()
-            e1.record()
+            e0.record(main)
+            round_(kind, reps)
+            e1.record(main)
             torch.cuda.synchronize(dev)
             times[th] = e0.elapsed_time(e1) * 1e3 / reps
         best = min(candidates, key=lambda t: (times[t], -t))
