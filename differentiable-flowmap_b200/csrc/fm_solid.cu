@@ -970,8 +970,11 @@ int fm_solid_stats(fm_solid* S, void* stream, int reset, fm_mg_stats* out) {
   fm::count_launch(h.bodies * S->loop_kernels);  // kernels run inside device-mode loops since the last read
   Stats z = h;
   z.bodies = 0;
-  if (reset) z.solves = z.iterations = z.not_converged = z.nonfinite = 0, z.last_iters = z.max_iters_seen = 0,
-             z.last_rtr = 0.0;
+  if (reset) {
+    z.solves = z.iterations = z.not_converged = z.nonfinite = 0;
+    z.last_iters = z.max_iters_seen = 0;
+    z.last_rtr = 0.0;
+  }
   *S->stats_host = z;
   if (cudaMemcpyAsync(S->stats, S->stats_host, sizeof(Stats), cudaMemcpyHostToDevice, s) != cudaSuccess)
     return FM_ERR_CUDA;
