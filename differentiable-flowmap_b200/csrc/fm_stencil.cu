@@ -19,7 +19,7 @@
 namespace fm {
 
 // 3D tile: TI x TJ x TK output nodes (k contiguous); 2D: TI x TJ (j contiguous)
-constexpr int kTI3 = 4, kTJ3 = 8, kTK3 = 32;
+constexpr int kTI3 = 8, kTJ3 = 8, kTK3 = 32;
 constexpr int kTI2 = 16, kTJ2 = 64;
 constexpr int kStThreads = 256;
 
