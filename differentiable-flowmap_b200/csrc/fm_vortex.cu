@@ -1,6 +1,6 @@
 // fm_vortex.cu -- the 2D vortex problem's initial-condition map and vorticity
-// loss, with their adjoints (gradient of a final-vorticity
-// loss with respect to the vortex parameters).
+// loss, with their adjoints (the 256^2 vortex optimisation workload: gradient
+// of a final-vorticity loss with respect to the vortex parameters).
 //
 //  * velocity law: a sum of Gaussian-core point vortices evaluated at the cell
 //    centres, u_c = sum_k f(|p_k|) w_k (-p_k.y, p_k.x), p_k = X - c_k,
