@@ -46,3 +46,27 @@ def test_block_sizes_change_no_result(fm, cuda):
     assert l0 == l1 == l2
     assert np.array_equal(d0, d1) and np.array_equal(d0, d2)
     assert set(report) == set(T.KINDS) and all(r["threads"] in T.CANDIDATES for r in report.values())
+
+
+def test_tune_python_table_helpers(fm):
+    T = importlib.import_module("differentiable-flowmap_b200.tune")
+    shape = (80, 48)
+    T.reset(shape)
+    assert all(T.get_threads(k, shape) == 256 for k in T.KINDS)
+    T.set_threads("march", shape, 96)
+    assert T.get_threads("march", shape) == 96 and T.get_threads("advect_u", shape) == 256
+    T._cache[(shape, torch.float32, 2, T.CANDIDATES, 1)] = {"march": {"threads": 96, "us": {}}}
+    T.reset(shape)
+    assert T.get_threads("march", shape) == 256
+    assert not any(key[0] == shape for key in T._cache)
+    with pytest.raises(KeyError):
+        T.set_threads("no_such_kernel", shape, 64)
+
+
+def test_pdl_switch_round_trips(fm):
+    prev = fm._lib.set_pdl(False)
+    try:
+        assert fm._lib.set_pdl(True) is False
+        assert fm._lib.set_pdl(True) is True
+    finally:
+        fm._lib.set_pdl(prev)
