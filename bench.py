@@ -795,13 +795,13 @@ def dominant_kernel_roofline(fm, sim, dev, stream):
                      "peak_source": ("measured here: the best of an FMA-chain probe (fm_fp32_fma_probe, scalar "
                                      "and paired-lane FMAs) and cuBLAS FP32 GEMM 8192^3 with TF32 off"),
                      "measured": fp32},
-            "note": "gather kernel: FP32-issue bound (ncu: 501 M warp instructions per launch, issue active 60 %, "
-                    "L1 hit 96 %); its HBM fraction is low by construction, the fp32 entry is its bound"}
+            "note": "gather kernel: instruction-issue bound (ncu: 527 M warp instructions per launch, issue active "
+                    "66 %, L1 hit 95 %); its HBM fraction is low by construction, the fp32 entry is its bound"}
 
 
 # dram bytes (read + write) of one k_march<float,3,4> launch on the 128^3
 # benchmark state, from the ncu capture summarised in profiles/k_march_rk4_3d128.txt
-MARCH_DRAM_BYTES_PER_LAUNCH = 365_579_264
+MARCH_DRAM_BYTES_PER_LAUNCH = 371_630_592
 
 
 def fp32_peak_tflops(dev, fm):
