@@ -7,6 +7,7 @@ same shapes instead (numpy PCG64 generators, seeds fixed per config).
 from __future__ import annotations
 
 import math
+import os
 from dataclasses import replace
 
 import numpy as np
@@ -63,6 +64,52 @@ def shape3d_inputs(res=128, seed_target=20, seed_u=21, u_std=0.01):
     uc = rng.normal(0.0, u_std, size=(3,) + shape)
     u0 = split_central_vector(uc)
     return u0, rho0, rho_t
+
+
+# ---------------------------------------------------------------------------
+# The reference's own data files (copied into tests/golden/reference_fixtures.npz
+# by tests/golden/make_reference_fixtures.py)
+# ---------------------------------------------------------------------------
+REFERENCE_FIXTURES = os.path.join(os.path.dirname(os.path.dirname(os.path.abspath(__file__))), "tests", "golden",
+                                  "reference_fixtures.npz")
+
+
+def reference_fixtures(path: str = REFERENCE_FIXTURES) -> dict:
+    """The reference's data arrays: leaf_mask (2D/vortex/data/leaf_mask_256_scaled.npz),
+    density_{G,R}_2d (2D/shape/data/density_*_arial_scaled_shifted_0.8.npy) and
+    density_{G,R}_3d (3D/model/density_*_centered_1.2x_128x128.npy)."""
+    with np.load(path) as d:
+        return {k: d[k] for k in d.files}
+
+
+def extrude_glyph(glyph: np.ndarray, nz: int = 128) -> np.ndarray:
+    """A 128x128 glyph density extruded along z the way the reference's 3D shape
+    experiment does it (3D/optimize_shape_G_R.py:204-218): planes nz/2-16 ..
+    nz/2+15 hold glyph * (1 - |k - nz/2| / 16)^0.1, the rest are zero (FP32)."""
+    nx, ny = glyph.shape
+    out = np.zeros((nx, ny, nz), dtype=np.float32)
+    c = nz // 2
+    for k in range(c - 16, c + 16):
+        out[:, :, k] = glyph * (1 - abs(k - c) / 16) ** 0.1
+    return out
+
+
+def shape3d_glyph_inputs(fixtures: dict, seed_u=21, u_std=0.01):
+    """The 3D shape experiment's own densities at 128^3: rho0 = the extruded G
+    glyph, rho* = the extruded R glyph; u0 cell-centred N(0, u_std^2) split to faces."""
+    rho0 = extrude_glyph(fixtures["density_G_3d"])
+    rho_t = extrude_glyph(fixtures["density_R_3d"])
+    rng = np.random.default_rng(seed_u)
+    u0 = split_central_vector(rng.normal(0.0, u_std, size=(3,) + rho0.shape))
+    return u0, rho0, rho_t
+
+
+def shape2d_glyph_inputs(fixtures: dict, seed_u=12, u_std=0.01):
+    """The 2D shape experiment's own densities at 256^2 (G glyph -> R glyph);
+    u0 cell-centred N(0, u_std^2) split to faces."""
+    rng = np.random.default_rng(seed_u)
+    u0 = split_central_vector(rng.normal(0.0, u_std, size=(2, 256, 256)))
+    return u0, fixtures["density_G_2d"].astype(np.float64), fixtures["density_R_2d"].astype(np.float64)
 
 
 def shape2d_config(res=256, steps=200, reinit_every=12, rk=2, dt=0.01, dtype=torch.float32, store_dtype=None,

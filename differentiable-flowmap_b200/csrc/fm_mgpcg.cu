@@ -1513,7 +1513,11 @@ const char* fm_status_string(int status) {
 // use the array's name as a device address (it names a host-side shadow), so
 // the address is fetched with cudaGetSymbolAddress once per device, with that
 // device current, on the first call made on it; that first call should
-// therefore come before any stream capture.  Kernels are launched directly (no
+// therefore come before any stream capture.  Under CUDA's lazy module loading
+// (the default) that first call is also when the array and this library's
+// kernels receive their device memory, so it must come before another runtime
+// claims the device's memory (or the process sets CUDA_MODULE_LOADING=EAGER,
+// which places them when the library loads).  Kernels are launched directly (no
 // CUDA graph, whose instantiation may allocate) and convergence is polled
 // through a host stack variable (no pinned buffer).
 // ---------------------------------------------------------------------------
@@ -1532,7 +1536,10 @@ static int noalloc_scratch(void** out) {
   std::lock_guard<std::mutex> lock(g_noalloc_mu);
   if (!g_noalloc_base[dev]) {
     void* p = nullptr;
-    if (cudaGetSymbolAddress(&p, g_noalloc_scratch) != cudaSuccess || !p) return FM_ERR_CUDA;
+    if (cudaGetSymbolAddress(&p, g_noalloc_scratch) != cudaSuccess || !p) {
+      cudaGetLastError();  // leave no pending error for an unrelated later check
+      return FM_ERR_CUDA;
+    }
     g_noalloc_base[dev] = p;
   }
   *out = g_noalloc_base[dev];
@@ -1595,7 +1602,7 @@ extern "C" int fm_project_noalloc(const fm_grid* g, int dtype, const fm_mg_param
                                   void* uz, void* stream, int* iters, double* rtr) {
   int st = validate_grid(g, dtype);
   if (st) return st;
-  if (!params || !ux || !uy || (g->dim == 3 && !uz)) return FM_ERR_ARG;
+  if (!params) return FM_ERR_ARG;
   const fm_mg_params& P = *params;
   if (P.levels < 2 || P.levels > kMaxLevels || P.pre_post < 1 || P.bottom < 0 || P.max_iters < 1 ||
       P.check_every < 0 || (P.bottom_mode != 0 && P.bottom_mode != 1) || P.coarse_bf16)
@@ -1608,7 +1615,9 @@ extern "C" int fm_project_noalloc(const fm_grid* g, int dtype, const fm_mg_param
   S.dtype = dtype;
   S.P = P;
   S.L = P.levels;
+  // capacity before the field pointers: a caller can ask whether a grid fits without passing any
   if (noalloc_layout(*g, dtype, P.levels, &S, nullptr) > kNoAllocScratchBytes) return FM_ERR_CAPACITY;
+  if (!ux || !uy || (g->dim == 3 && !uz)) return FM_ERR_ARG;
   void* base = nullptr;
   if ((st = noalloc_scratch(&base))) return st;
   noalloc_layout(*g, dtype, P.levels, &S, (unsigned char*)base);

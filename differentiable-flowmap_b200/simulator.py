@@ -899,16 +899,32 @@ class LFM_Diff_Simulator(LFM_Simulator):
         ``control_forces[n]`` is step n's control_force_para, and the per-step
         parameter gradients are kept in ``control_force_grads[n]`` = (adj_center,
         adj_strength, penalty_center, penalty_strength), device FP64 n x dim."""
+        self.run_forward(u0, passive0, control_forces)
+        return self.run_adjoint(target_passive, target_vorticity, control_forces)
+
+    def run_forward(self, u0, passive0=None, control_forces=None):
+        """The forward half of ``gradient``: init from u0 (and passive0) and every
+        leapfrog step, leaving the trajectory the adjoint reads in the stores.
+        ``forward_serial`` counts completed forward passes, so that a caller who
+        runs the adjoint later can tell whether the trajectory is still its own."""
         cf = self.cfg.add_control_force
         if cf and control_forces is None:
             raise FlowmapError(2, "add_control_force needs control_forces (one control_force_para per step)")
-        self.control_force_grads = {}
         self.init(theta=u0, init_passive_np=passive0)
         while True:
             para = control_forces[self.step_num[None] + 1] if cf else None
             _, final = self.forward_step_midpoint(control_force_para=para)
             if final:
                 break
+        self.forward_serial = getattr(self, "forward_serial", 0) + 1
+
+    def run_adjoint(self, target_passive=None, target_vorticity=None, control_forces=None):
+        """The adjoint half of ``gradient``, on the trajectory of the last
+        ``run_forward``: returns (loss, dL/du0 as a list of face tensors)."""
+        cf = self.cfg.add_control_force
+        if cf and control_forces is None:
+            raise FlowmapError(2, "add_control_force needs control_forces (one control_force_para per step)")
+        self.control_force_grads = {}
         self.init_gradient(target_passive=target_passive, target_vorticity=target_vorticity)
         while True:
             n = self.step_num[None] - 1

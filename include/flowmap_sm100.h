@@ -281,6 +281,12 @@ int fm_mgpcg_stats(fm_mgpcg *solver, void *stream, int reset, fm_mg_stats *out);
  * overlap on the GPU (other streams, other host threads) race and must be
  * serialised by the caller.  The first call on a device looks the array's
  * address up (cudaGetSymbolAddress) and should come before any stream capture.
+ * Under CUDA's lazy module loading (the default) that first call is also when
+ * the array and this library's kernels get their device memory: make it before
+ * another runtime claims the device's memory (e.g. right after loading the
+ * library, before ti.init), or run with CUDA_MODULE_LOADING=EAGER.  The
+ * capacity check comes before the field-pointer check, so a call with NULL
+ * fields tells whether a grid fits (FM_ERR_CAPACITY if not, FM_ERR_ARG if so).
  * Every call synchronises `stream` to poll convergence (params->check_every
  * iterations per poll; 0 means 4).  Result and status as fm_project. */
 int fm_project_noalloc(const fm_grid *g, int dtype, const fm_mg_params *params, void *ux, void *uy, void *uz,

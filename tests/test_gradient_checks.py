@@ -109,3 +109,34 @@ def test_autograd_function(cuda):
     assert abs(float(L) - loss) <= 1e-12 * abs(loss)
     for a, b in zip(u, grad):
         assert torch.allclose(a.grad, 3.0 * b, rtol=1e-12, atol=0)
+
+
+def test_autograd_loss_without_gradients_runs_no_adjoint(cuda):
+    """Under torch.no_grad the loss costs one forward pass: the same kernel
+    launches as run_forward alone, no adjoint kernel, and the same loss; a
+    backward after an intervening forward pass rebuilds its own trajectory."""
+    A = importlib.import_module("differentiable-flowmap_b200.autograd")
+    lib = importlib.import_module("differentiable-flowmap_b200._lib")
+    sim, u0, rho0, rho_t = _setup(steps=8)
+    loss, grad = sim.gradient(u0, rho0, rho_t)
+    torch.cuda.synchronize()
+    lib.launch_count(reset=True)
+    sim.run_forward(u0, rho0)
+    torch.cuda.synchronize()
+    n_forward = lib.launch_count(reset=True)
+    sim.gradient(u0, rho0, rho_t)
+    torch.cuda.synchronize()
+    n_gradient = lib.launch_count(reset=True)
+    with torch.no_grad():
+        L = A.flowmap_loss(sim, u0, rho0, rho_t)
+    torch.cuda.synchronize()
+    n_nograd = lib.launch_count(reset=True)
+    assert n_nograd == n_forward < n_gradient, (n_nograd, n_forward, n_gradient)
+    assert abs(float(L) - loss) <= 1e-12 * abs(loss)
+    # a forward pass of other inputs between forward and backward
+    u = [x.clone().requires_grad_(True) for x in u0]
+    L = A.flowmap_loss(sim, u, rho0, rho_t)
+    sim.run_forward([0.5 * x for x in u0], rho0)
+    L.backward()
+    for a, b in zip(u, grad):
+        assert torch.equal(a.grad, b)
