@@ -39,7 +39,11 @@ def parse():
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--form", default="all", choices=["plain", "mixed", "checkpointed", "both", "all"],
-                    help="both: plain + mixed; all: plain + checkpointed + mixed (the headline form last)")
+                    help="both: plain + checkpointed; all: plain + mixed + checkpointed (the headline form last)")
+    ap.add_argument("--ckpt-dtype", default="bf16", choices=["bf16", "f32"],
+                    help="storage of the interval checkpoints in the checkpointed form")
+    ap.add_argument("--rel-tol", type=float, default=1e-6,
+                    help="relative z.r tolerance of the FP32 projections (rTr < rel_tol * zTr0)")
     ap.add_argument("--no-error", action="store_true", help="skip the FP64 reference runs")
     ap.add_argument("--solver-check-every", type=int, default=0,
                     help="0: device-side PCG loop (CUDA-graph WHILE node); k: host polls every k iterations "
@@ -83,13 +87,40 @@ def form_config(C, a, form, dtype):
     store = torch.bfloat16 if (mixed and dtype == torch.float32) else None
     cfg = C.shape3d_config(res=a.res, steps=a.sim_steps, reinit_every=a.reinit, rk=4, dtype=dtype,
                            store_dtype=store, backward_u=not mixed, check_every=a.solver_check_every,
-                           coarse_bf16=mixed and dtype == torch.float32 and a.mixed_coarse == "bf16")
+                           coarse_bf16=mixed and dtype == torch.float32 and a.mixed_coarse == "bf16",
+                           rel_tol=a.rel_tol)
     # checkpointed: the mixed form with interval checkpointing (the adjoint replays each interval)
-    return replace(cfg, recompute=True) if ckpt else cfg
+    if not ckpt:
+        return cfg
+    cd = torch.bfloat16 if (a.ckpt_dtype == "bf16" and dtype == torch.float32) else None
+    return replace(cfg, recompute=True, ckpt_dtype=cd)
 
 
 def workload_name(a):
     return f"3D smoke shape transition {a.res}^3, {a.sim_steps} steps, reinit {a.reinit}, RK4, fwd+adjoint"
+
+
+FORM_ORDER = {"plain": ["plain"], "mixed": ["mixed"], "checkpointed": ["checkpointed"],
+              "both": ["plain", "checkpointed"], "all": ["plain", "mixed", "checkpointed"]}
+
+
+def bench_forms(a):
+    """The forms the GPU arm times, the headline (value) form last."""
+    return FORM_ORDER[a.form]
+
+
+def headline_form(a):
+    return bench_forms(a)[-1]
+
+
+def bench_config(a, cfg, head):
+    """The `config` of the JSON line: the workload and the headline form's
+    settings (the same dict on the GPU arm and the reference arm)."""
+    return {"workload": workload_name(a), "form": head, "res": a.res, "sim_steps": a.sim_steps,
+            "reinit_every": a.reinit, "rk": 4, "dt": cfg.dt, "backward_u": cfg.backward_u,
+            "solver_rel_tol_zr": cfg.solver.rel_tol, "solver_levels": cfg.solver.levels,
+            "inputs": "seeded: sphere r=0.15 -> union of two spheres (seed 20), u0 ~ N(0, 0.01^2) (seed 21)",
+            "l2": "working set and trajectory stores exceed the 126 MB L2; no flush needed"}
 
 
 # ---------------------------------------------------------------------------
@@ -149,44 +180,82 @@ class ClockSampler:
 # ---------------------------------------------------------------------------
 # CPU: the reference algorithm (oracle restatement, FP32) on the host cores
 # ---------------------------------------------------------------------------
-def cpu_sample(a, threads=None):
-    """One-step gradient (1 forward + 1 adjoint step incl. the adjoint's reinit
-    BFECC) at the bench resolution with the FP32 oracle; returns seconds."""
-    threads = threads or len(os.sched_getaffinity(0))
+def _oracle_sim(cfg, steps, threads):
+    """The FP32 oracle simulator (the reference algorithm restated in C, OpenMP)
+    with the GPU form's algorithm and solver settings: backward_u, RK order,
+    reinit interval and the MGPCG tolerances.  Storage precision (BF16 stores,
+    BF16 coarse levels) and interval checkpointing are GPU memory layouts and
+    are not modelled."""
     os.environ["OMP_NUM_THREADS"] = str(threads)
     sys.path.insert(0, os.path.join(ROOT, "oracle"))
-    from oracle import MGParams  # noqa: E402  (checker only: CPU baseline leg)
+    from oracle import MGParams  # noqa: E402  (checker only: CPU legs)
     from sim_oracle import OracleSim  # noqa: E402
-    C = importlib.import_module("differentiable-flowmap_b200.configs")
-    u0, rho0, rho_t = C.shape3d_inputs(a.res)
-    levels = int(__import__("math").log2(a.res)) - 3 + 1
-    mg = MGParams(levels, 2, 50, 0, 400, 0.0, 1e-6, 1e-12)
-    o = OracleSim((a.res,) * 3, 1.0 / a.res, 0.0085, a.reinit, 1, rk=4, backward_u=True, prec="f32", mg=mg)
-    f32 = lambda x: x.astype("float32")
+
+    sc = cfg.solver
+    mg = MGParams(sc.levels, sc.pre_post, sc.bottom, sc.bottom_mode, sc.max_iters, sc.abs_tol, sc.rel_tol, sc.eps)
+    return OracleSim(cfg.res, cfg.dx, cfg.dt, cfg.reinit_every, steps, rk=cfg.RK_number,
+                     backward_u=cfg.backward_u, prec="f32", mg=mg)
+
+
+def cpu_pairs(cfg, steps, threads, inputs):
+    """A `steps`-step gradient of the benchmark workload with the FP32 oracle:
+    init, `steps` forward leapfrog steps (reinit every R, so whole intervals
+    include their reinit work), init_gradient and `steps` adjoint steps (the
+    adjoint's reinit BFECC at each interval start).  Returns (seconds for the
+    init, seconds for the step pairs, loss, gradient)."""
+    import numpy as np
+
+    o = _oracle_sim(cfg, steps, threads)
+    u0, rho0, rho_t = inputs
+    f32 = lambda x: np.asarray(x, dtype=np.float32)
     t0 = time.perf_counter()
-    o.gradient([f32(x) for x in u0], f32(rho0), f32(rho_t))
-    return time.perf_counter() - t0, threads
+    o.init([f32(x) for x in u0], f32(rho0))
+    t1 = time.perf_counter()
+    while not o.step_midpoint():
+        pass
+    o.init_gradient(f32(rho_t))
+    while not o.backtrack_step_midpoint():
+        pass
+    t2 = time.perf_counter()
+    return t1 - t0, t2 - t1, o.loss, [x.copy() for x in o.adj_u]
 
 
 def run_reference(a):
+    """The reference arm: the reference algorithm on the host cores (the FP32
+    oracle restatement; the reference's Taichi CPU backend cannot be installed
+    here), same workload, form and solver settings as the GPU headline.  One
+    bench step = one forward + adjoint leapfrog step pair at the benchmark size:
+    the W warm-up and K timed steps run as a W-step and a K-step gradient
+    (reinit every R, so their whole intervals include the reinit work), and the
+    150-step gradient rate is value = 1 / (150 x seconds per pair + init)."""
     rank = int(os.environ.get("RANK", "0"))
     if rank != 0:
         return 0
-    times = []
+    import torch
+
+    C = importlib.import_module("differentiable-flowmap_b200.configs")
+    head = headline_form(a)
+    cfg = form_config(C, a, head, torch.float32)
     threads = len(os.sched_getaffinity(0))
-    for i in range(a.warmup + a.steps):
-        dt, threads = cpu_sample(a, threads)
-        if i >= a.warmup:
-            times.append(dt)
-    per_grad = statistics.mean(times) * a.sim_steps
+    inputs = C.shape3d_inputs(a.res)
+    if a.warmup > 0:
+        cpu_pairs(cfg, a.warmup, threads, inputs)
+    t_init, t_pairs, _, _ = cpu_pairs(cfg, a.steps, threads, inputs)
+    per_pair = t_pairs / a.steps
+    per_grad = a.sim_steps * per_pair + t_init
     v = 1.0 / per_grad
-    sample = (f"one-step gradient (1 forward + 1 adjoint step, incl. the adjoint reinit BFECC) at {a.res}^3, "
-              f"scaled x{a.sim_steps} steps; FP32 CPU restatement of the reference algorithm (Taichi CPU backend "
-              f"not installable here), OpenMP")
+    sample = (f"a {a.steps}-step gradient ({a.steps} forward + {a.steps} adjoint leapfrog steps, reinit every "
+              f"{a.reinit} with the reinit work of its intervals) at {a.res}^3 in the {head} form's algorithm "
+              f"(backward_u={cfg.backward_u}, solver rel_tol {cfg.solver.rel_tol}), after a {a.warmup}-step "
+              f"warm-up gradient; {per_pair:.2f} s per step pair, scaled to {a.sim_steps} pairs + the init "
+              f"projection ({t_init:.2f} s); FP32 CPU restatement of the reference algorithm in C with OpenMP "
+              f"(the Taichi CPU backend is not installable here)")
     line = {"metric": METRIC, "value": v, "unit": UNIT, "impl": "reference", "n_gpus": a.gpus, "steps": a.steps,
-            "warmup": a.warmup, "ms_per_step": per_grad * 1e3, "higher_is_better": True, "scaling": "weak",
+            "warmup": a.warmup, "ms_per_step": per_pair * 1e3, "higher_is_better": True, "scaling": "weak",
             "vs_baseline": None, "dtype": "f32", "data": "synthetic",
-            "config": {"workload": workload_name(a), "form": "reference (CPU)", "parallelism": "host threads"},
+            "config": bench_config(a, cfg, head),
+            "step_unit": "one forward + adjoint leapfrog step pair (value scaled to the 150-step gradient)",
+            "ms_per_gradient": per_grad * 1e3,
             "cpu_baseline": {"value": v, "unit": UNIT, "cores": threads, "kind": "port", "sample": sample},
             "e2e": {"value": v, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
     print(json.dumps(line), flush=True)
@@ -592,13 +661,15 @@ def main():
         from datetime import timedelta
         dist.init_process_group("nccl", timeout=timedelta(seconds=600), device_id=dev)
 
+    from dataclasses import replace
+
     fm = importlib.import_module("differentiable-flowmap_b200")
     C = importlib.import_module("differentiable-flowmap_b200.configs")
     S = importlib.import_module("differentiable-flowmap_b200.simulator")
     lib = fm._lib
 
-    forms = {"both": ["plain", "mixed"], "all": ["plain", "checkpointed", "mixed"]}.get(a.form, [a.form])
-    head = forms[-1]
+    forms = bench_forms(a)
+    head = headline_form(a)
     sims, cfgs = {}, {}
     for f in forms:
         cfgs[f] = form_config(C, a, f, torch.float32)
@@ -689,60 +760,107 @@ def main():
     if rank == 0 and not a.no_roofline:
         roof = dominant_kernel_roofline(fm, sim, dev, stream)
 
-    # gradient error of each form against an FP64 run of the same algorithm
-    errors = {}
+    # gradient error of each form against an FP64 run of the same algorithm with every
+    # projection solved to the FP64 floor (relative z.r 1e-22, no eps): solver truncation
+    # shows up in the error instead of cancelling against an equally loose FP64 run
+    errors, g64s = {}, {}
     if rank == 0 and not a.no_error:
         for f in forms:
-            s64 = S.LFM_Diff_Simulator(config=form_config(C, a, f, torch.float64), device=dev)
-            l64, g64 = s64.gradient([x.double() for x in d_u0], d_r0.double(), d_rt.double())
+            c64 = form_config(C, a, f, torch.float64)
+            c64 = replace(c64, recompute=False, solver=replace(c64.solver, rel_tol=1e-22, abs_tol=0.0, eps=0.0,
+                                                                max_iters=400))
+            key = c64.backward_u
+            if key not in g64s:
+                s64 = S.LFM_Diff_Simulator(config=c64, device=dev)
+                g64s[key] = s64.gradient([x.double() for x in d_u0], d_r0.double(), d_rt.double())
+                st64 = s64.solver_stats
+                del s64
+                torch.cuda.empty_cache()
+            l64, g64 = g64s[key]
             g32 = results[f]["grad"]
-            num = sum(float(((x.double() - y) ** 2).sum()) for x, y in zip(g32, g64))
-            den = sum(float((y ** 2).sum()) for y in g64)
-            errors[f] = {"grad_rel_l2": (num / den) ** 0.5, "loss_rel": abs(results[f]["loss"] - l64) / abs(l64)}
-            del s64, g64
-            torch.cuda.empty_cache()
+            errors[f] = {"grad_rel_l2": rel_l2(g32, g64), "loss_rel": abs(results[f]["loss"] - l64) / abs(l64),
+                         "fp64_reference": "same algorithm, projections to relative z.r 1e-22"}
+        if True in g64s and False in g64s:
+            # the mixed forms' algorithm (backward_u off) against the plain algorithm, both FP64
+            errors["algorithm_gap_fp64"] = rel_l2(g64s[False][1], g64s[True][1])
+        del g64s
 
-    solves = sum(r.get("solves", 0) for r in iters)
-    pcg_iters = sum(r.get("iterations", 0) for r in iters)
-    not_conv = sum(r.get("not_converged", 0) for r in iters)
+    def solver_stats(f):
+        its = results[f]["iters"]
+        solves = sum(r.get("solves", 0) for r in its)
+        return {"levels": sims[f].solver.n_mg_levels, "rel_tol_zr": cfgs[f].solver.rel_tol,
+                "mean_pcg_iters": sum(r.get("iterations", 0) for r in its) / solves if solves else None,
+                "solves_per_grad": solves // max(a.steps, 1),
+                "not_converged": sum(r.get("not_converged", 0) for r in its),
+                "mode": "device (graph WHILE loop)" if a.solver_check_every == 0
+                else f"host-checked every {a.solver_check_every} iterations"}
+
     line = None
     if rank == 0:
         line = {"metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": a.steps,
                 "warmup": a.warmup, "ms_per_step": ms_max / a.steps, "higher_is_better": True, "scaling": "weak",
                 "vs_baseline": None, "dtype": "f32", "data": "synthetic",
-                "config": {"workload": workload_name(a), "form": head, "value_form": head,
-                           "res": a.res, "sim_steps": a.sim_steps,
-                           "reinit_every": a.reinit, "rk": 4, "backward_u": backward_u,
-                           "store_dtype": "bf16" if store is not None else "f32",
-                           "mg_coarse_storage": "bf16" if cfg.solver.coarse_bf16 else "f32",
-                           "solver": {"levels": sim.solver.n_mg_levels, "rel_tol": cfg.solver.rel_tol,
-                                      "mean_pcg_iters": pcg_iters / solves if solves else None,
-                                      "solves_per_grad": solves // max(a.steps, 1),
-                                      "not_converged": not_conv,
-                                      "mode": "device (graph WHILE loop)" if a.solver_check_every == 0
-                                      else f"host-checked every {a.solver_check_every} iterations"},
-                           "parallelism": f"replicas x{world}" if world > 1 else "single GPU",
-                           "l2": "working set and trajectory stores exceed the 126 MB L2; no flush needed"},
+                "config": bench_config(a, cfg, head),
+                "parallelism": f"replicas x{world}" if world > 1 else "single GPU",
                 "e2e": e2e, "gpu_launches": launches, "clocks": clk, "roofline": roof,
                 "forms": {f: {"value": r["value"], "ms_per_step": r["ms_per_step"], "gpu_launches": r["launches"],
                               "backward_u": cfgs[f].backward_u,
-                              "velocity_store": ("f32 ring of one interval, replayed" if cfgs[f].recompute else
+                              "velocity_store": ("interval checkpoints + a replayed f32 ring of one interval"
+                                                 if cfgs[f].recompute else
                                                  "bf16" if cfgs[f].store_dtype == torch.bfloat16 else "f32"),
-                              "trajectory_gb": sims_bytes[f] / 1e9,
-                              "grad_error_vs_fp64": errors.get(f)} for f, r in results.items()}}
-        if "plain" in results and "mixed" in results:
-            line["mixed_over_plain"] = results["mixed"]["value"] / results["plain"]["value"]
+                              "checkpoint_dtype": (str(cfgs[f].ckpt_dtype or cfgs[f].dtype).replace("torch.", "")
+                                                   if cfgs[f].recompute else None),
+                              "mg_coarse_storage": "bf16" if cfgs[f].solver.coarse_bf16 else "f32",
+                              "trajectory_gb": sims_bytes[f] / 1e9, "solver": solver_stats(f),
+                              "grad_error_vs_fp64": errors.get(f)} for f, r in results.items()},
+                "algorithm_gap_fp64": errors.get("algorithm_gap_fp64")}
+        for f in ("mixed", "checkpointed"):
+            if "plain" in results and f in results:
+                line[f"{f}_over_plain"] = results[f]["value"] / results["plain"]["value"]
         if world == 1 and not a.no_cpu_baseline:
-            secs, threads = cpu_sample(a)
-            line["cpu_baseline"] = {
-                "value": 1.0 / (secs * a.sim_steps), "unit": UNIT, "cores": threads, "kind": "port",
-                "sample": (f"one-step gradient (1 forward + 1 adjoint step incl. the adjoint reinit) at {a.res}^3 "
-                           f"with the FP32 CPU restatement, {secs:.1f} s, scaled x{a.sim_steps} steps")}
+            line["cpu_baseline"], line["parity_one_step"] = cpu_leg(a, C, S, cfg, head, dev)
         print(json.dumps(line), flush=True)
     if world > 1:
         dist.barrier()
         dist.destroy_process_group()
     return 0
+
+
+def rel_l2(a, b):
+    num = sum(float(((x.double() - y.double()) ** 2).sum()) for x, y in zip(a, b))
+    den = sum(float((y.double() ** 2).sum()) for y in b)
+    return (num / den) ** 0.5
+
+
+def cpu_leg(a, C, S, cfg, head, dev):
+    """cpu_baseline: a one-step gradient (1 forward + 1 adjoint step, the
+    adjoint's reinit BFECC included) of the headline form's algorithm at the
+    benchmark size with the FP32 oracle on all host threads, scaled x150 (a
+    bounded sample: the reference arm times a longer one).  The same one-step
+    gradient is run on the GPU and compared with it (relative L2 of dL/du0):
+    implementation parity at the benchmark grid size."""
+    import numpy as np
+    import torch
+    from dataclasses import replace
+
+    threads = len(os.sched_getaffinity(0))
+    inputs = C.shape3d_inputs(a.res)
+    t_init, t_pairs, lo, go = cpu_pairs(cfg, 1, threads, inputs)
+    secs = t_init + t_pairs
+    one = replace(cfg, total_steps=1, recompute=False, store_dtype=None)
+    sim1 = S.LFM_Diff_Simulator(config=one, device=dev)
+    u0, rho0, rho_t = inputs
+    lg, gg = sim1.gradient(u0, rho0, rho_t)
+    gg = [x.double().cpu().numpy() for x in gg]
+    err = float(np.sqrt(sum(((x - y) ** 2).sum() for x, y in zip(gg, go)) / sum((y.astype(np.float64) ** 2).sum()
+                                                                               for y in go)))
+    base = {"value": 1.0 / (secs * a.sim_steps), "unit": UNIT, "cores": threads, "kind": "port",
+            "sample": (f"one-step gradient (1 forward + 1 adjoint step incl. the adjoint reinit) of the {head} "
+                       f"form's algorithm at {a.res}^3 with the FP32 CPU restatement, {secs:.1f} s, scaled "
+                       f"x{a.sim_steps} steps")}
+    parity = {"case": f"one-step gradient at {a.res}^3, {head} form's algorithm, FP32 GPU vs FP32 oracle",
+              "grad_rel_l2": err, "loss_rel": abs(lg - lo) / abs(lo)}
+    return base, parity
 
 
 def dominant_kernel_roofline(fm, sim, dev, stream):

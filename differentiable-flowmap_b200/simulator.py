@@ -82,6 +82,9 @@ class FlowmapConfig:
     # steps before undoing them (about 7x less trajectory memory at 128^3, one
     # more forward pass of time).  Needs backward_u=False.
     recompute: bool = False
+    # storage dtype of the interval checkpoints (None: the working dtype); BF16
+    # halves them, and the replay then starts from the rounded state
+    ckpt_dtype: Optional[torch.dtype] = None
     solver: SolverConfig = field(default_factory=SolverConfig)
 
     def validate(self):
@@ -296,9 +299,10 @@ class LFM_Simulator:
         self.store_mid = self.store_phi = self.store_phi_f = self.store_F_f = self.store_passive = None
         self.ckpt_u = self.ckpt_passive = self._ring_passive = None
         if self.cfg.recompute:
-            self.ckpt_u = [torch.zeros((n_int + 1,) + g.face_shape(c), dtype=wd, device=dev) for c in range(self.dim)]
+            cd = self.cfg.ckpt_dtype or wd
+            self.ckpt_u = [torch.zeros((n_int + 1,) + g.face_shape(c), dtype=cd, device=dev) for c in range(self.dim)]
             if self.cfg.add_passive_scalar:
-                self.ckpt_passive = torch.zeros((n_int + 1,) + g.shape, dtype=wd, device=dev)
+                self.ckpt_passive = torch.zeros((n_int + 1,) + g.shape, dtype=cd, device=dev)
                 self._ring_passive = torch.zeros((R + 1,) + g.shape, dtype=wd, device=dev)
             self._ring = [[torch.zeros(g.face_shape(c), dtype=wd, device=dev) for c in range(self.dim)]
                           for _ in range(R)]
@@ -336,9 +340,9 @@ class LFM_Simulator:
         """Interval checkpointing: the state at the start of interval k (slot
         n_int: the state after the last step)."""
         for c in range(self.dim):
-            self.ckpt_u[c][k].copy_(self.u[c])
+            K.store(self.u[c], self.ckpt_u[c][k])
         if self.ckpt_passive is not None:
-            self.ckpt_passive[k].copy_(self.passive)
+            K.store(self.passive, self.ckpt_passive[k])
 
     # ------------------------------------------------------------ kernels
     def reset_to_identity(self, psi, psi_f, T_f):
@@ -591,9 +595,9 @@ class LFM_Simulator:
         last = min(n0 + R - 1, self.total_steps - 1)
         saved = self.step_num[None]
         for c in range(self.dim):
-            self.u[c].copy_(self.ckpt_u[c][k])
+            K.store(self.ckpt_u[c][k], self.u[c])
         if self.ckpt_passive is not None:
-            self.passive.copy_(self.ckpt_passive[k])
+            K.store(self.ckpt_passive[k], self.passive)
             self.init_passive.copy_(self.passive)
         _copy_mac(self.init_u, self.u)
         self.reset_to_identity(self.phi, self.phi_f, self.F_f)
@@ -608,7 +612,7 @@ class LFM_Simulator:
             self._recomputing = False
             self.step_num[None] = saved
         if self._ring_passive is not None:
-            self._ring_passive[last + 1 - n0].copy_(self.ckpt_passive[k + 1])
+            K.store(self.ckpt_passive[k + 1], self._ring_passive[last + 1 - n0])
 
 
 class LFM_Diff_Simulator(LFM_Simulator):

@@ -1,0 +1,120 @@
+"""Parity at the benchmark configurations' own sizes: the CUDA simulator against
+the oracle's restatement of the reference control flow on the same inputs.
+
+* 3D 128^3 (the benchmark grid), one forward + one adjoint step (reinit 8,
+  RK4, dt 0.0085) started from the reference's own 3D shape densities (the G
+  glyph extruded along z as 3D/optimize_shape_G_R.py:204-218 does it, target
+  the R glyph), for the plain form (backward_u) and the mixed form's algorithm
+  (backward_u off).
+* 2D 256^2 with the 2D shape configuration (reinit 12, RK2, dt 0.01) over two
+  reinit intervals, on the seeded rectangles -> discs inputs and on the
+  reference's own 2D glyph densities (2D/shape/data).
+
+FP64 CUDA vs the FP64 oracle: loss to 1e-9 relative, dL/du0 to 1e-7 relative
+L2 (both solve every projection to machine precision).  FP32 CUDA with the
+accurate solver setting vs the FP64 oracle: dL/du0 to 1e-4 relative L2 (the
+accuracy bar of the benchmark), loss to 1e-5.
+"""
+import importlib
+
+import numpy as np
+import pytest
+import torch
+
+from oracle import MGParams
+from sim_oracle import OracleSim
+
+pytestmark = pytest.mark.gpu
+
+GRAD_TOL_FP64 = 1e-7
+LOSS_TOL_FP64 = 1e-9
+GRAD_TOL_FP32 = 1e-4
+LOSS_TOL_FP32 = 1e-5
+FP32_REL_TOL = 1e-12  # relative z.r criterion of the FP32 solves
+
+
+def _C():
+    return importlib.import_module("differentiable-flowmap_b200.configs")
+
+
+def _rel_l2(a, b):
+    num = np.sqrt(sum(np.sum((np.asarray(x, np.float64) - y) ** 2) for x, y in zip(a, b)))
+    den = np.sqrt(sum(np.sum(np.asarray(y, np.float64) ** 2) for y in b))
+    return num / den
+
+
+# name: (res, steps, R, rk, dt, backward_u, inputs)
+CASES = {
+    "3d128_plain_glyphs": ((128, 128, 128), 1, 8, 4, 0.0085, True, "glyph3d"),
+    "3d128_mixed_glyphs": ((128, 128, 128), 1, 8, 4, 0.0085, False, "glyph3d"),
+    "2d256_shape_config": ((256, 256), 24, 12, 2, 0.01, True, "shape2d"),
+    "2d256_glyphs": ((256, 256), 24, 12, 2, 0.01, True, "glyph2d"),
+}
+
+
+def _inputs(kind):
+    C = _C()
+    if kind == "shape2d":
+        return C.shape2d_inputs(256)
+    fx = C.reference_fixtures()
+    return C.shape3d_glyph_inputs(fx) if kind == "glyph3d" else C.shape2d_glyph_inputs(fx)
+
+
+def _levels(res):
+    # 3D: base level 3 (5 levels at 128^3); 2D: base level 4 (5 levels at 256^2)
+    return int(np.log2(min(res))) - (3 if len(res) == 3 else 4) + 1
+
+
+def _bottom(res):
+    return (50, 0) if len(res) == 3 else (20, 1)
+
+
+def _run_cuda(name, dtype):
+    res, steps, R, rk, dt, bu, kind = CASES[name]
+    S = importlib.import_module("differentiable-flowmap_b200.simulator")
+    tight = dtype == torch.float64
+    bottom, mode = _bottom(res)
+    solver = S.SolverConfig(levels=_levels(res), bottom=bottom, bottom_mode=mode, max_iters=400 if tight else 200,
+                            abs_tol=0.0, rel_tol=1e-22 if tight else FP32_REL_TOL, eps=0.0 if tight else 1e-12,
+                            check_every=0)
+    cfg = S.FlowmapConfig(res=res, dx=1.0 / res[0], dt=dt, total_steps=steps, reinit_every=R, RK_number=rk,
+                          backward_u=bu, dtype=dtype, solver=solver)
+    sim = S.LFM_Diff_Simulator(config=cfg)
+    u0, rho0, rho_t = _inputs(kind)
+    loss, grad = sim.gradient(u0, rho0, rho_t)
+    out = loss, [g.double().cpu().numpy() for g in grad]
+    del sim
+    torch.cuda.empty_cache()
+    return out
+
+
+def _run_oracle(name):
+    res, steps, R, rk, dt, bu, kind = CASES[name]
+    bottom, mode = _bottom(res)
+    mg = MGParams(_levels(res), 2, bottom, mode, 400, 0.0, 1e-22, 0.0)
+    o = OracleSim(res, 1.0 / res[0], dt, R, steps, rk=rk, backward_u=bu, prec="f64", mg=mg)
+    u0, rho0, rho_t = _inputs(kind)
+    return o.gradient(u0, rho0, rho_t)
+
+
+@pytest.fixture(scope="module")
+def oracle_results():
+    return {}
+
+
+@pytest.mark.parametrize("name", list(CASES))
+def test_full_size_fp64_matches_oracle(cuda, name, oracle_results):
+    lo, go = oracle_results.setdefault(name, _run_oracle(name))
+    lc, gc = _run_cuda(name, torch.float64)
+    assert np.linalg.norm(np.concatenate([g.ravel() for g in go])) > 0
+    assert abs(lc - lo) / abs(lo) < LOSS_TOL_FP64, (lc, lo)
+    assert _rel_l2(gc, go) < GRAD_TOL_FP64
+
+
+@pytest.mark.parametrize("name", list(CASES))
+def test_full_size_fp32_within_bar_of_fp64_oracle(cuda, name, oracle_results):
+    lo, go = oracle_results.setdefault(name, _run_oracle(name))
+    lc, gc = _run_cuda(name, torch.float32)
+    assert abs(lc - lo) / abs(lo) < LOSS_TOL_FP32, (lc, lo)
+    err = _rel_l2(gc, go)
+    assert err < GRAD_TOL_FP32, err
