@@ -61,7 +61,7 @@ def parse():
     ap.add_argument("--gaussians", type=int, default=3000, help="Gaussian control forces per step (shape3d-forces)")
     ap.add_argument("--workload", default="gradient",
                     choices=["gradient", "poisson", "vortex2d", "vortex2d-obstacle", "vortex2d-batch",
-                             "shape3d-forces", "force-kernels"],
+                             "shape2d", "shape3d-forces", "force-kernels"],
                     help="gradient: the headline 3D gradient benchmark; poisson: the mixed-precision Poisson solve "
                          "(seeded k^-5/3 divergence RHS, all-Neumann, --poisson-res^3); vortex2d: the 2D vortex "
                          "optimisation gradient dL/dtheta (256^2, 100 steps, 4 vortices); shape3d-forces: the 3D "
@@ -439,6 +439,100 @@ def run_vortex2d(a):
     return 0
 
 
+def run_shape2d(a):
+    """2D smoke shape transition (256^2 MAC, 200 steps, reinit 12, RK2, dt 0.01,
+    MGPCG 5 levels; rho0 = three seeded rectangles, rho* = three seeded discs,
+    control u0 ~ N(0, 0.01^2)): one bench step = one gradient dL/du0 of
+    L = sum (rho(T) - rho*)^2 in the plain FP32 drop-in form.  value: the gradient
+    replayed from one CUDA graph on device-resident inputs; e2e: the
+    torch.autograd path (flowmap_loss + backward) with pinned host inputs copied
+    in and the gradient and loss copied out every step."""
+    import torch
+    from dataclasses import replace
+
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    torch.cuda.set_device(local)
+    dev = torch.device("cuda", local)
+    S = importlib.import_module("differentiable-flowmap_b200.simulator")
+    C = importlib.import_module("differentiable-flowmap_b200.configs")
+    A = importlib.import_module("differentiable-flowmap_b200.autograd")
+    lib = importlib.import_module("differentiable-flowmap_b200._lib")
+    f32 = torch.float32
+    cfg = C.shape2d_config(res=256, steps=200, reinit_every=12, rk=2, dt=0.01, dtype=f32, rel_tol=a.rel_tol,
+                           check_every=0)
+    sim = S.LFM_Diff_Simulator(config=cfg, device=dev)
+    u0, rho0, rho_t = C.shape2d_inputs(256)
+    d_u0 = [torch.tensor(x, dtype=f32, device=dev) for x in u0]
+    d_r0 = torch.tensor(rho0, dtype=f32, device=dev)
+    d_rt = torch.tensor(rho_t, dtype=f32, device=dev)
+
+    def timed(fn):
+        for _ in range(a.warmup):
+            fn()
+        torch.cuda.synchronize(dev)
+        lib.launch_count(reset=True)
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record()
+        for _ in range(a.steps):
+            out = fn()
+        e1.record()
+        torch.cuda.synchronize(dev)
+        return e0.elapsed_time(e1) / a.steps, out, lib.launch_count(reset=True)
+
+    ms_eager, (loss, grad), _ = timed(lambda: sim.gradient(d_u0, d_r0, d_rt))
+    grad = [x.clone() for x in grad]
+    stats = sim.solver_stats
+    graph = sim.capture_gradient(d_u0, d_r0, d_rt)
+
+    def replay():
+        graph.replay()
+        return sim.adj_u
+
+    ms, gg, launches = timed(replay)
+    if any(not torch.equal(x, y) for x, y in zip(gg, grad)):
+        raise RuntimeError("graph replay differs from the eager gradient")
+    # end to end through torch.autograd with host buffers
+    h_u0 = [torch.tensor(x, dtype=f32).pin_memory() for x in u0]
+    h_r0 = torch.tensor(rho0, dtype=f32).pin_memory()
+    h_rt = torch.tensor(rho_t, dtype=f32).pin_memory()
+    h_g = [torch.empty(x.shape, dtype=f32).pin_memory() for x in u0]
+
+    def e2e_step():
+        u = [x.to(dev, non_blocking=True).requires_grad_(True) for x in h_u0]
+        L = A.flowmap_loss(sim, u, h_r0, h_rt)
+        L.backward()
+        for hg, x in zip(h_g, u):
+            hg.copy_(x.grad, non_blocking=True)
+        return float(L)
+
+    ms_e2e, _, _ = timed(e2e_step)
+    # FP64 run with every projection solved to the FP64 floor
+    c64 = C.shape2d_config(res=256, steps=200, reinit_every=12, rk=2, dt=0.01, dtype=torch.float64, rel_tol=1e-22,
+                           max_iters=400, check_every=0)
+    c64 = replace(c64, solver=replace(c64.solver, eps=0.0))
+    s64 = S.LFM_Diff_Simulator(config=c64, device=dev)
+    l64, g64 = s64.gradient([x.double() for x in d_u0], d_r0.double(), d_rt.double())
+    line = {"metric": "2D shape transition dL/du0 evaluations/s, 256^2, 200 steps", "value": 1e3 / ms,
+            "unit": "grads/s", "n_gpus": 1, "steps": a.steps, "warmup": a.warmup, "ms_per_step": ms,
+            "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic",
+            "config": {"workload": "2D smoke shape transition 256^2, 200 steps, reinit 12, RK2, dt 0.01, control u0",
+                       "form": "plain FP32 drop-in (backward_u)", "solver_rel_tol_zr": a.rel_tol,
+                       "inputs": "3 seeded rectangles (seed 10) -> 3 seeded discs (seed 11), u0 ~ N(0, 0.01^2) "
+                                 "(seed 12)", "launch": "one CUDA graph per gradient (capture_gradient)",
+                       "l2": "inputs (0.5 MB per field) fit in L2; the trajectory store (210 MB) does not"},
+            "gpu_launches": launches, "eager": {"grads_per_s": 1e3 / ms_eager, "ms": ms_eager},
+            "e2e": {"value": 1e3 / ms_e2e, "unit": "grads/s", "path": "autograd flowmap_loss + backward",
+                    "h2d_bytes_per_step": sum(x.numel() * 4 for x in h_u0) + 2 * h_r0.numel() * 4,
+                    "d2h_bytes_per_step": sum(x.numel() * 4 for x in h_g) + 8},
+            "solver": {"mean_pcg_iters": stats["iterations"] / max(stats["solves"], 1),
+                       "solves_per_grad": stats["solves"] // max(a.warmup + a.steps, 1)},
+            "loss": loss, "grad_error_vs_fp64": {"grad_rel_l2": rel_l2(grad, g64), "loss_rel": abs(loss - l64) / abs(l64),
+                                                 "fp64_reference": "projections to relative z.r 1e-22"},
+            "trajectory_gb": sim.trajectory_bytes() / 1e9}
+    print(json.dumps(line), flush=True)
+    return 0
+
+
 def run_vortex2d_batch(a):
     """16 vortex-optimisation instances (4 x 128^2, 4 x 192^2, 4 x 256^2,
     4 x 384^2; 100 steps, reinit 10, dt = 0.5 dx; control seeds 100+i, target
@@ -644,6 +738,8 @@ def main():
         return run_vortex2d(a)
     if a.workload == "vortex2d-batch":
         return run_vortex2d_batch(a)
+    if a.workload == "shape2d":
+        return run_shape2d(a)
     if a.workload == "shape3d-forces":
         return run_shape3d_forces(a)
     if a.workload == "force-kernels":
