@@ -30,7 +30,9 @@ GRAD_TOL_FP64 = 1e-7
 LOSS_TOL_FP64 = 1e-9
 GRAD_TOL_FP32 = 1e-4
 LOSS_TOL_FP32 = 1e-5
-FP32_REL_TOL = 1e-12  # relative z.r criterion of the FP32 solves
+# relative z.r criterion of the FP32 solves: 1e-8 is within FP32's reach at 128^3
+# (tighter ones stall near 1e-9 and run into the iteration cap), 1e-10 at 256^2
+FP32_REL_TOL = {3: 1e-8, 2: 1e-10}
 
 
 def _C():
@@ -75,7 +77,7 @@ def _run_cuda(name, dtype):
     tight = dtype == torch.float64
     bottom, mode = _bottom(res)
     solver = S.SolverConfig(levels=_levels(res), bottom=bottom, bottom_mode=mode, max_iters=400 if tight else 200,
-                            abs_tol=0.0, rel_tol=1e-22 if tight else FP32_REL_TOL, eps=0.0 if tight else 1e-12,
+                            abs_tol=0.0, rel_tol=1e-22 if tight else FP32_REL_TOL[len(res)], eps=0.0 if tight else 1e-12,
                             check_every=0)
     cfg = S.FlowmapConfig(res=res, dx=1.0 / res[0], dt=dt, total_steps=steps, reinit_every=R, RK_number=rk,
                           backward_u=bu, dtype=dtype, solver=solver)
@@ -97,14 +99,18 @@ def _run_oracle(name):
     return o.gradient(u0, rho0, rho_t)
 
 
-@pytest.fixture(scope="module")
-def oracle_results():
-    return {}
+_ORACLE = {}
+
+
+def _oracle(name):
+    if name not in _ORACLE:
+        _ORACLE[name] = _run_oracle(name)
+    return _ORACLE[name]
 
 
 @pytest.mark.parametrize("name", list(CASES))
-def test_full_size_fp64_matches_oracle(cuda, name, oracle_results):
-    lo, go = oracle_results.setdefault(name, _run_oracle(name))
+def test_full_size_fp64_matches_oracle(cuda, name):
+    lo, go = _oracle(name)
     lc, gc = _run_cuda(name, torch.float64)
     assert np.linalg.norm(np.concatenate([g.ravel() for g in go])) > 0
     assert abs(lc - lo) / abs(lo) < LOSS_TOL_FP64, (lc, lo)
@@ -112,9 +118,10 @@ def test_full_size_fp64_matches_oracle(cuda, name, oracle_results):
 
 
 @pytest.mark.parametrize("name", list(CASES))
-def test_full_size_fp32_within_bar_of_fp64_oracle(cuda, name, oracle_results):
-    lo, go = oracle_results.setdefault(name, _run_oracle(name))
+def test_full_size_fp32_within_bar_of_fp64_oracle(cuda, name):
+    lo, go = _oracle(name)
     lc, gc = _run_cuda(name, torch.float32)
     assert abs(lc - lo) / abs(lo) < LOSS_TOL_FP32, (lc, lo)
     err = _rel_l2(gc, go)
+    print(f"{name}: FP32 vs FP64 oracle dL/du0 {err:.3e}, loss {abs(lc - lo) / abs(lo):.3e}")
     assert err < GRAD_TOL_FP32, err

@@ -226,3 +226,21 @@ def test_simulator_with_obstacle_matches_oracle(fm, cuda, name):
     fluid = ~(mask > 0)
     for c in range(2):
         assert np.all(gc[c][SO.faces_of_solids(fluid, c)] == 0)  # the adjoint velocity is masked
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("dtype", [torch.float32, torch.float64])
+def test_solid_vcycle_bitwise_on_the_reference_leaf_mask(fm, cuda, dtype):
+    """The reference experiment's own obstacle (2D/vortex/data/leaf_mask_256_scaled.npz,
+    7922 solid cells) at its size, 256^2 with the vortex solver's 5 levels, 20
+    bottom sweeps as 10 x (R,B) + 10 x (B,R): bit-exact against the oracle."""
+    Cf = importlib.import_module("differentiable-flowmap_b200.configs")
+    mask = Cf.reference_fixtures()["leaf_mask"].astype(np.float32)
+    assert mask.shape == (256, 256) and int(mask.sum()) == 7922
+    npt = np.float32 if dtype == torch.float32 else np.float64
+    S = _solid((256, 256), mask, dtype, 5, bottom=20, bottom_mode=1)
+    r = np.random.default_rng(9).normal(size=(256, 256)).astype(npt)
+    z = S.apply_preconditioner(torch.tensor(r, device="cuda"))
+    torch.cuda.synchronize()
+    want = SO.vcycle(r, ~(mask > 0), 5, bottom=20)
+    np.testing.assert_array_equal(z.cpu().numpy(), want)

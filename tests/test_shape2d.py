@@ -78,7 +78,7 @@ def test_shape2d_gradient_vs_central_fd_on_32_cells(fp64_run):
 
 def test_shape2d_fp32_gradient_within_bar_of_fp64(fp64_run):
     _, _, _, _, l64, g64 = fp64_run
-    sim = _sim(torch.float32, 1e-12)
+    sim = _sim(torch.float32, 1e-10)
     u0, rho0, rho_t = _inputs(torch.float32)
     loss, grad = sim.gradient(u0, rho0, rho_t)
     num = sum(float(((x.double() - y) ** 2).sum()) for x, y in zip(grad, g64))
