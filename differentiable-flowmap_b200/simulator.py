@@ -24,7 +24,6 @@ Control flow and arithmetic follow the reference step for step; the flags of
 from __future__ import annotations
 
 import math
-from contextlib import contextmanager
 from dataclasses import dataclass, field, replace
 from typing import Dict, List, Optional, Sequence
 
@@ -86,11 +85,6 @@ class FlowmapConfig:
     # storage dtype of the interval checkpoints (None: the working dtype); BF16
     # halves them, and the replay then starts from the rounded state
     ckpt_dtype: Optional[torch.dtype] = None
-    # Run each step's flow-map march (and, in the adjoint, the accumulate_init
-    # pullbacks that read it) on a second CUDA stream, concurrently with the
-    # advections and the projection it does not depend on.  The kernels and their
-    # inputs are unchanged, so results are bit-identical either way.
-    overlap: bool = True
     solver: SolverConfig = field(default_factory=SolverConfig)
 
     def validate(self):
@@ -287,8 +281,6 @@ class LFM_Simulator:
         self.frame_idx = _Scalar(0)
         self.total_steps = cfg.total_steps
         self._recomputing = False
-        # the side stream of the overlapped march (FlowmapConfig.overlap)
-        self._side = torch.cuda.Stream(device=dev) if cfg.overlap else None
         self._alloc_stores()
         self.reset_to_identity(self.phi, self.phi_f, self.F_f)
 
@@ -351,29 +343,6 @@ class LFM_Simulator:
             K.store(self.u[c], self.ckpt_u[c][k])
         if self.ckpt_passive is not None:
             K.store(self.passive, self.ckpt_passive[k])
-
-    # ------------------------------------------------------------ streams
-    def _overlap_ok(self) -> bool:
-        """The march runs on the side stream in the plain leapfrog step; the
-        short-BFECC, control-force and viscosity variants read its result within
-        the step and stay on one stream."""
-        cfg = self.cfg
-        return (self._side is not None and not cfg.use_short_BFECC and not cfg.add_control_force
-                and self.vis is None)
-
-    @contextmanager
-    def _on_side(self):
-        """Launch on the side stream, after everything issued so far on the
-        current stream (works inside a CUDA-graph capture: the side stream
-        joins it)."""
-        main = torch.cuda.current_stream(self.device)
-        self._side.wait_stream(main)
-        with torch.cuda.stream(self._side):
-            yield
-
-    def _join_side(self):
-        """The current stream waits for the side stream's work."""
-        torch.cuda.current_stream(self.device).wait_stream(self._side)
 
     # ------------------------------------------------------------ kernels
     def reset_to_identity(self, psi, psi_f, T_f):
@@ -557,12 +526,7 @@ class LFM_Simulator:
                 K.store(self.u[c], self.store_mid[c][n])
             if self._ring is not None:
                 self._ring[j][c].copy_(self.u[c])
-        overlap = self._overlap_ok()
-        if overlap:  # the march reads this u (u_mid) only; the rest of the step does not read phi, F
-            with self._on_side():
-                self.march_phi_grid(self.u)
-        else:
-            self.march_phi_grid(self.u)
+        self.march_phi_grid(self.u)
         if cfg.use_short_BFECC:
             # BFECC through one-step maps instead of the semi-Lagrangian advection
             # (3D/lfm_midpoint_simulator.py:725-745); the BFECC result replaces u
@@ -587,8 +551,6 @@ class LFM_Simulator:
             K.accumulate_init(self.grid, self.dx, curr_dt, self.vis, self.init_u, self.F_f, self.phi_f)
         self.project(self.u)
         self._mask()  # 3D/lfm_midpoint_simulator.py:769-771
-        if overlap:
-            self._join_side()  # u_mid is overwritten next step; the reinit reads phi, F
 
         if self._recomputing:
             # an interval replayed for the adjoint: it needs the midpoint
@@ -788,19 +750,6 @@ class LFM_Diff_Simulator(LFM_Simulator):
             self.BFECC(self.u, self.final_u, self.err_u, *maps)
             self.u, self.final_u = self.final_u, self.u
 
-    def _adj_accumulate(self, n: int, curr_dt: float):
-        """The adjoint step's accumulate_init pullbacks of the sources into the
-        reinit frame (3D/lfm_midpoint_diff_simulator.py:513-524)."""
-        g, dx = self.grid, self.dx
-        # Adams-Bashforth index: adjoint steps already taken in this interval
-        # (= reinit_every-1-j for a full interval, as the reference computes it)
-        interval_last = min((n // self.reinit_every) * self.reinit_every + self.reinit_every - 1,
-                            self.total_steps - 1)
-        K.accumulate_init(g, dx, -2 * curr_dt, self.src, self.init_adj_u, self.T_f, self.psi_f, self.H_prev,
-                          self.H_prev_prev, interval_last - n)
-        if self.cfg.add_passive_scalar:
-            K.accumulate_init(g, dx, -curr_dt, self.adj_passive_f, self.init_adj_u, self.T_f, self.psi_f)
-
     def calculate_adj_gausion_force(self, adj_u, center, inverse_radius, strength, num):
         """3D/lfm_midpoint_diff_simulator.py:63-69: the four per-Gaussian sums into
         adj_gaussion_force_center / _strength and penalty_gaussion_force_center /
@@ -858,16 +807,9 @@ class LFM_Diff_Simulator(LFM_Simulator):
         if self.vis is not None:  # 2D/vortex/lfm_midpoint_diff_simulator.py:270-271
             K.viscous_force_2d(g, cfg.viscosity, dx, self.mid_u, self.vis, adj=self.adj_u, part=self._vis_part,
                                dot=self.adj_viscous.tensor)
-        overlap = self._overlap_ok()
-        if overlap:  # the march reads mid_u, psi, T only
-            with self._on_side():
-                self.march_psi_grid(curr_dt)
         K.nabla_u_w(g, dx, self.u if cfg.backward_u else self.mid_u, self.adj_u, self.src)
         if cfg.add_passive_scalar:
             K.nabla_scalar_adjoint(g, dx, self.passive, self.adj_passive, self.adj_passive_f)
-        if overlap:  # after the march and the sources; writes init_adj_u and the AB3 history only
-            with self._on_side():
-                self._adj_accumulate(n, curr_dt)
 
         rk = cfg.RK_number
         if cfg.use_short_BFECC:
@@ -895,9 +837,15 @@ class LFM_Diff_Simulator(LFM_Simulator):
                 for c in range(self.dim):
                     K.add_fields(self.adj_u[c], self.adj_passive_f[c], self.adj_u[c], -curr_dt)
 
-        if not overlap:
-            self.march_psi_grid(curr_dt)
-            self._adj_accumulate(n, curr_dt)
+        self.march_psi_grid(curr_dt)
+        # Adams-Bashforth index: adjoint steps already taken in this interval
+        # (= reinit_every-1-j for a full interval, as the reference computes it)
+        interval_last = min((n // self.reinit_every) * self.reinit_every + self.reinit_every - 1,
+                            self.total_steps - 1)
+        K.accumulate_init(g, dx, -2 * curr_dt, self.src, self.init_adj_u, self.T_f, self.psi_f, self.H_prev,
+                          self.H_prev_prev, interval_last - n)
+        if cfg.add_passive_scalar:
+            K.accumulate_init(g, dx, -curr_dt, self.adj_passive_f, self.init_adj_u, self.T_f, self.psi_f)
         if self.vis is not None:  # 2D/vortex/lfm_midpoint_diff_simulator.py:387-389
             for c in range(self.dim):
                 K.add_fields(self.adj_u[c], self.vis[c], self.adj_u[c], -curr_dt)
@@ -914,8 +862,6 @@ class LFM_Diff_Simulator(LFM_Simulator):
                 K.accumulate_init(g, dx, -curr_dt, self.vis, self.init_u, self.T_f, self.psi_f)
             self.project(self.u)
         self._mask(adjoint=True)  # 3D/lfm_midpoint_diff_simulator.py:534-538
-        if overlap:
-            self._join_side()  # the reinit below reads psi, T, init_adj_u; the next step rewrites mid_u
 
         if j == 0:
             k = n // self.reinit_every
