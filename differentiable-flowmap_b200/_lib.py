@@ -100,6 +100,7 @@ SIGNATURES = {
     "fm_advect_scalar_grid_pair": [GP, I, I, D, D] + [P] * 7 + [P],
     "fm_mg_vcycle": [P, P, P, P],
     "fm_mgpcg_solve_dc": [P, I, P, P, P, D, I, P, C.POINTER(I), C.POINTER(I), C.POINTER(D)],
+    "fm_project_dc": [P, P, P, P, P, D, I, P, P],
     "fm_clamp_extrema": [GP, I, I, P, P, P, P],
     "fm_tune_set": [I, GP, I],
     "fm_tune_get": [I, GP],

@@ -56,6 +56,9 @@ struct DevState {
   // outer defect correction (fm_mgpcg_solve_dc): mean of b, |b - mean|^2, |r|^2,
   // and an rTr floor for the inner solves (0 outside a defect correction)
   double dc_mean, dc_b2, dc_r2, dc_tol;
+  // device-side defect correction (fm_project_dc): set once |r| <= rel_tol |b|;
+  // every later correction, and the inner solves inside them, skip their work
+  int dc_done;
 };
 
 // ---------------------------------------------------------------------------
@@ -317,6 +320,128 @@ __global__ void k_dc_update(long n, double* __restrict__ x, const float* __restr
   FM_GRID_STRIDE(q, n) x[q] += s * (double)e[q];
 }
 
+// fm_project_dc: b = -div(u) of the FP32 velocity formed in FP64 (apply_bc
+// zeroes the wall faces, as k_div_bc does), x = 0, partial sums of b.
+template <int D>
+__global__ void __launch_bounds__(kRedThreads) k_dc_div(fm_grid g, MacW<float> u, double* __restrict__ b,
+                                                        double* __restrict__ x, double* __restrict__ part) {
+  pdl_begin();
+  const Shape cs = cell_shape(g);
+  double sum = 0;
+  FM_GRID_STRIDE(q, cs.size()) {
+    int I[3];
+    unflatten(cs, q, I[0], I[1], I[2]);
+    double acc = 0;
+#pragma unroll
+    for (int c = 0; c < D; ++c) {
+      const Shape fs = face_shape(g, c);
+      const long step = c == 0 ? (long)fs.s1 * fs.s2 : (c == 1 ? (long)fs.s2 : 1);
+      const long ql = fs.idx(I[0], I[1], I[2]);
+      double a = (double)u.c[c][ql], bb = (double)u.c[c][ql + step];
+      if (I[c] == 0) { a = 0; u.c[c][ql] = 0.f; }
+      if (I[c] == axis_len(cs, c) - 1) { bb = 0; u.c[c][ql + step] = 0.f; }
+      acc += bb - a;
+    }
+    b[q] = -acc;
+    x[q] = 0;
+    sum += -acc;
+  }
+  block_reduce2(sum, 0.0, part + 2 * blockIdx.x);
+}
+
+// fm_project_dc: after a residual, |r|^2 (which = 1 also |b|^2) and the stop
+// test |r| <= rel_tol |b|; nothing once the correction loop is done.
+__global__ void k_dc_check(DevState* st, const double* part, double rel_tol, int which) {
+  pdl_begin();
+  if (st->dc_done) return;
+  double a, b;
+  sum_partials(part, a, b);
+  if (threadIdx.x == 0) {
+    st->dc_r2 = b;
+    if (which == 1) st->dc_b2 = b;
+    if (!isfinite(b)) { st->dc_done = 1; st->nonfinite_count += 1; }
+    else if (st->dc_b2 == 0.0 || b <= rel_tol * rel_tol * st->dc_b2) st->dc_done = 1;
+  }
+}
+
+// The correction-loop versions of k_dc_residual / k_dc_load / k_dc_set_tol /
+// k_dc_update: each returns at once when the loop is done.
+template <int D>
+__global__ void __launch_bounds__(kRedThreads) k_dc_residual_g(Shape s, const double* __restrict__ b,
+                                                               const double* __restrict__ x, double* __restrict__ w,
+                                                               double* __restrict__ part, const DevState* st) {
+  pdl_begin();
+  if (st->dc_done) return;
+  const double mean = st->dc_mean;
+  double acc = 0;
+  FM_GRID_STRIDE(q, s.size()) {
+    int i, j, k;
+    unflatten(s, q, i, j, k);
+    double diag;
+    const double nb = nb_sum<double, D>(x, s, i, j, k, diag);
+    const double r = (b[q] - mean) - (diag * x[q] - nb);
+    w[q] = r;
+    acc += r * r;
+  }
+  block_reduce2(0.0, acc, part + 2 * blockIdx.x);
+}
+
+__global__ void __launch_bounds__(kRedThreads) k_dc_load_g(long n, const double* __restrict__ w,
+                                                           float* __restrict__ r, float* __restrict__ x,
+                                                           double* __restrict__ part, const DevState* st) {
+  pdl_begin();
+  if (st->dc_done) return;
+  const double inv = 1.0 / sqrt(st->dc_r2);
+  double sum = 0;
+  FM_GRID_STRIDE(q, n) {
+    const float v = (float)(w[q] * inv);
+    r[q] = v;
+    x[q] = 0.f;
+    sum += (double)v;
+  }
+  block_reduce2(sum, 0.0, part + 2 * blockIdx.x);
+}
+
+__global__ void k_dc_set_tol_g(DevState* st, double rel_tol) {
+  pdl_begin();
+  if (st->dc_done) return;
+  const double t = 0.5 * rel_tol * sqrt(st->dc_b2 / st->dc_r2);
+  st->dc_tol = t * t;
+}
+
+__global__ void k_dc_update_g(long n, double* __restrict__ x, const float* __restrict__ e, const DevState* st) {
+  pdl_begin();
+  if (st->dc_done) return;
+  const double sc = sqrt(st->dc_r2);
+  FM_GRID_STRIDE(q, n) x[q] += sc * (double)e[q];
+}
+
+// u -= grad x in FP64, rounded to FP32 (apply_bc: wall faces zero)
+template <int D>
+__global__ void k_dc_subgrad(fm_grid g, const double* __restrict__ x, MacW<float> u) {
+  pdl_begin();
+  const int c = blockIdx.y;
+  const Shape fs = face_shape(g, c);
+  const Shape cs = cell_shape(g);
+  const long q = (long)blockIdx.x * blockDim.x + threadIdx.x;
+  if (q >= fs.size()) return;
+  int I[3];
+  unflatten(fs, q, I[0], I[1], I[2]);
+  if (I[c] == 0 || I[c] == axis_len(cs, c)) { u.c[c][q] = 0.f; return; }
+  const long pc = cs.idx(I[0], I[1], I[2]);
+  const long step = c == 0 ? (long)cs.s1 * cs.s2 : (c == 1 ? cs.s2 : 1);
+  u.c[c][q] = (float)((double)u.c[c][q] - (x[pc] - x[pc - step]));
+}
+
+// End of fm_project_dc: an unconverged loop counts as a not-converged solve;
+// the state returns to plain solves (no floor, not done).
+__global__ void k_dc_finish(DevState* st) {
+  pdl_begin();
+  if (!st->dc_done) st->not_converged += 1;
+  st->dc_done = 0;
+  st->dc_tol = 0.0;
+}
+
 // subtract_grad_p + apply_bc (3D/mgpcg.py:401-427)
 template <typename T, int D>
 __global__ void k_subgrad_bc(fm_grid g, const T* __restrict__ p, MacW<T> u) {
@@ -343,7 +468,8 @@ __global__ void k_fin_mean(DevState* st, const double* part, double n) {
   sum_partials(part, a, b);
   if (threadIdx.x == 0) {
     st->mean = a / n;
-    st->done = 0; st->conv = 0; st->nonfinite = 0; st->it = 0; st->result_it = 0;
+    st->done = st->dc_done;  // 0 outside fm_project_dc
+    st->conv = 0; st->nonfinite = 0; st->it = 0; st->result_it = 0;
     st->beta = 0; st->alpha = 0;
   }
 }
@@ -381,6 +507,13 @@ __global__ void k_fin_conv(DevState* st, const double* part, double n) {
     if (!isfinite(a)) { st->nonfinite = 1; finish_solve(st); }
     else if (a < st->tol) { st->conv = 1; finish_solve(st); }
   }
+}
+
+// Node before a while loop: skip the loop when the solve is already done at
+// its start (an inner solve of a finished defect correction, a non-finite
+// start), instead of running one body of early-returning kernels.
+__global__ void k_loop_init(cudaGraphConditionalHandle h, const DevState* st) {
+  cudaGraphSetConditional(h, st->done ? 0u : 1u);
 }
 
 // Last node of the while-loop body: keep iterating until the solve is done.
@@ -1043,12 +1176,21 @@ static int build_loop_graph(fm_mgpcg* S) {
   do {
     cudaGraphConditionalHandle h;
     if (cudaGraphConditionalHandleCreate(&h, graph, 1, cudaGraphCondAssignDefault) != cudaSuccess) break;
+    cudaKernelNodeParams kp = {};
+    DevState* st_arg = S->st;
+    void* kargs[2] = {&h, &st_arg};
+    kp.func = (void*)k_loop_init;
+    kp.gridDim = dim3(1, 1, 1);
+    kp.blockDim = dim3(1, 1, 1);
+    kp.kernelParams = kargs;
+    cudaGraphNode_t init;
+    if (cudaGraphAddKernelNode(&init, graph, nullptr, 0, &kp) != cudaSuccess) break;
     cudaGraphNodeParams cp = {cudaGraphNodeTypeConditional};
     cp.conditional.handle = h;
     cp.conditional.type = cudaGraphCondTypeWhile;
     cp.conditional.size = 1;
     cudaGraphNode_t node;
-    if (cudaGraphAddNode(&node, graph, nullptr, 0, &cp) != cudaSuccess) break;
+    if (cudaGraphAddNode(&node, graph, &init, 1, &cp) != cudaSuccess) break;
     cudaGraph_t body = cp.conditional.phGraph_out[0];
     if (cudaStreamBeginCaptureToGraph(S->cap, body, nullptr, nullptr, 0, cudaStreamCaptureModeThreadLocal) !=
         cudaSuccess)
@@ -1113,6 +1255,9 @@ static int capture_solve(fm_mgpcg* S, cudaStream_t s) {
   cudaGraphConditionalHandle h;
   if ((e = cudaGraphConditionalHandleCreate(&h, graph, 1, cudaGraphCondAssignDefault)) != cudaSuccess)
     return cuda_fail(e);
+  k_loop_init<<<1, 1, 0, s>>>(h, S->st);
+  if ((e = cudaGetLastError()) != cudaSuccess) return cuda_fail(e);
+  if ((e = cudaStreamGetCaptureInfo(s, &cs, nullptr, &graph, &deps, &ndeps)) != cudaSuccess) return cuda_fail(e);
   cudaGraphNodeParams cp = {cudaGraphNodeTypeConditional};
   cp.conditional.handle = h;
   cp.conditional.type = cudaGraphCondTypeWhile;
@@ -1417,6 +1562,52 @@ int fm_mgpcg_solve_dc(fm_mgpcg* S, int b_dtype, const void* b, double* x, double
   if (rel_res) *rel_res = rel;
   if (check_cuda()) return FM_ERR_CUDA;
   return status;
+}
+
+int fm_project_dc(fm_mgpcg* S, void* ux, void* uy, void* uz, double* work, double rel_tol, int max_outer,
+                  double* p_out, void* stream) {
+  if (!S || !ux || !uy || (S->g.dim == 3 && !uz) || !work || max_outer < 1 || max_outer > 16 ||
+      !(rel_tol > 0.0))
+    return FM_ERR_ARG;
+  if (S->dtype != FM_F32) return FM_ERR_DTYPE;
+  if (S->P.check_every != 0) return FM_ERR_ARG;  // device-side loops only
+  cudaStream_t s = (cudaStream_t)stream;
+  const fm_grid g = S->g;
+  const Shape s0 = S->lv[0];
+  const long n = s0.size();
+  const int D = g.dim;
+  double* b = work;
+  double* x = work + n;
+  double* w = work + 2 * n;
+  MacW<float> u{{(float*)ux, (float*)uy, (float*)uz}};
+  const unsigned nb = blocks_for(n, 256, 148L * 16);
+  if (D == 3) launch_pdl(k_dc_div<3>, kRedBlocks, kRedThreads, 0, s, g, u, b, x, S->part);
+  else launch_pdl(k_dc_div<2>, kRedBlocks, kRedThreads, 0, s, g, u, b, x, S->part);
+  launch_pdl(k_dc_fin, 1, 256, 0, s, S->st, S->part, (double)n, 0);  // dc_mean
+  auto residual = [&](int which) {
+    if (D == 3) launch_pdl(k_dc_residual_g<3>, kRedBlocks, kRedThreads, 0, s, s0, (const double*)b, (const double*)x, w, S->part, (const DevState*)S->st);
+    else launch_pdl(k_dc_residual_g<2>, kRedBlocks, kRedThreads, 0, s, s0, (const double*)b, (const double*)x, w, S->part, (const DevState*)S->st);
+    launch_pdl(k_dc_check, 1, 256, 0, s, S->st, S->part, rel_tol, which);
+  };
+  residual(1);
+  for (int o = 0; o < max_outer; ++o) {
+    launch_pdl(k_dc_load_g, kRedBlocks, kRedThreads, 0, s, n, (const double*)w, (float*)S->r[0], (float*)S->x,
+               S->part, (const DevState*)S->st);
+    launch_pdl(k_dc_set_tol_g, 1, 1, 0, s, S->st, rel_tol);
+    const int st = run_solve<float>(S, s, nullptr, nullptr);
+    if (st) return st;
+    launch_pdl(k_dc_update_g, nb, 256, 0, s, n, x, (const float*)S->x, (const DevState*)S->st);
+    residual(2);
+  }
+  long maxf = 0;
+  for (int c = 0; c < D; ++c) maxf = face_shape(g, c).size() > maxf ? face_shape(g, c).size() : maxf;
+  dim3 fgrid((unsigned)((maxf + 255) / 256), (unsigned)D, 1);
+  if (D == 3) launch_pdl(k_dc_subgrad<3>, fgrid, 256, 0, s, g, (const double*)x, u);
+  else launch_pdl(k_dc_subgrad<2>, fgrid, 256, 0, s, g, (const double*)x, u);
+  launch_pdl(k_dc_finish, 1, 1, 0, s, S->st);
+  if (p_out) cudaMemcpyAsync(p_out, x, sizeof(double) * n, cudaMemcpyDeviceToDevice, s);
+  if (check_cuda()) return FM_ERR_CUDA;
+  return FM_OK;
 }
 
 int fm_mgpcg_stats(fm_mgpcg* S, void* stream, int reset, fm_mg_stats* out) {

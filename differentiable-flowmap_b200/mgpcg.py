@@ -30,10 +30,14 @@ class MGPCG:
     def __init__(self, N: Sequence[int], dtype=torch.float32, *, base_level: int = 3, levels: Optional[int] = None,
                  pre_post: int = 2, bottom: int = 50, bottom_mode: int = 0, max_iters: int = 400,
                  abs_tol: float = 1e-12, rel_tol: float = 0.0, eps: float = 1e-12, check_every: int = 4,
-                 raise_on_nonconvergence: bool = False, coarse_bf16: bool = False):
+                 raise_on_nonconvergence: bool = False, coarse_bf16: bool = False, dc_rel_tol: float = 0.0,
+                 dc_max_outer: int = 4):
         """coarse_bf16 (FP32 solvers): store the per-level coarse grids between the
         finest level and the shared-memory-resident ones in BF16 (arithmetic stays
-        FP32); the preconditioner then no longer equals the FP32 V-cycle bit for bit."""
+        FP32); the preconditioner then no longer equals the FP32 V-cycle bit for bit.
+        dc_rel_tol > 0 (FP32 solvers, check_every = 0): every ``project`` runs an FP64
+        outer defect correction around the FP32 solves (fm_project_dc) until the FP64
+        residual is below dc_rel_tol |b|, at most dc_max_outer corrections."""
         self.N = tuple(int(n) for n in N)
         self.grid = GridSpec(self.N)
         self.dtype = dtype
@@ -49,6 +53,13 @@ class MGPCG:
         self.last_rtr = 0.0
         self.last_converged = True
         self.history = []
+        self.dc_rel_tol, self.dc_max_outer = float(dc_rel_tol), int(dc_max_outer)
+        self._dc_work = None
+        if self.dc_rel_tol > 0:
+            if dtype != torch.float32 or check_every != 0:
+                raise _lib.FlowmapError(2, "defect correction needs an FP32 solver in device mode (check_every=0)")
+            n = self.grid.ncell
+            self._dc_work = torch.empty(3 * n, dtype=torch.float64, device="cuda")
 
     @property
     def n_mg_levels(self) -> int:
@@ -84,6 +95,13 @@ class MGPCG:
             if tuple(x.shape) != self.grid.face_shape(c) or x.dtype != self.dtype:
                 raise _lib.FlowmapError(1, f"project: component {c} shape/dtype mismatch")
         ps = [_lib.ptr(x) for x in u] + [None] * (3 - len(u))
+        if self._dc_work is not None:
+            if p_out is not None and (p_out.dtype != torch.float64 or tuple(p_out.shape) != self.N):
+                raise _lib.FlowmapError(1, "project with defect correction: p_out must be an FP64 cell grid")
+            _lib.check(_lib.lib().fm_project_dc(self._h, ps[0], ps[1], ps[2], _lib.ptr(self._dc_work),
+                                                self.dc_rel_tol, self.dc_max_outer, _lib.ptr(p_out),
+                                                _lib.stream_ptr(stream)), "fm_project_dc")
+            return
         if self.device_mode:
             # asynchronous: the outcome is folded into stats()
             st = _lib.lib().fm_project(self._h, ps[0], ps[1], ps[2], _lib.ptr(p_out), _lib.stream_ptr(stream),
@@ -245,6 +263,13 @@ class SolidMGPCG:
             if tuple(x.shape) != self.grid.face_shape(c) or x.dtype != self.dtype:
                 raise _lib.FlowmapError(1, f"project: component {c} shape/dtype mismatch")
         ps = [_lib.ptr(x) for x in u] + [None] * (3 - len(u))
+        if self._dc_work is not None:
+            if p_out is not None and (p_out.dtype != torch.float64 or tuple(p_out.shape) != self.N):
+                raise _lib.FlowmapError(1, "project with defect correction: p_out must be an FP64 cell grid")
+            _lib.check(_lib.lib().fm_project_dc(self._h, ps[0], ps[1], ps[2], _lib.ptr(self._dc_work),
+                                                self.dc_rel_tol, self.dc_max_outer, _lib.ptr(p_out),
+                                                _lib.stream_ptr(stream)), "fm_project_dc")
+            return
         if self.device_mode:
             st = _lib.lib().fm_solid_project(self._h, ps[0], ps[1], ps[2], _lib.ptr(p_out), _lib.stream_ptr(stream),
                                              None, None)

@@ -52,6 +52,10 @@ class SolverConfig:
     eps: float = 1e-12
     check_every: int = 4
     coarse_bf16: bool = False  # FP32 solvers: per-level coarse grids stored in BF16 (arithmetic FP32)
+    # FP32 solvers: FP64 outer defect correction in every projection until the FP64
+    # residual is below dc_rel_tol |b| (0: off), at most dc_max_outer corrections
+    dc_rel_tol: float = 0.0
+    dc_max_outer: int = 4
 
 
 @dataclass
@@ -230,7 +234,9 @@ class LFM_Simulator:
             self.solver = MGPCG(g.shape, dt_, base_level=sc.base_level, levels=sc.levels, pre_post=sc.pre_post,
                                 bottom=sc.bottom, bottom_mode=sc.bottom_mode, max_iters=sc.max_iters,
                                 abs_tol=sc.abs_tol, rel_tol=sc.rel_tol, eps=sc.eps, check_every=sc.check_every,
-                                coarse_bf16=sc.coarse_bf16 and dt_ == torch.float32)
+                                coarse_bf16=sc.coarse_bf16 and dt_ == torch.float32,
+                                dc_rel_tol=sc.dc_rel_tol if dt_ == torch.float32 else 0.0,
+                                dc_max_outer=sc.dc_max_outer)
 
         # flow maps: backward (psi, T) and forward (phi, F); centre maps for scalars
         self.psi = torch.zeros((self.dim,) + g.shape, dtype=dt_, device=dev)

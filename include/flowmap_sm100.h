@@ -254,6 +254,23 @@ int fm_mg_vcycle(fm_mgpcg *solver, const void *r, void *z, void *stream);
 int fm_mgpcg_solve_dc(fm_mgpcg *solver, int b_dtype, const void *b, double *x, double *work, double rel_tol,
                       int max_outer, void *stream, int *outer_iters, int *inner_iters, double *rel_res);
 
+/* Poisson(u) (3D/mgpcg.py:207-289 with apply_bc, divergence and
+ * subtract_grad_p, :368-427) with an FP64 outer defect correction around the
+ * FP32 MGPCG of `solver` (an FM_F32 handle in device mode, check_every == 0).
+ * The correction loop has no reference counterpart (the reference solves in
+ * FP32 only): b = -div u and every residual b - mean(b) - A x are formed in
+ * FP64; each correction solves A e = r/|r| with the FP32 MGPCG (its own
+ * tolerances, floored at what the outer target needs) and adds |r| e to x in
+ * FP64; the loop stops when |r| <= rel_tol |b - mean b| or after max_outer
+ * (1..16) corrections (counted as a not-converged solve in fm_mgpcg_stats);
+ * then u -= grad x in FP64, rounded to FP32.  Every stop decision is taken on
+ * the device: no host synchronisation, and on a capturing stream the whole
+ * projection is recorded (each inner solve a conditional while node).
+ * work: 3 x cells doubles of caller-owned scratch (b, x, r).  p_out (FP64 cell
+ * grid, may be NULL) receives x. */
+int fm_project_dc(fm_mgpcg *solver, void *ux, void *uy, void *uz, double *work, double rel_tol, int max_outer,
+                  double *p_out, void *stream);
+
 /* Cumulative solver outcome (synchronises `stream`).  reset != 0 zeroes the
  * counters afterwards.  The reference reports non-convergence only with a
  * print (3D/mgpcg.py:286-289); here it is counted. */

@@ -67,3 +67,10 @@ def test_launch_counter_exported(fm):
 def test_last_cuda_error_reported(fm):
     code, name = fm._lib.last_cuda_error()
     assert isinstance(code, int) and name.startswith("cuda")
+
+
+def test_project_dc_arguments_rejected(fm):
+    """fm_project_dc: a NULL solver, NULL fields or work, rel_tol <= 0: argument
+    errors returned before any device work."""
+    lib = fm._lib.lib()
+    assert lib.fm_project_dc(None, None, None, None, None, 1e-10, 4, None, None) == 2

@@ -123,3 +123,80 @@ def test_mixed_solve_fp64_rhs_and_limits(fm, cuda):
     assert float(x0.abs().max()) == 0.0
     z, oz, iz, rz = sol.solve_mixed(torch.zeros_like(b), rel_tol=1e-10)
     assert oz == 0 and float(z.abs().max()) == 0.0
+
+
+# ---------------------------------------------------------------- fm_project_dc
+def _div64(u):
+    """-div of a MAC velocity with the wall faces zeroed, in FP64 (numpy)."""
+    out = None
+    for c, f in enumerate(u):
+        f = np.array(f, dtype=np.float64, copy=True)
+        lo = [slice(None)] * f.ndim
+        hi = [slice(None)] * f.ndim
+        lo[c], hi[c] = 0, -1
+        f[tuple(lo)] = 0.0
+        f[tuple(hi)] = 0.0
+        d = np.diff(f, axis=c)
+        out = d if out is None else out + d
+    return -out
+
+
+@pytest.mark.parametrize("shape,levels", [((64, 64, 64), 4), ((256, 256), 5), ((48, 32, 40), 3)])
+def test_project_dc_matches_fp64_projection(fm, cuda, shape, levels):
+    """The FP32 projection with FP64 defect correction lands within FP32
+    rounding of the FP64 projection of the same velocity, while the plain FP32
+    projection at its tightest reachable tolerance stays far from it."""
+    rng = np.random.default_rng(11)
+    u = [rng.normal(size=tuple(n + (a == c) for a, n in enumerate(shape))).astype(np.float32)
+         for c in range(len(shape))]
+    s64 = fm.MGPCG(shape, torch.float64, levels=levels, abs_tol=0.0, rel_tol=1e-26, eps=0.0, max_iters=400,
+                   check_every=0)
+    u64 = [torch.tensor(x, dtype=torch.float64, device=cuda) for x in u]
+    s64.project(u64)
+    sdc = fm.MGPCG(shape, torch.float32, levels=levels, abs_tol=0.0, rel_tol=1e-6, max_iters=100, check_every=0,
+                   dc_rel_tol=1e-10, dc_max_outer=8)
+    udc = [torch.tensor(x, device=cuda) for x in u]
+    p = torch.empty(shape, dtype=torch.float64, device=cuda)
+    sdc.project(udc, p_out=p)
+    st = sdc.stats(reset=True)
+    assert st["not_converged"] == 0 and st["nonfinite"] == 0
+    assert 1 <= st["solves"] <= 8  # inner solves, one per correction
+    scale = max(float(x.abs().max()) for x in u64)
+    err = max(float((a.double() - b).abs().max()) for a, b in zip(udc, u64)) / scale
+    assert err < 2e-6, err
+    # the FP64 residual of the returned pressure
+    b = _div64(u)
+    bh = b - b.mean()
+    res = np.linalg.norm(bh - _laplacian64(p.cpu().numpy())) / np.linalg.norm(bh)
+    assert res <= 1e-10, res
+    # the plain FP32 projection at relative z.r 1e-8
+    s32 = fm.MGPCG(shape, torch.float32, levels=levels, abs_tol=0.0, rel_tol=1e-8, max_iters=100, check_every=0)
+    u32 = [torch.tensor(x, device=cuda) for x in u]
+    s32.project(u32)
+    err32 = max(float((a.double() - b).abs().max()) for a, b in zip(u32, u64)) / scale
+    assert err < err32, (err, err32)
+
+
+def test_project_dc_recorded_in_a_graph_equals_eager(fm, cuda):
+    shape = (32, 32, 32)
+    rng = np.random.default_rng(12)
+    u = [rng.normal(size=tuple(n + (a == c) for a, n in enumerate(shape))).astype(np.float32) for c in range(3)]
+    sdc = fm.MGPCG(shape, torch.float32, levels=3, abs_tol=0.0, rel_tol=1e-6, max_iters=100, check_every=0,
+                   dc_rel_tol=1e-10, dc_max_outer=8)
+    ue = [torch.tensor(x, device=cuda) for x in u]
+    sdc.project(ue)
+    ug = [torch.tensor(x, device=cuda) for x in u]
+    src = [x.clone() for x in ug]
+    s = torch.cuda.Stream()
+    torch.cuda.synchronize()
+    graph = torch.cuda.CUDAGraph()
+    with torch.cuda.graph(graph, stream=s):
+        for a, b in zip(ug, src):
+            a.copy_(b)
+        sdc.project(ug)
+    for _ in range(2):
+        graph.replay()
+        torch.cuda.synchronize()
+        for a, b in zip(ug, ue):
+            assert torch.equal(a, b)
+
