@@ -265,6 +265,229 @@ __global__ void __launch_bounds__(kStThreads) k_fixed_grad_dot2(fm_grid g, T dx,
   }
 }
 
+// ---------------------------------------------------------------------------
+// 3D: plane-streaming form.  A CTA owns a kSJ x kSK tile of output nodes in
+// (j, k) and walks an i-chunk of kSI outputs plane by plane.  For every input
+// plane it loads the (j, k) footprint of every term's two fields once, contracts
+// it along k (a sliding register window where the tile's stencils advance one
+// tap per node) and then along j, and keeps the last NZ+1 contracted planes in
+// registers; an output node is finished by the i contraction from that ring as
+// soon as its last plane has been read.  Each input value is read from memory
+// once per i-chunk (plus the chunk's NZ-1 halo planes), and all three terms of
+// nabla_u_w share one pass.  Stencil tables, the clamp band and sample()'s
+// index clamp are those of k_fixed_grad_dot3; only the summation order differs.
+// ---------------------------------------------------------------------------
+constexpr int kSJ = 16, kSK = 32, kSI = 16;
+constexpr int kSThreads = 256;  // 32 k-lanes x 8 j-pairs
+
+template <typename T, int ORDER, int NT>
+struct StreamSmem {
+  static constexpr int NZ = Taps<ORDER>::nz;
+  static constexpr int FJ = kSJ + NZ - 1, FK = kSK + NZ - 1;
+  static constexpr size_t plane = (size_t)NT * 2 * FJ * FK;   // footprints [a][f][jj][kk]
+  static constexpr size_t kpass = (size_t)NT * 2 * FJ * kSK;  // after the k pass [a][f][jj][k]
+  static constexpr size_t bytes = sizeof(T) * (plane + kpass);
+};
+
+template <typename T, int ORDER, int NT>
+__global__ void __launch_bounds__(kSThreads) k_src_stream3(fm_grid g, T dx, int c, StTerms<T> terms,
+                                                           T* __restrict__ out) {
+  using SM = StreamSmem<T, ORDER, NT>;
+  constexpr int NZ = SM::NZ, FJ = SM::FJ, FK = SM::FK, NR = NZ + 1;
+  extern __shared__ __align__(16) unsigned char ss_raw[];
+  T* sP = reinterpret_cast<T*>(ss_raw);
+  T* sA = sP + SM::plane;
+  __shared__ int bI[NT][kSI], bJ[NT][kSJ], bK[NT][kSK];
+  __shared__ T wI[NT][2][kSI][NZ], wJ[NT][2][kSJ][NZ], wK[NT][2][kSK][NZ];
+  __shared__ int fastJ[NT], fastK[NT];
+
+  const Shape so = face_shape(g, c);
+  const int i0 = blockIdx.z * kSI, j0 = blockIdx.y * kSJ, k0 = blockIdx.x * kSK;
+  const int iend = min(i0 + kSI, so.s0);
+  const int tx = threadIdx.x & 31, ty = threadIdx.x >> 5;
+  const T inv_dx = (T)1 / dx;
+
+  // per-term axis tables: first tap and weights of every node of the tile / chunk
+  // (field f: derivative weights along the output face axis c, value weights
+  // elsewhere; field h: value weights)
+  for (int e = threadIdx.x; e < NT * (kSI + kSJ + kSK); e += blockDim.x) {
+    const int a = e / (kSI + kSJ + kSK), r = e % (kSI + kSJ + kSK);
+    const StTerm<T> tm = pick_term(terms, a);
+    int ax, loc, len;
+    T bl;
+    if (r < kSI) { ax = 0; loc = r; len = tm.s0; bl = tm.bl0; }
+    else if (r < kSI + kSJ) { ax = 1; loc = r - kSI; len = tm.s1; bl = tm.bl1; }
+    else { ax = 2; loc = r - kSI - kSJ; len = tm.s2; bl = tm.bl2; }
+    const int node = (ax == 0 ? i0 : (ax == 1 ? j0 : k0)) + loc;
+    T fi = (T)node;
+    if (ax != c) fi = fi + (T)0.5;
+    int base;
+    T w[NZ], dw[NZ];
+    axis_stencil<T, ORDER>(fi * dx, dx, bl, len, base, w, dw);
+    int* bt = ax == 0 ? &bI[a][loc] : (ax == 1 ? &bJ[a][loc] : &bK[a][loc]);
+    T* wf = ax == 0 ? &wI[a][0][loc][0] : (ax == 1 ? &wJ[a][0][loc][0] : &wK[a][0][loc][0]);
+    T* wh = ax == 0 ? &wI[a][1][loc][0] : (ax == 1 ? &wJ[a][1][loc][0] : &wK[a][1][loc][0]);
+    *bt = base;
+#pragma unroll
+    for (int t = 0; t < NZ; ++t) {
+      wf[t] = ax == c ? dw[t] : w[t];
+      wh[t] = w[t];
+    }
+  }
+  __syncthreads();
+  // fast paths: the stencils of the whole tile advance one tap per node (no clamp
+  // band inside the tile), so all nodes share one set of weights
+  if (threadIdx.x < 2 * NT) {
+    const int a = threadIdx.x >> 1;
+    const bool alongK = threadIdx.x & 1;
+    const int n = alongK ? kSK : kSJ;
+    const int* b = alongK ? &bK[a][0] : &bJ[a][0];
+    bool ok = true;
+    for (int q = 1; q < n; ++q) ok = ok && b[q] == b[0] + q;
+    if (alongK) fastK[a] = ok; else fastJ[a] = ok;
+  }
+  __syncthreads();
+
+  // planes the chunk reads, over all terms
+  int pmin = bI[0][0], pmax = bI[0][iend - 1 - i0];
+#pragma unroll
+  for (int a = 1; a < NT; ++a) {
+    pmin = min(pmin, bI[a][0]);
+    pmax = max(pmax, bI[a][iend - 1 - i0]);
+  }
+  pmax += NZ - 1;
+
+  T ring[NT][2][2][NR];  // [term][field][j of the pair][plane p - slot]
+#pragma unroll
+  for (int a = 0; a < NT; ++a)
+#pragma unroll
+    for (int f = 0; f < 2; ++f)
+#pragma unroll
+      for (int m = 0; m < 2; ++m)
+#pragma unroll
+        for (int q = 0; q < NR; ++q) ring[a][f][m][q] = (T)0;
+  int inext = i0;
+
+  for (int p = pmin; p <= pmax; ++p) {
+    // 1. footprints of plane p: rows of FK values, a warp per row (sample()'s index clamp)
+    for (int row = ty; row < NT * 2 * FJ; row += kSThreads / 32) {
+      const int a = row / (2 * FJ), f = (row / FJ) & 1, jj = row % FJ;
+      const StTerm<T> tm = pick_term(terms, a);
+      const T* src = f == 0 ? tm.f : tm.h;
+      const int gi = clampi(p, 0, tm.s0 - 1), gj = clampi(bJ[a][0] + jj, 0, tm.s1 - 1);
+      const long rb = ((long)gi * tm.s1 + gj) * tm.s2;
+      T* dst = sP + (size_t)row * FK;
+      for (int kk = tx; kk < FK; kk += 32) dst[kk] = ldg(src + rb + clampi(bK[a][0] + kk, 0, tm.s2 - 1));
+    }
+    __syncthreads();
+    // 2. k pass: segments of 4 outputs of one row
+    for (int task = threadIdx.x; task < NT * 2 * FJ * (kSK / 4); task += kSThreads) {
+      const int row = task / (kSK / 4), seg = task % (kSK / 4);
+      const int a = row / (2 * FJ), f = (row / FJ) & 1;
+      const T* src = sP + (size_t)row * FK;
+      T* dst = sA + (size_t)row * kSK + seg * 4;
+      const int kb = seg * 4;
+      if (fastK[a]) {
+        const int o = bK[a][kb] - bK[a][0];
+        T v[NZ + 3], w[NZ];
+#pragma unroll
+        for (int q = 0; q < NZ + 3; ++q) v[q] = src[o + q];
+#pragma unroll
+        for (int t = 0; t < NZ; ++t) w[t] = wK[a][f][kb][t];
+#pragma unroll
+        for (int m = 0; m < 4; ++m) {
+          T acc = 0;
+#pragma unroll
+          for (int t = 0; t < NZ; ++t) acc += v[m + t] * w[t];
+          dst[m] = acc;
+        }
+      } else {
+#pragma unroll
+        for (int m = 0; m < 4; ++m) {
+          const int o = bK[a][kb + m] - bK[a][0];
+          T acc = 0;
+#pragma unroll
+          for (int t = 0; t < NZ; ++t) acc += src[o + t] * wK[a][f][kb + m][t];
+          dst[m] = acc;
+        }
+      }
+    }
+    __syncthreads();
+    // 3. j pass for this thread's nodes (j = 2 ty, 2 ty + 1; k = tx), into the ring
+    const int ja = 2 * ty;
+#pragma unroll
+    for (int a = 0; a < NT; ++a) {
+#pragma unroll
+      for (int f = 0; f < 2; ++f) {
+        const T* col = sA + (size_t)(a * 2 + f) * FJ * kSK + tx;
+        T r0 = 0, r1 = 0;
+        if (fastJ[a]) {
+          const int o = bJ[a][ja] - bJ[a][0];
+          T v[NZ + 1];
+#pragma unroll
+          for (int q = 0; q < NZ + 1; ++q) v[q] = col[(o + q) * kSK];
+#pragma unroll
+          for (int t = 0; t < NZ; ++t) {
+            const T w = wJ[a][f][ja][t];
+            r0 += v[t] * w;
+            r1 += v[t + 1] * w;
+          }
+        } else {
+          const int o0 = bJ[a][ja] - bJ[a][0], o1 = bJ[a][ja + 1] - bJ[a][0];
+#pragma unroll
+          for (int t = 0; t < NZ; ++t) {
+            r0 += col[(o0 + t) * kSK] * wJ[a][f][ja][t];
+            r1 += col[(o1 + t) * kSK] * wJ[a][f][ja + 1][t];
+          }
+        }
+#pragma unroll
+        for (int q = NR - 1; q > 0; --q) {
+          ring[a][f][0][q] = ring[a][f][0][q - 1];
+          ring[a][f][1][q] = ring[a][f][1][q - 1];
+        }
+        ring[a][f][0][0] = r0;
+        ring[a][f][1][0] = r1;
+      }
+    }
+    // 4. finish every output whose last plane (over all terms) is p
+    while (inext < iend) {
+      const int li = inext - i0;
+      int e = bI[0][li];
+#pragma unroll
+      for (int a = 1; a < NT; ++a) e = max(e, bI[a][li]);
+      if (e + NZ - 1 != p) break;
+      T acc0 = 0, acc1 = 0;
+#pragma unroll
+      for (int a = 0; a < NT; ++a) {
+        const int d = e - bI[a][li];  // 0 or 1: this term's window ended one plane earlier
+        T gf0 = 0, gf1 = 0, hh0 = 0, hh1 = 0;
+#pragma unroll
+        for (int t = 0; t < NZ; ++t) {
+          const int slot = NZ - 1 - t;  // plane bI + t sits at ring slot d + NZ - 1 - t
+          const T f0 = d ? ring[a][0][0][slot + 1] : ring[a][0][0][slot];
+          const T f1 = d ? ring[a][0][1][slot + 1] : ring[a][0][1][slot];
+          const T h0 = d ? ring[a][1][0][slot + 1] : ring[a][1][0][slot];
+          const T h1 = d ? ring[a][1][1][slot + 1] : ring[a][1][1][slot];
+          const T wf = wI[a][0][li][t], wh = wI[a][1][li][t];
+          gf0 += f0 * wf;
+          gf1 += f1 * wf;
+          hh0 += h0 * wh;
+          hh1 += h1 * wh;
+        }
+        acc0 += (gf0 * inv_dx) * hh0;
+        acc1 += (gf1 * inv_dx) * hh1;
+      }
+      const int k = k0 + tx;
+      if (k < so.s2) {
+        if (j0 + ja < so.s1) out[so.idx(inext, j0 + ja, k)] = acc0;
+        if (j0 + ja + 1 < so.s1) out[so.idx(inext, j0 + ja + 1, k)] = acc1;
+      }
+      ++inext;
+    }
+    __syncthreads();
+  }
+}
+
 template <typename T, int ORDER>
 static size_t fixed3_smem() {
   constexpr int NZ = Taps<ORDER>::nz;
@@ -276,14 +499,24 @@ template <typename T, int ORDER>
 static void launch_fixed(const fm_grid& g, T dx, int c, const StTerms<T>& terms, T* out, cudaStream_t s) {
   const Shape so = face_shape(g, c);
   if (g.dim == 3) {
-    const size_t smem = fixed3_smem<T, ORDER>();
-    static bool attr_set = false;  // per instantiation, set once
-    if (!attr_set && smem > 48 * 1024) {
-      cudaFuncSetAttribute(k_fixed_grad_dot3<T, ORDER>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
-      attr_set = true;
+    dim3 grid((so.s2 + kSK - 1) / kSK, (so.s1 + kSJ - 1) / kSJ, (so.s0 + kSI - 1) / kSI);
+    if (terms.n == 3) {
+      const size_t smem = StreamSmem<T, ORDER, 3>::bytes;
+      static bool attr_set = false;  // per instantiation, set once
+      if (!attr_set && smem > 48 * 1024) {
+        cudaFuncSetAttribute(k_src_stream3<T, ORDER, 3>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+        attr_set = true;
+      }
+      launch(k_src_stream3<T, ORDER, 3>, grid, kSThreads, smem, s, g, dx, c, terms, out);
+    } else {
+      const size_t smem = StreamSmem<T, ORDER, 1>::bytes;
+      static bool attr_set = false;
+      if (!attr_set && smem > 48 * 1024) {
+        cudaFuncSetAttribute(k_src_stream3<T, ORDER, 1>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+        attr_set = true;
+      }
+      launch(k_src_stream3<T, ORDER, 1>, grid, kSThreads, smem, s, g, dx, c, terms, out);
     }
-    dim3 grid((so.s2 + kTK3 - 1) / kTK3, (so.s1 + kTJ3 - 1) / kTJ3, (so.s0 + kTI3 - 1) / kTI3);
-    launch(k_fixed_grad_dot3<T, ORDER>, grid, kStThreads, smem, s, g, dx, c, terms, out);
   } else {
     dim3 grid((so.s1 + kTJ2 - 1) / kTJ2, (so.s0 + kTI2 - 1) / kTI2, 1);
     launch(k_fixed_grad_dot2<T, ORDER>, grid, kStThreads, 0, s, g, dx, c, terms, out);

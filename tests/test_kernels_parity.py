@@ -405,3 +405,33 @@ def test_paired_advection_equals_two_calls(fm, cuda, shape, rk):
     fm.kernels.advect_scalar_grid(g, rk, dx, -0.6 * dx, u0, s, s3)
     fm.kernels.advect_scalar_grid(g, rk, dx, -0.6 * dx, u0, t, t3)
     assert torch.equal(s2, s3) and torch.equal(t2, t3)
+
+
+@pytest.mark.parametrize("order", [3, 4])
+@pytest.mark.parametrize("big", [(40, 48, 72), (17, 35, 66)], ids=lambda s: "x".join(map(str, s)))
+def test_adjoint_sources_multi_tile(fm, cuda, big, prec, order):
+    """The 3D adjoint-source stencils on grids spanning several CTA tiles and
+    i-chunks in every direction, with interior tiles (shared-weight fast paths)
+    and ragged, clamped edges: nabla_u_w and nabla_scalar_adjoint vs the oracle."""
+    rng, o, dtype, tol, dx = setup(big, prec, 17)
+    g = fm.GridSpec(big)
+    u = _rand_mac(rng, big, 1.0)
+    w = _rand_mac(rng, big, 1.0)
+    ref = [np.zeros(g.face_shape(c), o.dtype) for c in range(3)]
+    cv = lambda L: [np.array(x, dtype=o.dtype, copy=True) for x in L]
+    o.calculate_nabla_u_w(cv(u), cv(w), ref, dx, order)
+    out = [torch.zeros(g.face_shape(c), dtype=dtype, device=cuda) for c in range(3)]
+    fm.kernels.nabla_u_w(g, dx, [_t(x, dtype, cuda) for x in u], [_t(x, dtype, cuda) for x in w], out, order)
+    torch.cuda.synchronize()
+    for c in range(3):
+        assert _rel(_np(out[c]), ref[c]) < tol
+    if order == 3:
+        s = rng.uniform(0, 1, size=big)
+        a = rng.uniform(-1, 1, size=big)
+        ref = [np.zeros(g.face_shape(c), o.dtype) for c in range(3)]
+        o.calculate_nabla_scalar_adjoint(s.astype(o.dtype), a.astype(o.dtype), ref, dx)
+        out = [torch.zeros(g.face_shape(c), dtype=dtype, device=cuda) for c in range(3)]
+        fm.kernels.nabla_scalar_adjoint(g, dx, _t(s, dtype, cuda), _t(a, dtype, cuda), out)
+        torch.cuda.synchronize()
+        for c in range(3):
+            assert _rel(_np(out[c]), ref[c]) < tol
