@@ -717,6 +717,109 @@ __global__ void __launch_bounds__(kPairBX* kPairBY) k_smooth_pair(Shape s, const
   z[q] = to_s<S>(div_nd((T)to_c(r[q]) + nb, nd));
 }
 
+// Two RBGS half-sweeps of a 3D level in one launch (temporal blocking).  A CTA
+// owns a kRbI x kRbJ x kRbK tile; it stages z on the tile plus a two-cell halo
+// and r on the tile plus a one-cell halo in shared memory, updates colour A on
+// the tile and its one-cell halo (which reads colour B on the two-cell halo),
+// then colour B on the tile (which reads the new colour A), and writes the
+// tile.  Halo cells are recomputed by every CTA that needs them with the same
+// operations, so the result equals the two separate half-sweeps bit for bit:
+// every update is div_nd(r + neighbour sum, nd) with the neighbours summed in
+// the reference order (+i, -i, +j, -j, +k, -k) from +0.0, cells outside the
+// domain contributing +0.0 (which leaves the sum unchanged), and colour-A
+// values rounded to the level's storage type before colour B reads them.
+// mode 0: the first pair from z = 0 (red = r / nd, black from it), r recentred
+// by st->mean when `recenter` (level 0 of the first V-cycle); 1: (red, black);
+// 2: (black, red).
+constexpr int kRbJ = 8, kRbK = 32, kRbThreads = 256;
+
+template <int TI>
+struct RbTile {
+  static constexpr int ZI = TI + 4, ZJ = kRbJ + 4, ZK = kRbK + 4;  // z: tile + 2
+  static constexpr int RI = TI + 2, RJ = kRbJ + 2, RK = kRbK + 2;  // r: tile + 1
+  static constexpr int nz = ZI * ZJ * ZK, nr = RI * RJ * RK;
+};
+
+template <typename T, typename S, int TI>
+__global__ void __launch_bounds__(kRbThreads) k_rb_pair3(Shape s, S* __restrict__ r, S* __restrict__ z, int mode,
+                                                         int recenter, const DevState* st) {
+  using G = RbTile<TI>;
+  pdl_begin();
+  if (st->done) return;
+  extern __shared__ __align__(16) unsigned char rb_raw[];
+  T* zs = reinterpret_cast<T*>(rb_raw);
+  T* rs = zs + G::nz;
+  const int i0 = blockIdx.z * TI, j0 = blockIdx.y * kRbJ, k0 = blockIdx.x * kRbK;
+  const T mean = recenter ? (T)st->mean : (T)0;
+  const unsigned si = (unsigned)s.s1 * s.s2, sj = s.s2;
+  // stage r (tile + 1) and z (tile + 2; zero outside the domain, all zero in mode 0)
+  for (int e = threadIdx.x; e < G::nr; e += kRbThreads) {
+    const int kk = e % G::RK, jj = (e / G::RK) % G::RJ, ii = e / (G::RK * G::RJ);
+    const int i = i0 - 1 + ii, j = j0 - 1 + jj, k = k0 - 1 + kk;
+    T v = 0;
+    if (i >= 0 && i < s.s0 && j >= 0 && j < s.s1 && k >= 0 && k < s.s2) {
+      v = (T)to_c(r[((unsigned)i * s.s1 + j) * s.s2 + k]);
+      if (recenter) v = v - mean;
+    }
+    rs[e] = v;
+  }
+  for (int e = threadIdx.x; e < G::nz; e += kRbThreads) {
+    const int kk = e % G::ZK, jj = (e / G::ZK) % G::ZJ, ii = e / (G::ZK * G::ZJ);
+    const int i = i0 - 2 + ii, j = j0 - 2 + jj, k = k0 - 2 + kk;
+    T v = 0;
+    if (mode != 0 && i >= 0 && i < s.s0 && j >= 0 && j < s.s1 && k >= 0 && k < s.s2)
+      v = (T)to_c(z[((unsigned)i * s.s1 + j) * s.s2 + k]);
+    zs[e] = v;
+  }
+  __syncthreads();
+  const int colA = mode == 2 ? 1 : 0;  // the colour updated first
+  // update of the colour-c cell of each (i, j, k-pair) in a box of the tile
+  // (lo = -1: with the one-cell halo), reading zs
+  auto half = [&](int c, int lo) {
+    const int ni = TI - 2 * lo, nj = kRbJ - 2 * lo, np = (kRbK - 2 * lo) / 2;
+    for (int e = threadIdx.x; e < ni * nj * np; e += kRbThreads) {
+      const int pk = e % np, jj = (e / np) % nj, ii = e / (np * nj);
+      const int i = i0 + lo + ii, j = j0 + lo + jj;
+      int k = k0 + lo + 2 * pk;
+      k += ((i + j + k) & 1) != c;  // the colour-c cell of the pair
+      if (i < 0 || i >= s.s0 || j < 0 || j >= s.s1 || k < 0 || k >= s.s2) continue;
+      const int zi = i - i0 + 2, zj = j - j0 + 2, zk = k - k0 + 2;
+      const int q = (zi * G::ZJ + zj) * G::ZK + zk;
+      const int nd = diag_of<3>(s, i, j, k);
+      const T rv = rs[((zi - 1) * G::RJ + (zj - 1)) * G::RK + (zk - 1)];
+      T v;
+      if (mode == 0 && c == colA) {
+        v = div_nd(rv, nd);
+      } else {
+        T acc = 0;
+        acc += zs[q + G::ZJ * G::ZK];
+        acc += zs[q - G::ZJ * G::ZK];
+        acc += zs[q + G::ZK];
+        acc += zs[q - G::ZK];
+        acc += zs[q + 1];
+        acc += zs[q - 1];
+        v = div_nd(rv + acc, nd);
+      }
+      zs[q] = (T)to_c(to_s<S>(v));
+    }
+  };
+  half(colA, -1);
+  __syncthreads();
+  half(colA ^ 1, 0);
+  __syncthreads();
+  // write the tile (both colours; r too when recentred)
+  for (int e = threadIdx.x; e < TI * kRbJ * kRbK; e += kRbThreads) {
+    const int kk = e % kRbK, jj = (e / kRbK) % kRbJ, ii = e / (kRbK * kRbJ);
+    const int i = i0 + ii, j = j0 + jj, k = k0 + kk;
+    if (i >= s.s0 || j >= s.s1 || k >= s.s2) continue;
+    const unsigned g = ((unsigned)i * s.s1 + j) * s.s2 + k;
+    z[g] = to_s<S>(zs[((ii + 2) * G::ZJ + (jj + 2)) * G::ZK + (kk + 2)]);
+    if (recenter) r[g] = to_s<S>(rs[((ii + 1) * G::RJ + (jj + 1)) * G::RK + (kk + 1)]);
+  }
+  (void)si;
+  (void)sj;
+}
+
 // First red sweep from z == 0 over pairs (fuses z.fill(0)); optionally recentres r.
 template <typename T, int D, typename S = T>
 __global__ void __launch_bounds__(kPairBX* kPairBY) k_smooth_first_pair(Shape s, S* __restrict__ r, S* __restrict__ z,
@@ -1062,10 +1165,32 @@ static void launch_vcycle(fm_mgpcg* S, cudaStream_t s, bool dot_last, bool recen
     if (bf(l)) launch_pdl(k_smooth_pair<T, D, BF>, pair_grid(sh), pblk, 0, s, sh, (const BF*)S->r[l], (BF*)S->z[l], phase, S->st);
     else launch_pdl(k_smooth_pair<T, D>, pair_grid(sh), pblk, 0, s, sh, (const T*)r[l], z[l], phase, S->st);
   };
+  // two half-sweeps per launch (k_rb_pair3) on 3D levels
+  auto rb_pair = [&](int l, int mode, int rec) {
+    const Shape sh = S->lv[l];
+    const bool wide = std::is_same<T, float>::value &&
+                      (long)((sh.s0 + 7) / 8) * ((sh.s1 + kRbJ - 1) / kRbJ) * ((sh.s2 + kRbK - 1) / kRbK) >= 2 * 148;
+    const int ti = wide ? 8 : 4;
+    const dim3 grid((unsigned)((sh.s2 + kRbK - 1) / kRbK), (unsigned)((sh.s1 + kRbJ - 1) / kRbJ),
+                    (unsigned)((sh.s0 + ti - 1) / ti));
+    if (wide) {
+      const size_t sm = sizeof(T) * (RbTile<8>::nz + RbTile<8>::nr);
+      if (bf(l)) launch_pdl(k_rb_pair3<T, BF, 8>, grid, kRbThreads, sm, s, sh, (BF*)S->r[l], (BF*)S->z[l], mode, rec, (const DevState*)S->st);
+      else launch_pdl(k_rb_pair3<T, T, 8>, grid, kRbThreads, sm, s, sh, r[l], z[l], mode, rec, (const DevState*)S->st);
+    } else {
+      const size_t sm = sizeof(T) * (RbTile<4>::nz + RbTile<4>::nr);
+      if (bf(l)) launch_pdl(k_rb_pair3<T, BF, 4>, grid, kRbThreads, sm, s, sh, (BF*)S->r[l], (BF*)S->z[l], mode, rec, (const DevState*)S->st);
+      else launch_pdl(k_rb_pair3<T, T, 4>, grid, kRbThreads, sm, s, sh, r[l], z[l], mode, rec, (const DevState*)S->st);
+    }
+  };
   for (int l = 0; l < lc; ++l) {
     const Shape sh = S->lv[l];
     const dim3 pg = pair_grid(sh);
     for (int it = 0; it < P.pre_post; ++it) {
+      if (D == 3) {
+        rb_pair(l, it == 0 ? 0 : 1, it == 0 && l == 0 && recenter ? 1 : 0);
+        continue;
+      }
       if (it == 0) {
         if (bf(l)) launch_pdl(k_smooth_first_pair<T, D, BF>, pg, pblk, 0, s, sh, (BF*)S->r[l], (BF*)S->z[l], S->st, 0);
         else launch_pdl(k_smooth_first_pair<T, D>, pg, pblk, 0, s, sh, r[l], z[l], S->st, l == 0 && recenter ? 1 : 0);
@@ -1124,8 +1249,12 @@ static void launch_vcycle(fm_mgpcg* S, cudaStream_t s, bool dot_last, bool recen
     else
       launch_pdl(k_prolong<T, D>, nb, 256, 0, s, sh, sc, z[l], (const T*)z[l + 1], S->st);
     for (int it = 0; it < P.pre_post; ++it) {
-      sweep(l, 1);
       const bool last = dot_last && l == 0 && it == P.pre_post - 1;
+      if (D == 3 && !last) {
+        rb_pair(l, 2, 0);
+        continue;
+      }
+      sweep(l, 1);
       if (last) launch_pdl(k_smooth<T, D, true>, kRedBlocks, kRedThreads, 0, s, sh, r[l], z[l], 0, S->part, S->st);
       else sweep(l, 0);
     }

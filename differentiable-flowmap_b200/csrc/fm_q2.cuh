@@ -45,6 +45,20 @@ struct Q2Lim {
   }
 };
 
+// floor(s) as a float and as an int for 1 <= s < 2^23: the integer is read
+// from the mantissa of floor(s) + 2^23 instead of a float->int conversion (an
+// XU-pipe instruction).  Exact: the same values as floor() and (int) floor().
+__device__ __forceinline__ float floor_pos(float s, int& i) {
+  const float f = floorf(s);
+  i = __float_as_int(__fadd_rn(f, 8388608.0f)) - 0x4B000000;  // exact: f is an integer below 2^23
+  return f;
+}
+__device__ __forceinline__ double floor_pos(double s, int& i) {
+  const double f = floor(s);
+  i = (int)f;
+  return f;
+}
+
 template <typename T, bool GRAD>
 struct Q2 {
   int i0;
@@ -54,11 +68,12 @@ struct Q2 {
     const T u = pos_scaled - bl;
     T s = u < hi ? u : hi;
     s = s > (T)1 ? s : (T)1;
-    const T iu = floor(s);
+    int ii;
+    const T iu = floor_pos(s, ii);  // s >= 1 after the clamp
     const T f = s - iu;
     const bool up = f >= (T)0.5;
     const T t = up ? f - (T)1 : f;
-    i0 = (int)iu - 1 + (up ? 1 : 0);
+    i0 = ii - 1 + (up ? 1 : 0);
     const T a = (T)0.5 - t, b = (T)0.5 + t;
     w0 = (T)0.5 * (a * a);
     w1 = (T)0.75 - t * t;
