@@ -263,13 +263,6 @@ class SolidMGPCG:
             if tuple(x.shape) != self.grid.face_shape(c) or x.dtype != self.dtype:
                 raise _lib.FlowmapError(1, f"project: component {c} shape/dtype mismatch")
         ps = [_lib.ptr(x) for x in u] + [None] * (3 - len(u))
-        if self._dc_work is not None:
-            if p_out is not None and (p_out.dtype != torch.float64 or tuple(p_out.shape) != self.N):
-                raise _lib.FlowmapError(1, "project with defect correction: p_out must be an FP64 cell grid")
-            _lib.check(_lib.lib().fm_project_dc(self._h, ps[0], ps[1], ps[2], _lib.ptr(self._dc_work),
-                                                self.dc_rel_tol, self.dc_max_outer, _lib.ptr(p_out),
-                                                _lib.stream_ptr(stream)), "fm_project_dc")
-            return
         if self.device_mode:
             st = _lib.lib().fm_solid_project(self._h, ps[0], ps[1], ps[2], _lib.ptr(p_out), _lib.stream_ptr(stream),
                                              None, None)
