@@ -71,7 +71,7 @@ __global__ void __launch_bounds__(kStThreads) k_fixed_grad_dot2(fm_grid g, T dx,
                                                                   T* __restrict__ out) {
   constexpr int NZ = Taps<ORDER>::nz;
   constexpr int TI = kTI2, TJ = kTJ2;
-  constexpr int FI = TI + NZ, FJ = TJ + NZ;  // first taps spread over up to TI / TJ cells (see below)
+  constexpr int FI = TI + NZ + 2, FJ = TJ + NZ + 2;  // one tap of margin on each side (see below)
   constexpr int NOUT = TI * TJ / kStThreads;
   __shared__ T sF[2 * FI * FJ];
   __shared__ T sA[2 * FI * TJ];
@@ -105,7 +105,7 @@ __global__ void __launch_bounds__(kStThreads) k_fixed_grad_dot2(fm_grid g, T dx,
       for (int t = 0; t < NZ; ++t) { wt[loc * NZ + t] = w[t]; dt[loc * NZ + t] = dw[t]; }
     }
     __syncthreads();
-    const int li = bI[0], lj = bJ[0];
+    const int li = bI[0] - 1, lj = bJ[0] - 1;
     for (int e = threadIdx.x; e < FI * FJ; e += blockDim.x) {
       const int jj = e % FJ, ii = e / FJ;
       const long q = (long)clampi(li + ii, 0, tm.s0 - 1) * tm.s1 + clampi(lj + jj, 0, tm.s1 - 1);
@@ -175,7 +175,7 @@ constexpr int kSThreads = 256;  // 32 k-lanes x 8 j-pairs
 template <typename T, int ORDER>
 struct StreamSmem {
   static constexpr int NZ = Taps<ORDER>::nz;
-  static constexpr int FJ = kSJ + NZ, FK = kSK + NZ;
+  static constexpr int FJ = kSJ + NZ + 2, FK = kSK + NZ + 2;  // one tap of margin on each side
   static constexpr int ROWS = 2 * FJ;                          // footprint rows of the two fields
   static constexpr int RPW = (ROWS + kSThreads / 32 - 1) / (kSThreads / 32);  // rows per warp
   static constexpr size_t plane = (size_t)ROWS * FK;           // [f][jj][kk]
@@ -248,8 +248,13 @@ __global__ void __launch_bounds__(kSThreads) k_src_stream3(fm_grid g, T dx, int 
 
   for (int a = 0; a < NT; ++a) {
     const StTerm<T> tm = pick_term(terms, a);
-    const int pmin = bI[a][0], pmax = bI[a][iend - 1 - i0] + NZ - 1;
-    const int lj = bJ[a][0], lk = bK[a][0];
+    int pmin = bI[a][0], pmax = bI[a][0];
+    for (int q = 1; q < iend - i0; ++q) {
+      pmin = min(pmin, bI[a][q]);
+      pmax = max(pmax, bI[a][q]);
+    }
+    pmax += NZ - 1;
+    const int lj = bJ[a][0] - 1, lk = bK[a][0] - 1;
     // this lane's footprint columns (sample()'s index clamp) and rows
     const int gk0 = clampi(lk + tx, 0, tm.s2 - 1), gk1 = clampi(lk + tx + 32, 0, tm.s2 - 1);
     const bool col1 = tx + 32 < FK;
@@ -299,7 +304,7 @@ __global__ void __launch_bounds__(kSThreads) k_src_stream3(fm_grid g, T dx, int 
         if (fastK[a]) {
           T v[NZ + 3], w[NZ];
 #pragma unroll
-          for (int q = 0; q < NZ + 3; ++q) v[q] = src[kb + q];
+          for (int q = 0; q < NZ + 3; ++q) v[q] = src[kb + 1 + q];
 #pragma unroll
           for (int t = 0; t < NZ; ++t) w[t] = wK[a][f][kb][t];
 #pragma unroll
@@ -329,7 +334,7 @@ __global__ void __launch_bounds__(kSThreads) k_src_stream3(fm_grid g, T dx, int 
         if (fastJ[a]) {
           T v[NZ + 1];
 #pragma unroll
-          for (int q = 0; q < NZ + 1; ++q) v[q] = col[(ja + q) * kSK];
+          for (int q = 0; q < NZ + 1; ++q) v[q] = col[(ja + 1 + q) * kSK];
 #pragma unroll
           for (int t = 0; t < NZ; ++t) {
             const T w = wJ[a][f][ja][t];
@@ -352,17 +357,21 @@ __global__ void __launch_bounds__(kSThreads) k_src_stream3(fm_grid g, T dx, int 
         ring[f][0][0] = r0;
         ring[f][1][0] = r1;
       }
-      // 4. this term of every output whose last plane is p (plane bI + t at ring slot NZ - 1 - t)
-      while (inext < iend && bI[a][inext - i0] + NZ - 1 == p) {
+      // 4. this term of every output whose last plane is p (or p - 1 where the
+      // first taps step back by one: plane bI + t then sits at ring slot
+      // d + NZ - 1 - t with d = p - (bI + NZ - 1))
+      while (inext < iend && bI[a][inext - i0] + NZ - 1 <= p) {
         const int li = inext - i0;
+        const bool d = bI[a][li] + NZ - 1 < p;
         T gf0 = 0, gf1 = 0, hh0 = 0, hh1 = 0;
 #pragma unroll
         for (int t = 0; t < NZ; ++t) {
           const T wf = wI[a][0][li][t], wh = wI[a][1][li][t];
-          gf0 += ring[0][0][NZ - 1 - t] * wf;
-          gf1 += ring[0][1][NZ - 1 - t] * wf;
-          hh0 += ring[1][0][NZ - 1 - t] * wh;
-          hh1 += ring[1][1][NZ - 1 - t] * wh;
+          const int sl = NZ - 1 - t;
+          gf0 += (d ? ring[0][0][sl + 1] : ring[0][0][sl]) * wf;
+          gf1 += (d ? ring[0][1][sl + 1] : ring[0][1][sl]) * wf;
+          hh0 += (d ? ring[1][0][sl + 1] : ring[1][0][sl]) * wh;
+          hh1 += (d ? ring[1][1][sl + 1] : ring[1][1][sl]) * wh;
         }
         T* o = sO + (li * kSJ + ja) * kSK + tx;
         o[0] += (gf0 * inv_dx) * hh0;
@@ -388,21 +397,14 @@ static void launch_fixed(const fm_grid& g, T dx, int c, const StTerms<T>& terms,
   const Shape so = face_shape(g, c);
   if (g.dim == 3) {
     dim3 grid((so.s2 + kSK - 1) / kSK, (so.s1 + kSJ - 1) / kSJ, (so.s0 + kSI - 1) / kSI);
+    // dynamic plus static shared memory exceeds the default 48 KB window: the
+    // dynamic limit is raised whatever the dynamic part alone needs
+    const size_t smem = StreamSmem<T, ORDER>::bytes;
     if (terms.n == 3) {
-      const size_t smem = StreamSmem<T, ORDER>::bytes;
-      static bool attr_set = false;  // per instantiation, set once
-      if (!attr_set && smem > 48 * 1024) {
-        cudaFuncSetAttribute(k_src_stream3<T, ORDER, 3>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
-        attr_set = true;
-      }
+      if (!raise_smem_limit(k_src_stream3<T, ORDER, 3>, smem)) return;
       launch(k_src_stream3<T, ORDER, 3>, grid, kSThreads, smem, s, g, dx, c, terms, out);
     } else {
-      const size_t smem = StreamSmem<T, ORDER>::bytes;
-      static bool attr_set = false;
-      if (!attr_set && smem > 48 * 1024) {
-        cudaFuncSetAttribute(k_src_stream3<T, ORDER, 1>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
-        attr_set = true;
-      }
+      if (!raise_smem_limit(k_src_stream3<T, ORDER, 1>, smem)) return;
       launch(k_src_stream3<T, ORDER, 1>, grid, kSThreads, smem, s, g, dx, c, terms, out);
     }
   } else {
