@@ -520,6 +520,18 @@ def run_shape2d(a):
     c64 = replace(c64, solver=replace(c64.solver, eps=0.0))
     s64 = S.LFM_Diff_Simulator(config=c64, device=dev)
     l64, g64 = s64.gradient([x.double() for x in d_u0], d_r0.double(), d_rt.double())
+    del s64
+    # the same gradient with the tightest FP32 solve that converges (relative z.r 1e-10)
+    c10 = C.shape2d_config(res=256, steps=200, reinit_every=12, rk=2, dt=0.01, dtype=f32, rel_tol=1e-10,
+                           max_iters=100, check_every=0)
+    s10 = S.LFM_Diff_Simulator(config=c10, device=dev)
+    ms10, (l10, g10), _ = timed(lambda: s10.gradient(d_u0, d_r0, d_rt))
+    st10 = s10.solver_stats
+    accurate = {"solver_rel_tol_zr": 1e-10, "ms": ms10, "grads_per_s": 1e3 / ms10,
+                "mean_pcg_iters": st10["iterations"] / max(st10["solves"], 1),
+                "grad_error_vs_fp64": {"grad_rel_l2": rel_l2(g10, g64), "loss_rel": abs(l10 - l64) / abs(l64)},
+                "launch": "eager"}
+    del s10
     line = {"metric": "2D shape transition dL/du0 evaluations/s, 256^2, 200 steps", "value": 1e3 / ms,
             "unit": "grads/s", "n_gpus": 1, "steps": a.steps, "warmup": a.warmup, "ms_per_step": ms,
             "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic",
@@ -536,6 +548,9 @@ def run_shape2d(a):
                        "solves_per_grad": stats["solves"] // max(a.warmup + a.steps, 1)},
             "loss": loss, "grad_error_vs_fp64": {"grad_rel_l2": rel_l2(grad, g64), "loss_rel": abs(loss - l64) / abs(l64),
                                                  "fp64_reference": "projections to relative z.r 1e-22"},
+            "accurate_solve": accurate,
+            "note": ("the rectangles' discontinuous density makes the adjoint sources amplify FP32 rounding: the "
+                     "gradient error vs FP64 stays near 3e-4 even with FP64 defect-corrected projections"),
             "trajectory_gb": sim.trajectory_bytes() / 1e9}
     print(json.dumps(line), flush=True)
     return 0

@@ -169,7 +169,7 @@ __global__ void __launch_bounds__(kStThreads) k_fixed_grad_dot2(fm_grid g, T dx,
 // rounding error, so over a tile of n nodes the first taps spread over up to n
 // (not n - 1) cells: the footprints hold n + NZ values.
 // ---------------------------------------------------------------------------
-constexpr int kSJ = 16, kSK = 32, kSI = 16;
+constexpr int kSJ = 16, kSK = 32, kSI = 4;
 constexpr int kSThreads = 256;  // 32 k-lanes x 8 j-pairs
 
 template <typename T, int ORDER>
@@ -185,7 +185,7 @@ struct StreamSmem {
 };
 
 template <typename T, int ORDER, int NT>
-__global__ void __launch_bounds__(kSThreads) k_src_stream3(fm_grid g, T dx, int c, StTerms<T> terms,
+__global__ void __launch_bounds__(kSThreads, 3) k_src_stream3(fm_grid g, T dx, int c, StTerms<T> terms,
                                                            T* __restrict__ out) {
   using SM = StreamSmem<T, ORDER>;
   constexpr int NZ = SM::NZ, FJ = SM::FJ, FK = SM::FK, NR = NZ + 1, RPW = SM::RPW;
