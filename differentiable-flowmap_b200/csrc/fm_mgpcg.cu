@@ -717,101 +717,6 @@ __global__ void __launch_bounds__(kPairBX* kPairBY) k_smooth_pair(Shape s, const
   z[q] = to_s<S>(div_nd((T)to_c(r[q]) + nb, nd));
 }
 
-// Two RBGS half-sweeps of a 3D level in one launch (temporal blocking).  A CTA
-// owns a TI x kRbJ x kRbK tile; it stages z on the tile plus a two-cell halo
-// and r on the tile plus a one-cell halo in shared memory, updates colour A on
-// the tile and its one-cell halo (which reads colour B on the two-cell halo),
-// then colour B on the tile (which reads the new colour A), and writes the
-// tile to a second buffer: the halo must be read before any CTA has
-// overwritten it, so the sweeps read `zin` and write `zout`.  Halo cells are
-// recomputed by every CTA that needs them with the same operations, so the
-// result equals the two separate half-sweeps bit for bit: every update is
-// div_nd(r + neighbour sum, nd) with the neighbours summed in the reference
-// order (+i, -i, +j, -j, +k, -k) from +0.0, cells outside the domain
-// contributing +0.0 (which leaves the sum unchanged), and colour-A values
-// rounded to the level's storage type before colour B reads them.
-// mode 0: the first pair from z = 0 (red = r / nd, black from it; zin unused);
-// 1: (red, black); 2: (black, red).
-constexpr int kRbJ = 8, kRbK = 32, kRbThreads = 256;
-
-template <int TI>
-struct RbTile {
-  static constexpr int ZI = TI + 4, ZJ = kRbJ + 4, ZK = kRbK + 4;  // z: tile + 2
-  static constexpr int RI = TI + 2, RJ = kRbJ + 2, RK = kRbK + 2;  // r: tile + 1
-  static constexpr int nz = ZI * ZJ * ZK, nr = RI * RJ * RK;
-};
-
-template <typename T, typename S, int TI>
-__global__ void __launch_bounds__(kRbThreads) k_rb_pair3(Shape s, const S* __restrict__ r, const S* __restrict__ zin,
-                                                         S* __restrict__ zout, int mode, const DevState* st) {
-  using G = RbTile<TI>;
-  pdl_begin();
-  if (st->done) return;
-  extern __shared__ __align__(16) unsigned char rb_raw[];
-  T* zs = reinterpret_cast<T*>(rb_raw);
-  T* rs = zs + G::nz;
-  const int i0 = blockIdx.z * TI, j0 = blockIdx.y * kRbJ, k0 = blockIdx.x * kRbK;
-  // stage r (tile + 1) and z (tile + 2; zero outside the domain, all zero in mode 0)
-  for (int e = threadIdx.x; e < G::nr; e += kRbThreads) {
-    const int kk = e % G::RK, jj = (e / G::RK) % G::RJ, ii = e / (G::RK * G::RJ);
-    const int i = i0 - 1 + ii, j = j0 - 1 + jj, k = k0 - 1 + kk;
-    T v = 0;
-    if (i >= 0 && i < s.s0 && j >= 0 && j < s.s1 && k >= 0 && k < s.s2)
-      v = (T)to_c(r[((unsigned)i * s.s1 + j) * s.s2 + k]);
-    rs[e] = v;
-  }
-  for (int e = threadIdx.x; e < G::nz; e += kRbThreads) {
-    const int kk = e % G::ZK, jj = (e / G::ZK) % G::ZJ, ii = e / (G::ZK * G::ZJ);
-    const int i = i0 - 2 + ii, j = j0 - 2 + jj, k = k0 - 2 + kk;
-    T v = 0;
-    if (mode != 0 && i >= 0 && i < s.s0 && j >= 0 && j < s.s1 && k >= 0 && k < s.s2)
-      v = (T)to_c(zin[((unsigned)i * s.s1 + j) * s.s2 + k]);
-    zs[e] = v;
-  }
-  __syncthreads();
-  const int colA = mode == 2 ? 1 : 0;  // the colour updated first
-  // update of the colour-c cell of each (i, j, k-pair) in a box of the tile
-  // (lo = -1: with the one-cell halo), reading zs
-  auto half = [&](int c, int lo) {
-    const int ni = TI - 2 * lo, nj = kRbJ - 2 * lo, np = (kRbK - 2 * lo) / 2;
-    for (int e = threadIdx.x; e < ni * nj * np; e += kRbThreads) {
-      const int pk = e % np, jj = (e / np) % nj, ii = e / (np * nj);
-      const int i = i0 + lo + ii, j = j0 + lo + jj;
-      int k = k0 + lo + 2 * pk;
-      k += ((i + j + k) & 1) != c;  // the colour-c cell of the pair
-      if (i < 0 || i >= s.s0 || j < 0 || j >= s.s1 || k < 0 || k >= s.s2) continue;
-      const int zi = i - i0 + 2, zj = j - j0 + 2, zk = k - k0 + 2;
-      const int q = (zi * G::ZJ + zj) * G::ZK + zk;
-      const int nd = diag_of<3>(s, i, j, k);
-      const T rv = rs[((zi - 1) * G::RJ + (zj - 1)) * G::RK + (zk - 1)];
-      T v;
-      if (mode == 0 && c == colA) {
-        v = div_nd(rv, nd);
-      } else {
-        T acc = 0;
-        acc += zs[q + G::ZJ * G::ZK];
-        acc += zs[q - G::ZJ * G::ZK];
-        acc += zs[q + G::ZK];
-        acc += zs[q - G::ZK];
-        acc += zs[q + 1];
-        acc += zs[q - 1];
-        v = div_nd(rv + acc, nd);
-      }
-      zs[q] = (T)to_c(to_s<S>(v));
-    }
-  };
-  half(colA, -1);
-  __syncthreads();
-  half(colA ^ 1, 0);
-  __syncthreads();
-  for (int e = threadIdx.x; e < TI * kRbJ * kRbK; e += kRbThreads) {
-    const int kk = e % kRbK, jj = (e / kRbK) % kRbJ, ii = e / (kRbK * kRbJ);
-    const int i = i0 + ii, j = j0 + jj, k = k0 + kk;
-    if (i >= s.s0 || j >= s.s1 || k >= s.s2) continue;
-    zout[((unsigned)i * s.s1 + j) * s.s2 + k] = to_s<S>(zs[((ii + 2) * G::ZJ + (jj + 2)) * G::ZK + (kk + 2)]);
-  }
-}
-
 // First red sweep from z == 0 over pairs (fuses z.fill(0)); optionally recentres r.
 template <typename T, int D, typename S = T>
 __global__ void __launch_bounds__(kPairBX* kPairBY) k_smooth_first_pair(Shape s, S* __restrict__ r, S* __restrict__ z,
@@ -1015,7 +920,6 @@ struct fm_mgpcg {
   Shape lv[kMaxLevels];
   void* r[kMaxLevels];
   void* z[kMaxLevels];
-  void* z2[kMaxLevels];  // second z of the levels smoothed by k_rb_pair3 (3D), 0 elsewhere
   void* x;
   void* p;
   void* Ap;
@@ -1140,11 +1044,7 @@ static void launch_vcycle(fm_mgpcg* S, cudaStream_t s, bool dot_last, bool recen
   const int L = S->L;
   const fm_mg_params& P = S->P;
   T** r = (T**)S->r;
-  // the buffer holding each level's current z: the fused pairs alternate
-  // between S->z[l] and S->z2[l]
-  void* zc[kMaxLevels];
-  for (int l = 0; l < kMaxLevels; ++l) zc[l] = S->z[l];
-  T** z = (T**)zc;
+  T** z = (T**)S->z;
   const long cap = 148L * 16;
   const int lc = S->lc > 0 ? S->lc : L - 1;  // first level not smoothed by per-level launches
   const dim3 pblk(kPairBX, kPairBY, 1);
@@ -1159,44 +1059,15 @@ static void launch_vcycle(fm_mgpcg* S, cudaStream_t s, bool dot_last, bool recen
   auto bf = [&](int l) { return std::is_same<T, float>::value && l >= 1 && l < S->bf16_hi; };
   auto sweep = [&](int l, int phase) {
     const Shape sh = S->lv[l];
-    if (bf(l)) launch_pdl(k_smooth_pair<T, D, BF>, pair_grid(sh), pblk, 0, s, sh, (const BF*)S->r[l], (BF*)zc[l], phase, S->st);
+    if (bf(l)) launch_pdl(k_smooth_pair<T, D, BF>, pair_grid(sh), pblk, 0, s, sh, (const BF*)S->r[l], (BF*)S->z[l], phase, S->st);
     else launch_pdl(k_smooth_pair<T, D>, pair_grid(sh), pblk, 0, s, sh, (const T*)r[l], z[l], phase, S->st);
   };
-  // two half-sweeps per launch (k_rb_pair3) on 3D levels; modes 1 and 2 read
-  // the current z and write the level's other buffer
-  auto rb_pair = [&](int l, int mode) {
-    const Shape sh = S->lv[l];
-    const bool wide = std::is_same<T, float>::value &&
-                      (long)((sh.s0 + 7) / 8) * ((sh.s1 + kRbJ - 1) / kRbJ) * ((sh.s2 + kRbK - 1) / kRbK) >= 2 * 148;
-    const int ti = wide ? 8 : 4;
-    const dim3 grid((unsigned)((sh.s2 + kRbK - 1) / kRbK), (unsigned)((sh.s1 + kRbJ - 1) / kRbJ),
-                    (unsigned)((sh.s0 + ti - 1) / ti));
-    void* zin = zc[l];
-    void* zout = mode == 0 ? zc[l] : (zc[l] == S->z[l] ? S->z2[l] : S->z[l]);
-    const DevState* stc = S->st;
-    if (wide) {
-      const size_t sm = sizeof(T) * (RbTile<8>::nz + RbTile<8>::nr);
-      if (bf(l)) launch_pdl(k_rb_pair3<T, BF, 8>, grid, kRbThreads, sm, s, sh, (const BF*)S->r[l], (const BF*)zin, (BF*)zout, mode, stc);
-      else launch_pdl(k_rb_pair3<T, T, 8>, grid, kRbThreads, sm, s, sh, (const T*)r[l], (const T*)zin, (T*)zout, mode, stc);
-    } else {
-      const size_t sm = sizeof(T) * (RbTile<4>::nz + RbTile<4>::nr);
-      if (bf(l)) launch_pdl(k_rb_pair3<T, BF, 4>, grid, kRbThreads, sm, s, sh, (const BF*)S->r[l], (const BF*)zin, (BF*)zout, mode, stc);
-      else launch_pdl(k_rb_pair3<T, T, 4>, grid, kRbThreads, sm, s, sh, (const T*)r[l], (const T*)zin, (T*)zout, mode, stc);
-    }
-    zc[l] = zout;
-  };
-  const bool fused = D == 3 && S->z2[0] != nullptr;
   for (int l = 0; l < lc; ++l) {
     const Shape sh = S->lv[l];
     const dim3 pg = pair_grid(sh);
     for (int it = 0; it < P.pre_post; ++it) {
-      // the recentring first sweep writes r in place: it stays a separate launch
-      if (fused && !(it == 0 && l == 0 && recenter)) {
-        rb_pair(l, it == 0 ? 0 : 1);
-        continue;
-      }
       if (it == 0) {
-        if (bf(l)) launch_pdl(k_smooth_first_pair<T, D, BF>, pg, pblk, 0, s, sh, (BF*)S->r[l], (BF*)zc[l], S->st, 0);
+        if (bf(l)) launch_pdl(k_smooth_first_pair<T, D, BF>, pg, pblk, 0, s, sh, (BF*)S->r[l], (BF*)S->z[l], S->st, 0);
         else launch_pdl(k_smooth_first_pair<T, D>, pg, pblk, 0, s, sh, r[l], z[l], S->st, l == 0 && recenter ? 1 : 0);
       } else {
         sweep(l, 0);
@@ -1206,9 +1077,9 @@ static void launch_vcycle(fm_mgpcg* S, cudaStream_t s, bool dot_last, bool recen
     const Shape sc = S->lv[l + 1];
     const unsigned rb = blocks_for(sc.size(), 256, cap);
     if (bf(l) && bf(l + 1))
-      launch_pdl(k_restrict<T, D, BF, BF>, rb, 256, 0, s, sh, sc, (const BF*)S->r[l], (const BF*)zc[l], (BF*)S->r[l + 1], S->st);
+      launch_pdl(k_restrict<T, D, BF, BF>, rb, 256, 0, s, sh, sc, (const BF*)S->r[l], (const BF*)S->z[l], (BF*)S->r[l + 1], S->st);
     else if (bf(l))
-      launch_pdl(k_restrict<T, D, BF, T>, rb, 256, 0, s, sh, sc, (const BF*)S->r[l], (const BF*)zc[l], r[l + 1], S->st);
+      launch_pdl(k_restrict<T, D, BF, T>, rb, 256, 0, s, sh, sc, (const BF*)S->r[l], (const BF*)S->z[l], r[l + 1], S->st);
     else if (bf(l + 1))
       launch_pdl(k_restrict<T, D, T, BF>, rb, 256, 0, s, sh, sc, (const T*)r[l], (const T*)z[l], (BF*)S->r[l + 1], S->st);
     else
@@ -1245,26 +1116,20 @@ static void launch_vcycle(fm_mgpcg* S, cudaStream_t s, bool dot_last, bool recen
     const Shape sc = S->lv[l + 1];
     const unsigned nb = blocks_for(sh.size(), 256, cap);
     if (bf(l) && bf(l + 1))
-      launch_pdl(k_prolong<T, D, BF, BF>, nb, 256, 0, s, sh, sc, (BF*)zc[l], (const BF*)zc[l + 1], S->st);
+      launch_pdl(k_prolong<T, D, BF, BF>, nb, 256, 0, s, sh, sc, (BF*)S->z[l], (const BF*)S->z[l + 1], S->st);
     else if (bf(l))
-      launch_pdl(k_prolong<T, D, BF, T>, nb, 256, 0, s, sh, sc, (BF*)zc[l], (const T*)z[l + 1], S->st);
+      launch_pdl(k_prolong<T, D, BF, T>, nb, 256, 0, s, sh, sc, (BF*)S->z[l], (const T*)z[l + 1], S->st);
     else if (bf(l + 1))
-      launch_pdl(k_prolong<T, D, T, BF>, nb, 256, 0, s, sh, sc, z[l], (const BF*)zc[l + 1], S->st);
+      launch_pdl(k_prolong<T, D, T, BF>, nb, 256, 0, s, sh, sc, z[l], (const BF*)S->z[l + 1], S->st);
     else
       launch_pdl(k_prolong<T, D>, nb, 256, 0, s, sh, sc, z[l], (const T*)z[l + 1], S->st);
     for (int it = 0; it < P.pre_post; ++it) {
-      const bool last = dot_last && l == 0 && it == P.pre_post - 1;
-      if (fused && !last) {
-        rb_pair(l, 2);
-        continue;
-      }
       sweep(l, 1);
+      const bool last = dot_last && l == 0 && it == P.pre_post - 1;
       if (last) launch_pdl(k_smooth<T, D, true>, kRedBlocks, kRedThreads, 0, s, sh, r[l], z[l], 0, S->part, S->st);
       else sweep(l, 0);
     }
   }
-  if (zc[0] != S->z[0])  // an odd number of fused pairs on the finest level
-    cudaMemcpyAsync(S->z[0], zc[0], sizeof(T) * S->lv[0].size(), cudaMemcpyDeviceToDevice, s);
   if (dot_last && L == 1) {
     // single-level: z.r over the bottom result
     launch_pdl(k_smooth<T, D, true>, kRedBlocks, kRedThreads, 0, s, sb, r[0], z[0], 2 /* no update */, S->part, S->st);
@@ -1525,14 +1390,6 @@ int fm_mgpcg_create(const fm_grid* g, int dtype, const fm_mg_params* params, fm_
     ok = ok && cudaMalloc(&S->r[l], e * S->lv[l].size()) == cudaSuccess;
     ok = ok && cudaMalloc(&S->z[l], e * S->lv[l].size()) == cudaSuccess;
   }
-  // second z buffers for the fused RBGS pairs of the per-level sweeps (3D)
-  if (g->dim == 3) {
-    const int lcs = S->lc > 0 ? S->lc : S->L - 1;
-    for (int l = 0; l < lcs; ++l) {
-      const size_t e = (l >= 1 && l < S->bf16_hi) ? sizeof(__nv_bfloat16) : es;
-      ok = ok && cudaMalloc(&S->z2[l], e * S->lv[l].size()) == cudaSuccess;
-    }
-  }
   const long n0 = S->lv[0].size();
   ok = ok && cudaMalloc(&S->x, es * n0) == cudaSuccess;
   ok = ok && cudaMalloc(&S->p, es * n0) == cudaSuccess;
@@ -1571,7 +1428,6 @@ int fm_mgpcg_destroy(fm_mgpcg* S) {
   for (int l = 0; l < kMaxLevels; ++l) {
     if (S->r[l]) cudaFree(S->r[l]);
     if (S->z[l]) cudaFree(S->z[l]);
-    if (S->z2[l]) cudaFree(S->z2[l]);
   }
   if (S->x) cudaFree(S->x);
   if (S->p) cudaFree(S->p);
