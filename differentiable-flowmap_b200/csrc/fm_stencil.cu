@@ -13,6 +13,8 @@
 // Weights, first taps and the clamp band follow the reference exactly
 // (s = clamp(X/dx - BL, 1, len-2-eps), taps iu+lo+t, sample() index clamp);
 // only the summation order differs.
+#include <cmath>
+
 #include "fm_common.cuh"
 #include "fm_internal.h"
 
@@ -20,7 +22,7 @@ namespace fm {
 
 // 3D tile: TI x TJ x TK output nodes (k contiguous); 2D: TI x TJ (j contiguous)
 constexpr int kTI3 = 8, kTJ3 = 8, kTK3 = 32;
-constexpr int kTI2 = 12, kTJ2 = 64;
+constexpr int kTI2 = 16, kTJ2 = 64;
 constexpr int kStThreads = 256;
 
 template <typename T>
@@ -67,13 +69,13 @@ __device__ __forceinline__ void axis_stencil(T pos, T dx, T bl, int len, int& ba
 
 __device__ __forceinline__ int clampi(int v, int lo, int hi) { return v < lo ? lo : (v > hi ? hi : v); }
 
-template <typename T, int ORDER>
+template <typename T, int ORDER, int M>
 __global__ void __launch_bounds__(kStThreads) k_fixed_grad_dot3(fm_grid g, T dx, int c, StTerms<T> terms,
                                                                   T* __restrict__ out) {
   constexpr int NZ = Taps<ORDER>::nz;
   constexpr int TI = kTI3, TJ = kTJ3, TK = kTK3;
-  // footprint: taps from the tile's first base - 1 (see fixed3_smem)
-  constexpr int FI = TI + NZ + 1, FJ = TJ + NZ + 1, FK = TK + NZ + 1;
+  // footprint: taps from the tile's first base - M (see fixed3_smem)
+  constexpr int FI = TI + NZ - 1 + 2 * M, FJ = TJ + NZ - 1 + 2 * M, FK = TK + NZ - 1 + 2 * M;
   constexpr int NOUT = TI * TJ * TK / kStThreads;
   // dynamic shared: [F | H] footprints, then [Af | Ah] after the k pass; the
   // j pass reuses the footprint region for [Bf | Bh]
@@ -115,7 +117,7 @@ __global__ void __launch_bounds__(kStThreads) k_fixed_grad_dot3(fm_grid g, T dx,
       for (int t = 0; t < NZ; ++t) { wt[loc * NZ + t] = w[t]; dt[loc * NZ + t] = dw[t]; }
     }
     __syncthreads();
-    const int li = bI[0] - 1, lj = bJ[0] - 1, lk = bK[0] - 1;
+    const int li = bI[0] - M, lj = bJ[0] - M, lk = bK[0] - M;
     // footprint (clamped indices: sample())
     for (int e = threadIdx.x; e < FI * FJ * FK; e += blockDim.x) {
       const int kk = e % FK, jj = (e / FK) % FJ, ii = e / (FK * FJ);
@@ -182,12 +184,12 @@ __global__ void __launch_bounds__(kStThreads) k_fixed_grad_dot3(fm_grid g, T dx,
   }
 }
 
-template <typename T, int ORDER>
+template <typename T, int ORDER, int M>
 __global__ void __launch_bounds__(kStThreads) k_fixed_grad_dot2(fm_grid g, T dx, int c, StTerms<T> terms,
                                                                   T* __restrict__ out) {
   constexpr int NZ = Taps<ORDER>::nz;
-  constexpr int TI = kTI2, TJ = kTJ2;
-  constexpr int FI = TI + NZ + 1, FJ = TJ + NZ + 1;  // taps from the first base - 1 (see fixed3_smem)
+  constexpr int TI = M ? kTI2 - 4 : kTI2, TJ = kTJ2;  // the wider footprint of M = 1 fits 48 KB in FP64
+  constexpr int FI = TI + NZ - 1 + 2 * M, FJ = TJ + NZ - 1 + 2 * M;  // taps from the first base - M (fixed3_smem)
   constexpr int NOUT = TI * TJ / kStThreads;
   __shared__ T sF[2 * FI * FJ];
   __shared__ T sA[2 * FI * TJ];
@@ -221,7 +223,7 @@ __global__ void __launch_bounds__(kStThreads) k_fixed_grad_dot2(fm_grid g, T dx,
       for (int t = 0; t < NZ; ++t) { wt[loc * NZ + t] = w[t]; dt[loc * NZ + t] = dw[t]; }
     }
     __syncthreads();
-    const int li = bI[0] - 1, lj = bJ[0] - 1;
+    const int li = bI[0] - M, lj = bJ[0] - M;
     for (int e = threadIdx.x; e < FI * FJ; e += blockDim.x) {
       const int jj = e % FJ, ii = e / FJ;
       const long q = (long)clampi(li + ii, 0, tm.s0 - 1) * tm.s1 + clampi(lj + jj, 0, tm.s1 - 1);
@@ -266,29 +268,46 @@ __global__ void __launch_bounds__(kStThreads) k_fixed_grad_dot2(fm_grid g, T dx,
   }
 }
 
-template <typename T, int ORDER>
+// A node's first tap is floor(node position / dx - BL) plus a constant.  With a
+// power-of-two dx the quotient is exact and the first taps of a tile of n nodes
+// lie within [b0, b0 + n - 1] of the first node's b0 (M = 0).  Otherwise the
+// quotient carries a rounding error and they lie within [b0 - 1, b0 + n]: the
+// footprints then hold n + NZ + 1 taps from b0 - 1 (M = 1).
+template <typename T, int ORDER, int M>
 static size_t fixed3_smem() {
   constexpr int NZ = Taps<ORDER>::nz;
-  // A node's first tap is floor(node position / dx - BL) plus a constant; when dx
-  // is not a power of two the quotient carries a rounding error (and the upper
-  // clamp band can move a tap), so across a tile of n nodes the first taps lie
-  // within [b0 - 1, b0 + n] of the first node's b0: footprints hold n + NZ + 1
-  // taps from b0 - 1.
-  constexpr int FI = kTI3 + NZ + 1, FJ = kTJ3 + NZ + 1, FK = kTK3 + NZ + 1;
+  constexpr int FI = kTI3 + NZ - 1 + 2 * M, FJ = kTJ3 + NZ - 1 + 2 * M, FK = kTK3 + NZ - 1 + 2 * M;
   return sizeof(T) * (2 * FI * FJ * FK + 2 * FI * FJ * kTK3);
+}
+
+static bool power_of_two(double x) {
+  int e;
+  return x > 0 && std::frexp(x, &e) == 0.5;
+}
+
+template <typename T, int ORDER, int M>
+static void launch_fixed3(const fm_grid& g, T dx, int c, const StTerms<T>& terms, T* out, cudaStream_t s) {
+  const Shape so = face_shape(g, c);
+  const size_t smem = fixed3_smem<T, ORDER, M>();
+  if (!raise_smem_limit(k_fixed_grad_dot3<T, ORDER, M>, smem)) return;
+  dim3 grid((so.s2 + kTK3 - 1) / kTK3, (so.s1 + kTJ3 - 1) / kTJ3, (so.s0 + kTI3 - 1) / kTI3);
+  launch(k_fixed_grad_dot3<T, ORDER, M>, grid, kStThreads, smem, s, g, dx, c, terms, out);
 }
 
 template <typename T, int ORDER>
 static void launch_fixed(const fm_grid& g, T dx, int c, const StTerms<T>& terms, T* out, cudaStream_t s) {
   const Shape so = face_shape(g, c);
   if (g.dim == 3) {
-    const size_t smem = fixed3_smem<T, ORDER>();
-    if (!raise_smem_limit(k_fixed_grad_dot3<T, ORDER>, smem)) return;
-    dim3 grid((so.s2 + kTK3 - 1) / kTK3, (so.s1 + kTJ3 - 1) / kTJ3, (so.s0 + kTI3 - 1) / kTI3);
-    launch(k_fixed_grad_dot3<T, ORDER>, grid, kStThreads, smem, s, g, dx, c, terms, out);
+    if (power_of_two((double)dx)) launch_fixed3<T, ORDER, 0>(g, dx, c, terms, out, s);
+    else launch_fixed3<T, ORDER, 1>(g, dx, c, terms, out, s);
   } else {
-    dim3 grid((so.s1 + kTJ2 - 1) / kTJ2, (so.s0 + kTI2 - 1) / kTI2, 1);
-    launch(k_fixed_grad_dot2<T, ORDER>, grid, kStThreads, 0, s, g, dx, c, terms, out);
+    if (power_of_two((double)dx)) {
+      dim3 grid((so.s1 + kTJ2 - 1) / kTJ2, (so.s0 + kTI2 - 1) / kTI2, 1);
+      launch(k_fixed_grad_dot2<T, ORDER, 0>, grid, kStThreads, 0, s, g, dx, c, terms, out);
+    } else {
+      dim3 grid((so.s1 + kTJ2 - 1) / kTJ2, (so.s0 + kTI2 - 5) / (kTI2 - 4), 1);
+      launch(k_fixed_grad_dot2<T, ORDER, 1>, grid, kStThreads, 0, s, g, dx, c, terms, out);
+    }
   }
 }
 
