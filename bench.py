@@ -789,6 +789,10 @@ def main():
 
     forms = bench_forms(a)
     head = headline_form(a)
+    # launch shapes (gather-kernel block sizes, adjoint-source tile height) picked by the
+    # project's autotuner on this grid shape; they change no result
+    T = importlib.import_module("differentiable-flowmap_b200.tune")
+    tuned = {k: v["threads"] for k, v in T.autotune((a.res,) * 3, rk=4, reps=5, device=dev).items()}
     sims, cfgs = {}, {}
     for f in forms:
         cfgs[f] = form_config(C, a, f, torch.float32)
@@ -932,7 +936,10 @@ def main():
                               "mg_coarse_storage": "bf16" if cfgs[f].solver.coarse_bf16 else "f32",
                               "trajectory_gb": sims_bytes[f] / 1e9, "solver": solver_stats(f),
                               "grad_error_vs_fp64": errors.get(f)} for f, r in results.items()},
-                "algorithm_gap_fp64": errors.get("algorithm_gap_fp64")}
+                "algorithm_gap_fp64": errors.get("algorithm_gap_fp64"),
+                "launch_shapes": {"autotuned": tuned,
+                                  "note": "threads per block of the gather kernels, tile height of the adjoint-source "
+                                          "stencil (tune.autotune on this grid)"}}
         for f in ("mixed", "checkpointed"):
             if "plain" in results and f in results:
                 line[f"{f}_over_plain"] = results[f]["value"] / results["plain"]["value"]

@@ -331,11 +331,13 @@ struct TuneHash {
 static std::mutex g_tune_mu;
 static std::unordered_map<TuneKey, int, TuneHash> g_tune;
 
-static inline int tuned_threads(int kind, const fm_grid& g) {
+int tuned_value(int kind, const fm_grid& g, int dflt) {
   std::lock_guard<std::mutex> lk(g_tune_mu);
   auto it = g_tune.find(TuneKey{kind, g.dim, g.n[0], g.n[1], g.n[2]});
-  return it == g_tune.end() ? kThreads : it->second;
+  return it == g_tune.end() ? dflt : it->second;
 }
+
+static inline int tuned_threads(int kind, const fm_grid& g) { return tuned_value(kind, g, kThreads); }
 
 template <typename T>
 static Mac<T> mac(const void* x, const void* y, const void* z) {
@@ -624,12 +626,18 @@ int fm_add_fields(int dtype, long n, const void* f1, const void* f2, void* dest,
 
 }  // extern "C"
 
-// Autotuner table (see tuned_threads): threads per block for one kernel class
-// on one grid shape; 32..256 in multiples of 32, or 0 to restore the default.
+// Autotuner table (see tuned_value): per kernel class and grid shape, the threads
+// per block of the gather kernels (32..256 in multiples of 32) or the adjoint-
+// source stencil's tile height (4 or 8 in 3D, 8 or 16 in 2D); 0 restores the default.
 int fm_tune_set(int kind, const fm_grid* g, int threads) {
   using namespace fm;
   if (!g || kind < 0 || kind >= FM_TUNE_KINDS) return FM_ERR_ARG;
-  if (threads != 0 && (threads < 32 || threads > kThreads || threads % 32 != 0)) return FM_ERR_ARG;
+  if (kind == FM_TUNE_ADJ_SOURCE_TILE) {
+    const bool ok = threads == 0 || (g->dim == 3 ? (threads == 4 || threads == 8) : (threads == 8 || threads == 16));
+    if (!ok) return FM_ERR_ARG;
+  } else if (threads != 0 && (threads < 32 || threads > kThreads || threads % 32 != 0)) {
+    return FM_ERR_ARG;
+  }
   std::lock_guard<std::mutex> lk(g_tune_mu);
   const TuneKey k{kind, g->dim, g->n[0], g->n[1], g->n[2]};
   if (threads == 0) g_tune.erase(k);
@@ -640,5 +648,6 @@ int fm_tune_set(int kind, const fm_grid* g, int threads) {
 int fm_tune_get(int kind, const fm_grid* g) {
   using namespace fm;
   if (!g || kind < 0 || kind >= FM_TUNE_KINDS) return -FM_ERR_ARG;
+  if (kind == FM_TUNE_ADJ_SOURCE_TILE) return tuned_value(kind, *g, g->dim == 3 ? 8 : 16);
   return tuned_threads(kind, *g);
 }

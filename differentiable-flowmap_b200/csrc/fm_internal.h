@@ -30,6 +30,9 @@ inline int validate_grid(const fm_grid* g, int dtype) {
 // Host-side count of kernels this library has launched (graph launches add
 // the number of kernel nodes they contain); read by fm_launch_count().
 extern std::atomic<long long> g_launch_count;
+// The autotuner's value for kernel class `kind` on grid g (fm_tune_set), else dflt.
+int tuned_value(int kind, const fm_grid& g, int dflt);
+
 inline void count_launch(long long n = 1) { g_launch_count.fetch_add(n, std::memory_order_relaxed); }
 
 // The CUDA error behind the most recent FM_ERR_CUDA (fm_last_cuda_error()).

@@ -21,8 +21,8 @@
 namespace fm {
 
 // 3D tile: TI x TJ x TK output nodes (k contiguous); 2D: TI x TJ (j contiguous)
-constexpr int kTI3 = 8, kTJ3 = 8, kTK3 = 32;
-constexpr int kTI2 = 16, kTJ2 = 64;
+constexpr int kTJ3 = 8, kTK3 = 32;  // the tile height along i is a template parameter (4 or 8)
+constexpr int kTJ2 = 64;  // the tile height along i is a template parameter (8, 12 or 16)
 constexpr int kStThreads = 256;
 
 template <typename T>
@@ -69,11 +69,11 @@ __device__ __forceinline__ void axis_stencil(T pos, T dx, T bl, int len, int& ba
 
 __device__ __forceinline__ int clampi(int v, int lo, int hi) { return v < lo ? lo : (v > hi ? hi : v); }
 
-template <typename T, int ORDER, int M>
+template <typename T, int ORDER, int M, int TI3>
 __global__ void __launch_bounds__(kStThreads) k_fixed_grad_dot3(fm_grid g, T dx, int c, StTerms<T> terms,
                                                                   T* __restrict__ out) {
   constexpr int NZ = Taps<ORDER>::nz;
-  constexpr int TI = kTI3, TJ = kTJ3, TK = kTK3;
+  constexpr int TI = TI3, TJ = kTJ3, TK = kTK3;
   // footprint: taps from the tile's first base - M (see fixed3_smem)
   constexpr int FI = TI + NZ - 1 + 2 * M, FJ = TJ + NZ - 1 + 2 * M, FK = TK + NZ - 1 + 2 * M;
   constexpr int NOUT = TI * TJ * TK / kStThreads;
@@ -184,11 +184,11 @@ __global__ void __launch_bounds__(kStThreads) k_fixed_grad_dot3(fm_grid g, T dx,
   }
 }
 
-template <typename T, int ORDER, int M>
+template <typename T, int ORDER, int M, int TI2>
 __global__ void __launch_bounds__(kStThreads) k_fixed_grad_dot2(fm_grid g, T dx, int c, StTerms<T> terms,
                                                                   T* __restrict__ out) {
   constexpr int NZ = Taps<ORDER>::nz;
-  constexpr int TI = M ? kTI2 - 4 : kTI2, TJ = kTJ2;  // the wider footprint of M = 1 fits 48 KB in FP64
+  constexpr int TI = TI2, TJ = kTJ2;
   constexpr int FI = TI + NZ - 1 + 2 * M, FJ = TJ + NZ - 1 + 2 * M;  // taps from the first base - M (fixed3_smem)
   constexpr int NOUT = TI * TJ / kStThreads;
   __shared__ T sF[2 * FI * FJ];
@@ -273,10 +273,10 @@ __global__ void __launch_bounds__(kStThreads) k_fixed_grad_dot2(fm_grid g, T dx,
 // lie within [b0, b0 + n - 1] of the first node's b0 (M = 0).  Otherwise the
 // quotient carries a rounding error and they lie within [b0 - 1, b0 + n]: the
 // footprints then hold n + NZ + 1 taps from b0 - 1 (M = 1).
-template <typename T, int ORDER, int M>
+template <typename T, int ORDER, int M, int TI>
 static size_t fixed3_smem() {
   constexpr int NZ = Taps<ORDER>::nz;
-  constexpr int FI = kTI3 + NZ - 1 + 2 * M, FJ = kTJ3 + NZ - 1 + 2 * M, FK = kTK3 + NZ - 1 + 2 * M;
+  constexpr int FI = TI + NZ - 1 + 2 * M, FJ = kTJ3 + NZ - 1 + 2 * M, FK = kTK3 + NZ - 1 + 2 * M;
   return sizeof(T) * (2 * FI * FJ * FK + 2 * FI * FJ * kTK3);
 }
 
@@ -285,28 +285,42 @@ static bool power_of_two(double x) {
   return x > 0 && std::frexp(x, &e) == 0.5;
 }
 
-template <typename T, int ORDER, int M>
+template <typename T, int ORDER, int M, int TI>
 static void launch_fixed3(const fm_grid& g, T dx, int c, const StTerms<T>& terms, T* out, cudaStream_t s) {
   const Shape so = face_shape(g, c);
-  const size_t smem = fixed3_smem<T, ORDER, M>();
-  if (!raise_smem_limit(k_fixed_grad_dot3<T, ORDER, M>, smem)) return;
-  dim3 grid((so.s2 + kTK3 - 1) / kTK3, (so.s1 + kTJ3 - 1) / kTJ3, (so.s0 + kTI3 - 1) / kTI3);
-  launch(k_fixed_grad_dot3<T, ORDER, M>, grid, kStThreads, smem, s, g, dx, c, terms, out);
+  const size_t smem = fixed3_smem<T, ORDER, M, TI>();
+  if (!raise_smem_limit(k_fixed_grad_dot3<T, ORDER, M, TI>, smem)) return;
+  dim3 grid((so.s2 + kTK3 - 1) / kTK3, (so.s1 + kTJ3 - 1) / kTJ3, (so.s0 + TI - 1) / TI);
+  launch(k_fixed_grad_dot3<T, ORDER, M, TI>, grid, kStThreads, smem, s, g, dx, c, terms, out);
 }
 
 template <typename T, int ORDER>
 static void launch_fixed(const fm_grid& g, T dx, int c, const StTerms<T>& terms, T* out, cudaStream_t s) {
   const Shape so = face_shape(g, c);
+  // tile height along i: the autotuner's choice (fm_tune_set, FM_TUNE_ADJ_SOURCE_TILE),
+  // else 8 in 3D and 16 in 2D; the tile changes only the speed, never a result
+  const int ti = tuned_value(FM_TUNE_ADJ_SOURCE_TILE, g, g.dim == 3 ? 8 : 16);
+  const bool exact = power_of_two((double)dx);
   if (g.dim == 3) {
-    if (power_of_two((double)dx)) launch_fixed3<T, ORDER, 0>(g, dx, c, terms, out, s);
-    else launch_fixed3<T, ORDER, 1>(g, dx, c, terms, out, s);
-  } else {
-    if (power_of_two((double)dx)) {
-      dim3 grid((so.s1 + kTJ2 - 1) / kTJ2, (so.s0 + kTI2 - 1) / kTI2, 1);
-      launch(k_fixed_grad_dot2<T, ORDER, 0>, grid, kStThreads, 0, s, g, dx, c, terms, out);
+    if (exact) {
+      if (ti == 4) launch_fixed3<T, ORDER, 0, 4>(g, dx, c, terms, out, s);
+      else launch_fixed3<T, ORDER, 0, 8>(g, dx, c, terms, out, s);
     } else {
-      dim3 grid((so.s1 + kTJ2 - 1) / kTJ2, (so.s0 + kTI2 - 5) / (kTI2 - 4), 1);
-      launch(k_fixed_grad_dot2<T, ORDER, 1>, grid, kStThreads, 0, s, g, dx, c, terms, out);
+      if (ti == 4) launch_fixed3<T, ORDER, 1, 4>(g, dx, c, terms, out, s);
+      else launch_fixed3<T, ORDER, 1, 8>(g, dx, c, terms, out, s);
+    }
+  } else {
+    // with margins a 16-row FP64 quartic tile would exceed 48 KB of static shared memory: 12 rows
+    if (ti == 8) {
+      dim3 grid((so.s1 + kTJ2 - 1) / kTJ2, (so.s0 + 7) / 8, 1);
+      if (exact) launch(k_fixed_grad_dot2<T, ORDER, 0, 8>, grid, kStThreads, 0, s, g, dx, c, terms, out);
+      else launch(k_fixed_grad_dot2<T, ORDER, 1, 8>, grid, kStThreads, 0, s, g, dx, c, terms, out);
+    } else if (exact) {
+      dim3 grid((so.s1 + kTJ2 - 1) / kTJ2, (so.s0 + 15) / 16, 1);
+      launch(k_fixed_grad_dot2<T, ORDER, 0, 16>, grid, kStThreads, 0, s, g, dx, c, terms, out);
+    } else {
+      dim3 grid((so.s1 + kTJ2 - 1) / kTJ2, (so.s0 + 11) / 12, 1);
+      launch(k_fixed_grad_dot2<T, ORDER, 1, 12>, grid, kStThreads, 0, s, g, dx, c, terms, out);
     }
   }
 }

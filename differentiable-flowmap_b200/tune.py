@@ -1,16 +1,19 @@
-"""Block-size autotuner for the gather kernels (advection, flow-map march,
-pullbacks, accumulate_init).
+"""Autotuner for launch shapes: the block size of the gather kernels
+(advection, flow-map march, pullbacks, accumulate_init) and the tile height of
+the adjoint-source stencils (nabla_u_w, nabla_scalar_adjoint).
 
-Those kernels compute every node independently, so the threads per block
-change only how the grid fills the 148 SMs -- which matters for the small 2D
-grids of the batched vortex instances (a 128^2 face grid is 64 blocks of 256).
-``autotune(shape)`` times each candidate block size on seeded fields of that
-grid shape with CUDA events, keeps the fastest per kernel class in the
-library's table (fm_tune_set) and returns the timings.  With concurrency = k
-the candidate runs as k copies on k streams at once (each on its own fields),
-which is how the kernel meets the GPU inside a batch of concurrent instances:
-a block size that is fastest alone can lose under contention.  Results are
-cached per (shape, dtype, RK order, concurrency) for the process.
+Those kernels compute every node independently, so the threads per block and
+the stencil tiles change only how the grid fills the 148 SMs (and, for the
+stencil, how much of each input footprint neighbouring tiles re-read) -- which
+matters for the small 2D grids of the batched vortex instances (a 128^2 face
+grid is 64 blocks of 256).  ``autotune(shape)`` times each candidate on seeded
+fields of that grid shape with CUDA events, keeps the fastest per kernel class
+in the library's table (fm_tune_set) and returns the timings.  With
+concurrency = k the candidate runs as k copies on k streams at once (each on
+its own fields), which is how the kernel meets the GPU inside a batch of
+concurrent instances: a launch shape that is fastest alone can lose under
+contention.  Results are cached per (shape, dtype, RK order, concurrency) for
+the process.
 """
 from __future__ import annotations
 
@@ -22,13 +25,16 @@ import torch
 from . import _lib
 from . import kernels as K
 
-KINDS = {"advect_u": 0, "advect_scalar": 1, "march": 2, "pullback_u": 3, "pullback_scalar": 4, "accumulate": 5}
-CANDIDATES = (64, 128, 256)
+KINDS = {"advect_u": 0, "advect_scalar": 1, "march": 2, "pullback_u": 3, "pullback_scalar": 4, "accumulate": 5,
+         "adjoint_sources": 6}
+CANDIDATES = (64, 128, 256)  # threads per block of the gather kernels
+TILE_CANDIDATES = {3: (4, 8), 2: (8, 16)}  # adjoint-source tile heights along i, by dimension
 _cache: Dict[Tuple, Dict[str, dict]] = {}
 
 
 def set_threads(kind: str, shape: Sequence[int], threads: int):
-    """fm_tune_set: threads per block for kernel class ``kind`` on grid ``shape`` (0: default)."""
+    """fm_tune_set: threads per block for kernel class ``kind`` on grid ``shape``
+    (the tile height for "adjoint_sources"; 0: default)."""
     g = K.GridSpec(tuple(shape))
     _lib.check(_lib.lib().fm_tune_set(KINDS[kind], C.byref(g.c_grid()), int(threads)), "fm_tune_set")
 
@@ -75,6 +81,7 @@ def _workloads(shape, dtype, rk, device):
         "pullback_u": lambda: K.pullback_u(g, dx, w, out, T_f, psi_f),
         "pullback_scalar": lambda: K.pullback_scalar(g, dx, s, s_out, psi_c),
         "accumulate": lambda: K.accumulate_init(g, dx, dt, w, init, T_f, psi_f),
+        "adjoint_sources": lambda: K.nabla_u_w(g, dx, u, w, out),
     }
 
 
@@ -104,9 +111,11 @@ def autotune(shape: Sequence[int], dtype=torch.float32, rk: int = 2, candidates:
             main.wait_stream(st)
 
     result = {}
+    dim = len(tuple(shape))
     for kind in works[0]:
         times = {}
-        for th in candidates:
+        cands = TILE_CANDIDATES[dim] if kind == "adjoint_sources" else candidates
+        for th in cands:
             set_threads(kind, shape, th)
             round_(kind, 3)
             torch.cuda.synchronize(dev)
@@ -115,7 +124,7 @@ def autotune(shape: Sequence[int], dtype=torch.float32, rk: int = 2, candidates:
             e1.record(main)
             torch.cuda.synchronize(dev)
             times[th] = e0.elapsed_time(e1) * 1e3 / reps
-        best = min(candidates, key=lambda t: (times[t], -t))
+        best = min(cands, key=lambda t: (times[t], -t))
         set_threads(kind, shape, best)
         result[kind] = {"threads": best, "us": times}
     _cache[key] = result

@@ -340,12 +340,17 @@ enum {
     FM_TUNE_PULLBACK_U = 3,      /* fm_pullback_u */
     FM_TUNE_PULLBACK_SCALAR = 4, /* fm_pullback_scalar */
     FM_TUNE_ACCUMULATE = 5,      /* fm_accumulate_init */
-    FM_TUNE_KINDS = 6
+    FM_TUNE_ADJ_SOURCE_TILE = 6, /* fm_nabla_u_w, fm_nabla_scalar_adjoint: output tile height along i */
+    FM_TUNE_KINDS = 7
 };
-/* Threads per block for kernel class `kind` on grid g: 32..256 in multiples of
- * 32, or 0 for the default (256).  Thread-safe; applies to later launches. */
+/* Kernel classes 0-5: threads per block on grid g, 32..256 in multiples of 32
+ * (default 256).  FM_TUNE_ADJ_SOURCE_TILE: the adjoint-source stencil's tile
+ * height along i, 4 or 8 output nodes in 3D (default 8), 8 or 16 in 2D
+ * (default 16; with a dx that is not a power of two, 16 runs as 12).  0
+ * restores the default.  Neither changes a result.  Thread-safe; applies to
+ * later launches. */
 int fm_tune_set(int kind, const fm_grid *g, int threads);
-/* The block size launches of `kind` on g use (256 unless set); -FM_ERR_ARG on a bad kind. */
+/* The value launches of `kind` on g use; -FM_ERR_ARG on a bad kind. */
 int fm_tune_get(int kind, const fm_grid *g);
 
 /* ------------------------------------------------------------------------
