@@ -115,8 +115,13 @@ def _vortex_setup(fm, n, steps, R, dtype, target_seed=1):
 
 
 @pytest.mark.gpu
-def test_vortex_gradient_matches_oracle_fp64(fm, cuda):
-    n, steps, R = 32, 8, 4
+@pytest.mark.parametrize("n,steps,R", [(32, 8, 4), (256, 20, 10), (192, 10, 10)],
+                         ids=["32", "256-config0-size", "192-batch-size"])
+def test_vortex_gradient_matches_oracle_fp64(fm, cuda, n, steps, R):
+    """The vortex gradient (theta -> u0 -> steps -> vorticity loss -> adjoint ->
+    dL/dtheta) against the oracle: at a small grid, at the 2D vortex benchmark's
+    256^2 over two reinit intervals, and at one of the batched instances' 192^2
+    grids, whose dx = 1/192 is not a power of two."""
     cfg, sim, prob, omt = _vortex_setup(fm, n, steps, R, torch.float64)
     theta = _C().vortex2d_theta(0)
     loss, dth = prob.gradient(theta, omt)
