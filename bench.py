@@ -1002,7 +1002,8 @@ def dominant_kernel_roofline(fm, sim, dev, stream):
     except Exception:
         pass
     hbm = peaks.get("hbm_gbs", 6650.0)
-    src = "measured" if "hbm_gbs" in peaks else "fallback"
+    src = ("measured (MEASURED_PEAKS.json hbm_gbs)" if "hbm_gbs" in peaks
+           else "fallback 6650 GB/s (no MEASURED_PEAKS.json on this machine)")
     g, K = sim.grid, fm.kernels
     psi, psi_f, T_f = sim.psi.clone(), [x.clone() for x in sim.psi_f], [x.clone() for x in sim.T_f]
     u = sim.u
@@ -1031,7 +1032,7 @@ def dominant_kernel_roofline(fm, sim, dev, stream):
     fp32_achieved = flops / (ms / 1e3) / 1e12
     return {"kernel": "k_march<float,3,4> (fm_march_map)", "bound": "hbm", "achieved": achieved, "peak": hbm,
             "unit": "GB/s", "frac": achieved / hbm, "traffic": MARCH_DRAM_BYTES_PER_LAUNCH, "ms_per_launch": ms,
-            "algorithmic_bytes_per_launch": algo, "peak_source": f"{src} (MEASURED_PEAKS.json hbm_gbs)",
+            "algorithmic_bytes_per_launch": algo, "peak_source": src,
             "traffic_source": "ncu dram__bytes_read.sum + dram__bytes_write.sum, one launch, "
                               "profiles/k_march_rk4_3d128.txt",
             "fp32": {"achieved": fp32_achieved, "peak": fp32_peak, "unit": "TFLOP/s", "frac": fp32_achieved / fp32_peak,

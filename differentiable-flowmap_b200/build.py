@@ -13,7 +13,8 @@ import sys
 HERE = os.path.dirname(os.path.abspath(__file__))
 CSRC = os.path.join(HERE, "csrc")
 LIB = os.path.join(HERE, "libflowmap_sm100.so")
-SOURCES = ["fm_flowmap.cu", "fm_mgpcg.cu", "fm_util.cu", "fm_stencil.cu", "fm_vortex.cu", "fm_force.cu", "fm_solid.cu"]
+SOURCES = ["fm_flowmap.cu", "fm_mgpcg.cu", "fm_util.cu", "fm_stencil.cu", "fm_vortex.cu", "fm_force.cu", "fm_solid.cu",
+           "fm_adjoint.cu"]
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
 
 

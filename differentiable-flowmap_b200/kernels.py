@@ -143,6 +143,49 @@ def pullback_scalar(g: GridSpec, dx: float, s0, out, psi, alpha=1.0, beta=0.0, b
                                         ptr(base), stream_ptr(stream)), "fm_pullback_scalar")
 
 
+def _mac_opt(g: GridSpec, u, name):
+    if u is not None:
+        _chk_mac(g, u, name)
+    return _mac3(u)
+
+
+def advect_scalar_grid_adj(g: GridSpec, rk: int, dx: float, dt: float, u0, s1, g_s2, g_u0=None, g_s1=None,
+                           stream=None):
+    """g_u0 += dL/du0, g_s1 += dL/ds1 for s2 = advect_scalar_grid(u0, s1), given g_s2 = dL/ds2."""
+    _chk_mac(g, u0, "u0")
+    check(_lib.lib().fm_advect_scalar_grid_adj(C.byref(g.c_grid()), _dt(u0[0]), rk, dx, dt, *_mac3(u0), ptr(s1),
+                                               ptr(g_s2), *_mac_opt(g, g_u0, "g_u0"), ptr(g_s1),
+                                               stream_ptr(stream)), "fm_advect_scalar_grid_adj")
+
+
+def advect_u_grid_adj(g: GridSpec, rk: int, dx: float, dt: float, u0, u1, g_u2, g_u0=None, g_u1=None, stream=None):
+    """g_u0 += dL/du0 (backtrace), g_u1 += dL/du1 (sampled field) for u2 = advect_u_grid(u0, u1)."""
+    for n, u in (("u0", u0), ("u1", u1), ("g_u2", g_u2)):
+        _chk_mac(g, u, n)
+    check(_lib.lib().fm_advect_u_grid_adj(C.byref(g.c_grid()), _dt(u0[0]), rk, dx, dt, *_mac3(u0), *_mac3(u1),
+                                          *_mac3(g_u2), *_mac_opt(g, g_u0, "g_u0"), *_mac_opt(g, g_u1, "g_u1"),
+                                          stream_ptr(stream)), "fm_advect_u_grid_adj")
+
+
+def pullback_u_adj(g: GridSpec, dx: float, u0, T_f, psi_f, g_out, alpha=1.0, beta=0.0, g_u0=None, g_T=None,
+                   g_psi=None, g_base=None, stream=None):
+    """Transpose of pullback_u: accumulates into g_u0, g_T, g_psi, g_base (any may be None)."""
+    _chk_mac(g, u0, "u0")
+    _chk_mac(g, g_out, "g_out")
+    check(_lib.lib().fm_pullback_u_adj(C.byref(g.c_grid()), _dt(u0[0]), dx, *_mac3(u0), *_mac3(T_f),
+                                       *_mac3(psi_f), alpha, beta, *_mac3(g_out), *_mac_opt(g, g_u0, "g_u0"),
+                                       *_mac3(g_T), *_mac3(g_psi), *_mac_opt(g, g_base, "g_base"),
+                                       stream_ptr(stream)), "fm_pullback_u_adj")
+
+
+def pullback_scalar_adj(g: GridSpec, dx: float, s0, psi, g_out, alpha=1.0, beta=0.0, g_s0=None, g_psi=None,
+                        g_base=None, stream=None):
+    """Transpose of pullback_scalar: accumulates into g_s0, g_psi, g_base (any may be None)."""
+    check(_lib.lib().fm_pullback_scalar_adj(C.byref(g.c_grid()), _dt(s0), dx, ptr(s0), ptr(psi), alpha, beta,
+                                            ptr(g_out), ptr(g_s0), ptr(g_psi), ptr(g_base), stream_ptr(stream)),
+          "fm_pullback_scalar_adj")
+
+
 def accumulate_init(g: GridSpec, dx: float, dt: float, f, init, F_f, phi_f, Hp=None, Hpp=None, ind=0, stream=None):
     ab3 = Hp is not None
     hs = []

@@ -187,6 +187,50 @@ int fm_add_fields(int dtype, long n, const void *f1, const void *f2, void *dest,
 int fm_convert(long n, int src_dtype, const void *src, int dst_dtype, void *dst, void *stream);
 
 /* ------------------------------------------------------------------------
+ * Discrete adjoints of the gather kernels (the backward passes of the
+ * per-kernel torch.autograd Functions).  Each is the exact transpose of its
+ * forward kernel's linearisation at the given inputs: the sampled field
+ * enters linearly (its gradient is a scatter of the B-spline weights), the
+ * sample position through the B-spline derivative weights (zero on an axis
+ * where the forward's position clamp is active), and an RK backtrace stage by
+ * stage in reverse.  Gradients are ADDED to the g_* buffers, which the caller
+ * zeroes; field gradients use atomic adds (their last bits depend on the
+ * order of the adds).  A g_* MAC argument is either complete or all NULL (not
+ * wanted).  The reference has no counterpart: its adjoint is the continuous
+ * one of 3D/lfm_midpoint_diff_simulator.py:390-594 (fm_nabla_* above).
+ * ------------------------------------------------------------------------ */
+/* Transpose of fm_advect_scalar_grid: g_s2 = dL/ds2 (cell grid) ->
+ * g_u0 += dL/du0, g_s1 += dL/ds1 (either may be NULL). */
+int fm_advect_scalar_grid_adj(const fm_grid *g, int dtype, int rk, double dx, double dt,
+                              const void *u0x, const void *u0y, const void *u0z, const void *s1,
+                              const void *g_s2, void *g_u0x, void *g_u0y, void *g_u0z, void *g_s1,
+                              void *stream);
+/* Transpose of fm_advect_u_grid: g_u2 = dL/du2 -> g_u0 += dL/du0 (through
+ * the backtrace), g_u1 += dL/du1 (the sampled field).  For self-advection
+ * (u1 == u0) the caller adds the two. */
+int fm_advect_u_grid_adj(const fm_grid *g, int dtype, int rk, double dx, double dt,
+                         const void *u0x, const void *u0y, const void *u0z,
+                         const void *u1x, const void *u1y, const void *u1z,
+                         const void *g_u2x, const void *g_u2y, const void *g_u2z,
+                         void *g_u0x, void *g_u0y, void *g_u0z, void *g_u1x, void *g_u1y, void *g_u1z,
+                         void *stream);
+/* Transpose of fm_pullback_u (out_c = alpha (T_c . u0(psi_c) + beta base_c)):
+ * g_out -> g_u0, g_T (D planes per face grid), g_psi (D planes), g_base. */
+int fm_pullback_u_adj(const fm_grid *g, int dtype, double dx,
+                      const void *u0x, const void *u0y, const void *u0z,
+                      const void *Tx, const void *Ty, const void *Tz,
+                      const void *psix, const void *psiy, const void *psiz,
+                      double alpha, double beta,
+                      const void *g_outx, const void *g_outy, const void *g_outz,
+                      void *g_u0x, void *g_u0y, void *g_u0z, void *g_Tx, void *g_Ty, void *g_Tz,
+                      void *g_psix, void *g_psiy, void *g_psiz, void *g_basex, void *g_basey, void *g_basez,
+                      void *stream);
+/* Transpose of fm_pullback_scalar (out = alpha (s0(psi) + beta base)):
+ * g_out -> g_s0, g_psi (D planes), g_base (each may be NULL). */
+int fm_pullback_scalar_adj(const fm_grid *g, int dtype, double dx, const void *s0, const void *psi, double alpha,
+                           double beta, const void *g_out, void *g_s0, void *g_psi, void *g_base, void *stream);
+
+/* ------------------------------------------------------------------------
  * MGPCG pressure projection.  Replaces MGPCG_3 / MGPCG_2 / MGPCG_2_solid
  * (3D/mgpcg.py:12-439, 2D/shape/mgpcg.py, 2D/vortex/mgpcg_solid.py) and the
  * 3D fast_mgpcg wrapper (3D/fast_mgpcg.py:241-323), empty obstacle mask.

@@ -74,3 +74,23 @@ def test_project_dc_arguments_rejected(fm):
     errors returned before any device work."""
     lib = fm._lib.lib()
     assert lib.fm_project_dc(None, None, None, None, None, 1e-10, 4, None, None) == 2
+
+
+def test_adjoint_entry_points_reject_arguments_without_device(fm):
+    """fm_*_adj: bad grids, dtypes, rk, missing inputs and partial gradient MACs
+    are argument errors returned before any device work (only NULL pointers
+    are passed)."""
+    lib = fm._lib.lib()
+    g = fm._lib.Grid(3, (C.c_int * 3)(8, 8, 8))
+    bad_dim = fm._lib.Grid(4, (C.c_int * 3)(8, 8, 8))
+    n = [None]
+    assert lib.fm_advect_scalar_grid_adj(C.byref(bad_dim), 0, 2, 0.1, 0.1, *(n * 9), None) == 1
+    assert lib.fm_advect_scalar_grid_adj(C.byref(g), 9, 2, 0.1, 0.1, *(n * 9), None) == 7
+    assert lib.fm_advect_scalar_grid_adj(C.byref(g), 0, 3, 0.1, 0.1, *(n * 9), None) == 2
+    assert lib.fm_advect_scalar_grid_adj(C.byref(g), 0, 2, 0.1, 0.1, *(n * 9), None) == 2
+    assert lib.fm_advect_u_grid_adj(C.byref(g), 1, 4, 0.1, 0.1, *(n * 15), None) == 2
+    assert lib.fm_pullback_u_adj(C.byref(g), 0, 0.1, *(n * 9), 1.0, 0.0, *(n * 15), None) == 2
+    assert lib.fm_pullback_scalar_adj(C.byref(g), 0, 0.1, None, None, 1.0, 0.0, None, None, None, None, None) == 2
+    tiny = fm._lib.Grid(2, (C.c_int * 3)(3, 8, 1))
+    assert lib.fm_pullback_scalar_adj(C.byref(tiny), 0, 0.1, None, None, 1.0, 0.0, None, None, None, None,
+                                      None) == 1
