@@ -87,6 +87,7 @@ SIGNATURES = {
     "fm_advect_u_grid_adj": [GP, I, I, D, D] + [P] * 15 + [P],
     "fm_pullback_u_adj": [GP, I, D] + [P] * 9 + [D, D] + [P] * 15 + [P],
     "fm_pullback_scalar_adj": [GP, I, D, P, P, D, D, P, P, P, P, P],
+    "fm_rk_grid_adj": [GP, I, I, D, D, I] + [P] * 12 + [P],
     "fm_accumulate_init": [GP, I, D, D, I, I] + [P] * 12 + [P] * 6 + [P],
     "fm_nabla_u_w": [GP, I, I, D] + [P] * 9 + [P],
     "fm_nabla_scalar_adjoint": [GP, I, D, P, P, P, P, P, P],

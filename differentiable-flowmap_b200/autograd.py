@@ -26,6 +26,13 @@ as the backward pass, for composing custom losses and solvers with torch):
   backward fm_pullback_u_adj (dL/du0, dL/dT, dL/dpsi, dL/dbase).
 * ``PullbackScalar`` / ``pullback_scalar``: alpha (s0(psi) + beta base)
   (fm_pullback_scalar); backward fm_pullback_scalar_adj.
+* ``RkGrid`` / ``rk_grid``: one RK2/RK4 march of a flow map psi and its
+  Jacobian row T through u (fm_rk_grid, RK_grid / RK_grid_only_psi);
+  backward fm_rk_grid_adj (dL/dpsi, dL/dT, dL/du, the Jacobian update
+  differentiated through the B-spline's second derivative).
+* ``AccumulateInit`` / ``accumulate_init``: init_c += dt F_c . f(phi_c), with
+  the Adams-Bashforth-3 history of accumulate_init_new (fm_accumulate_init);
+  backward through fm_pullback_u_adj and the AB3 coefficients.
 * ``Project`` / ``project``: the MGPCG pressure projection P (Poisson).  P is
   symmetric (u - G A^-1 D u with D = -G^T on the interior faces, wall faces
   zeroed), so the backward pass is the same projection of the incoming
@@ -204,6 +211,106 @@ class Project(torch.autograd.Function):
         g = [x.clone(memory_format=torch.contiguous_format) for x in g_out]
         ctx.solver.project(g)  # P^T = P
         return (None,) + tuple(g)
+
+
+class RkGrid(torch.autograd.Function):
+    @staticmethod
+    def forward(ctx, rk, dx, dt, face, psi, T, *u):
+        u = _c(u)
+        g = GridSpec.from_mac(u)
+        psi0 = psi.contiguous()
+        T0 = T.contiguous() if T is not None else None
+        psi1 = psi0.clone()
+        T1 = T0.clone() if T0 is not None else None
+        K.rk_grid(g, rk, dx, dt, face, psi1, T1, u)
+        ctx.args = (g, rk, dx, dt, face, T0 is not None)
+        ctx.save_for_backward(psi0, T0, *u)
+        return (psi1, T1) if T1 is not None else psi1
+
+    @staticmethod
+    def backward(ctx, *grads):
+        g, rk, dx, dt, face, has_T = ctx.args
+        psi0, T0, *u = ctx.saved_tensors
+        g_psi_out = grads[0].contiguous() if grads[0] is not None else torch.zeros_like(psi0)
+        g_T_out = None
+        if has_T:
+            g_T_out = grads[1].contiguous() if grads[1] is not None else torch.zeros_like(T0)
+        w_psi, w_T, w_u = ctx.needs_input_grad[4], ctx.needs_input_grad[5], any(ctx.needs_input_grad[6:])
+        g_psi = torch.zeros_like(psi0) if w_psi else None
+        g_T = torch.zeros_like(T0) if (w_T and has_T) else None
+        g_u = _zeros(u, w_u)
+        if w_psi or w_T or w_u:
+            K.rk_grid_adj(g, rk, dx, dt, face, psi0, T0, u, g_psi_out, g_T_out, g_psi, g_T, g_u)
+        return (None, None, None, None, g_psi, g_T) + (tuple(g_u) if w_u else (None,) * len(u))
+
+
+def _ab3_coefs(ab3: bool, ind: int, dt: float):
+    """d init' / d (F.f), d init' / d Hp, d init' / d Hpp of accumulate_init(_new)."""
+    if not ab3 or ind == 0:
+        return dt, 0.0, 0.0
+    if ind == 1:
+        return 7.0 / 12.0 * dt, 5.0 / 12.0 * dt, 0.0
+    return 23.0 / 12.0 * dt, -16.0 / 12.0 * dt, 5.0 / 12.0 * dt
+
+
+class AccumulateInit(torch.autograd.Function):
+    @staticmethod
+    def forward(ctx, dx, dt, ab3, ind, d, *fields):
+        f, init, F, phi = (_c(fields[i * d:(i + 1) * d]) for i in range(4))
+        Hp = [x.clone(memory_format=torch.contiguous_format) for x in fields[4 * d:5 * d]] if ab3 else None
+        Hpp = [x.clone(memory_format=torch.contiguous_format) for x in fields[5 * d:6 * d]] if ab3 else None
+        g = GridSpec.from_mac(f)
+        out = [x.clone() for x in init]
+        K.accumulate_init(g, dx, dt, f, out, F, phi, Hp, Hpp, ind)
+        ctx.args = (g, dx, dt, ab3, ind, d)
+        ctx.save_for_backward(*f, *F, *phi)
+        return tuple(out + (Hp + Hpp if ab3 else []))
+
+    @staticmethod
+    def backward(ctx, *grads):
+        g, dx, dt, ab3, ind, d = ctx.args
+        saved = ctx.saved_tensors
+        f, F, phi = list(saved[:d]), list(saved[d:2 * d]), list(saved[2 * d:])
+
+        def grad_or_zero(i, c):
+            return grads[i] if grads[i] is not None else torch.zeros_like(f[c])
+
+        G_init = [grad_or_zero(c, c) for c in range(d)]
+        c_fv, c_hp, c_hpp = _ab3_coefs(ab3, ind, dt)
+        fv_bar = [c_fv * x for x in G_init]  # dL/d(F_c . f(phi_c)) per node
+        g_hist = []
+        if ab3:  # Hp' = F . f(phi), Hpp' = Hp
+            G_hp = [grad_or_zero(d + c, c) for c in range(d)]
+            G_hpp = [grad_or_zero(2 * d + c, c) for c in range(d)]
+            fv_bar = [a + b for a, b in zip(fv_bar, G_hp)]
+            g_hist = [c_hp * a + b for a, b in zip(G_init, G_hpp)] + [c_hpp * a for a in G_init]
+        need = ctx.needs_input_grad[5:]
+        w_f, w_F, w_phi = any(need[:d]), any(need[2 * d:3 * d]), any(need[3 * d:4 * d])
+        g_f, g_F, g_phi = _zeros(f, w_f), _zeros(F, w_F), _zeros(phi, w_phi)
+        if w_f or w_F or w_phi:
+            K.pullback_u_adj(g, dx, f, F, phi, _c(fv_bar), 1.0, 0.0, g_f, g_F, g_phi)
+        res = [None] * 5
+        res += list(g_f) if w_f else [None] * d
+        res += G_init
+        res += list(g_F) if w_F else [None] * d
+        res += list(g_phi) if w_phi else [None] * d
+        return tuple(res + g_hist)
+
+
+def rk_grid(u, psi, T=None, face: int = -1, dx: float = 1.0, dt: float = 0.0, rk: int = 4):
+    """Differentiable RK_grid / RK_grid_only_psi (3D/flowmap.py:85-179): returns psi' (and T' when T is given)."""
+    return RkGrid.apply(rk, dx, dt, face, psi, T, *u)
+
+
+def accumulate_init(f, init, F_f, phi_f, dx: float, dt: float, Hp=None, Hpp=None, ind: int = 0):
+    """Differentiable accumulate_init (Hp/Hpp None) or accumulate_init_new (3D/flowmap.py:485-545).
+
+    Returns init' (a list), or (init', Hp', Hpp') with the AB3 history."""
+    d = len(f)
+    ab3 = Hp is not None
+    extra = list(Hp) + list(Hpp) if ab3 else []
+    out = list(AccumulateInit.apply(dx, dt, ab3, ind, d, *f, *init, *F_f, *phi_f, *extra))
+    return (out[:d], out[d:2 * d], out[2 * d:]) if ab3 else out
 
 
 def advect_scalar_grid(u0, s1, dx: float, dt: float, rk: int = 4):

@@ -292,6 +292,238 @@ __global__ void __launch_bounds__(kAdjThreads) k_pullback_scalar_adj(fm_grid g, 
 }
 
 // ---------------------------------------------------------------------------
+// RK_grid (flow map psi and Jacobian row T marched through u): the stage
+// k = u(pos), d = (grad u)(pos) t in reverse.  Besides the first derivatives
+// this needs the Hessian of the sample: the quadratic B-spline's second
+// derivative is 1, -2, 1 on the three taps of an axis (0 where the clamp is
+// active).
+// ---------------------------------------------------------------------------
+
+// At the stencil P: v = f, g = d f / d p (clamp-aware), graw = the gradient
+// the forward march uses in d = graw . t (the B-spline derivative at the
+// clamped position, scaled by 1/dx, not masked), Ht = d (graw . t) / d p.
+template <typename T, int D>
+__device__ __forceinline__ void val_grad_hess(const T* __restrict__ f, const Shape& s, const PointAdj<T, D>& P,
+                                              T inv_dx, const T* t, T& v, T* g, T* graw, T* Ht) {
+  T w[3][3], d[3][3], dd[3][3];
+#pragma unroll
+  for (int a = 0; a < 3; ++a) {
+    const Q2<T, true>& q = P.ax[a < D ? a : 0].q;
+    w[a][0] = q.w0, w[a][1] = q.w1, w[a][2] = q.w2;
+    d[a][0] = q.d0, d[a][1] = q.d1, d[a][2] = q.d2;
+    dd[a][0] = (T)1, dd[a][1] = (T)-2, dd[a][2] = (T)1;
+  }
+  T acc_v = 0, G[3] = {0, 0, 0}, H[3][3] = {{0, 0, 0}, {0, 0, 0}, {0, 0, 0}};
+  if constexpr (D == 3) {
+    const unsigned sj = s.s2, si = (unsigned)s.s1 * s.s2;
+    const unsigned b = ((unsigned)P.ax[0].q.i0 * s.s1 + P.ax[1].q.i0) * s.s2 + P.ax[2].q.i0;
+#pragma unroll
+    for (int i = 0; i < 3; ++i)
+#pragma unroll
+      for (int j = 0; j < 3; ++j)
+#pragma unroll
+        for (int k = 0; k < 3; ++k) {
+          const T x = ldg(f + b + i * si + j * sj + k);
+          acc_v += x * w[0][i] * w[1][j] * w[2][k];
+          G[0] += x * d[0][i] * w[1][j] * w[2][k];
+          G[1] += x * w[0][i] * d[1][j] * w[2][k];
+          G[2] += x * w[0][i] * w[1][j] * d[2][k];
+          H[0][0] += x * dd[0][i] * w[1][j] * w[2][k];
+          H[1][1] += x * w[0][i] * dd[1][j] * w[2][k];
+          H[2][2] += x * w[0][i] * w[1][j] * dd[2][k];
+          H[0][1] += x * d[0][i] * d[1][j] * w[2][k];
+          H[0][2] += x * d[0][i] * w[1][j] * d[2][k];
+          H[1][2] += x * w[0][i] * d[1][j] * d[2][k];
+        }
+  } else {
+    const unsigned si = s.s1;
+    const unsigned b = (unsigned)P.ax[0].q.i0 * s.s1 + P.ax[1].q.i0;
+#pragma unroll
+    for (int i = 0; i < 3; ++i)
+#pragma unroll
+      for (int j = 0; j < 3; ++j) {
+        const T x = ldg(f + b + i * si + j);
+        acc_v += x * w[0][i] * w[1][j];
+        G[0] += x * d[0][i] * w[1][j];
+        G[1] += x * w[0][i] * d[1][j];
+        H[0][0] += x * dd[0][i] * w[1][j];
+        H[1][1] += x * w[0][i] * dd[1][j];
+        H[0][1] += x * d[0][i] * d[1][j];
+      }
+  }
+  H[1][0] = H[0][1], H[2][0] = H[0][2], H[2][1] = H[1][2];
+  v = acc_v;
+#pragma unroll
+  for (int a = 0; a < D; ++a) {
+    graw[a] = G[a] * inv_dx;
+    g[a] = graw[a] * P.ax[a].live;
+    T h = 0;
+#pragma unroll
+    for (int b2 = 0; b2 < D; ++b2) h += H[a][b2] * inv_dx * t[b2];
+    Ht[a] = h * inv_dx * P.ax[a].live;
+  }
+}
+
+// f[taps] += kv * w + kd * (grad w . t)   (value and directional-derivative
+// adjoints; the derivative weights unmasked, as the forward's d uses them)
+template <typename T, int D>
+__device__ __forceinline__ void scatter_vd(T* f, const Shape& s, const PointAdj<T, D>& P, T inv_dx, T kv, T kd,
+                                           const T* t) {
+  T w[3][3], e[3][3];  // e = derivative weight * t_a / dx
+#pragma unroll
+  for (int a = 0; a < 3; ++a) {
+    const Q2<T, true>& q = P.ax[a < D ? a : 0].q;
+    const T sa = a < D ? inv_dx * t[a] : (T)0;
+    w[a][0] = q.w0, w[a][1] = q.w1, w[a][2] = q.w2;
+    e[a][0] = q.d0 * sa, e[a][1] = q.d1 * sa, e[a][2] = q.d2 * sa;
+  }
+  if constexpr (D == 3) {
+    const unsigned sj = s.s2, si = (unsigned)s.s1 * s.s2;
+    const unsigned b = ((unsigned)P.ax[0].q.i0 * s.s1 + P.ax[1].q.i0) * s.s2 + P.ax[2].q.i0;
+#pragma unroll
+    for (int i = 0; i < 3; ++i)
+#pragma unroll
+      for (int j = 0; j < 3; ++j)
+#pragma unroll
+        for (int k = 0; k < 3; ++k) {
+          const T wv = w[0][i] * w[1][j] * w[2][k];
+          const T wd = e[0][i] * w[1][j] * w[2][k] + w[0][i] * e[1][j] * w[2][k] + w[0][i] * w[1][j] * e[2][k];
+          atomicAdd(f + b + i * si + j * sj + k, kv * wv + kd * wd);
+        }
+  } else {
+    const unsigned si = s.s1;
+    const unsigned b = (unsigned)P.ax[0].q.i0 * s.s1 + P.ax[1].q.i0;
+#pragma unroll
+    for (int i = 0; i < 3; ++i)
+#pragma unroll
+      for (int j = 0; j < 3; ++j) {
+        const T wv = w[0][i] * w[1][j];
+        const T wd = e[0][i] * w[1][j] + w[0][i] * e[1][j];
+        atomicAdd(f + b + i * si + j, kv * wv + kd * wd);
+      }
+  }
+}
+
+// One march stage in reverse: k = u(pos), d = (grad u)(pos) t with adjoints
+// kbar, dbar (dbar unused when !WT) -> posbar, tbar; u's gradient scattered.
+template <typename T, int D, bool WT>
+__device__ __forceinline__ void march_stage_adj(const Mac<T>& u, const MacW<T>& gu, const fm_grid& g,
+                                                const Q2Lim<T>& lim, const T* pos, const T* t, T inv_dx,
+                                                const T* kbar, const T* dbar, T* posbar, T* tbar) {
+#pragma unroll
+  for (int a = 0; a < 3; ++a) posbar[a] = 0, tbar[a] = 0;
+#pragma unroll
+  for (int c = 0; c < D; ++c) {
+    PointAdj<T, D> P;
+    P.setup(lim, c, pos, inv_dx);
+    const Shape s = face_shape(g, c);
+    T v, gr[3] = {0, 0, 0}, graw[3] = {0, 0, 0}, Ht[3] = {0, 0, 0};
+    if constexpr (WT) {
+      val_grad_hess<T, D>(u.c[c], s, P, inv_dx, t, v, gr, graw, Ht);
+#pragma unroll
+      for (int a = 0; a < D; ++a) {
+        posbar[a] += kbar[c] * gr[a] + dbar[c] * Ht[a];
+        tbar[a] += dbar[c] * graw[a];
+      }
+      if (gu.c[0] != nullptr) scatter_vd<T, D>(gu.c[c], s, P, inv_dx, kbar[c], dbar[c], t);
+    } else {
+      val_grad<T, D>(u.c[c], s, P, inv_dx, v, gr);
+#pragma unroll
+      for (int a = 0; a < D; ++a) posbar[a] += kbar[c] * gr[a];
+      if (gu.c[0] != nullptr) scatter<T, D>(gu.c[c], s, P, kbar[c]);
+    }
+  }
+}
+
+// Adjoint of RK2/RK4_grid (WT) or RK*_grid_only_psi for one node: recomputes
+// the stage states (the same operations as the forward march), then
+//   RK2: psi' = P + (-dt) k2,  stage 2 at (P + h k1, T + h d1), h = -dt/2
+//   RK4: psi' = P + c6 (k1 + 2 k2 + 2 k3 + k4), c6 = -dt/6, stages at
+//        (P, T), (P + h k1, T + h d1), (P + h k2, T + h d2), (P - dt k3, T - dt d3)
+// and T' likewise with d.  g_psi / g_T receive dL/dpsi, dL/dT of the inputs.
+template <typename T, int D, int RK, bool WT>
+__global__ void __launch_bounds__(kAdjThreads) k_march_adj(fm_grid g, T dx, T dt, int face, Mac<T> u,
+                                                           const T* __restrict__ psi, const T* __restrict__ Tm,
+                                                           const T* __restrict__ g_psi_out,
+                                                           const T* __restrict__ g_T_out, MacW<T> gu, T* g_psi,
+                                                           T* g_T) {
+  const Shape s = face >= 0 ? face_shape(g, face) : cell_shape(g);
+  const long N = s.size();
+  const long n = (long)blockIdx.x * blockDim.x + threadIdx.x;
+  if (n >= N) return;
+  constexpr int S = RK == 2 ? 2 : 4;
+  T P0[3] = {0, 0, 0}, T0[3] = {0, 0, 0}, Pb[3] = {0, 0, 0}, Tb[3] = {0, 0, 0};
+#pragma unroll
+  for (int a = 0; a < D; ++a) {
+    P0[a] = psi[a * N + n];
+    Pb[a] = g_psi_out[a * N + n];
+    if constexpr (WT) {
+      T0[a] = Tm[a * N + n];
+      Tb[a] = g_T_out[a * N + n];
+    }
+  }
+  const T neg_dt = -dt;
+  const T h = (T)0.5 * neg_dt;
+  const T inv_dx = (T)1 / dx;
+  const Q2Lim<T> lim(g);
+  // forward stage states
+  T pos[S][3], tt[S][3], k[3], d[3] = {0, 0, 0};
+#pragma unroll
+  for (int a = 0; a < 3; ++a) pos[0][a] = P0[a], tt[0][a] = T0[a];
+#pragma unroll
+  for (int st = 1; st < S; ++st) {
+    if constexpr (WT) q2_mac_grad_dot<T, D>(u, g, lim, pos[st - 1], inv_dx, tt[st - 1], k, d);
+    else q2_mac_val<T, D>(u, g, lim, pos[st - 1], inv_dx, k);
+    const T hs = (RK == 4 && st == 3) ? (T)1.0 * neg_dt : h;
+#pragma unroll
+    for (int a = 0; a < 3; ++a) {
+      pos[st][a] = a < D ? P0[a] + hs * k[a] : (T)0;
+      tt[st][a] = (WT && a < D) ? T0[a] + hs * d[a] : (T)0;
+    }
+  }
+  // reverse sweep
+  T kb[3], db[3] = {0, 0, 0}, pb[3], tb[3];
+  if constexpr (RK == 2) {
+#pragma unroll
+    for (int a = 0; a < 3; ++a) kb[a] = neg_dt * Pb[a], db[a] = neg_dt * Tb[a];
+    march_stage_adj<T, D, WT>(u, gu, g, lim, pos[1], tt[1], inv_dx, kb, db, pb, tb);
+#pragma unroll
+    for (int a = 0; a < 3; ++a) {
+      kb[a] = h * pb[a], db[a] = h * tb[a];
+      Pb[a] += pb[a], Tb[a] += tb[a];
+    }
+    march_stage_adj<T, D, WT>(u, gu, g, lim, pos[0], tt[0], inv_dx, kb, db, pb, tb);
+  } else {
+    const T c6 = neg_dt * (T)1 / (T)6;
+    const T Po[3] = {Pb[0], Pb[1], Pb[2]}, To[3] = {Tb[0], Tb[1], Tb[2]};
+#pragma unroll
+    for (int a = 0; a < 3; ++a) kb[a] = c6 * Po[a], db[a] = c6 * To[a];
+#pragma unroll
+    for (int st = 3; st >= 1; --st) {
+      march_stage_adj<T, D, WT>(u, gu, g, lim, pos[st], tt[st], inv_dx, kb, db, pb, tb);
+      const T hs = st == 3 ? neg_dt : h;        // how stage st's state depends on the previous stage's k, d
+      const T wprev = st == 1 ? c6 : (T)2 * c6;  // weight of the previous stage's k, d in the update
+#pragma unroll
+      for (int a = 0; a < 3; ++a) {
+        Pb[a] += pb[a], Tb[a] += tb[a];
+        kb[a] = wprev * Po[a] + hs * pb[a];
+        db[a] = wprev * To[a] + hs * tb[a];
+      }
+    }
+    march_stage_adj<T, D, WT>(u, gu, g, lim, pos[0], tt[0], inv_dx, kb, db, pb, tb);
+  }
+#pragma unroll
+  for (int a = 0; a < D; ++a) {
+    Pb[a] += pb[a];
+    if (g_psi != nullptr) g_psi[a * N + n] += Pb[a];
+    if constexpr (WT) {
+      Tb[a] += tb[a];
+      if (g_T != nullptr) g_T[a * N + n] += Tb[a];
+    }
+  }
+}
+
+// ---------------------------------------------------------------------------
 // host side
 // ---------------------------------------------------------------------------
 template <typename T>
@@ -431,6 +663,41 @@ int fm_pullback_scalar_adj(const fm_grid* g, int dtype, double dx, const void* s
     else FM_PS_LAUNCH(double, 2);
   }
 #undef FM_PS_LAUNCH
+  return check_launch();
+}
+
+int fm_rk_grid_adj(const fm_grid* g, int dtype, int rk, double dx, double dt, int face, const void* psi,
+                   const void* T, const void* ux, const void* uy, const void* uz, const void* g_psi_out,
+                   const void* g_T_out, void* g_psi, void* g_T, void* g_ux, void* g_uy, void* g_uz, void* stream) {
+  int st = validate_grid(g, dtype);
+  if (st) return st;
+  if ((rk != 2 && rk != 4) || face < -1 || face >= g->dim || !psi || !g_psi_out || (face == -1 && T) ||
+      (!T != !g_T_out) || (!T && g_T) || !mac_args(*g, ux, uy, uz, false) || !mac_args(*g, g_ux, g_uy, g_uz, true))
+    return FM_ERR_ARG;
+  cudaStream_t s = (cudaStream_t)stream;
+  const long n = face >= 0 ? face_shape(*g, face).size() : cell_shape(*g).size();
+  const dim3 grid = blocks(n, 1);
+#define FM_MA_LAUNCH(Tp, D, RK, WT)                                                                             \
+  k_march_adj<Tp, D, RK, WT><<<grid, kAdjThreads, 0, s>>>(*g, (Tp)dx, (Tp)dt, face, cmac<Tp>(ux, uy, uz),        \
+                                                          (const Tp*)psi, (const Tp*)T, (const Tp*)g_psi_out,   \
+                                                          (const Tp*)g_T_out, wmac<Tp>(g_ux, g_uy, g_uz),       \
+                                                          (Tp*)g_psi, (Tp*)g_T)
+#define FM_MA_WT(Tp, D, RK)              \
+  if (T) FM_MA_LAUNCH(Tp, D, RK, true);  \
+  else FM_MA_LAUNCH(Tp, D, RK, false)
+#define FM_MA_RK(Tp, D)          \
+  if (rk == 2) { FM_MA_WT(Tp, D, 2); } \
+  else { FM_MA_WT(Tp, D, 4); }
+  if (dtype == FM_F32) {
+    if (g->dim == 3) { FM_MA_RK(float, 3) }
+    else { FM_MA_RK(float, 2) }
+  } else {
+    if (g->dim == 3) { FM_MA_RK(double, 3) }
+    else { FM_MA_RK(double, 2) }
+  }
+#undef FM_MA_RK
+#undef FM_MA_WT
+#undef FM_MA_LAUNCH
   return check_launch();
 }
 

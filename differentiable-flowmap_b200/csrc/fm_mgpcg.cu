@@ -538,6 +538,10 @@ __global__ void k_fin_beta(DevState* st, const double* part, double eps, double 
       st->tol = tol;
       st->beta = 0;
       if (!isfinite(a)) { st->nonfinite = 1; finish_solve(st); }
+      // z.r = 0 means r = 0 (the preconditioner is SPD on mean-zero fields): the
+      // zero start is the solution.  Stopping here keeps alpha = 0 / (0 + eps)
+      // from becoming NaN when eps = 0.
+      else if (a == 0.0) { st->conv = 1; finish_solve(st); }
     } else {
       st->beta = a / (st->zTr_old + eps);
       st->zTr_old = a;

@@ -364,6 +364,10 @@ __global__ void __launch_bounds__(kFinThreads) k_fin(int which, const double* __
   if (which == 0) {
     st->old_zr = s;
     st->tol = fmax(st->abs_tol, s * st->rel_tol);
+    if (s == 0.0) {  // r = 0: the zero start is the solution (and alpha would be 0 / 0 with eps = 0)
+      st->done = 1;
+      st->converged = 1;
+    }
   } else if (which == 1) {
     st->pAp = s;
     st->alpha = st->old_zr / (s + st->eps);

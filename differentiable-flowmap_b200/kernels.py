@@ -186,6 +186,16 @@ def pullback_scalar_adj(g: GridSpec, dx: float, s0, psi, g_out, alpha=1.0, beta=
           "fm_pullback_scalar_adj")
 
 
+def rk_grid_adj(g: GridSpec, rk: int, dx: float, dt: float, face: int, psi, T, u, g_psi_out, g_T_out=None,
+                g_psi=None, g_T=None, g_u=None, stream=None):
+    """Transpose of rk_grid at its inputs (psi, T, u): accumulates into g_psi, g_T, g_u."""
+    _chk_mac(g, u, "u")
+    _chk_vec(g, psi, face, "psi")
+    check(_lib.lib().fm_rk_grid_adj(C.byref(g.c_grid()), _dt(psi), rk, dx, dt, face, ptr(psi), ptr(T), *_mac3(u),
+                                    ptr(g_psi_out), ptr(g_T_out), ptr(g_psi), ptr(g_T), *_mac_opt(g, g_u, "g_u"),
+                                    stream_ptr(stream)), "fm_rk_grid_adj")
+
+
 def accumulate_init(g: GridSpec, dx: float, dt: float, f, init, F_f, phi_f, Hp=None, Hpp=None, ind=0, stream=None):
     ab3 = Hp is not None
     hs = []

@@ -229,6 +229,16 @@ int fm_pullback_u_adj(const fm_grid *g, int dtype, double dx,
  * g_out -> g_s0, g_psi (D planes), g_base (each may be NULL). */
 int fm_pullback_scalar_adj(const fm_grid *g, int dtype, double dx, const void *s0, const void *psi, double alpha,
                            double beta, const void *g_out, void *g_s0, void *g_psi, void *g_base, void *stream);
+/* Transpose of fm_rk_grid (one flow map psi, with its Jacobian row T when T is
+ * not NULL, marched through u): psi, T are the march's INPUTS; g_psi_out,
+ * g_T_out = dL/d(psi', T') of its outputs -> g_psi, g_T += dL/d(psi, T),
+ * g_u += dL/du.  The Jacobian update d = (grad u)(pos) . t is differentiated
+ * through the B-spline's second derivative.  g_T_out is required with T;
+ * g_psi, g_T, g_u may be NULL. */
+int fm_rk_grid_adj(const fm_grid *g, int dtype, int rk, double dx, double dt, int face,
+                   const void *psi, const void *T, const void *ux, const void *uy, const void *uz,
+                   const void *g_psi_out, const void *g_T_out, void *g_psi, void *g_T,
+                   void *g_ux, void *g_uy, void *g_uz, void *stream);
 
 /* ------------------------------------------------------------------------
  * MGPCG pressure projection.  Replaces MGPCG_3 / MGPCG_2 / MGPCG_2_solid

@@ -119,6 +119,53 @@ def test_pullback_scalar_gradcheck(fm, cuda, shape):
     _gradcheck(lambda s, p: A.pullback_scalar(s, p, dx), (s0, psi))
 
 
+@pytest.mark.parametrize("shape", SMALL, ids=lambda s: "x".join(map(str, s)))
+@pytest.mark.parametrize("rk", [2, 4])
+def test_rk_grid_gradcheck(fm, cuda, shape, rk):
+    """Flow map and Jacobian row marched through u: gradients in psi, T and u
+    (the T update differentiated through the B-spline's second derivative)."""
+    A = _A(fm)
+    rng = np.random.default_rng(19)
+    dx = 1.0 / shape[1]
+    d = len(shape)
+    u = _mac(rng, shape, 1.0, cuda)
+    for face in [0, d - 1, -1]:
+        node = _face(shape, face) if face >= 0 else shape
+        psi = _pos(rng, node, dx, cuda, spread=1.5)
+        if face >= 0:
+            T = torch.tensor(rng.uniform(-1, 1, size=(d,) + node), dtype=torch.float64, device=cuda,
+                             requires_grad=True)
+            _gradcheck(lambda p, t, *v: A.rk_grid(list(v), p, t, face, dx, 0.7 * dx, rk), (psi, T, *u))
+        else:
+            _gradcheck(lambda p, *v: A.rk_grid(list(v), p, None, face, dx, 0.7 * dx, rk), (psi, *u))
+
+
+@pytest.mark.parametrize("shape", SMALL, ids=lambda s: "x".join(map(str, s)))
+@pytest.mark.parametrize("ab3,ind", [(False, 0), (True, 0), (True, 1), (True, 3)])
+def test_accumulate_init_gradcheck(fm, cuda, shape, ab3, ind):
+    A = _A(fm)
+    rng = np.random.default_rng(20)
+    dx = 1.0 / shape[1]
+    d = len(shape)
+    f = _mac(rng, shape, 1.0, cuda)
+    init = _mac(rng, shape, 1.0, cuda)
+    F = [torch.tensor(rng.uniform(-1, 1, size=(d,) + _face(shape, c)), dtype=torch.float64, device=cuda,
+                      requires_grad=True) for c in range(d)]
+    phi = [_pos(rng, _face(shape, c), dx, cuda) for c in range(d)]
+    if ab3:
+        Hp, Hpp = _mac(rng, shape, 1.0, cuda), _mac(rng, shape, 1.0, cuda)
+
+        def fn(*x):
+            out = A.accumulate_init(list(x[:d]), list(x[d:2 * d]), list(x[2 * d:3 * d]), list(x[3 * d:4 * d]),
+                                    dx, 0.3, list(x[4 * d:5 * d]), list(x[5 * d:]), ind)
+            return tuple(out[0] + out[1] + out[2])
+
+        _gradcheck(fn, (*f, *init, *F, *phi, *Hp, *Hpp))
+    else:
+        _gradcheck(lambda *x: tuple(A.accumulate_init(list(x[:d]), list(x[d:2 * d]), list(x[2 * d:3 * d]),
+                                                      list(x[3 * d:]), dx, 0.3)), (*f, *init, *F, *phi))
+
+
 @pytest.mark.parametrize("shape", [(16, 16), (16, 16, 16)], ids=lambda s: "x".join(map(str, s)))
 def test_project_is_self_adjoint(fm, cuda, shape):
     A = _A(fm)
@@ -285,3 +332,73 @@ def test_fp32_adjoint_matches_fp64(fm, cuda):
         res[dt_] = [_np(x).astype(np.float64) for x in gu] + [_np(gs).astype(np.float64)]
     for a, b in zip(res[torch.float32], res[torch.float64]):
         assert np.abs(a - b).max() < 2e-5 * np.abs(b).max()
+
+
+@pytest.mark.parametrize("shape", MEDIUM, ids=lambda s: "x".join(map(str, s)))
+@pytest.mark.parametrize("rk", [2, 4])
+def test_rk_grid_adjoint_matches_oracle(fm, cuda, shape, rk):
+    """dL/du, dL/dpsi, dL/dT of one march against central differences of the
+    FP64 oracle's RK_grid (L = <psi', lam> + <T', mu>)."""
+    rng = np.random.default_rng(21)
+    o = Oracle(shape, "f64")
+    g = fm.GridSpec(shape)
+    d = len(shape)
+    dx = 1.0 / shape[1]
+    dt = 0.7 * dx
+    face = d - 1
+    node = _face(shape, face)
+    u = [rng.uniform(-1, 1, size=_face(shape, c)) for c in range(d)]
+    psi = _np(_pos(rng, node, dx, cuda, spread=1.5, grad=False))
+    Tm = rng.uniform(-1, 1, size=(d,) + node)
+    lam = rng.uniform(-1, 1, size=psi.shape)
+    mu = rng.uniform(-1, 1, size=Tm.shape)
+    T = lambda a: torch.tensor(np.ascontiguousarray(a), dtype=torch.float64, device=cuda)  # noqa: E731
+
+    def L(u_, psi_, T_):
+        p, t = psi_.copy(), T_.copy()
+        o.RK_grid(rk, face, p, t, [np.ascontiguousarray(x) for x in u_], dx, dt)
+        return _dot([p, t], [lam, mu])
+
+    g_psi, g_T = torch.zeros_like(T(psi)), torch.zeros_like(T(Tm))
+    g_u = [torch.zeros(_face(shape, c), dtype=torch.float64, device=cuda) for c in range(d)]
+    fm.kernels.rk_grid_adj(g, rk, dx, dt, face, T(psi), T(Tm), [T(x) for x in u], T(lam), T(mu), g_psi, g_T, g_u)
+    torch.cuda.synchronize()
+    h = 1e-6
+    for trial in range(2):
+        du = [rng.standard_normal(x.shape) for x in u]
+        dp = rng.standard_normal(psi.shape) * dx
+        dT = rng.standard_normal(Tm.shape)
+        fd = (L([x + h * y for x, y in zip(u, du)], psi, Tm) - L([x - h * y for x, y in zip(u, du)], psi, Tm)) / (2 * h)
+        an = _dot(du, [_np(x) for x in g_u])
+        assert abs(fd - an) < 1e-6 * max(abs(an), 1e-3), ("u", trial, fd, an)
+        fd = (L(u, psi + h * dp, Tm) - L(u, psi - h * dp, Tm)) / (2 * h)
+        an = _dot([dp], [_np(g_psi)])
+        assert abs(fd - an) < 1e-6 * max(abs(an), 1e-3), ("psi", trial, fd, an)
+        fd = (L(u, psi, Tm + h * dT) - L(u, psi, Tm - h * dT)) / (2 * h)
+        an = _dot([dT], [_np(g_T)])
+        assert abs(fd - an) < 1e-6 * max(abs(an), 1e-3), ("T", trial, fd, an)
+
+
+@pytest.mark.parametrize("check_every", [4, 0], ids=["host-checked", "device-loop"])
+@pytest.mark.parametrize("shape", [(16, 16), (16, 16, 16)], ids=lambda s: "x".join(map(str, s)))
+def test_projection_of_a_zero_field_with_eps_zero(fm, cuda, shape, check_every):
+    """A zero right-hand side (the backward pass of a loss that does not depend
+    on the projected field) ends the solve at once: z.r = 0 means r = 0, and
+    with eps = 0 the first step would otherwise divide 0 by 0."""
+    import importlib
+
+    M = importlib.import_module("differentiable-flowmap_b200.mgpcg")
+    sol = fm.MGPCG(shape, torch.float64, levels=2, bottom=50, max_iters=60, abs_tol=1e-24, rel_tol=1e-26, eps=0.0,
+                   check_every=check_every)
+    u = [torch.zeros(_face(shape, c), dtype=torch.float64, device=cuda) for c in range(len(shape))]
+    sol.project(u)
+    torch.cuda.synchronize()
+    assert all(torch.count_nonzero(x).item() == 0 for x in u)
+    if len(shape) == 2:  # the masked solver: a solid block in the middle
+        mask = torch.zeros(shape)
+        mask[5:9, 6:10] = 1.0
+        ssol = M.SolidMGPCG(shape, mask, torch.float64, levels=2, abs_tol=1e-24, rel_tol=1e-26, eps=0.0,
+                            check_every=check_every)
+        ssol.project(u)
+        torch.cuda.synchronize()
+        assert all(torch.count_nonzero(x).item() == 0 for x in u)
