@@ -1140,26 +1140,35 @@ static void launch_vcycle(fm_mgpcg* S, cudaStream_t s, bool dot_last, bool recen
   }
 }
 
-// One PCG iteration (3D/mgpcg.py:240-284) as a fixed launch sequence.
+// x += alpha p, r -= alpha A p and the convergence test: the second half of a
+// PCG iteration (3D/mgpcg.py:240-260).
 template <typename T, int D>
-static void launch_iteration(fm_mgpcg* S, cudaStream_t s) {
+static void launch_step(fm_mgpcg* S, cudaStream_t s) {
   const Shape s0 = S->lv[0];
   const long n = s0.size();
-  T* x = (T*)S->x;
-  T* p = (T*)S->p;
-  T* Ap = (T*)S->Ap;
-  T* r0 = (T*)S->r[0];
-  T* z0 = (T*)S->z[0];
-  launch_pdl(k_Ap_dot<T, D>, kRedBlocks, kRedThreads, 0, s, s0, p, Ap, S->part, S->st);
+  launch_pdl(k_Ap_dot<T, D>, kRedBlocks, kRedThreads, 0, s, s0, (T*)S->p, (T*)S->Ap, S->part, S->st);
   launch_pdl(k_fin_alpha, 1, 256, 0, s, S->st, S->part, S->P.eps);
-  launch_pdl(k_update_xr<T>, kRedBlocks, kRedThreads, 0, s, n, x, r0, p, Ap, S->part, S->st);
+  launch_pdl(k_update_xr<T>, kRedBlocks, kRedThreads, 0, s, n, (T*)S->x, (T*)S->r[0], (T*)S->p, (T*)S->Ap,
+             S->part, S->st);
   launch_pdl(k_fin_conv, 1, 256, 0, s, S->st, S->part, (double)n);
-  launch_vcycle<T, D>(S, s, true);
-  launch_pdl(k_fin_beta, 1, 256, 0, s, S->st, S->part, S->P.eps, S->P.abs_tol, S->P.rel_tol, S->P.max_iters, 0);
-  launch_pdl(k_update_p<T>, blocks_for(n, 256, 148L * 16), 256, 0, s, n, p, z0, S->st, 0);
 }
 
-// Prologue after r0 = b and partial sums of b: recentre, V-cycle, p = z, zTr.
+// One PCG iteration (3D/mgpcg.py:240-284) as a fixed launch sequence, rotated
+// so that the convergence test ends it: z = M r, beta, p = z + beta p, then the
+// next x / r update and its test.  A solve that converges stops right after
+// its test, with no V-cycle of early-returning kernels behind it; the kernels
+// run in the same order as the unrotated loop, so results are unchanged.
+template <typename T, int D>
+static void launch_iteration(fm_mgpcg* S, cudaStream_t s) {
+  const long n = S->lv[0].size();
+  launch_vcycle<T, D>(S, s, true);
+  launch_pdl(k_fin_beta, 1, 256, 0, s, S->st, S->part, S->P.eps, S->P.abs_tol, S->P.rel_tol, S->P.max_iters, 0);
+  launch_pdl(k_update_p<T>, blocks_for(n, 256, 148L * 16), 256, 0, s, n, (T*)S->p, (T*)S->z[0], S->st, 0);
+  launch_step<T, D>(S, s);
+}
+
+// Prologue after r0 = b and partial sums of b: recentre, V-cycle, p = z, zTr,
+// and the first x / r update with its convergence test.
 template <typename T, int D>
 static void launch_prologue(fm_mgpcg* S, cudaStream_t s) {
   const long n = S->lv[0].size();
@@ -1167,6 +1176,7 @@ static void launch_prologue(fm_mgpcg* S, cudaStream_t s) {
   launch_vcycle<T, D>(S, s, true);
   launch_pdl(k_fin_beta, 1, 256, 0, s, S->st, S->part, S->P.eps, S->P.abs_tol, S->P.rel_tol, S->P.max_iters, 1);
   launch_pdl(k_update_p<T>, blocks_for(n, 256, 148L * 16), 256, 0, s, n, (T*)S->p, (T*)S->z[0], S->st, 1);
+  launch_step<T, D>(S, s);
 }
 
 // Device mode: one graph holding a conditional WHILE node whose body is one PCG
