@@ -46,7 +46,8 @@ def parse():
     ap.add_argument("--rel-tol", type=float, default=None,
                     help="relative z.r tolerance of the FP32 projections (rTr < rel_tol * zTr0); default: the "
                          "loosest setting whose gradient is within 1e-4 of an FP64 run solved to its floor "
-                         "(3D gradient 1e-6, vortex2d 1e-10, shape2d 1e-8)")
+                         "(3D gradient 3e-6: 1e-6 and 3e-6 measure 1.3e-5, 1e-5 2.5e-4; vortex2d 1e-10, "
+                         "shape2d 1e-8)")
     ap.add_argument("--no-error", action="store_true", help="skip the FP64 reference runs")
     ap.add_argument("--solver-check-every", type=int, default=0,
                     help="0: device-side PCG loop (CUDA-graph WHILE node); k: host polls every k iterations "
@@ -74,7 +75,7 @@ def parse():
                     help="relative z.r tolerance of the FP32 inner solves of the mixed Poisson solve")
     a = ap.parse_args()
     if a.rel_tol is None:
-        a.rel_tol = {"vortex2d": 1e-10, "vortex2d-obstacle": 1e-8, "shape2d": 1e-8}.get(a.workload, 1e-6)
+        a.rel_tol = {"vortex2d": 1e-10, "vortex2d-obstacle": 1e-8, "shape2d": 1e-8}.get(a.workload, 3e-6)
     return a
 
 
