@@ -48,6 +48,11 @@ def parse():
                          "loosest setting whose gradient is within 1e-4 of an FP64 run solved to its floor "
                          "(3D gradient 3e-6: 1e-6 and 3e-6 measure 1.3e-5, 1e-5 2.5e-4; vortex2d 1e-10, "
                          "shape2d 1e-8)")
+    ap.add_argument("--pre-post", type=int, default=None,
+                    help="RBGS iterations before and after each coarse correction in the FP32 forms' V-cycle "
+                         "(default: the reference's 2)")
+    ap.add_argument("--bottom", type=int, default=None,
+                    help="bottom-level RBGS iterations of the FP32 forms' V-cycle (default: the reference's 50)")
     ap.add_argument("--no-error", action="store_true", help="skip the FP64 reference runs")
     ap.add_argument("--solver-check-every", type=int, default=0,
                     help="0: device-side PCG loop (CUDA-graph WHILE node); k: host polls every k iterations "
@@ -96,6 +101,10 @@ def form_config(C, a, form, dtype):
                            store_dtype=store, backward_u=not mixed, check_every=a.solver_check_every,
                            coarse_bf16=mixed and dtype == torch.float32 and a.mixed_coarse == "bf16",
                            rel_tol=a.rel_tol)
+    if dtype == torch.float32 and (a.pre_post is not None or a.bottom is not None):
+        sv = cfg.solver
+        cfg = replace(cfg, solver=replace(sv, pre_post=sv.pre_post if a.pre_post is None else a.pre_post,
+                                          bottom=sv.bottom if a.bottom is None else a.bottom))
     # checkpointed: the mixed form with interval checkpointing (the adjoint replays each interval)
     if not ckpt:
         return cfg
@@ -126,6 +135,7 @@ def bench_config(a, cfg, head):
     return {"workload": workload_name(a), "form": head, "res": a.res, "sim_steps": a.sim_steps,
             "reinit_every": a.reinit, "rk": 4, "dt": cfg.dt, "backward_u": cfg.backward_u,
             "solver_rel_tol_zr": cfg.solver.rel_tol, "solver_levels": cfg.solver.levels,
+            "solver_pre_post": cfg.solver.pre_post, "solver_bottom": cfg.solver.bottom,
             "inputs": "seeded: sphere r=0.15 -> union of two spheres (seed 20), u0 ~ N(0, 0.01^2) (seed 21)",
             "l2": "working set and trajectory stores exceed the 126 MB L2; no flush needed"}
 
