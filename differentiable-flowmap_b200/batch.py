@@ -20,6 +20,7 @@ import numpy as np
 import torch
 
 from . import _lib
+from . import kernels as K
 from .configs import vortex2d_config, vortex2d_theta
 from .simulator import LFM_Diff_Simulator
 from .vortex import VortexProblem
@@ -119,13 +120,40 @@ class BatchedVortex:
             self.instances.append(VortexInstance(n, vortex2d_theta(control_seed0 + i), omt, prob, stream))
         torch.cuda.synchronize(self.device)
 
-    def capture(self):
-        """Record every instance's gradient as one CUDA graph (untimed setup;
-        runs one eager gradient per instance first)."""
-        for inst in self.instances:
-            with torch.cuda.device(self.device), torch.cuda.stream(inst.stream):
-                inst.problem.capture(inst.theta, inst.omega_target)
-        torch.cuda.synchronize(self.device)
+    def capture(self, single_graph: bool = False):
+        """Record every instance's gradient as a CUDA graph (untimed setup; runs one
+        eager gradient per instance first).  single_graph=False: one graph per
+        instance, replayed on its own stream.  single_graph=True: ONE graph for the
+        whole batch, each instance's forward + adjoint a branch forked from the
+        capturing stream onto the instance's stream and joined back, so a batch
+        gradient is one graph launch; the branches have no dependencies between
+        them and run concurrently."""
+        self.batch_graph = None
+        if not single_graph:
+            for inst in self.instances:
+                with torch.cuda.device(self.device), torch.cuda.stream(inst.stream):
+                    inst.problem.capture(inst.theta, inst.omega_target)
+            torch.cuda.synchronize(self.device)
+            self.captured = True
+            return
+        with torch.cuda.device(self.device):
+            for inst in self.instances:
+                with torch.cuda.stream(inst.stream):
+                    inst.problem.prepare_record(inst.theta, inst.omega_target)
+            torch.cuda.synchronize(self.device)
+            main = torch.cuda.Stream(device=self.device)
+            graph = torch.cuda.CUDAGraph()
+            recorded = []
+            with torch.cuda.graph(graph, stream=main, capture_error_mode="thread_local"):
+                for inst in self.instances:
+                    inst.stream.wait_stream(main)  # fork
+                    with torch.cuda.stream(inst.stream):
+                        recorded.append(inst.problem.record())
+                    main.wait_stream(inst.stream)  # join
+        self.batch_graph = graph
+        self.batch_roles = [r[0] for r in recorded]
+        self.batch_loss = [r[1] for r in recorded]
+        self.batch_kernels = sum(r[2] for r in recorded)
         self.captured = True
 
     def _run(self, inst: VortexInstance):
@@ -135,9 +163,23 @@ class BatchedVortex:
     def gradients(self, concurrent: bool = True, graphs: bool = False):
         """One gradient per instance; concurrent=False runs them one after another.
         graphs=True replays the captured graphs (capture() first): one graph
-        launch per instance on its stream, all issued from this thread, then the
+        launch per instance on its stream, all issued from this thread, or, after
+        capture(single_graph=True), one graph launch for the whole batch; then the
         losses and dL/dtheta are read back instance by instance."""
-        if graphs:
+        if graphs and getattr(self, "batch_graph", None) is not None:
+            # the whole batch as one graph launch on the current stream
+            with torch.cuda.device(self.device):
+                for inst in self.instances:
+                    K.vortex_velocity_2d(inst.problem.grid, inst.problem.dx, inst.theta, inst.problem._u0[0],
+                                         inst.problem._u0[1])
+                self.batch_graph.replay()
+                for inst, roles, loss in zip(self.instances, self.batch_roles, self.batch_loss):
+                    for k, v in roles.items():
+                        setattr(inst.problem.sim, k, v)
+                    inst.loss = float(loss.item())
+                    inst.problem.loss = inst.loss
+                    inst.dtheta = inst.problem.calculate_dtheta(inst.theta)
+        elif graphs:
             if not getattr(self, "captured", False):
                 raise RuntimeError("gradients(graphs=True): call capture() first")
             with torch.cuda.device(self.device):

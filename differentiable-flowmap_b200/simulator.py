@@ -964,6 +964,17 @@ class LFM_Diff_Simulator(LFM_Simulator):
         capture and leaves the same results).  Not available with control forces (their
         parameters are staged from the host every step), a trajectory loss (read on
         the host) or a host-checked solver (check_every > 0)."""
+        self.prepare_capture(u0, passive0, target_passive, target_vorticity)
+        s = stream if stream is not None else torch.cuda.Stream(device=self.device)
+        torch.cuda.synchronize(self.device)
+        graph = torch.cuda.CUDAGraph()
+        with torch.cuda.graph(graph, stream=s, capture_error_mode="thread_local"):
+            roles, loss_dev, kernels = self.record_gradient(u0, passive0, target_passive, target_vorticity)
+        return GradientGraph(self, graph, roles, loss_dev, kernels)
+
+    def prepare_capture(self, u0, passive0=None, target_passive=None, target_vorticity=None):
+        """Checks that a gradient with these inputs can be recorded, and runs it
+        once eagerly (every lazily allocated buffer exists afterwards)."""
         cfg = self.cfg
         if cfg.add_control_force or cfg.trajectory_loss:
             raise FlowmapError(2, "capture_gradient: control forces and a trajectory loss are not capturable")
@@ -973,19 +984,20 @@ class LFM_Diff_Simulator(LFM_Simulator):
             if x is not None and not (isinstance(x, torch.Tensor) and x.is_cuda):
                 raise FlowmapError(2, "capture_gradient: inputs must be device tensors")
         self.gradient(u0, passive0, target_passive, target_vorticity)
-        s = stream if stream is not None else torch.cuda.Stream(device=self.device)
-        torch.cuda.synchronize(self.device)
+
+    def record_gradient(self, u0, passive0=None, target_passive=None, target_vorticity=None):
+        """Record one gradient on the current stream, which must be capturing (after
+        prepare_capture).  Returns (roles, loss tensor, kernels recorded outside the
+        PCG loop bodies): what a GradientGraph needs to replay it."""
         before = _lib.launch_count()
-        graph = torch.cuda.CUDAGraph()
         self._capturing = True
         try:
-            with torch.cuda.graph(graph, stream=s, capture_error_mode="thread_local"):
-                self.gradient(u0, passive0, target_passive, target_vorticity)
+            self.gradient(u0, passive0, target_passive, target_vorticity)
         finally:
             self._capturing = False
         kernels = _lib.launch_count() - before
         roles = {k: getattr(self, k) for k in _ROLES if hasattr(self, k)}
-        return GradientGraph(self, graph, roles, self._loss_dev, kernels)
+        return roles, self._loss_dev, kernels
 
 
 # fields whose tensors the steps exchange by reference (ping-pong buffers)

@@ -78,6 +78,19 @@ class VortexProblem:
         self.graph = self.sim.capture_gradient(self._u0, target_vorticity=omega_target)
         return self.graph
 
+    def prepare_record(self, theta, omega_target: torch.Tensor):
+        """First half of recording this gradient into a graph shared with other
+        problems (BatchedVortex.capture(single_graph=True)): the graph's input
+        tensor and one eager gradient."""
+        self._u0 = self.velocity(theta)
+        self._omega_target = omega_target
+        self.sim.prepare_capture(self._u0, target_vorticity=omega_target)
+
+    def record(self):
+        """Second half: record the gradient on the current (capturing) stream;
+        returns (roles, loss tensor, kernels) for the shared graph's replay."""
+        return self.sim.record_gradient(self._u0, target_vorticity=self._omega_target)
+
     def launch_gradient(self, theta):
         """The asynchronous part of graph_gradient: u0(theta) into the graph's
         input and one graph launch, on the current stream."""
