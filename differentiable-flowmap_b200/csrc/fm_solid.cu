@@ -81,6 +81,12 @@ __global__ void k_loop_cond(cudaGraphConditionalHandle h, State* st, Stats* stat
   cudaGraphSetConditional(h, (!st->done && st->loops <= st->max_iters) ? 1u : 0u);
 }
 
+// Before the WHILE node: skip the loop when the prologue's test already ended
+// the solve.
+__global__ void k_loop_init(cudaGraphConditionalHandle h, const State* st) {
+  cudaGraphSetConditional(h, st->done ? 0u : 1u);
+}
+
 __global__ void k_stats(const State* st, Stats* out) {
   const bool nf = !isfinite(st->rtr);
   out->solves += 1;
@@ -661,9 +667,11 @@ void vcycle(fm_solid* S, cudaStream_t s, const State* st) {
   }
 }
 
-// one PCG iteration (solve(), :318-363), every kernel frozen once st->done is set
+// The second half of a PCG iteration (2D/vortex/mgpcg_solid.py solve(), :318-363):
+// x += alpha p, r -= alpha A p and the convergence test; every kernel frozen once
+// st->done is set.
 template <typename T, int D>
-void iteration(fm_solid* S, cudaStream_t s) {
+void step(fm_solid* S, cudaStream_t s) {
   const long n = S->sh[0].size();
   const unsigned nb = blocks_for(n);
   State* st = S->st;
@@ -677,6 +685,20 @@ void iteration(fm_solid* S, cudaStream_t s) {
   launch(k_update_xr<T>, nb, kThreads, 0, s, n, (T*)S->x, r, (const T*)p, (const T*)Ap, fl, (const State*)st);
   launch(k_dot<T>, kRedBlocks, kThreads, 0, s, n, (const T*)r, (const T*)r, fl, S->part, (const State*)st);
   launch(k_fin, 1, kFinThreads, 0, s, 2, (const double*)S->part, st, n);
+}
+
+// One PCG iteration, rotated so that the convergence test ends it: recentre r,
+// z = M r, beta, p = z + beta p, then the next x / r update and its test (step).
+// A converged solve leaves the loop right after its test; the kernels run in
+// the order of the unrotated loop, so results are unchanged.
+template <typename T, int D>
+void iteration(fm_solid* S, cudaStream_t s) {
+  const long n = S->sh[0].size();
+  const unsigned nb = blocks_for(n);
+  State* st = S->st;
+  T* r = (T*)S->r[0];
+  T* p = (T*)S->p;
+  const uint8_t* fl = S->fl[0];
   launch(k_dot<T>, kRedBlocks, kThreads, 0, s, n, (const T*)r, (const T*)nullptr, (const uint8_t*)nullptr, S->part,
          (const State*)st);
   launch(k_fin, 1, kFinThreads, 0, s, 3, (const double*)S->part, st, n);
@@ -685,17 +707,43 @@ void iteration(fm_solid* S, cudaStream_t s) {
   launch(k_dot<T>, kRedBlocks, kThreads, 0, s, n, (const T*)S->z[0], (const T*)r, fl, S->part, (const State*)st);
   launch(k_fin, 1, kFinThreads, 0, s, 4, (const double*)S->part, st, n);
   launch(k_update_p<T>, nb, kThreads, 0, s, n, p, (const T*)S->z[0], fl, (const State*)st);
+  step<T, D>(S, s);
 }
 
 // The PCG loop as a conditional WHILE node appended to `graph` after `deps`
-// (the body, one iteration and k_loop_cond, recorded from S->cap); *node_out
-// receives the node.
+// (the body, one iteration and k_loop_cond, recorded from S->cap), preceded by
+// k_loop_init; *node_out receives the node.  `capturing`: the caller's stream
+// when `graph` is the graph it is recording (k_loop_init is then recorded from
+// that stream and the node follows the stream's current dependencies).
 template <typename T, int D>
-int add_loop_node(fm_solid* S, cudaGraph_t graph, const cudaGraphNode_t* deps, size_t ndeps, cudaGraphNode_t* node_out) {
+int add_loop_node(fm_solid* S, cudaGraph_t graph, const cudaGraphNode_t* deps, size_t ndeps, cudaGraphNode_t* node_out,
+                  cudaStream_t capturing) {
   cudaGraphConditionalHandle h;
   cudaError_t e;
   if ((e = cudaGraphConditionalHandleCreate(&h, graph, 1, cudaGraphCondAssignDefault)) != cudaSuccess)
     return cuda_fail(e);
+  // k_loop_init ahead of the node: recorded from the capturing stream inside a
+  // caller's capture, else added as a kernel node
+  cudaGraphNode_t init;
+  if (capturing) {
+    k_loop_init<<<1, 1, 0, capturing>>>(h, S->st);
+    if ((e = cudaGetLastError()) != cudaSuccess) return cuda_fail(e);
+    cudaStreamCaptureStatus cs;
+    if ((e = cudaStreamGetCaptureInfo(capturing, &cs, nullptr, &graph, &deps, &ndeps)) != cudaSuccess)
+      return cuda_fail(e);
+    if (cs != cudaStreamCaptureStatusActive) return cuda_fail(cudaErrorStreamCaptureInvalidated);
+  } else {
+    cudaKernelNodeParams kp = {};
+    State* st_arg = S->st;
+    void* kargs[2] = {&h, &st_arg};
+    kp.func = (void*)k_loop_init;
+    kp.gridDim = dim3(1, 1, 1);
+    kp.blockDim = dim3(1, 1, 1);
+    kp.kernelParams = kargs;
+    if ((e = cudaGraphAddKernelNode(&init, graph, deps, ndeps, &kp)) != cudaSuccess) return cuda_fail(e);
+    deps = &init;
+    ndeps = 1;
+  }
   cudaGraphNodeParams cp = {cudaGraphNodeTypeConditional};
   cp.conditional.handle = h;
   cp.conditional.type = cudaGraphCondTypeWhile;
@@ -728,7 +776,7 @@ int device_loop(fm_solid* S, cudaStream_t s, bool capturing) {
     cudaError_t e;
     if ((e = cudaStreamGetCaptureInfo(s, &cs, nullptr, &graph, &deps, &ndeps)) != cudaSuccess) return cuda_fail(e);
     cudaGraphNode_t node;
-    const int st = add_loop_node<T, D>(S, graph, deps, ndeps, &node);
+    const int st = add_loop_node<T, D>(S, graph, deps, ndeps, &node, s);
     if (st) return st;
     if ((e = cudaStreamUpdateCaptureDependencies(s, &node, 1, cudaStreamSetCaptureDependencies)) != cudaSuccess)
       return cuda_fail(e);
@@ -739,7 +787,7 @@ int device_loop(fm_solid* S, cudaStream_t s, bool capturing) {
     cudaError_t e;
     if ((e = cudaGraphCreate(&graph, 0)) != cudaSuccess) return cuda_fail(e);
     cudaGraphNode_t node;
-    int st = add_loop_node<T, D>(S, graph, nullptr, 0, &node);
+    int st = add_loop_node<T, D>(S, graph, nullptr, 0, &node, nullptr);
     if (!st && (e = cudaGraphInstantiate(&S->loop, graph, 0)) != cudaSuccess) {
       S->loop = nullptr;
       st = cuda_fail(e);
@@ -781,6 +829,7 @@ int solve(fm_solid* S, const void* b, double k, void* x, cudaStream_t s, int* it
   launch(k_update_p<T>, nb, kThreads, 0, s, n, p, (const T*)z, fl, (const State*)st);
   launch(k_dot<T>, kRedBlocks, kThreads, 0, s, n, (const T*)z, (const T*)r, fl, S->part, (const State*)st);
   launch(k_fin, 1, kFinThreads, 0, s, 0, (const double*)S->part, st, n);
+  step<T, D>(S, s);  // the first x / r update and its convergence test
   if (device) {
     const int dl = device_loop<T, D>(S, s, capturing);
     if (dl) return dl;
