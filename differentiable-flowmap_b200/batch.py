@@ -145,11 +145,15 @@ class BatchedVortex:
             graph = torch.cuda.CUDAGraph()
             recorded = []
             with torch.cuda.graph(graph, stream=main, capture_error_mode="thread_local"):
+                # every fork before any join: a branch forked after an earlier branch's
+                # join would depend on that branch and run after it
                 for inst in self.instances:
-                    inst.stream.wait_stream(main)  # fork
+                    inst.stream.wait_stream(main)
+                for inst in self.instances:
                     with torch.cuda.stream(inst.stream):
                         recorded.append(inst.problem.record())
-                    main.wait_stream(inst.stream)  # join
+                for inst in self.instances:
+                    main.wait_stream(inst.stream)
         self.batch_graph = graph
         self.batch_roles = [r[0] for r in recorded]
         self.batch_loss = [r[1] for r in recorded]
