@@ -62,6 +62,9 @@ def parse():
     ap.add_argument("--reinit", type=int, default=8)
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-e2e", action="store_true")
+    ap.add_argument("--no-other-workloads", action="store_true",
+                    help="3D gradient at N=1: skip the short runs of the vortex2d, shape2d and vortex2d-batch "
+                         "workloads whose summaries the line carries under other_workloads")
     ap.add_argument("--no-roofline", action="store_true",
                     help="skip the dominant-kernel roofline timing (used for profiler runs, which need W >= 1 only; "
                          "a reported bench value needs W >= 3)")
@@ -486,10 +489,12 @@ def run_shape2d(a):
     d_r0 = torch.tensor(rho0, dtype=f32, device=dev)
     d_rt = torch.tensor(rho_t, dtype=f32, device=dev)
 
-    def timed(fn):
+    def timed(fn, settle=None):
         for _ in range(a.warmup):
             fn()
         torch.cuda.synchronize(dev)
+        if settle:
+            settle()
         lib.launch_count(reset=True)
         e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
         e0.record()
@@ -497,6 +502,8 @@ def run_shape2d(a):
             out = fn()
         e1.record()
         torch.cuda.synchronize(dev)
+        if settle:
+            settle()  # the solver's loop bodies of the timed replays enter the launch count here
         return e0.elapsed_time(e1) / a.steps, out, lib.launch_count(reset=True)
 
     ms_eager, (loss, grad), _ = timed(lambda: sim.gradient(d_u0, d_r0, d_rt))
@@ -508,7 +515,8 @@ def run_shape2d(a):
         graph.replay()
         return sim.adj_u
 
-    ms, gg, launches = timed(replay)
+    ms, gg, launches = timed(replay, settle=graph.stats)
+    launches += graph.kernels * a.steps  # kernels recorded outside the PCG loop bodies
     if any(not torch.equal(x, y) for x, y in zip(gg, grad)):
         raise RuntimeError("graph replay differs from the eager gradient")
     # end to end through torch.autograd with host buffers
@@ -773,6 +781,38 @@ def run_force_kernels(a):
     return 0
 
 
+OTHER_WORKLOADS = (("vortex2d", ["--steps", "3", "--warmup", "3"]),
+                   ("shape2d", ["--steps", "3", "--warmup", "3"]),
+                   ("vortex2d-batch", ["--steps", "2", "--warmup", "2"]))
+OTHER_KEYS = ("metric", "value", "unit", "ms_per_step", "steps", "warmup", "solver", "solver_rel_tol_zr",
+              "dtheta_rel_err_vs_fp64", "grad_error_vs_fp64", "e2e", "graph_launches_per_batch",
+              "per_instance_dtheta_rel_err_vs_unbatched", "clocks")
+
+
+def other_workloads():
+    """The other benchmark configurations, each run once as its own process on this
+    GPU (`bench.py --workload W`), summarised so that one default run records them
+    all: 2D vortex 256^2 (config 0), 2D shape transition 256^2 (config 1) and the
+    16-instance batch (config 4)."""
+    import subprocess
+
+    out = {}
+    for name, extra in OTHER_WORKLOADS:
+        cmd = [sys.executable, os.path.join(ROOT, "bench.py"), "--workload", name, *extra]
+        try:
+            p = subprocess.run(cmd, capture_output=True, text=True, timeout=900)
+            lines = [l for l in p.stdout.splitlines() if l.startswith("{")]
+            if p.returncode != 0 or not lines:
+                out[name] = {"error": f"exit {p.returncode}: {p.stderr.strip().splitlines()[-1:]}"}
+                continue
+            d = json.loads(lines[-1])
+            out[name] = {k: d[k] for k in OTHER_KEYS if k in d}
+            out[name]["command"] = "python bench.py --workload " + name + " " + " ".join(extra)
+        except Exception as e:  # recorded, never fatal to the headline line
+            out[name] = {"error": f"{type(e).__name__}: {e}"}
+    return out
+
+
 def main():
     a = parse()
     if a.impl == "reference":
@@ -967,6 +1007,8 @@ def main():
                 line[f"{f}_over_plain"] = results[f]["value"] / results["plain"]["value"]
         if world == 1 and not a.no_cpu_baseline:
             line["cpu_baseline"], line["parity_one_step"] = cpu_leg(a, C, S, cfg, head, dev)
+        if world == 1 and not a.no_other_workloads and a.res == 128 and a.sim_steps == 150:
+            line["other_workloads"] = other_workloads()
         print(json.dumps(line), flush=True)
     if world > 1:
         dist.barrier()
