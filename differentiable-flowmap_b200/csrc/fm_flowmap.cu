@@ -20,8 +20,9 @@ namespace fm {
 constexpr int kThreads = 256;
 
 // CTAs per SM the march kernel is compiled for: 3 in FP32 (80 registers; 0.697
-// vs 0.723 ms per 128^3 RK4 launch at 2 CTAs / 128 registers), 2 in FP64 (80
-// registers would spill over 1 KB per thread there).
+// vs 0.723 ms per 128^3 RK4 launch at 2 CTAs / 128 registers; 4 CTAs force 64
+// registers with spills and measure no faster), 2 in FP64 (80 registers would
+// spill over 1 KB per thread there).
 template <typename T>
 constexpr int march_min_blocks() {
   return sizeof(T) == 4 ? 3 : 2;
