@@ -287,6 +287,7 @@ class LFM_Simulator:
         self.frame_idx = _Scalar(0)
         self.total_steps = cfg.total_steps
         self._recomputing = False
+        self._replay_tail = False
         self._alloc_stores()
         self.reset_to_identity(self.phi, self.phi_f, self.F_f)
 
@@ -533,6 +534,11 @@ class LFM_Simulator:
             if self._ring is not None:
                 self._ring[j][c].copy_(self.u[c])
         self.march_phi_grid(self.u)
+        if self._recomputing and self._replay_tail:
+            # the last step of a replayed interval: the adjoint needs its midpoint
+            # velocity and the interval-end maps, not the end state (the next
+            # checkpoint holds it)
+            return
         if cfg.use_short_BFECC:
             # BFECC through one-step maps instead of the semi-Lagrangian advection
             # (3D/lfm_midpoint_simulator.py:725-745); the BFECC result replaces u
@@ -613,9 +619,11 @@ class LFM_Simulator:
                 self.step_num[None] = n
                 if self._ring_passive is not None:
                     self._ring_passive[n - n0].copy_(self.passive)
+                self._replay_tail = n == last
                 self.step_flow_map(n - n0, self.dt)
         finally:
             self._recomputing = False
+            self._replay_tail = False
             self.step_num[None] = saved
         if self._ring_passive is not None:
             K.store(self.ckpt_passive[k + 1], self._ring_passive[last + 1 - n0])
