@@ -1108,6 +1108,7 @@ def main():
         its = results[f]["iters"]
         solves = sum(r.get("solves", 0) for r in its)
         return {"levels": sims[f].solver.n_mg_levels, "rel_tol_zr": cfgs[f].solver.rel_tol,
+                "pre_post": cfgs[f].solver.pre_post, "bottom": cfgs[f].solver.bottom,
                 "mean_pcg_iters": sum(r.get("iterations", 0) for r in its) / solves if solves else None,
                 "solves_per_grad": solves // max(a.steps, 1),
                 "not_converged": sum(r.get("not_converged", 0) for r in its),
