@@ -288,6 +288,7 @@ class LFM_Simulator:
         self.total_steps = cfg.total_steps
         self._recomputing = False
         self._replay_tail = False
+        self._replayed = None  # interval whose replay state the last forward pass left in place
         self._alloc_stores()
         self.reset_to_identity(self.phi, self.phi_f, self.F_f)
 
@@ -481,15 +482,29 @@ class LFM_Simulator:
         if n >= self.total_steps:
             raise FlowmapError(2, f"step {n} beyond total_steps={self.total_steps}")
         j = n % self.reinit_every
+        R = self.reinit_every
+        self._replayed = None
+        # interval checkpointing with a partial last interval: the forward keeps that
+        # interval's replay state (midpoint ring, passive ring, maps never reset), so
+        # the adjoint's first step need not replay it
+        keep_tail = (self.ckpt_u is not None and self.total_steps % R != 0
+                     and n // R == (self.total_steps - 1) // R)
         if self.store_passive is not None:
             K.store(self.passive, self.store_passive[n])
         if self.ckpt_u is not None and j == 0:
-            self._checkpoint(n // self.reinit_every)
+            self._checkpoint(n // R)
+        if keep_tail and self._ring_passive is not None:
+            self._ring_passive[j].copy_(self.passive)
         self.step_flow_map(j, self.dt, control_force_para)
         if self.final_condition() and self.store_passive is not None:
             K.store(self.passive, self.store_passive[n + 1])
         if self.final_condition() and self.ckpt_u is not None:
-            self._checkpoint((self.total_steps + self.reinit_every - 1) // self.reinit_every)
+            k_end = (self.total_steps + R - 1) // R
+            self._checkpoint(k_end)
+            if keep_tail:
+                if self._ring_passive is not None:  # as the replay sets it: from the checkpoint
+                    K.store(self.ckpt_passive[k_end], self._ring_passive[j + 1])
+                self._replayed = n // R
         return False, self.final_condition()
 
     def march_phi_grid(self, u):
@@ -789,7 +804,10 @@ class LFM_Diff_Simulator(LFM_Simulator):
         j = n % self.reinit_every
         n0 = n - j
         if self.ckpt_u is not None and n == min(n0 + self.reinit_every, self.total_steps) - 1:
-            self._recompute_interval(n // self.reinit_every)  # first adjoint step of this interval
+            if self._replayed == n // self.reinit_every:
+                self._replayed = None  # the forward left this interval's replay state in place
+            else:
+                self._recompute_interval(n // self.reinit_every)  # first adjoint step of this interval
         if self.cfg.add_passive_scalar and not self.cfg.backward_u:
             if self._ring_passive is not None:
                 self.passive.copy_(self._ring_passive[n + 1 - n0])
