@@ -89,6 +89,7 @@ SIGNATURES = {
     "fm_pullback_scalar_adj": [GP, I, D, P, P, D, D, P, P, P, P, P],
     "fm_rk_grid_adj": [GP, I, I, D, D, I] + [P] * 12 + [P],
     "fm_accumulate_init": [GP, I, D, D, I, I] + [P] * 12 + [P] * 6 + [P],
+    "fm_accumulate_init_pair": [GP, I, D, D, I, I] + [P] * 12 + [P] * 6 + [P] * 3 + [D, P],
     "fm_nabla_u_w": [GP, I, I, D] + [P] * 9 + [P],
     "fm_nabla_scalar_adjoint": [GP, I, D, P, P, P, P, P, P],
     "fm_reset_to_identity": [GP, I, D] + [P] * 7 + [P],

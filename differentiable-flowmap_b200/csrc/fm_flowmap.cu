@@ -240,9 +240,14 @@ __global__ void __launch_bounds__(kThreads) k_pullback_scalar(fm_grid g, T dx, c
   out[q] = alpha * acc;
 }
 
-template <typename T, int D, bool AB3>
+// With TWO, a second field f2 is accumulated afterwards with coefficient dt2 and
+// no history, from the same positions and rows (the adjoint's passive-scalar
+// source, 3D/lfm_midpoint_diff_simulator.py:519-523): the same operations as a
+// second plain launch on the first one's result.
+template <typename T, int D, bool AB3, bool TWO = false>
 __global__ void __launch_bounds__(kThreads) k_accumulate(fm_grid g, T dx, T dt, int ind, Mac<T> f, MacW<T> init,
-                                                         Mac<T> F, Mac<T> phi, MacW<T> Hp, MacW<T> Hpp) {
+                                                         Mac<T> F, Mac<T> phi, MacW<T> Hp, MacW<T> Hpp,
+                                                         Mac<T> f2 = Mac<T>{}, T dt2 = 0) {
   const int c = blockIdx.y;
   const Shape s = face_shape(g, c);
   const long N = s.size();
@@ -250,10 +255,18 @@ __global__ void __launch_bounds__(kThreads) k_accumulate(fm_grid g, T dx, T dt, 
   if (q >= N) return;
   const T* phi_c = pick(phi, c);
   const T* F_c = pick(F, c);
-  T p[3] = {0, 0, 0}, v[3];
+  T p[3] = {0, 0, 0}, v[3], v2[3] = {0, 0, 0};
 #pragma unroll
   for (int a = 0; a < D; ++a) p[a] = phi_c[a * N + q];
-  q2_mac_val<T, D>(f, g, Q2Lim<T>(g), p, (T)1 / dx, v);
+  {
+    MacStencil<T, D, false> st;
+    st.setup(Q2Lim<T>(g), p, (T)1 / dx);
+#pragma unroll
+    for (int b = 0; b < D; ++b) {
+      v[b] = q2_val<T, D, false>(f.c[b], face_shape(g, b), st.ax(b, 0), st.ax(b, 1), st.ax(b, 2 % D));
+      if constexpr (TWO) v2[b] = q2_val<T, D, false>(f2.c[b], face_shape(g, b), st.ax(b, 0), st.ax(b, 1), st.ax(b, 2 % D));
+    }
+  }
   T Fv = 0, Fv23 = 0, Fv16 = 0;
 #pragma unroll
   for (int a = 0; a < D; ++a) {
@@ -274,6 +287,12 @@ __global__ void __launch_bounds__(kThreads) k_accumulate(fm_grid g, T dx, T dt, 
     T* hp_c = pick(Hp, c);
     pick(Hpp, c)[q] = hp_c[q];
     hp_c[q] = Fv;
+  }
+  if constexpr (TWO) {
+    T Fv2 = 0;
+#pragma unroll
+    for (int a = 0; a < D; ++a) Fv2 += F_c[a * N + q] * v2[a];
+    acc += Fv2 * dt2;
   }
   init_c[q] = acc;
 }
@@ -397,6 +416,20 @@ static int march_t(const fm_grid& g, int rk, double dx, double dt, const MarchJo
   dim3 grid = grid_for(n, njobs, th);
   FM_DISPATCH_D(g, if (rk == 2) k_march<T, D, 2><<<grid, th, 0, st>>>(g, (T)dx, (T)dt, jobs, u);
                 else k_march<T, D, 4><<<grid, th, 0, st>>>(g, (T)dx, (T)dt, jobs, u));
+  return check_launch();
+}
+
+template <typename T>
+static int accumulate_t(const fm_grid& g, double dx, double dt, int ab3, int ind, Mac<T> f, MacW<T> in, Mac<T> F,
+                        Mac<T> ph, MacW<T> hp, MacW<T> hpp, Mac<T> f2, double dt2, cudaStream_t s) {
+  const int th = tuned_threads(FM_TUNE_ACCUMULATE, g);
+  dim3 grid = grid_for(max_face(g), g.dim, th);
+  const bool two = f2.c[0] != nullptr;
+#define FM_ACC(AB, TW) \
+  k_accumulate<T, D, AB, TW><<<grid, th, 0, s>>>(g, (T)dx, (T)dt, ind, f, in, F, ph, hp, hpp, f2, (T)dt2)
+  FM_DISPATCH_D(g, if (ab3) { if (two) FM_ACC(true, true); else FM_ACC(true, false); }
+                   else { if (two) FM_ACC(false, true); else FM_ACC(false, false); });
+#undef FM_ACC
   return check_launch();
 }
 
@@ -546,43 +579,44 @@ int fm_pullback_scalar(const fm_grid* g, int dtype, double dx, const void* s0, v
   return check_launch();
 }
 
-int fm_accumulate_init(const fm_grid* g, int dtype, double dx, double dt, int ab3, int ind, const void* fx,
-                       const void* fy, const void* fz, void* initx, void* inity, void* initz, const void* Fx,
-                       const void* Fy, const void* Fz, const void* phix, const void* phiy, const void* phiz,
-                       void* Hpx, void* Hppx, void* Hpy, void* Hppy, void* Hpz, void* Hppz, void* stream) {
+static int accumulate_entry(const fm_grid* g, int dtype, double dx, double dt, int ab3, int ind, const void* fx,
+                            const void* fy, const void* fz, void* initx, void* inity, void* initz, const void* Fx,
+                            const void* Fy, const void* Fz, const void* phix, const void* phiy, const void* phiz,
+                            void* Hpx, void* Hppx, void* Hpy, void* Hppy, void* Hpz, void* Hppz, const void* f2x,
+                            const void* f2y, const void* f2z, double dt2, void* stream) {
   int st = validate_grid(g, dtype);
   if (st) return st;
   if (!mac_ok(*g, fx, fy, fz) || !mac_ok(*g, initx, inity, initz) || !mac_ok(*g, Fx, Fy, Fz) ||
       !mac_ok(*g, phix, phiy, phiz) || ind < 0)
     return FM_ERR_ARG;
   if (ab3 && (!mac_ok(*g, Hpx, Hpy, Hpz) || !mac_ok(*g, Hppx, Hppy, Hppz))) return FM_ERR_ARG;
-  const int th = tuned_threads(FM_TUNE_ACCUMULATE, *g);
-  dim3 grid = grid_for(max_face(*g), g->dim, th);
+  if ((f2x || f2y || f2z) && !mac_ok(*g, f2x, f2y, f2z)) return FM_ERR_ARG;
   cudaStream_t s = FM_STREAM(stream);
-  if (dtype == FM_F32) {
-    auto f = mac<float>(fx, fy, fz);
-    auto in = macw<float>(initx, inity, initz);
-    auto F = mac<float>(Fx, Fy, Fz);
-    auto ph = mac<float>(phix, phiy, phiz);
-    auto hp = macw<float>(Hpx, Hpy, Hpz);
-    auto hpp = macw<float>(Hppx, Hppy, Hppz);
-    FM_DISPATCH_D(*g, if (ab3) k_accumulate<float, D, true><<<grid, th, 0, s>>>(*g, (float)dx, (float)dt, ind,
-                                                                                       f, in, F, ph, hp, hpp);
-                  else k_accumulate<float, D, false><<<grid, th, 0, s>>>(*g, (float)dx, (float)dt, ind, f,
-                                                                               in, F, ph, hp, hpp));
-  } else {
-    auto f = mac<double>(fx, fy, fz);
-    auto in = macw<double>(initx, inity, initz);
-    auto F = mac<double>(Fx, Fy, Fz);
-    auto ph = mac<double>(phix, phiy, phiz);
-    auto hp = macw<double>(Hpx, Hpy, Hpz);
-    auto hpp = macw<double>(Hppx, Hppy, Hppz);
-    FM_DISPATCH_D(*g, if (ab3) k_accumulate<double, D, true><<<grid, th, 0, s>>>(*g, dx, dt, ind, f, in, F,
-                                                                                        ph, hp, hpp);
-                  else k_accumulate<double, D, false><<<grid, th, 0, s>>>(*g, dx, dt, ind, f, in, F, ph, hp,
-                                                                                hpp));
-  }
-  return check_launch();
+  if (dtype == FM_F32)
+    return accumulate_t<float>(*g, dx, dt, ab3, ind, mac<float>(fx, fy, fz), macw<float>(initx, inity, initz),
+                               mac<float>(Fx, Fy, Fz), mac<float>(phix, phiy, phiz), macw<float>(Hpx, Hpy, Hpz),
+                               macw<float>(Hppx, Hppy, Hppz), mac<float>(f2x, f2y, f2z), dt2, s);
+  return accumulate_t<double>(*g, dx, dt, ab3, ind, mac<double>(fx, fy, fz), macw<double>(initx, inity, initz),
+                              mac<double>(Fx, Fy, Fz), mac<double>(phix, phiy, phiz), macw<double>(Hpx, Hpy, Hpz),
+                              macw<double>(Hppx, Hppy, Hppz), mac<double>(f2x, f2y, f2z), dt2, s);
+}
+
+int fm_accumulate_init(const fm_grid* g, int dtype, double dx, double dt, int ab3, int ind, const void* fx,
+                       const void* fy, const void* fz, void* initx, void* inity, void* initz, const void* Fx,
+                       const void* Fy, const void* Fz, const void* phix, const void* phiy, const void* phiz,
+                       void* Hpx, void* Hppx, void* Hpy, void* Hppy, void* Hpz, void* Hppz, void* stream) {
+  return accumulate_entry(g, dtype, dx, dt, ab3, ind, fx, fy, fz, initx, inity, initz, Fx, Fy, Fz, phix, phiy, phiz,
+                          Hpx, Hppx, Hpy, Hppy, Hpz, Hppz, nullptr, nullptr, nullptr, 0.0, stream);
+}
+
+int fm_accumulate_init_pair(const fm_grid* g, int dtype, double dx, double dt, int ab3, int ind, const void* fx,
+                            const void* fy, const void* fz, void* initx, void* inity, void* initz, const void* Fx,
+                            const void* Fy, const void* Fz, const void* phix, const void* phiy, const void* phiz,
+                            void* Hpx, void* Hppx, void* Hpy, void* Hppy, void* Hpz, void* Hppz, const void* f2x,
+                            const void* f2y, const void* f2z, double dt2, void* stream) {
+  if (!f2x) return FM_ERR_ARG;
+  return accumulate_entry(g, dtype, dx, dt, ab3, ind, fx, fy, fz, initx, inity, initz, Fx, Fy, Fz, phix, phiy, phiz,
+                          Hpx, Hppx, Hpy, Hppy, Hpz, Hppz, f2x, f2y, f2z, dt2, stream);
 }
 
 int fm_reset_to_identity(const fm_grid* g, int dtype, double dx, void* psi_c, void* psi_x, void* psi_y, void* psi_z,

@@ -206,6 +206,19 @@ def accumulate_init(g: GridSpec, dx: float, dt: float, f, init, F_f, phi_f, Hp=N
           "fm_accumulate_init")
 
 
+def accumulate_init_pair(g: GridSpec, dx: float, dt: float, f, init, F_f, phi_f, f2, dt2: float, Hp=None, Hpp=None,
+                         ind=0, stream=None):
+    """accumulate_init(f, dt, ...) then a plain accumulate_init(f2, dt2) through the same maps, in one pass."""
+    _chk_mac(g, f2, "f2")
+    ab3 = Hp is not None
+    hs = []
+    for c in range(3):
+        hs += [ptr(Hp[c]) if ab3 and c < g.dim else None, ptr(Hpp[c]) if ab3 and c < g.dim else None]
+    check(_lib.lib().fm_accumulate_init_pair(C.byref(g.c_grid()), _dt(f[0]), dx, dt, int(ab3), ind, *_mac3(f),
+                                             *_mac3(init), *_mac3(F_f), *_mac3(phi_f), *hs, *_mac3(f2), dt2,
+                                             stream_ptr(stream)), "fm_accumulate_init_pair")
+
+
 def nabla_u_w(g: GridSpec, dx: float, u, w, r, order: Optional[int] = None, stream=None):
     if order is None:
         order = 3 if g.dim == 3 else 4

@@ -874,10 +874,12 @@ class LFM_Diff_Simulator(LFM_Simulator):
         # (= reinit_every-1-j for a full interval, as the reference computes it)
         interval_last = min((n // self.reinit_every) * self.reinit_every + self.reinit_every - 1,
                             self.total_steps - 1)
-        K.accumulate_init(g, dx, -2 * curr_dt, self.src, self.init_adj_u, self.T_f, self.psi_f, self.H_prev,
-                          self.H_prev_prev, interval_last - n)
-        if cfg.add_passive_scalar:
-            K.accumulate_init(g, dx, -curr_dt, self.adj_passive_f, self.init_adj_u, self.T_f, self.psi_f)
+        if cfg.add_passive_scalar:  # the two accumulations in one pass (equal to two launches)
+            K.accumulate_init_pair(g, dx, -2 * curr_dt, self.src, self.init_adj_u, self.T_f, self.psi_f,
+                                   self.adj_passive_f, -curr_dt, self.H_prev, self.H_prev_prev, interval_last - n)
+        else:
+            K.accumulate_init(g, dx, -2 * curr_dt, self.src, self.init_adj_u, self.T_f, self.psi_f, self.H_prev,
+                              self.H_prev_prev, interval_last - n)
         if self.vis is not None:  # 2D/vortex/lfm_midpoint_diff_simulator.py:387-389
             for c in range(self.dim):
                 K.add_fields(self.adj_u[c], self.vis[c], self.adj_u[c], -curr_dt)

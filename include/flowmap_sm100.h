@@ -157,6 +157,19 @@ int fm_accumulate_init(const fm_grid *g, int dtype, double dx, double dt, int ab
                        void *Hpx, void *Hppx, void *Hpy, void *Hppy, void *Hpz, void *Hppz,
                        void *stream);
 
+/* fm_accumulate_init followed by a plain accumulate_init of a second face
+ * field f2 with coefficient dt2 through the same phi and F, in one pass (the
+ * adjoint step's two accumulations, 3D/lfm_midpoint_diff_simulator.py:513-523):
+ * the same result as the two calls, with the positions, rows and stencils
+ * loaded once.  f2 is required. */
+int fm_accumulate_init_pair(const fm_grid *g, int dtype, double dx, double dt, int ab3, int ind,
+                            const void *fx, const void *fy, const void *fz,
+                            void *initx, void *inity, void *initz,
+                            const void *Fx, const void *Fy, const void *Fz,
+                            const void *phix, const void *phiy, const void *phiz,
+                            void *Hpx, void *Hppx, void *Hpy, void *Hppy, void *Hpz, void *Hppz,
+                            const void *f2x, const void *f2y, const void *f2z, double dt2, void *stream);
+
 /* calculate_nabla_u_w: r_c = ((grad u)^T w)_c at face nodes, B-spline of
  * `order` (3 = cubic, as 3D/flowmap.py:359-380; 4 = quartic, as
  * 2D/vortex/flowmap.py:361-377). */

@@ -216,6 +216,34 @@ def test_accumulate_init(fm, cuda, shape, prec, ab3, ind):
             assert _rel(_np(Hpp_d[c]), Hpp_r[c]) < tol
 
 
+@pytest.mark.parametrize("ab3,ind", [(0, 0), (1, 1), (1, 4)])
+def test_accumulate_init_pair_equals_two_calls(fm, cuda, shape, prec, ab3, ind):
+    """fm_accumulate_init_pair equals accumulate_init followed by a plain one of the
+    second field through the same maps, bit for bit (histories included)."""
+    rng, o, dtype, tol, dx = setup(shape, prec, 7)
+    g = fm.GridSpec(shape)
+    dim = len(shape)
+    T_ = lambda xs: [_t(x, dtype, cuda) for x in xs]  # noqa: E731
+    f, f2, init = (_rand_mac(rng, shape, 1.0) for _ in range(3))
+    F = [rng.uniform(-1, 1, size=(dim,) + g.face_shape(c)) for c in range(dim)]
+    phi = [_rand_pos(rng, shape, g.face_shape(c), dx) for c in range(dim)]
+    Hp, Hpp = _rand_mac(rng, shape, 1.0), _rand_mac(rng, shape, 1.0)
+    a_init, a_hp, a_hpp = T_(init), T_(Hp), T_(Hpp)
+    b_init, b_hp, b_hpp = T_(init), T_(Hp), T_(Hpp)
+    if ab3:
+        fm.kernels.accumulate_init(g, dx, -0.02, T_(f), a_init, T_(F), T_(phi), a_hp, a_hpp, ind)
+    else:
+        fm.kernels.accumulate_init(g, dx, -0.02, T_(f), a_init, T_(F), T_(phi))
+    fm.kernels.accumulate_init(g, dx, -0.01, T_(f2), a_init, T_(F), T_(phi))
+    fm.kernels.accumulate_init_pair(g, dx, -0.02, T_(f), b_init, T_(F), T_(phi), T_(f2), -0.01,
+                                    b_hp if ab3 else None, b_hpp if ab3 else None, ind)
+    torch.cuda.synchronize()
+    for c in range(dim):
+        assert torch.equal(a_init[c], b_init[c])
+        if ab3:
+            assert torch.equal(a_hp[c], b_hp[c]) and torch.equal(a_hpp[c], b_hpp[c])
+
+
 @pytest.mark.parametrize("order", [3, 4])
 def test_nabla_u_w(fm, cuda, shape, prec, order):
     rng, o, dtype, tol, dx = setup(shape, prec, 7)
