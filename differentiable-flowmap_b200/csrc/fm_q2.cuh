@@ -73,11 +73,7 @@ struct Q2 {
     const T f = s - iu;
     const bool up = f >= (T)0.5;
     const T t = up ? f - (T)1 : f;
-    fill(t, ii - 1 + (up ? 1 : 0));
-  }
-  // weights of the taps i0..i0+2 for the offset t in [-0.5, 0.5)
-  __device__ __forceinline__ void fill(T t, int first) {
-    i0 = first;
+    i0 = ii - 1 + (up ? 1 : 0);
     const T a = (T)0.5 - t, b = (T)0.5 + t;
     w0 = (T)0.5 * (a * a);
     w1 = (T)0.75 - t * t;
@@ -89,27 +85,6 @@ struct Q2 {
     }
   }
 };
-
-// The face-staggered (BL = 0) and cell-centred (BL = 0.5) stencils of one axis
-// at the scaled position ps.  When neither clamp is active the second follows
-// from the first: with f = ps - floor(ps), t = f - 0.5 and base floor(ps) - 1
-// for BL = 0.5 (both cases f < 0.5 and f >= 0.5), every step exact, so the
-// result equals the two separate setups bit for bit.
-template <typename T, bool G>
-__device__ __forceinline__ void q2_setup_pair(T ps, T h0, T h5, Q2<T, G>& q0, Q2<T, G>& q5) {
-  const T u5 = ps - (T)0.5;
-  if (u5 > (T)1 && u5 < h5 && ps < h0) {
-    int ii;
-    const T iu = floor_pos(ps, ii);
-    const T f = ps - iu;
-    const bool up = f >= (T)0.5;
-    q0.fill(up ? f - (T)1 : f, ii - 1 + (up ? 1 : 0));
-    q5.fill(f - (T)0.5, ii - 1);
-  } else {
-    q0.setup(ps, (T)0, h0);
-    q5.setup(ps, (T)0.5, h5);
-  }
-}
 
 __device__ __forceinline__ float2 f2(float a, float b) { return make_float2(a, b); }
 __device__ __forceinline__ float2 f2(float a) { return make_float2(a, a); }
@@ -267,7 +242,11 @@ struct MacStencil {
   Q2<T, G> s5[3];  // BL = 0.5
   __device__ __forceinline__ void setup(const Q2Lim<T>& lim, const T* p, T inv_dx) {
 #pragma unroll
-    for (int a = 0; a < D; ++a) q2_setup_pair<T, G>(p[a] * inv_dx, lim.h0[a], lim.h5[a], s0[a], s5[a]);
+    for (int a = 0; a < D; ++a) {
+      const T ps = p[a] * inv_dx;
+      s0[a].setup(ps, (T)0, lim.h0[a]);
+      s5[a].setup(ps, (T)0.5, lim.h5[a]);
+    }
   }
   __device__ __forceinline__ const Q2<T, G>& ax(int c, int a) const { return a == c ? s0[a] : s5[a]; }
 };
