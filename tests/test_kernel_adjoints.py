@@ -402,3 +402,34 @@ def test_projection_of_a_zero_field_with_eps_zero(fm, cuda, shape, check_every):
         ssol.project(u)
         torch.cuda.synchronize()
         assert all(torch.count_nonzero(x).item() == 0 for x in u)
+
+
+def test_fp32_march_and_pullback_adjoints_match_fp64(fm, cuda):
+    """The FP32 march and pullback adjoint kernels agree with their FP64 versions to
+    FP32 rounding (relative to each gradient's scale)."""
+    rng = np.random.default_rng(22)
+    shape = (16, 20, 24)
+    g = fm.GridSpec(shape)
+    d = 3
+    dx = 1.0 / shape[1]
+    u = [rng.uniform(-1, 1, size=_face(shape, c)) for c in range(d)]
+    node = _face(shape, 2)
+    psi = _np(_pos(rng, node, dx, cuda, spread=1.5, grad=False))
+    Tm = rng.uniform(-1, 1, size=(d,) + node)
+    lam, mu = rng.uniform(-1, 1, size=psi.shape), rng.uniform(-1, 1, size=Tm.shape)
+    Tf = [rng.uniform(-1, 1, size=(d,) + _face(shape, c)) for c in range(d)]
+    pf = [_np(_pos(rng, _face(shape, c), dx, cuda, grad=False)) for c in range(d)]
+    lo = [rng.uniform(-1, 1, size=_face(shape, c)) for c in range(d)]
+    res = {}
+    for dt_ in (torch.float32, torch.float64):
+        T = lambda a: torch.tensor(np.ascontiguousarray(a), dtype=dt_, device=cuda)  # noqa: E731
+        Z = lambda a: torch.zeros(np.shape(a), dtype=dt_, device=cuda)  # noqa: E731
+        gp, gT, gu = Z(psi), Z(Tm), [Z(x) for x in u]
+        fm.kernels.rk_grid_adj(g, 4, dx, 0.7 * dx, 2, T(psi), T(Tm), [T(x) for x in u], T(lam), T(mu), gp, gT, gu)
+        hu, hT, hp = [Z(x) for x in u], [Z(x) for x in Tf], [Z(x) for x in pf]
+        fm.kernels.pullback_u_adj(g, dx, [T(x) for x in u], [T(x) for x in Tf], [T(x) for x in pf],
+                                  [T(x) for x in lo], 1.0, 0.0, hu, hT, hp)
+        res[dt_] = [gp, gT] + gu + hu + hT + hp
+    for a, b in zip(res[torch.float32], res[torch.float64]):
+        a, b = _np(a).astype(np.float64), _np(b)
+        assert np.abs(a - b).max() < 1e-4 * max(np.abs(b).max(), 1e-30)
