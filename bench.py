@@ -40,9 +40,10 @@ def parse():
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--form", default="all", choices=["plain", "mixed", "checkpointed", "both", "all"],
                     help="both: plain + checkpointed; all: plain + mixed + checkpointed (the headline form last)")
-    ap.add_argument("--ckpt-dtype", default="f32", choices=["bf16", "f32"],
-                    help="storage of the interval checkpoints in the checkpointed form (BF16 ones put the 128^3 "
-                         "gradient error at 1.7e-4 vs FP64, over the 1e-4 bar)")
+    ap.add_argument("--ckpt-dtype", default="f32", choices=["bf16", "bf16-delta", "f32"],
+                    help="storage of the interval checkpoints in the checkpointed form: f32; bf16 (the 128^3 "
+                         "gradient error 1.7e-4 vs FP64, over the 1e-4 bar); bf16-delta (velocity checkpoints as BF16 "
+                         "differences from the previous one, the first and the passive scalar in FP32)")
     ap.add_argument("--rel-tol", type=float, default=None,
                     help="relative z.r tolerance of the FP32 projections (rTr < rel_tol * zTr0); default: the "
                          "loosest setting whose gradient is within 1e-4 of an FP64 run solved to its floor "
@@ -121,8 +122,9 @@ def form_config(C, a, form, dtype):
     # checkpointed: the mixed form with interval checkpointing (the adjoint replays each interval)
     if not ckpt:
         return cfg
-    cd = torch.bfloat16 if (a.ckpt_dtype == "bf16" and dtype == torch.float32) else None
-    return replace(cfg, recompute=True, ckpt_dtype=cd)
+    f32 = dtype == torch.float32
+    cd = torch.bfloat16 if (a.ckpt_dtype == "bf16" and f32) else None
+    return replace(cfg, recompute=True, ckpt_dtype=cd, ckpt_delta=a.ckpt_dtype == "bf16-delta" and f32)
 
 
 def workload_name(a):
@@ -1128,7 +1130,9 @@ def main():
                               "velocity_store": ("interval checkpoints + a replayed f32 ring of one interval"
                                                  if cfgs[f].recompute else
                                                  "bf16" if cfgs[f].store_dtype == torch.bfloat16 else "f32"),
-                              "checkpoint_dtype": (str(cfgs[f].ckpt_dtype or cfgs[f].dtype).replace("torch.", "")
+                              "checkpoint_dtype": (("bf16 differences of u (first checkpoint and passive in f32)"
+                                                    if cfgs[f].ckpt_delta else
+                                                    str(cfgs[f].ckpt_dtype or cfgs[f].dtype).replace("torch.", ""))
                                                    if cfgs[f].recompute else None),
                               "mg_coarse_storage": "bf16" if cfgs[f].solver.coarse_bf16 else "f32",
                               "trajectory_gb": sims_bytes[f] / 1e9, "solver": solver_stats(f),

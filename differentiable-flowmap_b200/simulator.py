@@ -89,6 +89,13 @@ class FlowmapConfig:
     # storage dtype of the interval checkpoints (None: the working dtype); BF16
     # halves them, and the replay then starts from the rounded state
     ckpt_dtype: Optional[torch.dtype] = None
+    # velocity checkpoints in BF16 as differences from the previous checkpoint's
+    # reconstruction (the first one in the working dtype): the rounding then applies
+    # to one interval's change of u, not to u itself, and never accumulates (each
+    # difference is taken against the reconstruction the replay will rebuild).
+    # The passive-scalar checkpoints stay in the working dtype.  Needs recompute
+    # and an FP32 working dtype.
+    ckpt_delta: bool = False
     solver: SolverConfig = field(default_factory=SolverConfig)
 
     def validate(self):
@@ -99,6 +106,8 @@ class FlowmapConfig:
                                          ("trajectory_loss", self.trajectory_loss)) if on]
             if bad:
                 raise FlowmapError(2, f"recompute (interval checkpointing) does not support {', '.join(bad)}")
+        if self.ckpt_delta and (not self.recompute or self.dtype != torch.float32):
+            raise FlowmapError(2, "ckpt_delta needs recompute=True and an FP32 working dtype")
 
     @property
     def dim(self) -> int:
@@ -306,11 +315,16 @@ class LFM_Simulator:
         sd, wd = self.store_dtype, self.cfg.dtype
         self.store_mid = self.store_phi = self.store_phi_f = self.store_F_f = self.store_passive = None
         self.ckpt_u = self.ckpt_passive = self._ring_passive = None
+        self._ckpt_u0 = self._ckpt_base = self._ckpt_tmp = None
         if self.cfg.recompute:
-            cd = self.cfg.ckpt_dtype or wd
+            delta = self.cfg.ckpt_delta
+            cd = torch.bfloat16 if delta else (self.cfg.ckpt_dtype or wd)
             self.ckpt_u = [torch.zeros((n_int + 1,) + g.face_shape(c), dtype=cd, device=dev) for c in range(self.dim)]
+            if delta:  # checkpoint 0 in full, the running reconstruction, a difference buffer
+                self._ckpt_u0, self._ckpt_base, self._ckpt_tmp = (
+                    [torch.zeros(g.face_shape(c), dtype=wd, device=dev) for c in range(self.dim)] for _ in range(3))
             if self.cfg.add_passive_scalar:
-                self.ckpt_passive = torch.zeros((n_int + 1,) + g.shape, dtype=cd, device=dev)
+                self.ckpt_passive = torch.zeros((n_int + 1,) + g.shape, dtype=wd if delta else cd, device=dev)
                 self._ring_passive = torch.zeros((R + 1,) + g.shape, dtype=wd, device=dev)
             self._ring = [[torch.zeros(g.face_shape(c), dtype=wd, device=dev) for c in range(self.dim)]
                           for _ in range(R)]
@@ -337,7 +351,8 @@ class LFM_Simulator:
     def trajectory_bytes(self) -> int:
         """Device bytes held for the adjoint (stores, checkpoints, rings)."""
         ts = []
-        for x in (self.store_mid, self.store_phi_f, self.store_F_f, self.ckpt_u, self._ring):
+        for x in (self.store_mid, self.store_phi_f, self.store_F_f, self.ckpt_u, self._ring, self._ckpt_u0,
+                  self._ckpt_base, self._ckpt_tmp):
             if x is not None:
                 ts += [t for row in x for t in (row if isinstance(row, list) else [row])]
         ts += [x for x in (self.store_phi, self.store_passive, self.ckpt_passive, self._ring_passive)
@@ -347,10 +362,34 @@ class LFM_Simulator:
     def _checkpoint(self, k: int):
         """Interval checkpointing: the state at the start of interval k (slot
         n_int: the state after the last step)."""
-        for c in range(self.dim):
-            K.store(self.u[c], self.ckpt_u[c][k])
+        if self.cfg.ckpt_delta:
+            for c in range(self.dim):
+                if k == 0:
+                    self._ckpt_u0[c].copy_(self.u[c])
+                    self._ckpt_base[c].copy_(self.u[c])
+                    continue
+                # d = u - base rounded to BF16; base += d as the replay will add it
+                K.add_fields(self.u[c], self._ckpt_base[c], self._ckpt_tmp[c], -1.0)
+                K.store(self._ckpt_tmp[c], self.ckpt_u[c][k])
+                K.store(self.ckpt_u[c][k], self._ckpt_tmp[c])
+                K.add_fields(self._ckpt_base[c], self._ckpt_tmp[c], self._ckpt_base[c], 1.0)
+        else:
+            for c in range(self.dim):
+                K.store(self.u[c], self.ckpt_u[c][k])
         if self.ckpt_passive is not None:
             K.store(self.passive, self.ckpt_passive[k])
+
+    def _load_ckpt_u(self, k: int):
+        """u = the velocity checkpoint k (rebuilt from the differences in the delta
+        form, with the forward's operations in its order)."""
+        for c in range(self.dim):
+            if not self.cfg.ckpt_delta:
+                K.store(self.ckpt_u[c][k], self.u[c])
+                continue
+            self.u[c].copy_(self._ckpt_u0[c])
+            for j in range(1, k + 1):
+                K.store(self.ckpt_u[c][j], self._ckpt_tmp[c])
+                K.add_fields(self.u[c], self._ckpt_tmp[c], self.u[c], 1.0)
 
     # ------------------------------------------------------------ kernels
     def reset_to_identity(self, psi, psi_f, T_f):
@@ -621,8 +660,7 @@ class LFM_Simulator:
         n0 = k * R
         last = min(n0 + R - 1, self.total_steps - 1)
         saved = self.step_num[None]
-        for c in range(self.dim):
-            K.store(self.ckpt_u[c][k], self.u[c])
+        self._load_ckpt_u(k)
         if self.ckpt_passive is not None:
             K.store(self.ckpt_passive[k], self.passive)
             self.init_passive.copy_(self.passive)
