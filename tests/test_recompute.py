@@ -74,6 +74,33 @@ def test_recompute_with_bf16_store_dtype_is_closer_to_fp64(fm, cuda):
 
 
 @pytest.mark.gpu
+def test_delta_checkpoints_error_and_memory(fm, cuda):
+    """ckpt_delta: velocity checkpoints as BF16 differences.  The gradient stays
+    within 1e-4 of the FP64 run, closer than with plain BF16 checkpoints, and the
+    checkpoints take less memory than FP32 ones."""
+    from dataclasses import replace
+
+    cfg, u0, rho0, rho_t = _shape_case(32, 24, 4)
+    base = replace(cfg, recompute=True, backward_u=False)
+    runs = {}
+    for name, extra in (("f32", {}), ("bf16", dict(ckpt_dtype=torch.bfloat16)), ("delta", dict(ckpt_delta=True))):
+        sim = S.LFM_Diff_Simulator(config=replace(base, **extra))
+        runs[name] = (sim.gradient(u0, rho0, rho_t)[1], sim.trajectory_bytes())
+    c64 = replace(base, dtype=torch.float64, recompute=False)
+    _, g64 = S.LFM_Diff_Simulator(config=c64).gradient([x.double() for x in u0], rho0.double(), rho_t.double())
+
+    def err(g):
+        num = sum(float(((a.double() - b) ** 2).sum()) for a, b in zip(g, g64))
+        return (num / sum(float((b ** 2).sum()) for b in g64)) ** 0.5
+
+    assert err(runs["delta"][0]) < 1e-4
+    assert err(runs["delta"][0]) <= err(runs["bf16"][0])
+    assert runs["delta"][1] < runs["f32"][1]
+    with pytest.raises(fm.FlowmapError):
+        S.LFM_Diff_Simulator(config=replace(cfg, ckpt_delta=True))  # needs recompute
+
+
+@pytest.mark.gpu
 def test_recompute_vortex_and_graph_capture(fm, cuda):
     from dataclasses import replace
 
