@@ -40,10 +40,11 @@ def parse():
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--form", default="all", choices=["plain", "mixed", "checkpointed", "both", "all"],
                     help="both: plain + checkpointed; all: plain + mixed + checkpointed (the headline form last)")
-    ap.add_argument("--ckpt-dtype", default="f32", choices=["bf16", "bf16-delta", "f32"],
+    ap.add_argument("--ckpt-dtype", default="bf16-delta", choices=["bf16", "bf16-delta", "f32"],
                     help="storage of the interval checkpoints in the checkpointed form: f32; bf16 (the 128^3 "
                          "gradient error 1.7e-4 vs FP64, over the 1e-4 bar); bf16-delta (velocity checkpoints as BF16 "
-                         "differences from the previous one, the first and the passive scalar in FP32)")
+                         "differences from the previous one, the first and the passive scalar in FP32: 2.3e-6, "
+                         "the default)")
     ap.add_argument("--rel-tol", type=float, default=None,
                     help="relative z.r tolerance of the FP32 projections (rTr < rel_tol * zTr0); default: the "
                          "loosest setting whose gradient is within 1e-4 of an FP64 run solved to its floor "
