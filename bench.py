@@ -1177,7 +1177,7 @@ def cpu_leg(a, C, S, cfg, head, dev):
     inputs = C.shape3d_inputs(a.res)
     t_init, t_pairs, lo, go = cpu_pairs(cfg, 1, threads, inputs)
     secs = t_init + t_pairs
-    one = replace(cfg, total_steps=1, recompute=False, store_dtype=None)
+    one = replace(cfg, total_steps=1, recompute=False, ckpt_delta=False, store_dtype=None)
     sim1 = S.LFM_Diff_Simulator(config=one, device=dev)
     u0, rho0, rho_t = inputs
     lg, gg = sim1.gradient(u0, rho0, rho_t)
