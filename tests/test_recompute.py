@@ -25,6 +25,14 @@ def test_recompute_rejects_unsupported_options(bad):
 
 def test_recompute_accepts_the_checkpointed_form():
     S.FlowmapConfig(recompute=True, backward_u=False, store_dtype=torch.bfloat16).validate()
+    S.FlowmapConfig(recompute=True, backward_u=False, ckpt_delta=True).validate()
+
+
+@pytest.mark.parametrize("bad", [dict(recompute=False, backward_u=False),
+                                 dict(recompute=True, backward_u=False, dtype=torch.float64)])
+def test_checkpoint_differences_need_recompute_and_fp32(bad):
+    with pytest.raises(S.FlowmapError):
+        S.FlowmapConfig(ckpt_delta=True, **bad).validate()
 
 
 def _shape_case(res, steps, R, **kw):
